@@ -1,0 +1,417 @@
+// extern "C" boundary (include/fides_b200.h).  Converts exceptions into status codes and
+// a thread-local message, the C counterpart of the reference's OPENFHE_THROW / CudaError
+// (api/engine/cuda/CudaEngine.cpp, src/CudaUtils.cuh:706-757).
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fides_b200.h"
+#include "context.hpp"
+#include "ntt.cuh"
+#include "ops.hpp"
+
+struct fides_ctx {
+  fides::Context* c;
+  cudaStream_t host_stream;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return FIDES_OK;
+  } catch (const fides::Error& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return FIDES_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return FIDES_ERR_STATE;
+  }
+}
+
+fides::Context* C(fides_ctx* x) {
+  if (!x || !x->c) throw fides::Error(FIDES_ERR_ARG, "null context");
+  FIDES_CUDA(cudaSetDevice(x->c->device));
+  return x->c;
+}
+
+void need(const void* p, const char* what) {
+  if (!p) throw fides::Error(FIDES_ERR_ARG, std::string("null pointer: ") + what);
+}
+
+cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+const char* fides_last_error(void) { return g_err.c_str(); }
+
+int fides_ctx_create(const fides_params* p, fides_ctx** out) {
+  return guard([&] {
+    need(p, "params");
+    need(out, "out");
+    need(p->primes, "primes");
+    auto* x = new fides_ctx{nullptr, nullptr};
+    try {
+      x->c = fides::create_context(p->logN, p->n_q, p->n_special, p->dnum, p->primes, p->psi, p->device);
+      FIDES_CUDA(cudaStreamCreateWithFlags(&x->host_stream, cudaStreamNonBlocking));
+    } catch (...) {
+      if (x->c) fides::destroy_context(x->c);
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
+int fides_ctx_destroy(fides_ctx* x) {
+  return guard([&] {
+    if (!x) return;
+    if (x->host_stream) cudaStreamDestroy(x->host_stream);
+    fides::destroy_context(x->c);
+    delete x;
+  });
+}
+
+int fides_ctx_psi(const fides_ctx* x, uint64_t* psi_out) {
+  return guard([&] {
+    need(x, "ctx");
+    need(psi_out, "psi_out");
+    std::memcpy(psi_out, x->c->psi.data(), sizeof(uint64_t) * x->c->psi.size());
+  });
+}
+
+int fides_ctx_alpha(const fides_ctx* x) { return x && x->c ? x->c->alpha : FIDES_ERR_ARG; }
+
+size_t fides_ctx_scratch_bytes(const fides_ctx* x) { return x && x->c ? x->c->scratch_in_use.load() : 0; }
+
+int fides_ctx_set_scratch_limit(fides_ctx* x, size_t bytes) {
+  return guard([&] { C(x)->scratch_limit = bytes; });
+}
+
+uint64_t fides_ctx_launch_count(const fides_ctx* x) { return x && x->c ? x->c->launches.load() : 0; }
+
+int fides_ctx_profile(fides_ctx* x, int enable) {
+  return guard([&] {
+    auto* c = C(x);
+    std::lock_guard<std::mutex> g(c->prof_mu);
+    c->profiling = enable != 0;
+  });
+}
+
+int fides_ctx_profile_read(fides_ctx* x, int kind, double* ms, double* bytes, uint64_t* launches) {
+  return guard([&] {
+    auto* c = C(x);
+    if (kind < 0 || kind >= fides::KK_COUNT) throw fides::Error(FIDES_ERR_ARG, "bad kernel family");
+    std::lock_guard<std::mutex> g(c->prof_mu);
+    double t = 0, b = 0;
+    uint64_t n = 0;
+    std::vector<fides::ProfileRec> keep;
+    for (auto& r : c->prof) {
+      if (r.kind != kind) {
+        keep.push_back(r);
+        continue;
+      }
+      FIDES_CUDA(cudaEventSynchronize(r.end));
+      float e = 0;
+      FIDES_CUDA(cudaEventElapsedTime(&e, r.beg, r.end));
+      t += e;
+      b += r.bytes;
+      ++n;
+      c->ev_pool.push_back(r.beg);
+      c->ev_pool.push_back(r.end);
+    }
+    c->prof.swap(keep);
+    if (ms) *ms = t;
+    if (bytes) *bytes = b;
+    if (launches) *launches = n;
+  });
+}
+
+uint32_t fides_rotation_auto_index(int logN, int rotation) { return fides::h_auto_index(logN, rotation); }
+
+int fides_ntt_limbs(fides_ctx* x, uint64_t* const* limbs, const int* prime_ids, int n_limbs, int inverse,
+                    void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(limbs, "limbs");
+    need(prime_ids, "prime_ids");
+    std::vector<fides::LimbRef> v(n_limbs);
+    for (int i = 0; i < n_limbs; ++i) {
+      need(limbs[i], "limb");
+      if (prime_ids[i] < 0 || prime_ids[i] >= c->n_q + c->K) throw fides::Error(FIDES_ERR_ARG, "bad prime id");
+      v[i] = fides::LimbRef{limbs[i], prime_ids[i], 0};
+    }
+    fides::ntt_limbs(c, v.data(), n_limbs, inverse != 0, S(stream));
+  });
+}
+
+int fides_ntt_polys(fides_ctx* x, uint64_t* data, int n_polys, int n_limbs, int inverse, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(data, "data");
+    if (n_polys < 0 || n_limbs < 1 || n_limbs > c->n_q) throw fides::Error(FIDES_ERR_ARG, "bad poly shape");
+    std::vector<int> ids(n_limbs);
+    for (int i = 0; i < n_limbs; ++i) ids[i] = i;
+    fides::ntt_polys(c, data, n_polys, n_limbs, ids.data(), inverse != 0, S(stream));
+  });
+}
+
+int fides_modup(fides_ctx* x, const uint64_t* in, int level, uint64_t* digits, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(in, "x");
+    need(digits, "digits");
+    fides::op_modup(c, in, level, digits, S(stream));
+  });
+}
+
+int fides_ksk_inner_product(fides_ctx* x, const uint64_t* digits, int level, const uint64_t* key, uint64_t* out_a,
+                            uint64_t* out_b, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(digits, "digits");
+    need(out_a, "out_a");
+    need(out_b, "out_b");
+    fides::op_ksk_ip(c, nullptr, digits, level, key, out_a, out_b, S(stream));
+  });
+}
+
+int fides_moddown(fides_ctx* x, const uint64_t* x_ext, int level, uint64_t* out, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(x_ext, "x_ext");
+    need(out, "out");
+    fides::op_moddown(c, x_ext, level, out, S(stream));
+  });
+}
+
+int fides_keyswitch(fides_ctx* x, const uint64_t* d, int level, const uint64_t* key, uint64_t* f0, uint64_t* f1,
+                    void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(d, "d");
+    need(f0, "f0");
+    need(f1, "f1");
+    fides::KeySwitchItem it{d, level, key, f0, f1};
+    fides::op_keyswitch_batch(c, &it, 1, S(stream));
+  });
+}
+
+int fides_tensor(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
+                 int level, uint64_t* d0, uint64_t* d1, uint64_t* d2, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    for (const void* p : {(const void*)a0, (const void*)a1, (const void*)b0, (const void*)b1, (const void*)d0,
+                          (const void*)d1, (const void*)d2})
+      need(p, "tensor operand");
+    fides::op_tensor(c, a0, a1, b0, b1, level, d0, d1, d2, S(stream));
+  });
+}
+
+int fides_rescale(fides_ctx* x, const uint64_t* in, int level, uint64_t* out, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(in, "x");
+    need(out, "out");
+    uint64_t* o = out;
+    fides::op_rescale_batch(c, &in, &level, &o, 1, S(stream));
+  });
+}
+
+int fides_hmult(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
+                int level, const uint64_t* relin_key, int rescale, uint64_t* out0, uint64_t* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    for (const void* p : {(const void*)a0, (const void*)a1, (const void*)b0, (const void*)b1, (const void*)out0,
+                          (const void*)out1})
+      need(p, "hmult operand");
+    fides::HMultItem it{a0, a1, b0, b1, out0, out1, level};
+    fides::op_hmult_batch(c, &it, 1, relin_key, rescale != 0, S(stream));
+  });
+}
+
+int fides_rotate_auto(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int level, const uint64_t* key,
+                      uint32_t auto_index, uint64_t* out0, uint64_t* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(c0, "c0");
+    need(c1, "c1");
+    need(out0, "out0");
+    need(out1, "out1");
+    if ((auto_index & 1) == 0 || auto_index >= 2u * (uint32_t)c->N)
+      throw fides::Error(FIDES_ERR_ARG, "automorphism index must be odd and < 2N");
+    fides::RotateItem it{c0, c1, out0, out1, key, level, auto_index};
+    fides::op_rotate_batch(c, &it, 1, S(stream));
+  });
+}
+
+int fides_rotate(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int level, const uint64_t* rot_key,
+                 int rotation, uint64_t* out0, uint64_t* out1, void* stream) {
+  if (!x || !x->c) {
+    g_err = "null context";
+    return FIDES_ERR_ARG;
+  }
+  return fides_rotate_auto(x, c0, c1, level, rot_key, fides::h_auto_index(x->c->logN, rotation), out0, out1,
+                           stream);
+}
+
+int fides_rotate_hoisted(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int level,
+                         const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                         uint64_t* const* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(c0, "c0");
+    need(c1, "c1");
+    need(keys, "keys");
+    need(rotations, "rotations");
+    need(out0, "out0");
+    need(out1, "out1");
+    fides::HoistItem it;
+    it.c0 = c0;
+    it.c1 = c1;
+    it.l = level;
+    for (int j = 0; j < n; ++j) {
+      need(out0[j], "out0[j]");
+      need(out1[j], "out1[j]");
+      it.keys.push_back(keys[j]);
+      it.ks.push_back(fides::h_auto_index(c->logN, rotations[j]));
+      it.out0.push_back(out0[j]);
+      it.out1.push_back(out1[j]);
+    }
+    fides::op_hoisted(c, it, S(stream));
+  });
+}
+
+int fides_hmult_batch(fides_ctx* x, const fides_hmult_item* items, int n, const uint64_t* relin_key, int rescale,
+                      void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative batch");
+    if (n && !items) throw fides::Error(FIDES_ERR_ARG, "null items");
+    std::vector<fides::HMultItem> v(n);
+    for (int i = 0; i < n; ++i) {
+      const fides_hmult_item& s = items[i];
+      for (const void* p : {(const void*)s.a0, (const void*)s.a1, (const void*)s.b0, (const void*)s.b1,
+                            (const void*)s.out0, (const void*)s.out1})
+        need(p, "hmult item operand");
+      v[i] = fides::HMultItem{s.a0, s.a1, s.b0, s.b1, s.out0, s.out1, s.level};
+    }
+    fides::op_hmult_batch(c, v.data(), n, relin_key, rescale != 0, S(stream));
+  });
+}
+
+int fides_rotate_batch(fides_ctx* x, const fides_rotate_item* items, int n, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative batch");
+    if (n && !items) throw fides::Error(FIDES_ERR_ARG, "null items");
+    std::vector<fides::RotateItem> v(n);
+    for (int i = 0; i < n; ++i) {
+      const fides_rotate_item& s = items[i];
+      for (const void* p : {(const void*)s.c0, (const void*)s.c1, (const void*)s.out0, (const void*)s.out1})
+        need(p, "rotate item operand");
+      if ((s.auto_index & 1) == 0 || s.auto_index >= 2u * (uint32_t)c->N)
+        throw fides::Error(FIDES_ERR_ARG, "automorphism index must be odd and < 2N");
+      v[i] = fides::RotateItem{s.c0, s.c1, s.out0, s.out1, s.key, s.level, s.auto_index};
+    }
+    fides::op_rotate_batch(c, v.data(), n, S(stream));
+  });
+}
+
+int fides_key_upload(fides_ctx* x, const uint64_t* host_key, uint64_t** dev_key) {
+  return guard([&] {
+    auto* c = C(x);
+    need(host_key, "host_key");
+    need(dev_key, "dev_key");
+    size_t bytes = sizeof(uint64_t) * 2 * (size_t)c->dnum * (c->n_q + c->K) * c->N;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw fides::Error(FIDES_ERR_OOM, std::string("key allocation failed: ") + cudaGetErrorString(e));
+    }
+    e = cudaMemcpy(p, host_key, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(p);
+      throw fides::Error(FIDES_ERR_CUDA, std::string("key upload failed: ") + cudaGetErrorString(e));
+    }
+    *dev_key = static_cast<uint64_t*>(p);
+  });
+}
+
+int fides_key_free(fides_ctx* x, uint64_t* dev_key) {
+  return guard([&] {
+    C(x);
+    if (dev_key) FIDES_CUDA(cudaFree(dev_key));
+  });
+}
+
+}  // extern "C"
+
+namespace {
+// Host-buffer round trip: H2D inputs, op on device scratch, D2H outputs, synchronise.
+template <typename Op>
+void host_roundtrip(fides_ctx* x, const std::vector<const uint64_t*>& ins, int in_limbs, int n_out, int out_limbs,
+                    const std::vector<uint64_t*>& outs, Op&& op) {
+  auto* c = C(x);
+  const size_t N = c->N;
+  cudaStream_t s = x->host_stream;
+  size_t total = (size_t)ins.size() * in_limbs + (size_t)n_out * out_limbs;
+  fides::Scratch sc(c, sizeof(uint64_t) * N * total, s);
+  std::vector<uint64_t*> din(ins.size()), dout(n_out);
+  uint64_t* p = sc.u64();
+  for (size_t i = 0; i < ins.size(); ++i) {
+    need(ins[i], "host input");
+    din[i] = p;
+    p += (size_t)in_limbs * N;
+    FIDES_CUDA(cudaMemcpyAsync(din[i], ins[i], sizeof(uint64_t) * N * in_limbs, cudaMemcpyHostToDevice, s));
+  }
+  for (int i = 0; i < n_out; ++i) {
+    need(outs[i], "host output");
+    dout[i] = p;
+    p += (size_t)out_limbs * N;
+  }
+  op(din, dout, s);
+  for (int i = 0; i < n_out; ++i)
+    FIDES_CUDA(cudaMemcpyAsync(outs[i], dout[i], sizeof(uint64_t) * N * out_limbs, cudaMemcpyDeviceToHost, s));
+  FIDES_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+extern "C" {
+
+int fides_hmult_host(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
+                     int level, const uint64_t* relin_key_dev, int rescale, uint64_t* out0, uint64_t* out1) {
+  return guard([&] {
+    auto* c = C(x);
+    if (level < (rescale ? 2 : 1) || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    host_roundtrip(x, {a0, a1, b0, b1}, level, 2, rescale ? level - 1 : level, {out0, out1},
+                   [&](std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {
+                     fides::HMultItem it{in[0], in[1], in[2], in[3], out[0], out[1], level};
+                     fides::op_hmult_batch(c, &it, 1, relin_key_dev, rescale != 0, s);
+                   });
+  });
+}
+
+int fides_rotate_host(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int level, const uint64_t* rot_key_dev,
+                      int rotation, uint64_t* out0, uint64_t* out1) {
+  return guard([&] {
+    auto* c = C(x);
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    host_roundtrip(x, {c0, c1}, level, 2, level, {out0, out1},
+                   [&](std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {
+                     fides::RotateItem it{in[0], in[1], out[0], out[1], rot_key_dev, level,
+                                          fides::h_auto_index(c->logN, rotation)};
+                     fides::op_rotate_batch(c, &it, 1, s);
+                   });
+  });
+}
+
+}  // extern "C"

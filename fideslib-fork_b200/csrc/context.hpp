@@ -1,0 +1,134 @@
+// Internal context of the CKKS evaluation core: parameters, device-resident tables and
+// the scratch allocator.  Replaces the reference's ContextData (src/CKKS/Context.cu:74-138)
+// and the __constant__ Constants / Global::Globals tables (src/ConstantsGPU.cuh:49-198):
+// every table lives in global memory sized to the parameter set, so there is no
+// MAXP/MAXD ceiling (ConstantsGPU.cuh:12-32).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "modarith.cuh"
+
+namespace fides {
+
+// Error carried from the internals to the C ABI.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define FIDES_CUDA(call)                                                                           \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      throw ::fides::Error(-2, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + __FILE__ + \
+                                   ":" + std::to_string(__LINE__));                                \
+  } while (0)
+
+// A Shoup-precomputed constant.
+struct __align__(16) ShoupConst {
+  uint64_t w, ws;
+};
+
+// Table of one approximate basis conversion (ApproxSwitchCRTBasis):
+//   y_i = [x_i * pre_i]_{q_src_i};  out_j = [sum_i y_i * mat[i][j]]_{q_dst_j}.
+struct ConvTable {
+  int n_src = 0, n_dst = 0;
+  const int* src_pos = nullptr;    // limb index of source i in the input poly
+  const int* src_prime = nullptr;  // prime id of source i
+  const ShoupConst* pre = nullptr; // [n_src]
+  const int* dst_pos = nullptr;    // limb index of output j in the output poly
+  const int* dst_prime = nullptr;  // prime id of output j
+  const uint64_t* mat = nullptr;   // [n_src][n_dst]
+};
+
+struct RescaleConst {
+  uint64_t qinv, qinv_s;  // q_top^-1 mod q_j
+  uint64_t m, m_s;        // QlQlInvModqlDivqlModq_j = -q_top^-1 mod q_j
+};
+
+// Kernel families timed by the profiling mode (fides_ctx_profile).
+enum KernelKind { KK_NTT = 0, KK_CONV = 1, KK_KSK = 2, KK_ELEM = 3, KK_COUNT = 4 };
+
+struct ProfileRec {
+  int kind;
+  cudaEvent_t beg, end;
+  double bytes;  // algorithmic bytes of this launch
+};
+
+struct Context {
+  int device = 0;
+  int logN = 0, N = 0, n_q = 0, K = 0, dnum = 0, alpha = 0;
+  std::vector<uint64_t> primes, psi;
+
+  // device tables
+  DevPrime* d_prime = nullptr;       // [n_q + K]
+  ShoupConst* d_tw_fwd = nullptr;    // [n_q + K][N]: psi_rev (bit-reversed powers of psi)
+  ShoupConst* d_tw_inv = nullptr;    // [n_q + K][N]: psi^-1 bit-reversed
+  ShoupConst* d_inv_last = nullptr;  // [n_q + K]: psi_rev^-1[1] * N^-1 (last GS stage)
+  ShoupConst* d_pinv = nullptr;      // [n_q]: P^-1 mod q_j
+  ShoupConst* d_pmod = nullptr;      // [n_q]: P mod q_j
+  RescaleConst* d_rescale = nullptr; // [n_q + 1][n_q]: row l = rescale from level l
+  void* d_tables = nullptr;          // backing store of the conversion tables
+  std::vector<std::vector<ConvTable>> modup_tab;  // [l][d]
+  std::vector<ConvTable> moddown_tab;              // [l]
+
+  // scratch: stream-ordered allocations from the device's memory pool
+  cudaMemPool_t pool = nullptr;
+  std::atomic<size_t> scratch_in_use{0};
+  std::atomic<size_t> scratch_peak{0};
+  size_t scratch_limit = 0;
+  std::atomic<uint64_t> launches{0};
+  // profiling mode: CUDA events around every launch, per kernel family
+  bool profiling = false;
+  std::mutex prof_mu;
+  std::vector<ProfileRec> prof;
+  std::vector<cudaEvent_t> ev_pool;
+  std::mutex host_mu;                // guards the pinned staging buffers of the host entry points
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+
+  int beta(int l) const { return (l + alpha - 1) / alpha; }
+  size_t limb_bytes() const { return sizeof(uint64_t) * (size_t)N; }
+};
+
+// RAII stream-ordered scratch buffer.
+struct Scratch {
+  Context* ctx = nullptr;
+  cudaStream_t s = nullptr;
+  void* p = nullptr;
+  size_t bytes = 0;
+  Scratch(Context* c, size_t b, cudaStream_t st);
+  ~Scratch();
+  uint64_t* u64() const { return static_cast<uint64_t*>(p); }
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+};
+
+Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* primes, const uint64_t* psi, int device);
+void destroy_context(Context* c);
+
+// Launch bracket: counts the launch and, in profiling mode, records events around it.
+struct LaunchScope {
+  Context* c;
+  cudaStream_t s;
+  int idx = -1;
+  LaunchScope(Context* ctx, cudaStream_t st, int kind, double bytes);
+  ~LaunchScope();
+};
+
+// host number theory (same rules as the reference's Math.cu / ConstantsGPU.cu)
+uint64_t h_mulmod(uint64_t a, uint64_t b, uint64_t q);
+uint64_t h_powmod(uint64_t a, uint64_t e, uint64_t q);
+uint64_t h_invmod(uint64_t a, uint64_t q);
+uint64_t h_root_2n(uint64_t q, int logN);
+ShoupConst h_shoup(uint64_t w, uint64_t q);
+uint32_t h_auto_index(int logN, int rotation);
+
+}  // namespace fides

@@ -1,0 +1,103 @@
+// Elementwise RNS kernels, basis conversion and the key-switch-key inner product.
+//
+// Every kernel takes a by-value job list so that one launch covers many polynomials at
+// uneven levels (blockIdx.z = job, blockIdx.y = limb, blockIdx.x = coefficient tile).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "context.hpp"
+
+namespace fides {
+
+constexpr int EW_THREADS = 256;  // coefficients per CTA tile
+
+// ---- basis conversion (ModUp: DecompAndModUpConv, Conv.cu:274-423; ModDown: ModDown2, Conv.cu:27-133)
+struct ConvJob {
+  ConvTable t;
+  const uint64_t* src;  // source limb i at src + t.src_pos[i] * N (coefficient domain)
+  uint64_t* dst;        // output j at dst + t.dst_pos[j] * N
+};
+constexpr int MAX_CONV_JOBS = 96;
+struct ConvJobList {
+  int n, max_src, max_dst, pad;
+  ConvJob j[MAX_CONV_JOBS];
+};
+void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s);
+
+// ---- KSK inner product (fusedDotKSK_2_, ElemenwiseBatchKernels.cu:202-274) with the
+// hoisted-rotation extras of hoistedRotateDotKSK_2_ (:277-377): + P c0 on the b side and an
+// automorphism scatter of both outputs.
+struct KskJob {
+  const uint64_t* x;       // EVAL input at level l (own-digit limbs)
+  const uint64_t* digits;  // [beta][l + K][N] ModUp output (EVAL)
+  const uint64_t* key;     // [2][dnum][n_q + K][N]
+  const uint64_t* c0;      // optional: add P * c0 to out_b's Q limbs
+  uint64_t* out_a;         // [l + K][N]
+  uint64_t* out_b;
+  int l;
+  uint32_t auto_k;  // 0 = no automorphism
+};
+constexpr int MAX_KSK_JOBS = 64;
+struct KskJobList {
+  int n, max_ext, pad0, pad1;
+  KskJob j[MAX_KSK_JOBS];
+};
+void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s);
+
+// ---- ModDown epilogue (NTT_MODDOWN, NTTfusions.cuh:237-252): out = (x - conv) P^-1 (+ add)
+struct FinJob {
+  const uint64_t* x;     // Q limbs of the extended poly
+  const uint64_t* conv;  // converted special part, EVAL
+  const uint64_t* add;   // optional addend
+  uint64_t* out;
+  int l;
+  int pad;
+};
+constexpr int MAX_FIN_JOBS = 128;
+struct FinJobList {
+  int n, max_l, pad0, pad1;
+  FinJob j[MAX_FIN_JOBS];
+};
+void launch_moddown_finish(Context* c, const FinJob* jobs, int n, cudaStream_t s);
+
+// ---- tensor product (binomialMult_, ElemenwiseBatchKernels.cu:1363-1510)
+struct TensorJob {
+  const uint64_t *a0, *a1, *b0, *b1;
+  uint64_t *d0, *d1, *d2;
+  int l;
+  int pad;
+};
+constexpr int MAX_TENSOR_JOBS = 64;
+struct TensorJobList {
+  int n, max_l, pad0, pad1;
+  TensorJob j[MAX_TENSOR_JOBS];
+};
+void launch_tensor(Context* c, const TensorJob* jobs, int n, cudaStream_t s);
+
+// ---- rescale (rescale_fusion, NTTfusions.cuh:214-235; SwitchModulus, Rescale.cuh:44-64)
+struct SwitchJob {
+  const uint64_t* top;  // top limb, coefficient domain
+  uint64_t* out;        // l - 1 limbs
+  int l;
+  int pad;
+};
+struct RescaleJob {
+  const uint64_t* x;  // EVAL, level l
+  const uint64_t* t;  // NTT(SwitchModulus(top)), l - 1 limbs
+  uint64_t* out;      // l - 1 limbs
+  int l;
+  int pad;
+};
+constexpr int MAX_RS_JOBS = 128;
+struct SwitchJobList {
+  int n, max_l, pad0, pad1;
+  SwitchJob j[MAX_RS_JOBS];
+};
+struct RescaleJobList {
+  int n, max_l, pad0, pad1;
+  RescaleJob j[MAX_RS_JOBS];
+};
+void launch_switch_modulus(Context* c, const SwitchJob* jobs, int n, cudaStream_t s);
+void launch_rescale_finish(Context* c, const RescaleJob* jobs, int n, cudaStream_t s);
+
+}  // namespace fides

@@ -1,0 +1,60 @@
+// Ciphertext-level operations composed from the kernels.  Every operation is written for
+// a batch of items at arbitrary (uneven) levels; each stage is one launch over all items.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "context.hpp"
+
+namespace fides {
+
+struct KeySwitchItem {
+  const uint64_t* d;  // EVAL, level l
+  int l;
+  const uint64_t* key;
+  uint64_t* f0;  // ModDown(sum d b) (+ add0)
+  uint64_t* f1;  // ModDown(sum d a) (+ add1)
+  const uint64_t* add0 = nullptr;
+  const uint64_t* add1 = nullptr;
+};
+
+struct HMultItem {
+  const uint64_t *a0, *a1, *b0, *b1;
+  uint64_t *out0, *out1;
+  int l;
+};
+
+struct RotateItem {
+  const uint64_t *c0, *c1;
+  uint64_t *out0, *out1;
+  const uint64_t* key;
+  int l;
+  uint32_t k;  // automorphism index
+};
+
+// Hoisted rotations of one ciphertext.
+struct HoistItem {
+  const uint64_t *c0, *c1;
+  int l;
+  std::vector<const uint64_t*> keys;
+  std::vector<uint32_t> ks;
+  std::vector<uint64_t*> out0, out1;
+};
+
+void op_modup(Context* c, const uint64_t* x, int l, uint64_t* digits, cudaStream_t s);
+void op_ksk_ip(Context* c, const uint64_t* x, const uint64_t* digits, int l, const uint64_t* key, uint64_t* out_a,
+               uint64_t* out_b, cudaStream_t s);
+void op_moddown(Context* c, const uint64_t* x_ext, int l, uint64_t* out, cudaStream_t s);
+void op_tensor(Context* c, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1, int l,
+               uint64_t* d0, uint64_t* d1, uint64_t* d2, cudaStream_t s);
+
+void op_keyswitch_batch(Context* c, const KeySwitchItem* items, int n, cudaStream_t s);
+void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint64_t* const* outs, int n,
+                      cudaStream_t s);
+void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* relin_key, bool rescale,
+                    cudaStream_t s);
+void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s);
+void op_hoisted(Context* c, const HoistItem& item, cudaStream_t s);
+
+}  // namespace fides

@@ -1,0 +1,352 @@
+"""Python binding of the B200 CKKS evaluation core (libfides_b200.so, C ABI in
+include/fides_b200.h).
+
+The library is the product; this module only marshals arguments.  Device memory comes
+from torch (uint64 CUDA tensors); every call runs the CUDA kernels on the caller's
+current torch stream.  There is no CPU fallback: a missing library or GPU raises.
+
+Names follow the reference's CKKS ciphertext API (src/CKKS/Ciphertext.cuh: mult, rescale,
+rotate, rotate_hoisted, keySwitch) and engine plug-in (api/engine/Engine.hpp:75-408:
+evalMult, evalRotate, evalFastRotation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import torch
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "libfides_b200.so")
+_lib = None
+
+u64p = C.POINTER(C.c_uint64)
+vp = C.c_void_p
+
+FIDES_OK = 0
+ERRORS = {-1: "ARG", -2: "CUDA", -3: "OOM", -4: "LEVEL", -5: "KEY", -6: "TIMEOUT", -7: "STATE"}
+
+
+class FidesError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fides error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [("logN", C.c_int), ("n_q", C.c_int), ("n_special", C.c_int), ("dnum", C.c_int),
+                ("primes", u64p), ("psi", u64p), ("device", C.c_int)]
+
+
+class _HMultItem(C.Structure):
+    _fields_ = [("a0", vp), ("a1", vp), ("b0", vp), ("b1", vp), ("out0", vp), ("out1", vp), ("level", C.c_int)]
+
+
+class _RotateItem(C.Structure):
+    _fields_ = [("c0", vp), ("c1", vp), ("out0", vp), ("out1", vp), ("key", vp), ("level", C.c_int),
+                ("auto_index", C.c_uint32)]
+
+
+def build(force: bool = False) -> str:
+    """Compile libfides_b200.so for sm_100a with nvcc (make, in-tree)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", _PKG], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FidesError(-7, f"{LIB_PATH} is not built (run build())")
+        L = C.CDLL(LIB_PATH)
+        L.fides_last_error.restype = C.c_char_p
+        L.fides_ctx_create.argtypes = [C.POINTER(_Params), C.POINTER(vp)]
+        L.fides_ctx_destroy.argtypes = [vp]
+        L.fides_ctx_psi.argtypes = [vp, u64p]
+        L.fides_ctx_alpha.argtypes = [vp]
+        L.fides_ctx_scratch_bytes.argtypes = [vp]
+        L.fides_ctx_scratch_bytes.restype = C.c_size_t
+        L.fides_ctx_set_scratch_limit.argtypes = [vp, C.c_size_t]
+        L.fides_ctx_launch_count.argtypes = [vp]
+        L.fides_ctx_launch_count.restype = C.c_uint64
+        L.fides_ctx_profile.argtypes = [vp, C.c_int]
+        L.fides_ctx_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                             C.POINTER(C.c_uint64)]
+        L.fides_rotation_auto_index.argtypes = [C.c_int, C.c_int]
+        L.fides_rotation_auto_index.restype = C.c_uint32
+        L.fides_ntt_limbs.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int), C.c_int, C.c_int, vp]
+        L.fides_ntt_polys.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp]
+        L.fides_modup.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.fides_ksk_inner_product.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp]
+        L.fides_moddown.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.fides_keyswitch.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp]
+        L.fides_tensor.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp]
+        L.fides_rescale.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.fides_hmult.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp]
+        L.fides_rotate.argtypes = [vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp]
+        L.fides_rotate_auto.argtypes = [vp, vp, vp, C.c_int, vp, C.c_uint32, vp, vp, vp]
+        L.fides_rotate_hoisted.argtypes = [vp, vp, vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_int), C.c_int,
+                                           C.POINTER(vp), C.POINTER(vp), vp]
+        L.fides_hmult_batch.argtypes = [vp, C.POINTER(_HMultItem), C.c_int, vp, C.c_int, vp]
+        L.fides_rotate_batch.argtypes = [vp, C.POINTER(_RotateItem), C.c_int, vp]
+        L.fides_key_upload.argtypes = [vp, u64p, C.POINTER(vp)]
+        L.fides_key_free.argtypes = [vp, vp]
+        L.fides_hmult_host.argtypes = [vp, u64p, u64p, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
+        L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != FIDES_OK:
+        raise FidesError(rc, lib().fides_last_error().decode())
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    assert t.dtype == torch.uint64 and t.is_contiguous(), "expected a contiguous uint64 tensor"
+    return t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def auto_index(logN: int, rotation: int) -> int:
+    return int(lib().fides_rotation_auto_index(logN, rotation))
+
+
+@dataclass
+class Ciphertext:
+    """Device ciphertext (c0, c1) in EVALUATION format at `level` active Q limbs."""
+    c0: torch.Tensor
+    c1: torch.Tensor
+
+    @property
+    def level(self) -> int:
+        return int(self.c0.shape[0])
+
+
+class Context:
+    """One parameter set on one GPU (reference: CKKS::Context / ContextData)."""
+
+    def __init__(self, logN: int, q_primes, p_primes, dnum: int, psi=None, device: int = 0):
+        import numpy as np
+        self.logN, self.N = logN, 1 << logN
+        self.q, self.p = [int(x) for x in q_primes], [int(x) for x in p_primes]
+        self.n_q, self.K, self.dnum = len(self.q), len(self.p), dnum
+        self.device = device
+        self._primes = np.array(self.q + self.p, dtype=np.uint64)
+        self._psi = None if psi is None else np.array(psi, dtype=np.uint64)
+        prm = _Params(logN, self.n_q, self.K, dnum, self._primes.ctypes.data_as(u64p),
+                      None if self._psi is None else self._psi.ctypes.data_as(u64p), device)
+        h = vp()
+        _check(lib().fides_ctx_create(C.byref(prm), C.byref(h)))
+        self._h = h
+        self.alpha = int(lib().fides_ctx_alpha(h))
+        ps = np.zeros(len(self._primes), dtype=np.uint64)
+        _check(lib().fides_ctx_psi(h, ps.ctypes.data_as(u64p)))
+        self.psi = [int(x) for x in ps]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fides_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- bookkeeping --
+    def beta(self, l: int) -> int:
+        return (l + self.alpha - 1) // self.alpha
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().fides_ctx_launch_count(self._h))
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(lib().fides_ctx_scratch_bytes(self._h))
+
+    def set_scratch_limit(self, nbytes: int):
+        _check(lib().fides_ctx_set_scratch_limit(self._h, nbytes))
+
+    KERNEL_FAMILIES = {"ntt": 0, "conv": 1, "ksk": 2, "elem": 3}
+
+    def profile(self, enable: bool = True):
+        _check(lib().fides_ctx_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self, family: str) -> dict:
+        ms, by, n = C.c_double(), C.c_double(), C.c_uint64()
+        _check(lib().fides_ctx_profile_read(self._h, self.KERNEL_FAMILIES[family], C.byref(ms), C.byref(by),
+                                            C.byref(n)))
+        return {"ms": ms.value, "bytes": by.value, "launches": int(n.value)}
+
+    def empty(self, *shape) -> torch.Tensor:
+        return torch.empty(*shape, self.N, dtype=torch.uint64, device=f"cuda:{self.device}")
+
+    # -- transforms --
+    def ntt_limbs(self, limbs, prime_ids, inverse=False):
+        n = len(limbs)
+        ptrs = (vp * n)(*[_ptr(t) for t in limbs])
+        ids = (C.c_int * n)(*prime_ids)
+        _check(lib().fides_ntt_limbs(self._h, ptrs, ids, n, 1 if inverse else 0, _stream()))
+
+    def ntt(self, polys: torch.Tensor, inverse=False):
+        """In-place NTT of [n_polys][n_limbs][N] (or [n_limbs][N]) Q-limb polynomials."""
+        t = polys if polys.dim() == 3 else polys.unsqueeze(0)
+        _check(lib().fides_ntt_polys(self._h, _ptr(t), t.shape[0], t.shape[1], 1 if inverse else 0, _stream()))
+        return polys
+
+    def intt(self, polys):
+        return self.ntt(polys, inverse=True)
+
+    # -- key switching pieces --
+    def modup(self, x: torch.Tensor) -> torch.Tensor:
+        l = x.shape[0]
+        out = self.empty(self.beta(l), l + self.K)
+        _check(lib().fides_modup(self._h, _ptr(x), l, _ptr(out), _stream()))
+        return out
+
+    def ksk_inner_product(self, digits, l, key):
+        a, b = self.empty(l + self.K), self.empty(l + self.K)
+        _check(lib().fides_ksk_inner_product(self._h, _ptr(digits), l, _ptr(key), _ptr(a), _ptr(b), _stream()))
+        return a, b
+
+    def moddown(self, x_ext):
+        l = x_ext.shape[0] - self.K
+        out = self.empty(l)
+        _check(lib().fides_moddown(self._h, _ptr(x_ext), l, _ptr(out), _stream()))
+        return out
+
+    def keyswitch(self, d, key):
+        l = d.shape[0]
+        f0, f1 = self.empty(l), self.empty(l)
+        _check(lib().fides_keyswitch(self._h, _ptr(d), l, _ptr(key), _ptr(f0), _ptr(f1), _stream()))
+        return f0, f1
+
+    # -- ciphertext ops --
+    def tensor(self, a: Ciphertext, b: Ciphertext):
+        l = a.level
+        d = [self.empty(l) for _ in range(3)]
+        _check(lib().fides_tensor(self._h, _ptr(a.c0), _ptr(a.c1), _ptr(b.c0), _ptr(b.c1), l,
+                                  *[_ptr(x) for x in d], _stream()))
+        return d
+
+    def rescale_poly(self, x):
+        l = x.shape[0]
+        out = self.empty(l - 1)
+        _check(lib().fides_rescale(self._h, _ptr(x), l, _ptr(out), _stream()))
+        return out
+
+    def rescale(self, ct: Ciphertext) -> Ciphertext:
+        return Ciphertext(self.rescale_poly(ct.c0), self.rescale_poly(ct.c1))
+
+    def mult(self, a: Ciphertext, b: Ciphertext, relin_key, rescale=True, out: Ciphertext | None = None) -> Ciphertext:
+        l = a.level
+        lo = l - 1 if rescale else l
+        out = out or Ciphertext(self.empty(lo), self.empty(lo))
+        _check(lib().fides_hmult(self._h, _ptr(a.c0), _ptr(a.c1), _ptr(b.c0), _ptr(b.c1), l, _ptr(relin_key),
+                                 1 if rescale else 0, _ptr(out.c0), _ptr(out.c1), _stream()))
+        return out
+
+    def rotate(self, ct: Ciphertext, key, rotation: int, out: Ciphertext | None = None) -> Ciphertext:
+        l = ct.level
+        out = out or Ciphertext(self.empty(l), self.empty(l))
+        _check(lib().fides_rotate(self._h, _ptr(ct.c0), _ptr(ct.c1), l, _ptr(key), rotation, _ptr(out.c0),
+                                  _ptr(out.c1), _stream()))
+        return out
+
+    def rotate_auto(self, ct: Ciphertext, key, k: int) -> Ciphertext:
+        l = ct.level
+        out = Ciphertext(self.empty(l), self.empty(l))
+        _check(lib().fides_rotate_auto(self._h, _ptr(ct.c0), _ptr(ct.c1), l, _ptr(key), k, _ptr(out.c0),
+                                       _ptr(out.c1), _stream()))
+        return out
+
+    def rotate_hoisted(self, ct: Ciphertext, keys, rotations) -> list[Ciphertext]:
+        n, l = len(rotations), ct.level
+        outs = [Ciphertext(self.empty(l), self.empty(l)) for _ in range(n)]
+        kp = (vp * n)(*[_ptr(k) for k in keys])
+        rs = (C.c_int * n)(*rotations)
+        o0 = (vp * n)(*[_ptr(o.c0) for o in outs])
+        o1 = (vp * n)(*[_ptr(o.c1) for o in outs])
+        _check(lib().fides_rotate_hoisted(self._h, _ptr(ct.c0), _ptr(ct.c1), l, kp, rs, n, o0, o1, _stream()))
+        return outs
+
+    # -- batched forms --
+    def mult_batch(self, pairs, relin_key, rescale=True) -> list[Ciphertext]:
+        n = len(pairs)
+        outs, items = [], (_HMultItem * n)()
+        for i, (a, b) in enumerate(pairs):
+            lo = a.level - 1 if rescale else a.level
+            o = Ciphertext(self.empty(lo), self.empty(lo))
+            outs.append(o)
+            items[i] = _HMultItem(_ptr(a.c0), _ptr(a.c1), _ptr(b.c0), _ptr(b.c1), _ptr(o.c0), _ptr(o.c1), a.level)
+        _check(lib().fides_hmult_batch(self._h, items, n, _ptr(relin_key), 1 if rescale else 0, _stream()))
+        return outs
+
+    def rotate_batch(self, jobs) -> list[Ciphertext]:
+        """jobs: list of (ciphertext, key, rotation)."""
+        n = len(jobs)
+        outs, items = [], (_RotateItem * n)()
+        for i, (ct, key, r) in enumerate(jobs):
+            o = Ciphertext(self.empty(ct.level), self.empty(ct.level))
+            outs.append(o)
+            items[i] = _RotateItem(_ptr(ct.c0), _ptr(ct.c1), _ptr(o.c0), _ptr(o.c1), _ptr(key), ct.level,
+                                   auto_index(self.logN, r))
+        _check(lib().fides_rotate_batch(self._h, items, n, _stream()))
+        return outs
+
+    # -- host-buffer path --
+    def key_upload(self, host_key) -> int:
+        import numpy as np
+        hk = np.ascontiguousarray(host_key, dtype=np.uint64)
+        assert hk.shape == (2, self.dnum, self.n_q + self.K, self.N)
+        d = vp()
+        _check(lib().fides_key_upload(self._h, hk.ctypes.data_as(u64p), C.byref(d)))
+        return int(d.value)
+
+    def key_free(self, dev_key: int):
+        _check(lib().fides_key_free(self._h, dev_key))
+
+    def mult_host(self, a0, a1, b0, b1, dev_key: int, rescale=True, out0=None, out1=None):
+        import numpy as np
+        l = a0.shape[0]
+        lo = l - 1 if rescale else l
+        out0 = np.empty((lo, self.N), dtype=np.uint64) if out0 is None else out0
+        out1 = np.empty((lo, self.N), dtype=np.uint64) if out1 is None else out1
+        P = lambda a: a.ctypes.data_as(u64p)
+        _check(lib().fides_hmult_host(self._h, P(a0), P(a1), P(b0), P(b1), l, dev_key, 1 if rescale else 0,
+                                      P(out0), P(out1)))
+        return out0, out1
+
+    def rotate_host(self, c0, c1, dev_key: int, rotation: int, out0=None, out1=None):
+        import numpy as np
+        l = c0.shape[0]
+        out0 = np.empty((l, self.N), dtype=np.uint64) if out0 is None else out0
+        out1 = np.empty((l, self.N), dtype=np.uint64) if out1 is None else out1
+        P = lambda a: a.ctypes.data_as(u64p)
+        _check(lib().fides_rotate_host(self._h, P(c0), P(c1), l, dev_key, rotation, P(out0), P(out1)))
+        return out0, out1
+
+
+def to_device(a, device: int = 0) -> torch.Tensor:
+    """Host uint64 array -> device uint64 tensor (copied through an int64 view)."""
+    import numpy as np
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return torch.from_numpy(a.view(np.int64)).to(f"cuda:{device}").view(torch.uint64)
+
+
+def to_host(t: torch.Tensor):
+    import numpy as np
+    return t.contiguous().view(torch.int64).cpu().numpy().view(np.uint64)

@@ -1,0 +1,167 @@
+/*
+ * fides_b200.h -- C ABI of the B200-native CKKS evaluation core (libfides_b200.so).
+ *
+ * Plain pointers and sizes only.  Polynomials are limb-major uint64 arrays: limb i is
+ * N = 2^logN consecutive words.  Unless a function says "host", every polynomial or
+ * key pointer is DEVICE memory on the context's GPU.  Data are in EVALUATION format
+ * (negacyclic NTT, bit-reversed order) unless stated otherwise -- the same layout as the
+ * reference's RawCipherText limbs (src/CKKS/openfhe-interface/RawCiphertext.cuh:21-37).
+ *
+ * "level" l = number of active Q limbs of a ciphertext (1 <= l <= n_q).  An extended
+ * polynomial at level l has l Q limbs followed by the K special limbs.
+ *
+ * Key-switching keys are [2][dnum][n_q + K][N] (index 0 = a, feeds c1; index 1 = b,
+ * feeds c0), the layout of the reference's RawKeySwitchKey::r_key
+ * (RawCiphertext.cuh:90-95, KeySwitchingKey.cu:19-35).
+ *
+ * Every call returns FIDES_OK (0) or a negative status; fides_last_error() returns the
+ * calling thread's message.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ * Calls enqueue work and return without synchronising unless stated otherwise.
+ */
+#ifndef FIDES_B200_H
+#define FIDES_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIDES_OK 0
+#define FIDES_ERR_ARG (-1)     /* bad argument (null pointer, size, level) */
+#define FIDES_ERR_CUDA (-2)    /* a CUDA runtime call failed */
+#define FIDES_ERR_OOM (-3)     /* device allocation failed / over budget */
+#define FIDES_ERR_LEVEL (-4)   /* level out of range for the operation */
+#define FIDES_ERR_KEY (-5)     /* missing or malformed key */
+#define FIDES_ERR_TIMEOUT (-6) /* a bounded device-side wait gave up */
+#define FIDES_ERR_STATE (-7)   /* object in the wrong state */
+
+/* Parameters.  Replaces FIDESlib::CKKS::Parameters (src/CKKS/Parameters.cuh:20-129) and
+ * the RawParams moduli/roots (RawCiphertext.cuh:53-66).  psi[i] = primitive 2N-th root of
+ * primes[i]; NULL (or a zero entry) derives it as g^((q-1)/2N), g the smallest primitive
+ * root (reference src/ConstantsGPU.cu:39-69). */
+typedef struct fides_params {
+  int logN;
+  int n_q;       /* L + 1 */
+  int n_special; /* K */
+  int dnum;
+  const uint64_t* primes; /* n_q Q primes then K special primes, each < 2^62 */
+  const uint64_t* psi;    /* optional */
+  int device;             /* CUDA device ordinal */
+} fides_params;
+
+typedef struct fides_ctx fides_ctx;
+
+/* Context: replaces GenCryptoContextGPU + ContextData (src/CKKS/Context.cu:74-138) and
+ * SetupConstants (src/ConstantsGPU.cu:132-640). */
+int fides_ctx_create(const fides_params* params, fides_ctx** out);
+int fides_ctx_destroy(fides_ctx* ctx);
+const char* fides_last_error(void);
+int fides_ctx_psi(const fides_ctx* ctx, uint64_t* psi_out); /* n_q + K roots */
+int fides_ctx_alpha(const fides_ctx* ctx);
+/* Bytes of device scratch the context currently holds. */
+size_t fides_ctx_scratch_bytes(const fides_ctx* ctx);
+/* Cap on scratch growth (0 = unlimited); exceeding it returns FIDES_ERR_OOM. */
+int fides_ctx_set_scratch_limit(fides_ctx* ctx, size_t bytes);
+/* Count of kernels this context has launched (for launch accounting). */
+uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
+
+/* Profiling mode: when enabled, every kernel launch is bracketed by CUDA events on its
+ * stream and attributed to a family (0 = NTT passes, 1 = basis conversion, 2 = KSK inner
+ * product, 3 = other elementwise).  fides_ctx_profile_read synchronises on the recorded
+ * events and returns, for one family, the summed device time, the summed algorithmic
+ * bytes (compulsory HBM traffic of each launch) and the launch count, then clears that
+ * family's records.  Counterpart of the reference's NVTX ranges (src/CudaUtils.cuh:662-690). */
+int fides_ctx_profile(fides_ctx* ctx, int enable);
+int fides_ctx_profile_read(fides_ctx* ctx, int kind, double* ms, double* bytes, uint64_t* launches);
+
+/* ---- transforms --------------------------------------------------------------------- */
+/* Batched NTT / INTT over an arbitrary list of limbs (each limb: device pointer + prime
+ * index into params.primes).  Replaces NTT_/INTT_/NTTBatch_ + ApplyNTT/ApplyINTT
+ * (src/NTT.cu:42-802, src/CKKS/LimbPartition.cu:433-550).  In place. */
+int fides_ntt_limbs(fides_ctx* ctx, uint64_t* const* limbs, const int* prime_ids, int n_limbs, int inverse,
+                    void* stream);
+/* n_polys contiguous polynomials of n_limbs Q limbs each (prime ids 0..n_limbs-1). */
+int fides_ntt_polys(fides_ctx* ctx, uint64_t* data, int n_polys, int n_limbs, int inverse, void* stream);
+
+/* ---- hybrid key-switching pieces ---------------------------------------------------- */
+/* ModUp of an EVAL poly at level l into beta extended digits [beta][l+K][N] (own-digit
+ * limbs are copied through).  Replaces RNSPoly::modup / LimbPartition::modupMGPU
+ * (src/CKKS/LimbPartitionMGPU.cu:1981+) with DecompAndModUpConv (src/CKKS/Conv.cu:274-423). */
+int fides_modup(fides_ctx* ctx, const uint64_t* x, int level, uint64_t* digits, void* stream);
+/* KSK inner product over the digits: replaces fusedDotKSK_2_
+ * (src/CKKS/ElemenwiseBatchKernels.cu:202-274).  out_a/out_b are [l+K][N]. */
+int fides_ksk_inner_product(fides_ctx* ctx, const uint64_t* digits, int level, const uint64_t* key,
+                            uint64_t* out_a, uint64_t* out_b, void* stream);
+/* ModDown [l+K][N] -> [l][N]: replaces LimbPartition::moddown (src/CKKS/LimbPartition.cu:
+ * 2145-2217) with ModDown2 (src/CKKS/Conv.cu:27-133) and NTT_MODDOWN (NTTfusions.cuh:237). */
+int fides_moddown(fides_ctx* ctx, const uint64_t* x_ext, int level, uint64_t* out, void* stream);
+/* Full key switch of d: f0 = ModDown(sum d_j b_j), f1 = ModDown(sum d_j a_j).  Replaces
+ * LimbPartition::modup_ksk_moddown_mgpu (src/CKKS/LimbPartitionMGPU.cu:669-1980). */
+int fides_keyswitch(fides_ctx* ctx, const uint64_t* d, int level, const uint64_t* key, uint64_t* f0,
+                    uint64_t* f1, void* stream);
+
+/* ---- ciphertext operations (device buffers) ----------------------------------------- */
+/* Tensor product: replaces binomialMult_ (ElemenwiseBatchKernels.cu:1363-1510). */
+int fides_tensor(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
+                 int level, uint64_t* d0, uint64_t* d1, uint64_t* d2, void* stream);
+/* Rescale of n_polys polynomials at level l (FIXEDMANUAL DropLastElementAndScale);
+ * out has l-1 limbs per poly.  Replaces Ciphertext::rescale (src/CKKS/Ciphertext.cpp:
+ * 569-607) / LimbPartition::rescale (src/CKKS/LimbPartition.cu:711-797). */
+int fides_rescale(fides_ctx* ctx, const uint64_t* x, int level, uint64_t* out, void* stream);
+/* HMult + relinearize (+ rescale): replaces CKKS::Ciphertext::mult
+ * (src/CKKS/Ciphertext.cpp:660-869) behind CudaEngine::evalMult (CudaEngine.cpp:429-437). */
+int fides_hmult(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
+                int level, const uint64_t* relin_key, int rescale, uint64_t* out0, uint64_t* out1, void* stream);
+/* HRotate by `rotation` slots: replaces CKKS::Ciphertext::rotate (Ciphertext.cpp:1102-1168)
+ * behind CudaEngine::evalRotate (CudaEngine.cpp:527-533). */
+int fides_rotate(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, const uint64_t* rot_key,
+                 int rotation, uint64_t* out0, uint64_t* out1, void* stream);
+/* Same with an explicit automorphism index (2N-1 = conjugation, Ciphertext.cpp:1175-1219). */
+int fides_rotate_auto(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, const uint64_t* key,
+                      uint32_t auto_index, uint64_t* out0, uint64_t* out1, void* stream);
+/* Hoisted rotations (one ModUp, n rotations): replaces Ciphertext::rotate_hoisted
+ * (Ciphertext.cpp:1221-1394) / EvalFastRotation (CudaEngine.cpp:536-585). */
+int fides_rotate_hoisted(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
+                         const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                         uint64_t* const* out1, void* stream);
+/* Rotation index -> automorphism index (Context.cu:916-944 + RNSPoly.cpp:656-658). */
+uint32_t fides_rotation_auto_index(int logN, int rotation);
+
+/* ---- batched forms: many ciphertexts at uneven levels per launch -------------------- */
+/* Replaces the reference's same-level batches (LimbPartitionBatch.cu:526+,
+ * CudaEngine::evalRotateMany, CudaEngine.cpp:656-702) with mixed-level batching. */
+typedef struct fides_hmult_item {
+  const uint64_t *a0, *a1, *b0, *b1;
+  uint64_t *out0, *out1;
+  int level;
+} fides_hmult_item;
+int fides_hmult_batch(fides_ctx* ctx, const fides_hmult_item* items, int n, const uint64_t* relin_key,
+                      int rescale, void* stream);
+
+typedef struct fides_rotate_item {
+  const uint64_t *c0, *c1;
+  uint64_t *out0, *out1;
+  const uint64_t* key;
+  int level;
+  uint32_t auto_index;
+} fides_rotate_item;
+int fides_rotate_batch(fides_ctx* ctx, const fides_rotate_item* items, int n, void* stream);
+
+/* ---- host-buffer entry points (end-to-end path) ------------------------------------- */
+/* Upload a key from host memory into a new device buffer owned by the context. */
+int fides_key_upload(fides_ctx* ctx, const uint64_t* host_key, uint64_t** dev_key);
+int fides_key_free(fides_ctx* ctx, uint64_t* dev_key);
+/* HMult(+rescale) of host ciphertexts: copies in, computes, copies out, synchronises.
+ * Mirrors CudaEngine::evalMult's load -> op -> RecoverHostCiphertext cycle
+ * (CudaEngine.cpp:429-437, 1156-1227, 1768-1795). */
+int fides_hmult_host(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
+                     const uint64_t* b1, int level, const uint64_t* relin_key_dev, int rescale, uint64_t* out0,
+                     uint64_t* out1);
+int fides_rotate_host(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
+                      const uint64_t* rot_key_dev, int rotation, uint64_t* out0, uint64_t* out1);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

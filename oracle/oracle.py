@@ -129,8 +129,11 @@ class Oracle:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().or_ctx_destroy(h)
+        if h and _lib is not None:
+            try:
+                _lib.or_ctx_destroy(h)
+            except Exception:
+                pass
             self._h = None
 
     # -- helpers --

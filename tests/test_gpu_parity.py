@@ -1,0 +1,300 @@
+"""GPU parity: every residue of the CUDA path (through the C ABI) equals the CPU oracle
+on the same seeded inputs and keys.  Bit-exact: integer arithmetic only."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from ckks_host import KeyGen, decode, encode, uniform_limbs, xrng
+
+pytestmark = pytest.mark.gpu
+
+
+def eq(gpu_t, host):
+    import fides_b200 as F
+    return np.array_equal(F.to_host(gpu_t), host)
+
+
+class Setup:
+    def __init__(self, F, prm, keys=True, rot=()):
+        self.prm = prm
+        self.o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+        self.ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+        assert self.ctx.psi == self.o.psi
+        self.F = F
+        if keys:
+            self.kg = KeyGen(self.o)
+            self.rk = self.kg.relin_key()
+            self.rk_d = F.to_device(self.rk)
+            self.rot = {r: self.kg.rotation_key(r) for r in rot}
+            self.rot_d = {r: F.to_device(k) for r, k in self.rot.items()}
+
+    def rand_ct(self, l, stream):
+        rng = xrng(stream)
+        c0 = uniform_limbs(rng, self.prm.q[:l], self.o.N)
+        c1 = uniform_limbs(rng, self.prm.q[:l], self.o.N)
+        return c0, c1
+
+    def dev_ct(self, c):
+        return self.F.Ciphertext(self.F.to_device(c[0]), self.F.to_device(c[1]))
+
+
+@pytest.fixture(scope="module")
+def A(fides):
+    from fides_b200 import params as P
+    return Setup(fides, P.config_a(), rot=(1, -1, 5))
+
+
+@pytest.fixture(scope="module")
+def Cfg(fides):
+    from fides_b200 import params as P
+    return Setup(fides, P.config_c(4), rot=(1, -1, 2, 128, -128))
+
+
+# ---------------------------------------------------------------- NTT (config B)
+@pytest.mark.parametrize("batch", [1, 8])
+def test_ntt_config_b_bit_exact(fides, batch):
+    from fides_b200 import params as P
+    prm = P.config_b()
+    o = O.Oracle(16, prm.q, [], 1)
+    ctx = fides.Context(16, prm.q, [], 1)
+    rng = xrng(200 + batch)
+    x = np.stack([uniform_limbs(rng, prm.q, o.N) for _ in range(batch)])
+    d = fides.to_device(x)
+    ctx.ntt(d)
+    got = fides.to_host(d)
+    ids = list(range(36))
+    for b in range(batch):
+        assert np.array_equal(got[b], o.ntt(x[b], ids)), f"poly {b}"
+    ctx.intt(d)
+    assert eq(d, x)
+
+
+def test_ntt_config_b_batch64_roundtrip(fides):
+    """Full 64-polynomial batch: INTT(NTT(x)) == x everywhere, and every 9th polynomial
+    bit-exact against the oracle (size-independent check of the whole batch)."""
+    from fides_b200 import params as P
+    prm = P.config_b()
+    o = O.Oracle(16, prm.q, [], 1)
+    ctx = fides.Context(16, prm.q, [], 1)
+    rng = xrng(264)
+    x = np.stack([uniform_limbs(rng, prm.q, o.N) for _ in range(64)])
+    d = fides.to_device(x)
+    ctx.ntt(d)
+    got = fides.to_host(d)
+    for b in range(0, 64, 9):
+        assert np.array_equal(got[b], o.ntt(x[b], list(range(36))))
+    ctx.intt(d)
+    assert eq(d, x)
+
+
+@pytest.mark.parametrize("logN", [10, 11, 12, 13, 14, 15, 17])
+def test_ntt_all_sizes(fides, logN):
+    q = O.gen_primes(logN, 60, 1) + O.gen_primes(logN, 50, 2)
+    o = O.Oracle(logN, q, [], 1)
+    ctx = fides.Context(logN, q, [], 1)
+    x = uniform_limbs(xrng(logN), q, o.N)
+    d = fides.to_device(x)
+    ctx.ntt(d)
+    assert eq(d, o.ntt(x, [0, 1, 2]))
+    ctx.intt(d)
+    assert eq(d, x)
+
+
+def test_ntt_uneven_limb_list(fides):
+    """One launch over limbs of different primes and different polynomials."""
+    from fides_b200 import params as P
+    prm = P.config_a()
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    ctx = fides.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    ids = [3, 0, 7, 7, 1, 8, 2]
+    x = np.stack([xrng(i).integers(0, o.primes[p], o.N, dtype=np.uint64) for i, p in enumerate(ids)])
+    ts = [fides.to_device(x[i]) for i in range(len(ids))]
+    ctx.ntt_limbs(ts, ids)
+    for i, p in enumerate(ids):
+        assert eq(ts[i], o.ntt(x[i:i + 1], [p])[0])
+
+
+def test_ntt_reference_primes(fides):
+    """The reference's own NTT test moduli (p64 / sp64, up to 62 bits)."""
+    import json, os
+    from conftest import GOLDEN
+    rp = json.load(open(os.path.join(GOLDEN, "ref_params.json")))
+    q = rp["p64"][:6] + rp["sp64"][:3]
+    for logN in (13, 16):
+        o = O.Oracle(logN, q, [], 1)
+        ctx = fides.Context(logN, q, [], 1)
+        x = uniform_limbs(xrng(77), q, o.N)
+        d = fides.to_device(x)
+        ctx.ntt(d)
+        assert eq(d, o.ntt(x, list(range(len(q)))))
+        ctx.intt(d)
+        assert eq(d, x)
+
+
+# ---------------------------------------------------------------- key switching pieces
+@pytest.mark.parametrize("level", [30, 16, 6])
+def test_modup_ksk_moddown_config_c(Cfg, level):
+    F, o = Cfg.F, Cfg.o
+    x = Cfg.rand_ct(level, 300 + level)[0]
+    xd = F.to_device(x)
+    dig = Cfg.ctx.modup(xd)
+    dig_ref = o.modup(x)
+    assert eq(dig, dig_ref)
+    a, b = Cfg.ctx.ksk_inner_product(dig, level, Cfg.rk_d)
+    a_ref, b_ref = o.ksk_ip(dig_ref, level, Cfg.rk)
+    assert eq(a, a_ref) and eq(b, b_ref)
+    assert eq(Cfg.ctx.moddown(a), o.moddown(a_ref))
+    f0, f1 = Cfg.ctx.keyswitch(xd, Cfg.rk_d)
+    g0, g1 = o.keyswitch(x, Cfg.rk)
+    assert eq(f0, g0) and eq(f1, g1)
+
+
+def test_moddown_of_scaled_input_is_identity(Cfg):
+    """ModDown(P * x) == x exactly: special limbs are zero (size-independent property)."""
+    F, o, l = Cfg.F, Cfg.o, 30
+    x = Cfg.rand_ct(l, 31)[0]
+    Pm = []
+    for q in Cfg.prm.q[:l]:
+        v = 1
+        for p in Cfg.prm.p:
+            v = v * p % q
+        Pm.append(v)
+    ext = np.zeros((l + Cfg.prm.K, o.N), dtype=np.uint64)
+    ext[:l] = o.mul(x, np.array([[v] * o.N for v in Pm], dtype=np.uint64), list(range(l)))
+    assert eq(Cfg.ctx.moddown(F.to_device(ext)), x)
+
+
+# ---------------------------------------------------------------- ciphertext ops
+@pytest.mark.parametrize("level", [30, 16, 6, 2])
+def test_rescale(Cfg, level):
+    x = Cfg.rand_ct(level, 400 + level)[0]
+    assert eq(Cfg.ctx.rescale_poly(Cfg.F.to_device(x)), Cfg.o.rescale(x))
+
+
+@pytest.mark.parametrize("rescale", [True, False])
+def test_hmult_config_a(A, rescale):
+    a, b = A.rand_ct(6, 1), A.rand_ct(6, 2)
+    out = A.ctx.mult(A.dev_ct(a), A.dev_ct(b), A.rk_d, rescale=rescale)
+    r0, r1 = A.o.hmult(*a, *b, A.rk, rescale=rescale)
+    assert eq(out.c0, r0) and eq(out.c1, r1)
+
+
+@pytest.mark.parametrize("level", [30, 16, 6])
+def test_hmult_config_c(Cfg, level):
+    a, b = Cfg.rand_ct(level, 10 + level), Cfg.rand_ct(level, 20 + level)
+    out = Cfg.ctx.mult(Cfg.dev_ct(a), Cfg.dev_ct(b), Cfg.rk_d, rescale=True)
+    r0, r1 = Cfg.o.hmult(*a, *b, Cfg.rk, rescale=True)
+    assert eq(out.c0, r0) and eq(out.c1, r1)
+
+
+@pytest.mark.parametrize("r", [1, -1, 5])
+def test_rotate_config_a(A, r):
+    c = A.rand_ct(6, 50 + r)
+    out = A.ctx.rotate(A.dev_ct(c), A.rot_d[r], r)
+    r0, r1 = A.o.rotate(*c, A.rot[r], r)
+    assert eq(out.c0, r0) and eq(out.c1, r1)
+
+
+def test_conjugate_config_a(A):
+    c = A.rand_ct(6, 60)
+    k = 2 * A.o.N - 1
+    key = A.kg.auto_key(k)
+    out = A.ctx.rotate_auto(A.dev_ct(c), A.F.to_device(key), k)
+    r0, r1 = A.o.rotate_auto(*c, key, k)
+    assert eq(out.c0, r0) and eq(out.c1, r1)
+
+
+@pytest.mark.parametrize("level", [30, 16, 6])
+def test_rotate_config_c(Cfg, level):
+    c = Cfg.rand_ct(level, 70 + level)
+    out = Cfg.ctx.rotate(Cfg.dev_ct(c), Cfg.rot_d[1], 1)
+    r0, r1 = Cfg.o.rotate(*c, Cfg.rot[1], 1)
+    assert eq(out.c0, r0) and eq(out.c1, r1)
+
+
+@pytest.mark.parametrize("level", [16, 6])
+def test_hoisted_config_c(Cfg, level):
+    c = Cfg.rand_ct(level, 80 + level)
+    rs = [1, -1, 2, 128, -128]
+    outs = Cfg.ctx.rotate_hoisted(Cfg.dev_ct(c), [Cfg.rot_d[r] for r in rs], rs)
+    h0, h1 = Cfg.o.rotate_hoisted(*c, [Cfg.rot[r] for r in rs], rs)
+    for j in range(len(rs)):
+        assert eq(outs[j].c0, h0[j]) and eq(outs[j].c1, h1[j])
+
+
+def test_batched_mixed_levels_equal_singles(Cfg):
+    """One batched launch sequence over uneven levels == per-op results == oracle."""
+    levels = [30, 7, 16, 2, 23]
+    pairs = [(Cfg.dev_ct(Cfg.rand_ct(l, 500 + l)), Cfg.dev_ct(Cfg.rand_ct(l, 600 + l))) for l in levels]
+    outs = Cfg.ctx.mult_batch(pairs, Cfg.rk_d, rescale=True)
+    for (a, b), o in zip(pairs, outs):
+        s = Cfg.ctx.mult(a, b, Cfg.rk_d, rescale=True)
+        assert torch.equal(s.c0, o.c0) and torch.equal(s.c1, o.c1)
+    l = 7
+    a, b = Cfg.rand_ct(l, 500 + l), Cfg.rand_ct(l, 600 + l)
+    r0, r1 = Cfg.o.hmult(*a, *b, Cfg.rk, rescale=True)
+    assert eq(outs[1].c0, r0) and eq(outs[1].c1, r1)
+    jobs = [(Cfg.dev_ct(Cfg.rand_ct(l, 700 + l)), Cfg.rot_d[r], r) for l, r in zip(levels, [1, -1, 2, 128, -128])]
+    routs = Cfg.ctx.rotate_batch(jobs)
+    for (ct, key, r), o in zip(jobs, routs):
+        s = Cfg.ctx.rotate(ct, key, r)
+        assert torch.equal(s.c0, o.c0) and torch.equal(s.c1, o.c1)
+
+
+def test_host_entry_points(Cfg):
+    l = 16
+    a, b = Cfg.rand_ct(l, 900), Cfg.rand_ct(l, 901)
+    key = Cfg.ctx.key_upload(Cfg.rk)
+    try:
+        o0, o1 = Cfg.ctx.mult_host(*a, *b, key, rescale=True)
+        r0, r1 = Cfg.o.hmult(*a, *b, Cfg.rk, rescale=True)
+        assert np.array_equal(o0, r0) and np.array_equal(o1, r1)
+    finally:
+        Cfg.ctx.key_free(key)
+    rk = Cfg.ctx.key_upload(Cfg.rot[2])
+    try:
+        o0, o1 = Cfg.ctx.rotate_host(*a, rk, 2)
+        r0, r1 = Cfg.o.rotate(*a, Cfg.rot[2], 2)
+        assert np.array_equal(o0, r0) and np.array_equal(o1, r1)
+    finally:
+        Cfg.ctx.key_free(rk)
+
+
+def test_error_statuses(Cfg):
+    F = Cfg.F
+    c = Cfg.dev_ct(Cfg.rand_ct(4, 1))
+    with pytest.raises(F.FidesError) as e:
+        Cfg.ctx.mult(c, c, None)
+    assert e.value.code == -5
+    bad = F.Ciphertext(Cfg.ctx.empty(31), Cfg.ctx.empty(31))
+    with pytest.raises(F.FidesError) as e:
+        Cfg.ctx.rotate(bad, Cfg.rot_d[1], 1)
+    assert e.value.code == -4
+    Cfg.ctx.set_scratch_limit(1 << 20)
+    try:
+        with pytest.raises(F.FidesError) as e:
+            Cfg.ctx.mult(c, c, Cfg.rk_d)
+        assert e.value.code == -3
+    finally:
+        Cfg.ctx.set_scratch_limit(0)
+    out = Cfg.ctx.mult(c, c, Cfg.rk_d)  # context still usable
+    assert out.level == 3
+
+
+def test_decrypt_valid_config_c_k9(fides):
+    """K = 9 (reference sizing rule): results decrypt to the FP64 product / rotation."""
+    from fides_b200 import params as P
+    s = Setup(fides, P.config_c(9), rot=(1,))
+    N, D, l = s.o.N, 2.0 ** 50, 30
+    rng = xrng(33)
+    z1 = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    z2 = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    c = s.kg.encrypt(encode(z1, N, D).astype(np.int64), l)
+    d = s.kg.encrypt(encode(z2, N, D).astype(np.int64), l)
+    out = s.ctx.mult(s.dev_ct(c), s.dev_ct(d), s.rk_d, rescale=True)
+    got = decode(s.kg.decrypt_limb0(fides.to_host(out.c0), fides.to_host(out.c1)), N, D * D / s.prm.q[l - 1])
+    assert np.abs(got - z1 * z2).max() < 1e-6
+    rot = s.ctx.rotate(s.dev_ct(c), s.rot_d[1], 1)
+    got = decode(s.kg.decrypt_limb0(fides.to_host(rot.c0), fides.to_host(rot.c1)), N, D)
+    assert np.abs(got - np.roll(z1, -1)).max() < 1e-6

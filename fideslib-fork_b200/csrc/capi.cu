@@ -146,7 +146,7 @@ int fides_ntt_limbs(fides_ctx* x, uint64_t* const* limbs, const int* prime_ids, 
     for (int i = 0; i < n_limbs; ++i) {
       need(limbs[i], "limb");
       if (prime_ids[i] < 0 || prime_ids[i] >= c->n_q + c->K) throw fides::Error(FIDES_ERR_ARG, "bad prime id");
-      v[i] = fides::LimbRef{limbs[i], prime_ids[i], 0};
+      v[i] = fides::lref(limbs[i], prime_ids[i]);
     }
     fides::ntt_limbs(c, v.data(), n_limbs, inverse != 0, S(stream));
   });

@@ -1,5 +1,6 @@
 // Elementwise RNS kernels, basis conversion and KSK inner product.
 #include <algorithm>
+#include <vector>
 
 #include "kernels.cuh"
 
@@ -17,39 +18,60 @@ __device__ __forceinline__ uint32_t auto_slot(int logN, uint32_t k, uint32_t j) 
 constexpr int MAX_SRC = 64;   // limbs on the source side of one conversion
 constexpr int MAX_DST = 128;  // limbs on the destination side
 
+// Basis conversion.  NS (source limbs) is a template parameter so that the pre-scaled
+// sources stay in registers; NS = 0 is the generic width.  Each thread converts two
+// adjacent coefficients (16-byte accesses); destination primes, output positions and the
+// conversion matrix are staged in shared memory (broadcast reads).
+template <int NS>
 __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant__ ConvJobList L, const DevPrime* primes,
                                                           int logN) {
   const ConvJob& J = L.j[blockIdx.y];
   const ConvTable& T = J.t;
   extern __shared__ uint64_t sm[];
-  const int ns = T.n_src, nd = T.n_dst;
-  ShoupConst* pre = reinterpret_cast<ShoupConst*>(sm);  // [n_src], 16-byte aligned
-  uint64_t* mat = sm + 2 * ns;                          // [n_src][n_dst]
+  const int ns = NS ? NS : T.n_src, nd = T.n_dst;
+  ShoupConst* pre = reinterpret_cast<ShoupConst*>(sm);       // [ns]
+  DevPrime* dp = reinterpret_cast<DevPrime*>(sm + 2 * ns);   // [nd]
+  uint64_t* mat = sm + 2 * ns + 8 * nd;                      // [ns][nd]
+  int* dpos = reinterpret_cast<int*>(mat + ns * nd);         // [nd]
   for (int i = threadIdx.x; i < ns * nd; i += blockDim.x) mat[i] = T.mat[i];
   for (int i = threadIdx.x; i < ns; i += blockDim.x) pre[i] = T.pre[i];
+  for (int j = threadIdx.x; j < nd; j += blockDim.x) {
+    dp[j] = primes[T.dst_prime[j]];
+    dpos[j] = T.dst_pos[j];
+  }
   __syncthreads();
   const int N = 1 << logN;
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  uint64_t y[MAX_SRC];
-#pragma unroll 4
-  for (int i = 0; i < ns; ++i) {
-    const DevPrime& p = primes[T.src_prime[i]];
-    uint64_t v = J.src[(size_t)T.src_pos[i] * N + n];
-    y[i] = shoup(v, pre[i].w, pre[i].ws, p.q);
+  const int n = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  constexpr int R = NS ? NS : MAX_SRC;
+  uint64_t y0[R], y1[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    if (NS == 0 && i >= ns) break;
+    const uint64_t q = primes[T.src_prime[i]].q;
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(J.src + (size_t)T.src_pos[i] * N + n);
+    y0[i] = shoup(v.x, pre[i].w, pre[i].ws, q);
+    y1[i] = shoup(v.y, pre[i].w, pre[i].ws, q);
   }
+  uint64_t* dst = J.dst + n;
   for (int j = 0; j < nd; ++j) {
-    const DevPrime p = primes[T.dst_prime[j]];
-    U128 acc{0, 0};
-    int i = 0;
-    while (i < ns) {
-      const int e = min(ns, i + 8);
-      for (; i < e; ++i) mac128(acc, y[i], mat[i * nd + j]);
-      if (i < ns) acc = U128{reduce128(acc, p), 0};  // keep the sum below 2^128
+    const DevPrime p = dp[j];
+    U128 a0{0, 0}, a1{0, 0};
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      if (NS == 0 && i >= ns) break;
+      if (i && (i & 7) == 0) {  // keep the sums below 2^128
+        a0 = U128{reduce128(a0, p), 0};
+        a1 = U128{reduce128(a1, p), 0};
+      }
+      const uint64_t m = mat[i * nd + j];
+      mac128(a0, y0[i], m);
+      mac128(a1, y1[i], m);
     }
-    J.dst[(size_t)T.dst_pos[j] * N + n] = reduce128(acc, p);
+    *reinterpret_cast<ulonglong2*>(dst + (size_t)dpos[j] * N) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
   }
 }
 
+// Two adjacent coefficients per thread (16-byte loads of every stream).
 __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
                                                          const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
                                                          int alpha) {
@@ -58,28 +80,53 @@ __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__
   const int i = blockIdx.y;
   if (i >= ext) return;
   const int N = 1 << logN;
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int pid = i < l ? i : n_q + (i - l);
   const DevPrime p = primes[pid];
   const int beta = (l + alpha - 1) / alpha;
   const int own = i < l ? i / alpha : -1;
   const size_t kstride = (size_t)(n_q + K) * N;
-  U128 sa{0, 0}, sb{0, 0};
+  auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
+  U128 sa0{0, 0}, sb0{0, 0}, sa1{0, 0}, sb1{0, 0};
   for (int d = 0; d < beta; ++d) {
-    uint64_t v = (d == own && J.x) ? J.x[(size_t)i * N + n] : J.digits[((size_t)d * ext + i) * N + n];
-    uint64_t ka = J.key[(size_t)d * kstride + (size_t)pid * N + n];
-    uint64_t kb = J.key[(size_t)(dnum + d) * kstride + (size_t)pid * N + n];
-    mac128(sa, v, ka);
-    mac128(sb, v, kb);
+    ulonglong2 v;
+    if (d == own && J.x) {
+      v = ld2(J.x + (size_t)i * N + n);
+      if (J.x2) {
+        ulonglong2 w = ld2(J.x2 + (size_t)i * N + n);
+        v.x = mulmod(v.x, w.x, p);
+        v.y = mulmod(v.y, w.y, p);
+      }
+    } else {
+      v = ld2(J.digits + ((size_t)d * ext + i) * N + n);
+    }
+    const ulonglong2 ka = ld2(J.key + (size_t)d * kstride + (size_t)pid * N + n);
+    const ulonglong2 kb = ld2(J.key + (size_t)(dnum + d) * kstride + (size_t)pid * N + n);
+    mac128(sa0, v.x, ka.x);
+    mac128(sb0, v.x, kb.x);
+    mac128(sa1, v.y, ka.y);
+    mac128(sb1, v.y, kb.y);
   }
-  uint64_t ra = reduce128(sa, p), rb = reduce128(sb, p);
+  uint64_t ra0 = reduce128(sa0, p), rb0 = reduce128(sb0, p);
+  uint64_t ra1 = reduce128(sa1, p), rb1 = reduce128(sb1, p);
   if (J.c0 && i < l) {
     const ShoupConst pm = pmod[i];
-    rb = addmod(rb, shoup(J.c0[(size_t)i * N + n], pm.w, pm.ws, p.q), p.q);
+    const ulonglong2 c = ld2(J.c0 + (size_t)i * N + n);
+    rb0 = addmod(rb0, shoup(c.x, pm.w, pm.ws, p.q), p.q);
+    rb1 = addmod(rb1, shoup(c.y, pm.w, pm.ws, p.q), p.q);
   }
-  const uint32_t o = J.auto_k ? auto_slot(logN, J.auto_k, (uint32_t)n) : (uint32_t)n;
-  J.out_a[(size_t)i * N + o] = ra;
-  J.out_b[(size_t)i * N + o] = rb;
+  uint64_t* oa = J.out_a + (size_t)i * N;
+  uint64_t* ob = J.out_b + (size_t)i * N;
+  if (J.auto_k) {
+    const uint32_t o0 = auto_slot(logN, J.auto_k, (uint32_t)n), o1 = auto_slot(logN, J.auto_k, (uint32_t)n + 1);
+    oa[o0] = ra0;
+    ob[o0] = rb0;
+    oa[o1] = ra1;
+    ob[o1] = rb1;
+  } else {
+    *reinterpret_cast<ulonglong2*>(oa + n) = make_ulonglong2(ra0, ra1);
+    *reinterpret_cast<ulonglong2*>(ob + n) = make_ulonglong2(rb0, rb1);
+  }
 }
 
 __global__ void __launch_bounds__(EW_THREADS) moddown_finish_kernel(const __grid_constant__ FinJobList L,
@@ -109,20 +156,7 @@ __global__ void __launch_bounds__(EW_THREADS) tensor_kernel(const __grid_constan
   mac128(acc, x0, y1);
   mac128(acc, x1, y0);
   J.d1[off] = reduce128(acc, p);
-  J.d2[off] = mulmod(x1, y1, p);
-}
-
-// OpenFHE SwitchModulus as restated in the reference (src/CKKS/Rescale.cuh:44-64).
-__device__ __forceinline__ uint64_t switch_modulus(uint64_t a, const DevPrime& om, const DevPrime& nm) {
-  const uint64_t half = om.q >> 1;
-  if (nm.q > om.q) {
-    if (a > half) a += nm.q - om.q;
-    return a;
-  }
-  const uint64_t diff = nm.q - shoup(om.q, 1, nm.one_s, nm.q);  // nm - (om mod nm)
-  if (a > half) a += diff;
-  if (a >= nm.q) a = shoup(a, 1, nm.one_s, nm.q);
-  return a;
+  if (J.d2) J.d2[off] = mulmod(x1, y1, p);
 }
 
 __global__ void __launch_bounds__(EW_THREADS) switch_kernel(const __grid_constant__ SwitchJobList L,
@@ -160,26 +194,54 @@ int fill(List& L, const Job* jobs, int n) {
 
 void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
   static thread_local ConvJobList L;
-  for (int off = 0; off < n; off += MAX_CONV_JOBS) {
-    int m = std::min(MAX_CONV_JOBS, n - off);
-    fill(L, jobs + off, m);
-    size_t smem = 0;
-    for (int i = 0; i < m; ++i) {
-      const ConvTable& t = L.j[i].t;
-      if (t.n_src > MAX_SRC || t.n_dst > MAX_DST) throw Error(-1, "basis conversion too wide");
-      smem = std::max(smem, (size_t)t.n_src * t.n_dst * 8 + (size_t)t.n_src * 16);
+  // Group jobs by source width so each launch uses one specialised kernel.
+  std::vector<ConvJob> byw[MAX_SRC + 1];
+  for (int i = 0; i < n; ++i) {
+    const ConvTable& t = jobs[i].t;
+    if (t.n_src > MAX_SRC || t.n_dst > MAX_DST || t.n_src < 1) throw Error(-1, "basis conversion width out of range");
+    byw[t.n_src].push_back(jobs[i]);
+  }
+  for (int w = 1; w <= MAX_SRC; ++w) {
+    const auto& v = byw[w];
+    for (size_t off = 0; off < v.size(); off += MAX_CONV_JOBS) {
+      int m = (int)std::min<size_t>(MAX_CONV_JOBS, v.size() - off);
+      fill(L, v.data() + off, m);
+      size_t smem = 0;
+      double bytes = 0;
+      for (int i = 0; i < m; ++i) {
+        const ConvTable& t = L.j[i].t;
+        smem = std::max(smem, (size_t)t.n_src * t.n_dst * 8 + (size_t)t.n_src * 16 + (size_t)t.n_dst * 68);
+        bytes += 8.0 * c->N * (t.n_src + t.n_dst);
+      }
+      dim3 grid(c->N / (2 * EW_THREADS), m);
+      LaunchScope ls(c, s, KK_CONV, bytes);
+      switch (w) {
+#define FIDES_CONV_CASE(K)                                                                                    \
+  case K: {                                                                                                   \
+    static bool attr = false;                                                                                 \
+    if (!attr) {                                                                                              \
+      FIDES_CUDA(cudaFuncSetAttribute(conv_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); \
+      attr = true;                                                                                            \
+    }                                                                                                         \
+    conv_kernel<K><<<grid, EW_THREADS, smem, s>>>(L, c->d_prime, c->logN);                                    \
+    break;                                                                                                    \
+  }
+        FIDES_CONV_CASE(1) FIDES_CONV_CASE(2) FIDES_CONV_CASE(3) FIDES_CONV_CASE(4) FIDES_CONV_CASE(5)
+        FIDES_CONV_CASE(6) FIDES_CONV_CASE(7) FIDES_CONV_CASE(8) FIDES_CONV_CASE(9) FIDES_CONV_CASE(10)
+        FIDES_CONV_CASE(11) FIDES_CONV_CASE(12) FIDES_CONV_CASE(13) FIDES_CONV_CASE(14) FIDES_CONV_CASE(15)
+        FIDES_CONV_CASE(16)
+#undef FIDES_CONV_CASE
+        default: {
+          static bool attr = false;
+          if (!attr) {
+            FIDES_CUDA(cudaFuncSetAttribute(conv_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr = true;
+          }
+          conv_kernel<0><<<grid, EW_THREADS, smem, s>>>(L, c->d_prime, c->logN);
+        }
+      }
+      FIDES_CUDA(cudaGetLastError());
     }
-    static bool attr = false;
-    if (!attr) {
-      FIDES_CUDA(cudaFuncSetAttribute(conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-      attr = true;
-    }
-    dim3 grid(c->N / EW_THREADS, m);
-    double bytes = 0;
-    for (int i = 0; i < m; ++i) bytes += 8.0 * c->N * (L.j[i].t.n_src + L.j[i].t.n_dst);
-    LaunchScope ls(c, s, KK_CONV, bytes);
-    conv_kernel<<<grid, EW_THREADS, smem, s>>>(L, c->d_prime, c->logN);
-    FIDES_CUDA(cudaGetLastError());
   }
 }
 
@@ -190,7 +252,7 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     fill(L, jobs + off, m);
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
-    dim3 grid(c->N / EW_THREADS, mx, m);
+    dim3 grid(c->N / (2 * EW_THREADS), mx, m);
     double bytes = 0;
     for (int i = 0; i < m; ++i) {
       const int l = L.j[i].l, ext = l + c->K, b = c->beta(l);
@@ -227,7 +289,7 @@ void launch_tensor(Context* c, const TensorJob* jobs, int n, cudaStream_t s) {
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l);
     dim3 grid(c->N / EW_THREADS, mx, m);
     double bytes = 0;
-    for (int i = 0; i < m; ++i) bytes += 8.0 * c->N * (7.0 * L.j[i].l);
+    for (int i = 0; i < m; ++i) bytes += 8.0 * c->N * ((L.j[i].d2 ? 7.0 : 6.0) * L.j[i].l);
     LaunchScope ls(c, s, KK_ELEM, bytes);
     tensor_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->logN);
     FIDES_CUDA(cudaGetLastError());

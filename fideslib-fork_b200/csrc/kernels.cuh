@@ -29,6 +29,7 @@ void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s);
 // automorphism scatter of both outputs.
 struct KskJob {
   const uint64_t* x;       // EVAL input at level l (own-digit limbs)
+  const uint64_t* x2;      // optional: the input is x * x2 (tensor term a1 b1, never materialised)
   const uint64_t* digits;  // [beta][l + K][N] ModUp output (EVAL)
   const uint64_t* key;     // [2][dnum][n_q + K][N]
   const uint64_t* c0;      // optional: add P * c0 to out_b's Q limbs

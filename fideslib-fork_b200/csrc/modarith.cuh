@@ -67,4 +67,18 @@ __device__ __forceinline__ uint64_t mulmod(uint64_t a, uint64_t b, const DevPrim
   return reduce128(t, p);
 }
 
+// OpenFHE SwitchModulus as restated in the reference (src/CKKS/Rescale.cuh:44-64): a
+// residue of the old prime `om` re-expressed modulo `nm` with the centred lift.
+__device__ __forceinline__ uint64_t switch_modulus(uint64_t a, const DevPrime& om, const DevPrime& nm) {
+  const uint64_t half = om.q >> 1;
+  if (nm.q > om.q) {
+    if (a > half) a += nm.q - om.q;
+    return a;
+  }
+  const uint64_t diff = nm.q - shoup(om.q, 1, nm.one_s, nm.q);  // nm - (om mod nm)
+  if (a > half) a += diff;
+  if (a >= nm.q) a = shoup(a, 1, nm.one_s, nm.q);
+  return a;
+}
+
 }  // namespace fides

@@ -10,10 +10,16 @@
 //     inverse = ROW then COL; each pass reads and writes every limb once.
 //   * each thread keeps 2^LOGE elements in registers and runs LOGE stages per chunk;
 //     chunks exchange through padded shared memory (conflict-free);
-//   * Harvey lazy butterflies: values stay in [0, 4q) (forward) / [0, 2q) (inverse)
-//     between stages, one 64-bit Shoup product per butterfly, so primes must be < 2^62;
+//   * lazy butterflies with one 64-bit Shoup product each (primes < 2^62): the forward
+//     transform skips every conditional subtraction for q < 2^58 (values stay below 35q)
+//     and uses Harvey's [0, 4q) form otherwise; the inverse tracks a bound B (a multiple
+//     of q) and subtracts only once B passes 2^62;
 //   * one launch covers any list of limbs (any polynomials, any levels): blockIdx.y
-//     indexes a limb descriptor (pointer + prime id) passed by value.
+//     indexes a limb descriptor (pointer + prime id) passed by value;
+//   * the first pass may read from a separate source (out of place) or compute its input
+//     (prologue), and the last pass may combine its result with other operands before
+//     storing (epilogue) -- the reference's NTT fusion modes (src/NTT.cuh:39-69,
+//     src/NTTfusions.cuh:12-336) as compile-time variants.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -21,13 +27,33 @@
 
 namespace fides {
 
-struct LimbRef {
-  uint64_t* ptr;
-  int prime;
-  int pad;
+// What the first pass loads.
+enum NttIn {
+  IN_PLAIN = 0,   // x = src[i]  (src = ptr when in place)
+  IN_MUL = 1,     // inverse only: x = src[i] * pro[i] mod q   (tensor term a1 b1)
+  IN_SWITCH = 2,  // forward only: x = SwitchModulus(pro[i]) from prime aux - 1 (rescale)
+};
+// What the last pass stores to ptr.
+enum NttOut {
+  OUT_PLAIN = 0,
+  OUT_MODDOWN = 1,  // forward only: out = (ep0[i] - v) P^-1 (+ ep1[i])     (ModDown finish)
+  OUT_RESCALE = 2,  // forward only: out = qinv_l ep0[i] + QlQlInv_l v, l = aux (rescale finish)
 };
 
-constexpr int MAX_NTT_LIMBS = 1024;
+struct LimbRef {
+  uint64_t* ptr;          // output (and input of the first pass when src is null)
+  const uint64_t* src;    // optional input of the first pass
+  const uint64_t* pro;    // prologue operand
+  const uint64_t* ep0;    // epilogue operands
+  const uint64_t* ep1;
+  int prime;
+  int aux;  // IN_SWITCH / OUT_RESCALE: the level l being rescaled (top prime l - 1)
+  uint64_t pad;
+};
+
+inline LimbRef lref(uint64_t* p, int prime) { return LimbRef{p, nullptr, nullptr, nullptr, nullptr, prime, 0, 0}; }
+
+constexpr int MAX_NTT_LIMBS = 448;
 
 struct NttLimbList {
   int n;
@@ -36,7 +62,9 @@ struct NttLimbList {
 };
 
 // Launch a full forward or inverse transform over `n` limbs (any n; split internally).
-void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream_t s);
+// The prologue/epilogue modes apply to every limb of the call.
+void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream_t s, NttIn in = IN_PLAIN,
+               NttOut out = OUT_PLAIN);
 // Convenience: n_polys polynomials of `n_limbs` consecutive limbs starting at `data`,
 // limb i of each poly using prime id prime_ids[i].
 void ntt_polys(Context* c, uint64_t* data, int n_polys, int n_limbs, const int* prime_ids, bool inverse,

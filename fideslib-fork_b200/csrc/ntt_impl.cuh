@@ -1,0 +1,353 @@
+// Templates of the NTT pass kernels (see ntt.cuh).  Each ntt_inst_<logN>.cu instantiates
+// the passes of one ring dimension so that the variants compile in parallel.
+#pragma once
+#include <algorithm>
+
+#include "ntt.cuh"
+
+namespace fides {
+namespace nttk {
+
+constexpr int COL = 0, ROW = 1;
+
+constexpr int LOGE = 4;  // 16 elements per thread
+constexpr int G = 16;    // sub-transforms per CTA
+
+__device__ __forceinline__ ShoupConst ld_tw(const ShoupConst* p) {
+  ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+  return ShoupConst{v.x, v.y};
+}
+
+// Cooley-Tukey butterfly, Harvey lazy form: x, y in [0, 4q) -> [0, 4q).
+__device__ __forceinline__ void ct_bf(uint64_t& x, uint64_t& y, ShoupConst w, uint64_t q, uint64_t q2) {
+  uint64_t a = csub(x, q2);
+  uint64_t t = shoup_lazy(y, w.w, w.ws, q);
+  x = a + t;
+  y = a - t + q2;
+}
+
+// Cooley-Tukey butterfly without any conditional subtraction, for q < 2^58: inputs below
+// B give outputs below B + 2q; over at most 17 stages from [0, q) values stay below 35q.
+__device__ __forceinline__ void ct_bf_small(uint64_t& x, uint64_t& y, ShoupConst w, uint64_t q, uint64_t q2) {
+  uint64_t t = shoup_lazy(y, w.w, w.ws, q);
+  uint64_t a = x;
+  x = a + t;
+  y = a - t + q2;
+}
+
+// Gentleman-Sande butterfly with a tracked bound B (a multiple of q, values < B <= 2^63):
+// the sum doubles the bound unless `red` (B > 2^62), in which case it is brought back
+// below B by one conditional subtraction; the difference path leaves a Shoup product in
+// [0, 2q).  With q < 2^62 this degenerates to Harvey's form once B reaches 2q.
+__device__ __forceinline__ void gs_bf(uint64_t& x, uint64_t& y, ShoupConst w, uint64_t q, uint64_t B, bool red) {
+  uint64_t s = x + y;
+  if (red) s = csub(s, B);
+  uint64_t d = x - y + B;
+  y = shoup_lazy(d, w.w, w.ws, q);
+  x = s;
+}
+
+struct PassArgs {
+  const DevPrime* primes;
+  const ShoupConst* tw;        // forward or inverse twiddles, [prime][N]
+  const ShoupConst* inv_last;  // [prime]: psi_rev^-1[1] * N^-1
+  const ShoupConst* pinv;      // [Q prime]: P^-1 mod q (OUT_MODDOWN)
+  const RescaleConst* rescale; // [level][Q prime] (OUT_RESCALE)
+  int logN;
+  int log1;  // size of the column sub-transform
+  int n_q;
+};
+
+// Element index u of register r for thread t, when the register index spans bits
+// [lo, lo + LOGE) of u.
+template <int LO>
+__device__ __forceinline__ int u_of(int t, int r) {
+  // disjoint bit fields: '+' lets the compiler fold the register-index part into offsets
+  return ((t >> LO) << (LO + LOGE)) + (r << LO) + (t & ((1 << LO) - 1));
+}
+
+template <int LOGP>
+__device__ __forceinline__ int padu(int u) {
+  return u + (u >> LOGE);
+}
+
+// Butterflies of pair bits [BLO, BHI] (in u) for a thread whose registers span bits
+// [LO, LO + LOGE).  FWD walks bits high -> low, inverse low -> high.
+template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS, bool SMALL>
+__device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int sub, int sbase, const ShoupConst* tw,
+                                          const DevPrime& pr, ShoupConst last, uint64_t& B) {
+  constexpr int E = 1 << LOGE;
+  const int th = t >> LO;
+#pragma unroll
+  for (int k = 0; k <= BHI - BLO; ++k) {
+    const int b = FWD ? (BHI - k) : (BLO + k);
+    const int rb = b - LO;
+    const int sig = LOGP - 1 - b;  // stage within this pass
+    const int s = sbase + sig;     // global stage
+    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LOGE - b - 1));
+    const bool red = !FWD && B > (1ull << 62);
+#pragma unroll
+    for (int hi = 0; hi < (E >> (rb + 1)); ++hi) {
+      if (!FWD && PASS == COL && b == LOGP - 1) {
+        // last inverse stage (global stage 0): fold N^-1 into both outputs
+#pragma unroll
+        for (int lr = 0; lr < (1 << rb); ++lr) {
+          const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
+          uint64_t a = x[r0], c = x[r1];
+          x[r0] = shoup(a + c, pr.ninv, pr.ninv_s, pr.q);
+          x[r1] = shoup(a - c + B, last.w, last.ws, pr.q);
+        }
+      } else {
+        const ShoupConst w = ld_tw(tw + base + hi);
+#pragma unroll
+        for (int lr = 0; lr < (1 << rb); ++lr) {
+          const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
+          if (FWD && SMALL)
+            ct_bf_small(x[r0], x[r1], w, pr.q, pr.q2);
+          else if (FWD)
+            ct_bf(x[r0], x[r1], w, pr.q, pr.q2);
+          else
+            gs_bf(x[r0], x[r1], w, pr.q, B, red);
+        }
+      }
+    }
+    if (!FWD && !red) B <<= 1;
+  }
+}
+
+// Bound of the inverse transform's values after `stages` stages from reduced input.
+__device__ __forceinline__ uint64_t inv_bound(uint64_t q, int stages) {
+  uint64_t B = q;
+  for (int i = 0; i < stages; ++i)
+    if (B <= (1ull << 62)) B <<= 1;
+  return B;
+}
+
+
+
+// Register span of chunk c.
+template <int LOGP, bool FWD, int C>
+struct Chunk {
+  // forward: bits from the top; inverse: bits from the bottom
+  static constexpr int BHI = FWD ? (LOGP - 1 - C * LOGE) : (C * LOGE + LOGE - 1 < LOGP - 1 ? C * LOGE + LOGE - 1 : LOGP - 1);
+  static constexpr int BLO = FWD ? (LOGP - (C + 1) * LOGE > 0 ? LOGP - (C + 1) * LOGE : 0) : C * LOGE;
+  static constexpr int LO = FWD ? BLO : (BLO + LOGE <= LOGP ? BLO : LOGP - LOGE);
+};
+
+// The register chunks of one pass, separated by shared-memory exchanges.
+template <int LOGP, int PASS, bool FWD, bool SMALL, typename SIDX>
+__device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, SIDX sidx, int g, int t, int subtw,
+                                       int sbase, const ShoupConst* tw, const DevPrime& pr, ShoupConst last,
+                                       uint64_t& B, bool direct_load) {
+  constexpr int E = 1 << LOGE;
+  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
+  using C0 = Chunk<LOGP, FWD, 0>;
+  run_chunk<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+  if constexpr (NCH > 1) {
+    using C1 = Chunk<LOGP, FWD, 1>;
+    if (!direct_load) __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO>(t, r))] = x[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
+    run_chunk<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+  }
+  if constexpr (NCH > 2) {
+    using C1 = Chunk<LOGP, FWD, 1>;
+    using C2 = Chunk<LOGP, FWD, 2>;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO>(t, r))] = x[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
+    run_chunk<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+  }
+  static_assert(NCH <= 3, "sub-transform too large");
+}
+
+template <int LOGN, int PASS>
+struct PassShape {
+  static constexpr int LOG1 = (LOGN + 1) / 2, LOG2 = LOGN / 2;
+  static constexpr int LOGP = PASS == COL ? LOG1 : LOG2;
+};
+
+// One pass of a transform of 2^LOGN points.  Every index is a compile-time function of
+// LOGN, so global and shared addresses are a per-thread base plus immediate offsets.
+template <int LOGN, int PASS, bool FWD, int IN, int OUT>
+__global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G)
+    ntt_pass(const PassArgs a, const __grid_constant__ NttLimbList L) {
+  constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
+  constexpr int P = 1 << LOGP, E = 1 << LOGE, T = P / E, NT = T * G;
+  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
+  constexpr int PADP = P + P / E;
+  extern __shared__ uint64_t sm[];
+
+  const LimbRef lr = L.limbs[blockIdx.y];
+  const DevPrime pr = a.primes[lr.prime];
+  constexpr int N = 1 << LOGN;
+  const ShoupConst* tw = a.tw + (size_t)lr.prime * N;
+  const ShoupConst last = FWD ? ShoupConst{0, 0} : a.inv_last[lr.prime];
+  uint64_t* data = lr.ptr;
+  const int tid = threadIdx.x;
+  int g, t;
+  if (PASS == COL) {
+    g = tid % G;
+    t = tid / G;
+  } else {
+    t = tid % T;
+    g = tid / T;
+  }
+  constexpr int S = N >> LOGP;  // stride of a column (COL) / number of rows (ROW)
+  const int sub0 = blockIdx.x * G;
+  const int sub = sub0 + g;
+  constexpr int sbase = PASS == COL ? 0 : PassShape<LOGN, COL>::LOGP;
+  const int subtw = PASS == COL ? 0 : sub;
+
+  auto gidx = [&](int s_, int u) -> int { return PASS == COL ? s_ + u * S : s_ * P + u; };
+  auto sidx = [&](int gg, int u) -> int { return PASS == COL ? u * G + gg : gg * PADP + padu<LOGP>(u); };
+
+  uint64_t x[E];
+
+  // ---- input of this pass: the first pass applies the prologue
+  constexpr bool first_pass = FWD ? (PASS == COL) : (PASS == ROW);
+  const uint64_t* in = (first_pass && lr.src) ? lr.src : data;
+  DevPrime opr;
+  if (IN == IN_SWITCH) opr = a.primes[lr.aux - 1];
+  auto load = [&](size_t i) -> uint64_t {
+    if (first_pass && IN == IN_SWITCH) return switch_modulus(lr.pro[i], opr, pr);
+    if (first_pass && IN == IN_MUL) return mulmod(in[i], lr.pro[i], pr);
+    return in[i];
+  };
+
+  // ---- load chunk 0 (direct when lanes map to consecutive addresses, else staged)
+  constexpr int LO0 = Chunk<LOGP, FWD, 0>::LO;
+  constexpr bool direct_load = (PASS == COL) || (LO0 == LOGP - LOGE);
+  if (direct_load) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = load(gidx(sub, u_of<LO0>(t, r)));
+  } else {
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      int e = k * NT + tid;
+      int gg = e / P, u = e % P;
+      sm[sidx(gg, u)] = load(gidx(sub0 + gg, u));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<LO0>(t, r))];
+  }
+
+  // ---- chunks
+  uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
+  if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
+  if (FWD && pr.q < (1ull << 58))
+    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load);
+  else
+    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load);
+
+  // ---- final reduction of the completed transform
+  if (FWD && PASS == ROW) {
+    if (pr.q < (1ull << 58)) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) x[r] = shoup(x[r], 1, pr.one_s, pr.q);  // x < 35q
+    } else {
+#pragma unroll
+      for (int r = 0; r < E; ++r) x[r] = csub(csub(x[r], pr.q2), pr.q);   // x < 4q
+    }
+  }
+
+  // ---- store (the last pass applies the epilogue)
+  ShoupConst pinv{0, 0};
+  RescaleConst rsc{0, 0, 0, 0};
+  if (OUT == OUT_MODDOWN) pinv = a.pinv[lr.prime];
+  if (OUT == OUT_RESCALE) rsc = a.rescale[(size_t)lr.aux * a.n_q + lr.prime];
+  auto store = [&](size_t i, uint64_t v) {
+    if (OUT == OUT_MODDOWN) {
+      v = shoup(submod(lr.ep0[i], v, pr.q), pinv.w, pinv.ws, pr.q);
+      if (lr.ep1) v = addmod(v, lr.ep1[i], pr.q);
+    } else if (OUT == OUT_RESCALE) {
+      v = addmod(shoup(lr.ep0[i], rsc.qinv, rsc.qinv_s, pr.q), shoup(v, rsc.m, rsc.m_s, pr.q), pr.q);
+    }
+    data[i] = v;
+  };
+  constexpr int LOL = Chunk<LOGP, FWD, NCH - 1>::LO;
+  constexpr bool direct_store = (PASS == COL) || (LOL == LOGP - LOGE);
+  if (direct_store) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) store(gidx(sub, u_of<LOL>(t, r)), x[r]);
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<LOL>(t, r))] = x[r];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      int e = k * NT + tid;
+      int gg = e / P, u = e % P;
+      store(gidx(sub0 + gg, u), sm[sidx(gg, u)]);
+    }
+  }
+}
+
+
+template <int LOGN, int PASS, bool FWD, int IN, int OUT>
+void launch_pass(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
+  constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
+  constexpr int P = 1 << LOGP, T = P / (1 << LOGE);
+  constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LOGE))) * (int)sizeof(uint64_t);
+  static bool attr_set = false;  // per instantiation; set before first launch
+  if (!attr_set) {
+    FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+    attr_set = true;
+  }
+  dim3 grid(((1 << LOGN) >> LOGP) / G, L.n);
+  // algorithmic bytes: half of a transform's read + write of each limb (two passes)
+  LaunchScope ls(c, s, KK_NTT, 8.0 * (1 << LOGN) * L.n);
+  ntt_pass<LOGN, PASS, FWD, IN, OUT><<<grid, T * G, smem, s>>>(a, L);
+  FIDES_CUDA(cudaGetLastError());
+}
+
+// The pass sequence of one transform for a given ring dimension.
+template <int LOGN>
+void run_transform(Context* c, const PassArgs& a, const NttLimbList& L, bool inverse, NttIn in, NttOut out,
+                   cudaStream_t s) {
+  if (!inverse) {
+    if (in == IN_SWITCH)
+      launch_pass<LOGN, COL, true, IN_SWITCH, OUT_PLAIN>(c, a, L, s);
+    else
+      launch_pass<LOGN, COL, true, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
+    if (out == OUT_MODDOWN)
+      launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_MODDOWN>(c, a, L, s);
+    else if (out == OUT_RESCALE)
+      launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_RESCALE>(c, a, L, s);
+    else
+      launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
+  } else {
+    if (in == IN_MUL)
+      launch_pass<LOGN, ROW, false, IN_MUL, OUT_PLAIN>(c, a, L, s);
+    else
+      launch_pass<LOGN, ROW, false, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
+    launch_pass<LOGN, COL, false, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
+  }
+}
+
+}  // namespace nttk
+
+// Defined in ntt_inst_<logN>.cu.
+#define FIDES_NTT_DECL(LN)                                                                                  \
+  void ntt_transform_##LN(Context* c, const nttk::PassArgs& a, const NttLimbList& L, bool inverse, NttIn in, \
+                          NttOut out, cudaStream_t s);
+FIDES_NTT_DECL(10)
+FIDES_NTT_DECL(11)
+FIDES_NTT_DECL(12)
+FIDES_NTT_DECL(13)
+FIDES_NTT_DECL(14)
+FIDES_NTT_DECL(15)
+FIDES_NTT_DECL(16)
+FIDES_NTT_DECL(17)
+#undef FIDES_NTT_DECL
+
+}  // namespace fides

@@ -1,0 +1,9 @@
+// Pass kernels of the 2^16-point transform.
+#include "ntt_impl.cuh"
+
+namespace fides {
+void ntt_transform_16(Context* c, const nttk::PassArgs& a, const NttLimbList& L, bool inverse, NttIn in, NttOut out,
+                       cudaStream_t s) {
+  nttk::run_transform<16>(c, a, L, inverse, in, out, s);
+}
+}  // namespace fides

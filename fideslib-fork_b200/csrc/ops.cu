@@ -6,7 +6,14 @@
 //   -> INTT(special limbs) -> ModDown conversion -> NTT -> (x - conv) P^-1
 // and, for rotations, the fused hoisted form (LimbPartitionMGPU.cu:517-667): ModUp(c1),
 // then one KSK pass that adds P c0 and applies the automorphism as a scatter, then ModDown.
-// Each stage is ONE launch over all items of a batch, whatever their levels.
+// Each stage is ONE launch over all items of a batch, whatever their levels, and the
+// elementwise steps around the transforms are fused into them:
+//   * the INTT before ModUp reads its input directly (out of place), or computes the tensor
+//     term a1 b1 on the fly (HMult), so d2 is never written;
+//   * the ModDown finish (x - conv) P^-1 (+ the tensor terms d0 / d1) is the epilogue of the
+//     forward NTT of the converted limbs;
+//   * rescale is INTT(top limb) followed by one forward NTT whose prologue applies
+//     SwitchModulus to the top limb and whose epilogue forms q_l^-1 x + QlQlInv t.
 #include <algorithm>
 #include <cstring>
 
@@ -32,16 +39,20 @@ void check_level(Context* c, int l, int min_l = 1) {
   if (l < min_l || l > c->n_q) throw Error(-4, "level " + std::to_string(l) + " out of range");
 }
 
-// INTT copies of xs into tmps, ModUp conversions into digits, NTT of the new limbs.
-void modup_stage(Context* c, const uint64_t* const* xs, const int* ls, uint64_t* const* tmps,
-                 uint64_t* const* digits, int n, cudaStream_t s) {
+// ModUp of n inputs: INTT of xs[i] (times ys[i] when given) into tmps[i], conversion of each
+// digit into digits[i], NTT of the new limbs.  Own-digit limbs of digits[i] are not written.
+void modup_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
+                 uint64_t* const* tmps, uint64_t* const* digits, int n, cudaStream_t s) {
   const size_t N = c->N;
   std::vector<LimbRef> refs;
-  for (int i = 0; i < n; ++i) {
-    FIDES_CUDA(cudaMemcpyAsync(tmps[i], xs[i], sizeof(uint64_t) * N * ls[i], cudaMemcpyDeviceToDevice, s));
-    for (int j = 0; j < ls[i]; ++j) refs.push_back(LimbRef{tmps[i] + j * N, j, 0});
-  }
-  ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < ls[i]; ++j) {
+      LimbRef r = lref(tmps[i] + j * N, j);
+      r.src = xs[i] + j * N;
+      if (ys) r.pro = ys[i] + j * N;
+      refs.push_back(r);
+    }
+  ntt_limbs(c, refs.data(), (int)refs.size(), true, s, ys ? IN_MUL : IN_PLAIN);
   std::vector<ConvJob> jobs;
   refs.clear();
   for (int i = 0; i < n; ++i) {
@@ -51,44 +62,81 @@ void modup_stage(Context* c, const uint64_t* const* xs, const int* ls, uint64_t*
       jobs.push_back(ConvJob{c->modup_tab[l][d], tmps[i], D});
       const int s0 = d * c->alpha, s1 = std::min(l, (d + 1) * c->alpha);
       for (int j = 0; j < l; ++j)
-        if (j < s0 || j >= s1) refs.push_back(LimbRef{D + j * N, j, 0});
-      for (int k = 0; k < c->K; ++k) refs.push_back(LimbRef{D + (l + k) * N, c->n_q + k, 0});
+        if (j < s0 || j >= s1) refs.push_back(lref(D + j * N, j));
+      for (int k = 0; k < c->K; ++k) refs.push_back(lref(D + (l + k) * N, c->n_q + k));
     }
   }
   launch_conv(c, jobs.data(), (int)jobs.size(), s);
   ntt_limbs(c, refs.data(), (int)refs.size(), false, s);
 }
 
-// ModDown of extended polys exts[i] (special limbs are transformed in place) into outs[i].
+// ModDown of extended polys exts[i] (special limbs are transformed in place) into outs[i],
+// adding adds[i] when given.
 void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs, uint64_t* const* outs,
                    const uint64_t* const* adds, int n, cudaStream_t s) {
   const size_t N = c->N;
   const int K = c->K;
+  if (K == 0) throw Error(-1, "ModDown needs special primes");
   std::vector<LimbRef> refs;
   for (int i = 0; i < n; ++i)
-    for (int k = 0; k < K; ++k) refs.push_back(LimbRef{exts[i] + (ls[i] + k) * N, c->n_q + k, 0});
+    for (int k = 0; k < K; ++k) refs.push_back(lref(exts[i] + (ls[i] + k) * N, c->n_q + k));
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
   std::vector<ConvJob> jobs;
   refs.clear();
-  std::vector<FinJob> fin;
   for (int i = 0; i < n; ++i) {
     const int l = ls[i];
     jobs.push_back(ConvJob{c->moddown_tab[l], exts[i] + l * N, convs[i]});
-    for (int j = 0; j < l; ++j) refs.push_back(LimbRef{convs[i] + j * N, j, 0});
-    fin.push_back(FinJob{exts[i], convs[i], adds ? adds[i] : nullptr, outs[i], l, 0});
+    for (int j = 0; j < l; ++j) {
+      LimbRef r = lref(outs[i] + j * N, j);
+      r.src = convs[i] + j * N;
+      r.ep0 = exts[i] + j * N;
+      r.ep1 = (adds && adds[i]) ? adds[i] + j * N : nullptr;
+      refs.push_back(r);
+    }
   }
-  if (K > 0) {
-    launch_conv(c, jobs.data(), (int)jobs.size(), s);
-    ntt_limbs(c, refs.data(), (int)refs.size(), false, s);
-  } else {
-    for (int i = 0; i < n; ++i) FIDES_CUDA(cudaMemsetAsync(convs[i], 0, sizeof(uint64_t) * N * ls[i], s));
-  }
-  launch_moddown_finish(c, fin.data(), (int)fin.size(), s);
+  launch_conv(c, jobs.data(), (int)jobs.size(), s);
+  ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_PLAIN, OUT_MODDOWN);
 }
 
+// Scratch limbs of one key switch at level l: INTT copy, digits, A, B, two conversions.
 size_t ks_limbs(Context* c, int l) {
   const int ext = l + c->K;
   return (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l;
+}
+
+// Key switch of n items whose inputs are xs[i] (or xs[i] * ys[i]).
+void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
+                     const uint64_t* const* keys, uint64_t* const* f0, uint64_t* const* f1,
+                     const uint64_t* const* add0, const uint64_t* const* add1, int n, cudaStream_t s) {
+  const size_t N = c->N;
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) total += ks_limbs(c, ls[i]);
+  Scratch sc(c, sizeof(uint64_t) * N * total, s);
+  Bump bp{sc.u64(), N};
+  std::vector<int> ls2(2 * n);
+  std::vector<uint64_t*> tmp(n), dig(n), ex(2 * n), conv(2 * n), outs(2 * n);
+  std::vector<const uint64_t*> adds(2 * n);
+  std::vector<KskJob> kj;
+  for (int i = 0; i < n; ++i) {
+    const int l = ls[i], ext = l + c->K;
+    tmp[i] = bp.take(l);
+    dig[i] = bp.take((size_t)c->beta(l) * ext);
+    uint64_t* A = bp.take(ext);
+    uint64_t* B = bp.take(ext);
+    kj.push_back(KskJob{xs[i], ys ? ys[i] : nullptr, dig[i], keys[i], nullptr, A, B, l, 0});
+    ex[2 * i] = B;
+    ex[2 * i + 1] = A;
+    conv[2 * i] = bp.take(l);
+    conv[2 * i + 1] = bp.take(l);
+    outs[2 * i] = f0[i];
+    outs[2 * i + 1] = f1[i];
+    adds[2 * i] = add0 ? add0[i] : nullptr;
+    adds[2 * i + 1] = add1 ? add1[i] : nullptr;
+    ls2[2 * i] = ls2[2 * i + 1] = l;
+  }
+  modup_stage(c, xs, ys, ls, tmp.data(), dig.data(), n, s);
+  launch_ksk(c, kj.data(), n, s);
+  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), adds.data(), 2 * n, s);
 }
 
 }  // namespace
@@ -98,7 +146,7 @@ void op_modup(Context* c, const uint64_t* x, int l, uint64_t* digits, cudaStream
   const size_t N = c->N;
   Scratch sc(c, sizeof(uint64_t) * N * l, s);
   uint64_t* tmp = sc.u64();
-  modup_stage(c, &x, &l, &tmp, &digits, 1, s);
+  modup_stage(c, &x, nullptr, &l, &tmp, &digits, 1, s);
   const int ext = l + c->K;
   for (int d = 0; d < c->beta(l); ++d) {
     const int s0 = d * c->alpha, s1 = std::min(l, (d + 1) * c->alpha);
@@ -111,7 +159,7 @@ void op_ksk_ip(Context* c, const uint64_t* x, const uint64_t* digits, int l, con
                uint64_t* out_b, cudaStream_t s) {
   check_level(c, l);
   if (!key) throw Error(-5, "null key");
-  KskJob j{x, digits, key, nullptr, out_a, out_b, l, 0};
+  KskJob j{x, nullptr, digits, key, nullptr, out_a, out_b, l, 0};
   launch_ksk(c, &j, 1, s);
 }
 
@@ -135,73 +183,66 @@ void op_tensor(Context* c, const uint64_t* a0, const uint64_t* a1, const uint64_
 
 void op_keyswitch_batch(Context* c, const KeySwitchItem* items, int n, cudaStream_t s) {
   if (n <= 0) return;
-  const size_t N = c->N;
-  size_t total = 0;
+  std::vector<const uint64_t*> xs(n), keys(n), a0(n), a1(n);
+  std::vector<uint64_t*> f0(n), f1(n);
+  std::vector<int> ls(n);
   for (int i = 0; i < n; ++i) {
     check_level(c, items[i].l);
     if (!items[i].key) throw Error(-5, "null key");
-    total += ks_limbs(c, items[i].l);
+    xs[i] = items[i].d;
+    ls[i] = items[i].l;
+    keys[i] = items[i].key;
+    f0[i] = items[i].f0;
+    f1[i] = items[i].f1;
+    a0[i] = items[i].add0;
+    a1[i] = items[i].add1;
   }
-  Scratch sc(c, sizeof(uint64_t) * N * total, s);
-  Bump bp{sc.u64(), N};
-  std::vector<const uint64_t*> xs(n);
-  std::vector<int> ls(n), ls2(2 * n);
-  std::vector<uint64_t*> tmp(n), dig(n), ex(2 * n), conv(2 * n), outs(2 * n);
-  std::vector<const uint64_t*> adds(2 * n);
-  std::vector<KskJob> kj;
-  for (int i = 0; i < n; ++i) {
-    const KeySwitchItem& it = items[i];
-    const int l = it.l, ext = l + c->K;
-    xs[i] = it.d;
-    ls[i] = l;
-    tmp[i] = bp.take(l);
-    dig[i] = bp.take((size_t)c->beta(l) * ext);
-    uint64_t* A = bp.take(ext);
-    uint64_t* B = bp.take(ext);
-    kj.push_back(KskJob{it.d, dig[i], it.key, nullptr, A, B, l, 0});
-    ex[2 * i] = B;
-    ex[2 * i + 1] = A;
-    conv[2 * i] = bp.take(l);
-    conv[2 * i + 1] = bp.take(l);
-    outs[2 * i] = it.f0;
-    outs[2 * i + 1] = it.f1;
-    adds[2 * i] = it.add0;
-    adds[2 * i + 1] = it.add1;
-    ls2[2 * i] = ls2[2 * i + 1] = l;
-  }
-  modup_stage(c, xs.data(), ls.data(), tmp.data(), dig.data(), n, s);
-  launch_ksk(c, kj.data(), n, s);
-  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), adds.data(), 2 * n, s);
+  keyswitch_stage(c, xs.data(), nullptr, ls.data(), keys.data(), f0.data(), f1.data(), a0.data(), a1.data(), n, s);
 }
 
 void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint64_t* const* outs, int n,
                       cudaStream_t s) {
   if (n <= 0) return;
   const size_t N = c->N;
-  size_t total = 0;
+  // The fused NTT writes its output before its epilogue reads x, so an output that
+  // overlaps its input is produced in scratch and copied.
+  std::vector<bool> alias(n);
+  size_t extra = 0;
   for (int i = 0; i < n; ++i) {
     check_level(c, ls[i], 2);
-    total += 1 + (size_t)(ls[i] - 1);
+    const uint64_t *x0 = xs[i], *x1 = xs[i] + (size_t)ls[i] * N;
+    const uint64_t *o0 = outs[i], *o1 = outs[i] + (size_t)(ls[i] - 1) * N;
+    alias[i] = o0 < x1 && x0 < o1;
+    if (alias[i]) extra += ls[i] - 1;
   }
-  Scratch sc(c, sizeof(uint64_t) * N * total, s);
+  Scratch sc(c, sizeof(uint64_t) * N * (n + extra), s);
   Bump bp{sc.u64(), N};
   std::vector<LimbRef> refs, refs2;
-  std::vector<SwitchJob> sw;
-  std::vector<RescaleJob> fin;
+  std::vector<std::pair<uint64_t*, int>> copies;
   for (int i = 0; i < n; ++i) {
     const int l = ls[i];
+    uint64_t* dst = outs[i];
+    if (alias[i]) {
+      dst = bp.take(l - 1);
+      copies.push_back({dst, i});
+    }
     uint64_t* top = bp.take(1);
-    uint64_t* t = bp.take(l - 1);
-    FIDES_CUDA(cudaMemcpyAsync(top, xs[i] + (size_t)(l - 1) * N, sizeof(uint64_t) * N, cudaMemcpyDeviceToDevice, s));
-    refs.push_back(LimbRef{top, l - 1, 0});
-    sw.push_back(SwitchJob{top, t, l, 0});
-    for (int j = 0; j < l - 1; ++j) refs2.push_back(LimbRef{t + j * N, j, 0});
-    fin.push_back(RescaleJob{xs[i], t, outs[i], l, 0});
+    LimbRef r = lref(top, l - 1);
+    r.src = xs[i] + (size_t)(l - 1) * N;
+    refs.push_back(r);
+    for (int j = 0; j < l - 1; ++j) {
+      LimbRef t = lref(dst + j * N, j);
+      t.pro = top;
+      t.ep0 = xs[i] + j * N;
+      t.aux = l;
+      refs2.push_back(t);
+    }
   }
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
-  launch_switch_modulus(c, sw.data(), n, s);
-  ntt_limbs(c, refs2.data(), (int)refs2.size(), false, s);
-  launch_rescale_finish(c, fin.data(), n, s);
+  ntt_limbs(c, refs2.data(), (int)refs2.size(), false, s, IN_SWITCH, OUT_RESCALE);
+  for (auto& cp : copies)
+    FIDES_CUDA(cudaMemcpyAsync(outs[cp.second], cp.first, sizeof(uint64_t) * N * (ls[cp.second] - 1),
+                               cudaMemcpyDeviceToDevice, s));
 }
 
 void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* relin_key, bool rescale,
@@ -212,38 +253,41 @@ void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* r
   size_t total = 0;
   for (int i = 0; i < n; ++i) {
     check_level(c, items[i].l, rescale ? 2 : 1);
-    total += (size_t)items[i].l * (rescale ? 5 : 3);
+    total += (size_t)items[i].l * (rescale ? 4 : 2);
   }
   Scratch sc(c, sizeof(uint64_t) * N * total, s);
   Bump bp{sc.u64(), N};
   std::vector<TensorJob> tj;
-  std::vector<KeySwitchItem> ks;
-  std::vector<const uint64_t*> rx;
-  std::vector<uint64_t*> ro;
-  std::vector<int> rl;
+  std::vector<const uint64_t*> xs(n), ys(n), keys(n, relin_key), d0s(n), d1s(n), rx;
+  std::vector<uint64_t*> f0(n), f1(n), ro;
+  std::vector<int> ls(n), rl;
   for (int i = 0; i < n; ++i) {
     const HMultItem& it = items[i];
     const int l = it.l;
     uint64_t* d0 = bp.take(l);
     uint64_t* d1 = bp.take(l);
-    uint64_t* d2 = bp.take(l);
-    tj.push_back(TensorJob{it.a0, it.a1, it.b0, it.b1, d0, d1, d2, l, 0});
-    uint64_t* o0 = it.out0;
-    uint64_t* o1 = it.out1;
+    tj.push_back(TensorJob{it.a0, it.a1, it.b0, it.b1, d0, d1, nullptr, l, 0});
+    xs[i] = it.a1;
+    ys[i] = it.b1;
+    ls[i] = l;
+    d0s[i] = d0;
+    d1s[i] = d1;
+    f0[i] = it.out0;
+    f1[i] = it.out1;
     if (rescale) {
-      o0 = bp.take(l);
-      o1 = bp.take(l);
-      rx.push_back(o0);
-      rx.push_back(o1);
+      f0[i] = bp.take(l);
+      f1[i] = bp.take(l);
+      rx.push_back(f0[i]);
+      rx.push_back(f1[i]);
       ro.push_back(it.out0);
       ro.push_back(it.out1);
       rl.push_back(l);
       rl.push_back(l);
     }
-    ks.push_back(KeySwitchItem{d2, l, relin_key, o0, o1, d0, d1});
   }
   launch_tensor(c, tj.data(), n, s);
-  op_keyswitch_batch(c, ks.data(), n, s);
+  keyswitch_stage(c, xs.data(), ys.data(), ls.data(), keys.data(), f0.data(), f1.data(), d0s.data(), d1s.data(), n,
+                  s);
   if (rescale) op_rescale_batch(c, rx.data(), rl.data(), ro.data(), (int)rx.size(), s);
 }
 
@@ -271,7 +315,7 @@ void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s)
     dig[i] = bp.take((size_t)c->beta(l) * ext);
     uint64_t* A = bp.take(ext);
     uint64_t* B = bp.take(ext);
-    kj.push_back(KskJob{it.c1, dig[i], it.key, it.c0, A, B, l, it.k});
+    kj.push_back(KskJob{it.c1, nullptr, dig[i], it.key, it.c0, A, B, l, it.k});
     ex[2 * i] = B;
     ex[2 * i + 1] = A;
     conv[2 * i] = bp.take(l);
@@ -280,7 +324,7 @@ void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s)
     outs[2 * i + 1] = it.out1;
     ls2[2 * i] = ls2[2 * i + 1] = l;
   }
-  modup_stage(c, xs.data(), ls.data(), tmp.data(), dig.data(), n, s);
+  modup_stage(c, xs.data(), nullptr, ls.data(), tmp.data(), dig.data(), n, s);
   launch_ksk(c, kj.data(), n, s);
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
 }
@@ -298,14 +342,14 @@ void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) {
   Bump bp{sc.u64(), N};
   uint64_t* tmp = bp.take(l);
   uint64_t* dig = bp.take((size_t)c->beta(l) * ext);
-  modup_stage(c, &it.c1, &l, &tmp, &dig, 1, s);
+  modup_stage(c, &it.c1, nullptr, &l, &tmp, &dig, 1, s);
   std::vector<KskJob> kj;
   std::vector<uint64_t*> ex(2 * n), conv(2 * n), outs(2 * n);
   std::vector<int> ls2(2 * n, l);
   for (int j = 0; j < n; ++j) {
     uint64_t* A = bp.take(ext);
     uint64_t* B = bp.take(ext);
-    kj.push_back(KskJob{it.c1, dig, it.keys[j], it.c0, A, B, l, it.ks[j]});
+    kj.push_back(KskJob{it.c1, nullptr, dig, it.keys[j], it.c0, A, B, l, it.ks[j]});
     ex[2 * j] = B;
     ex[2 * j + 1] = A;
     conv[2 * j] = bp.take(l);

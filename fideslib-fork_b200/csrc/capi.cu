@@ -6,14 +6,10 @@
 #include <vector>
 
 #include "../../include/fides_b200.h"
+#include "capi_internal.hpp"
 #include "context.hpp"
 #include "ntt.cuh"
 #include "ops.hpp"
-
-struct fides_ctx {
-  fides::Context* c;
-  cudaStream_t host_stream;
-};
 
 namespace {
 thread_local std::string g_err;
@@ -47,6 +43,8 @@ void need(const void* p, const char* what) {
 
 cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 }  // namespace
+
+void fides::set_last_error(const std::string& msg) { g_err = msg; }
 
 extern "C" {
 

@@ -96,6 +96,7 @@ def lib():
         L.fides_key_free.argtypes = [vp, vp]
         L.fides_hmult_host.argtypes = [vp, u64p, u64p, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
+        L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         _lib = L
     return _lib
 
@@ -246,6 +247,12 @@ class Context:
         l = x.shape[0]
         out = self.empty(l - 1)
         _check(lib().fides_rescale(self._h, _ptr(x), l, _ptr(out), _stream()))
+        return out
+
+    def rescale_poly_noalloc(self, x, out):
+        """fides_rescale_noalloc: same result as rescale_poly, scratch from the library's
+        static array (no device allocation); `out` is caller-owned, l - 1 limbs."""
+        _check(lib().fides_rescale_noalloc(self._h, _ptr(x), x.shape[0], _ptr(out), _stream()))
         return out
 
     def rescale(self, ct: Ciphertext) -> Ciphertext:

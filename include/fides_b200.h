@@ -161,6 +161,20 @@ int fides_hmult_host(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, con
 int fides_rotate_host(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                       const uint64_t* rot_key_dev, int rotation, uint64_t* out0, uint64_t* out1);
 
+/* ---- allocation-free entry point ----------------------------------------------------
+ * No counterpart in the reference.  fides_rescale_noalloc computes exactly what
+ * fides_rescale computes for one polynomial, but takes its scratch (one limb) from a
+ * 512 KiB array compiled into the library instead of allocating device memory, for
+ * callers that cannot allocate on the call path: hosts whose HBM is entirely reserved
+ * by another allocator (every extra cudaMalloc fails) and latency-bound loops that cannot
+ * take the synchronisation cudaMalloc / cudaFree bring.  Limits and rules:
+ *   - N <= 2^16 (a larger ring returns FIDES_ERR_ARG), 2 <= level <= n_q;
+ *   - out (level - 1 limbs) must not overlap x (FIDES_ERR_ARG);
+ *   - the array is shared by every call on a device: calls that overlap on the GPU race;
+ *   - the first call on a device looks up the array's device address (with that device
+ *     current) and caches it; make that first call before any stream capture. */
+int fides_rescale_noalloc(fides_ctx* ctx, const uint64_t* x, int level, uint64_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@
 #include "../../include/fides_b200.h"
 #include "capi_internal.hpp"
 #include "context.hpp"
+#include "kernels.cuh"
 #include "ntt.cuh"
 #include "ops.hpp"
 
@@ -211,6 +212,27 @@ int fides_tensor(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uin
       need(p, "tensor operand");
     fides::op_tensor(c, a0, a1, b0, b1, level, d0, d1, d2, S(stream));
   });
+}
+
+static int addsub(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream,
+                  int sub) {
+  return guard([&] {
+    auto* c = C(x);
+    need(a, "a");
+    need(b, "b");
+    need(out, "out");
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    fides::AddSubJob j{a, b, out, level, sub};
+    fides::launch_addsub(c, &j, 1, S(stream));
+  });
+}
+
+int fides_add(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
+  return addsub(x, a, b, level, out, stream, 0);
+}
+
+int fides_sub(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
+  return addsub(x, a, b, level, out, stream, 1);
 }
 
 int fides_rescale(fides_ctx* x, const uint64_t* in, int level, uint64_t* out, void* stream) {

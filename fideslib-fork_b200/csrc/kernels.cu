@@ -183,6 +183,26 @@ __global__ void __launch_bounds__(EW_THREADS) rescale_finish_kernel(const __grid
   J.out[off] = addmod(a, b, p.q);
 }
 
+__global__ void __launch_bounds__(EW_THREADS) addsub_kernel(const __grid_constant__ AddSubJobList L,
+                                                            const DevPrime* primes, int logN) {
+  const AddSubJob& J = L.j[blockIdx.z];
+  const int j = blockIdx.y;
+  if (j >= J.l) return;
+  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const uint64_t q = primes[j].q;
+  const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(J.a + off);
+  const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(J.b + off);
+  ulonglong2 r;
+  if (J.sub) {
+    r.x = submod(x.x, y.x, q);
+    r.y = submod(x.y, y.y, q);
+  } else {
+    r.x = addmod(x.x, y.x, q);
+    r.y = addmod(x.y, y.y, q);
+  }
+  *reinterpret_cast<ulonglong2*>(J.out + off) = r;
+}
+
 template <typename List, typename Job>
 int fill(List& L, const Job* jobs, int n) {
   L.n = n;
@@ -324,6 +344,24 @@ void launch_rescale_finish(Context* c, const RescaleJob* jobs, int n, cudaStream
     for (int i = 0; i < m; ++i) bytes += 8.0 * c->N * (3.0 * (L.j[i].l - 1));
     LaunchScope ls(c, s, KK_ELEM, bytes);
     rescale_finish_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_rescale, c->logN, c->n_q);
+    FIDES_CUDA(cudaGetLastError());
+  }
+}
+
+void launch_addsub(Context* c, const AddSubJob* jobs, int n, cudaStream_t s) {
+  static thread_local AddSubJobList L;
+  for (int off = 0; off < n; off += MAX_ADDSUB_JOBS) {
+    int m = std::min(MAX_ADDSUB_JOBS, n - off);
+    fill(L, jobs + off, m);
+    int mx = 1;
+    double bytes = 0;
+    for (int i = 0; i < m; ++i) {
+      mx = std::max(mx, L.j[i].l);
+      bytes += 8.0 * c->N * 3.0 * L.j[i].l;
+    }
+    dim3 grid(c->N / (2 * EW_THREADS), mx, m);
+    LaunchScope ls(c, s, KK_ELEM, bytes);
+    addsub_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->logN);
     FIDES_CUDA(cudaGetLastError());
   }
 }

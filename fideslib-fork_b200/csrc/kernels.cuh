@@ -101,4 +101,18 @@ struct RescaleJobList {
 void launch_switch_modulus(Context* c, const SwitchJob* jobs, int n, cudaStream_t s);
 void launch_rescale_finish(Context* c, const RescaleJob* jobs, int n, cudaStream_t s);
 
+// ---- RNS add / sub (reference add_ / sub_, src/AddSub.cu:10-123)
+struct AddSubJob {
+  const uint64_t *a, *b;
+  uint64_t* out;
+  int l;
+  int sub;  // 0: a + b, 1: a - b
+};
+constexpr int MAX_ADDSUB_JOBS = 128;
+struct AddSubJobList {
+  int n, max_l, pad0, pad1;
+  AddSubJob j[MAX_ADDSUB_JOBS];
+};
+void launch_addsub(Context* c, const AddSubJob* jobs, int n, cudaStream_t s);
+
 }  // namespace fides

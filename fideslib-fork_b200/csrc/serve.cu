@@ -1,0 +1,338 @@
+// Continuous-batching request loop over resident evaluation keys.
+//
+// The reference runs one issuing host thread per context and lets independent host threads
+// share it through per-thread scratch slots (FIDESLIB_CONCURRENT_OPS, api/ConcurrentOps.hpp:
+// 30-64; test/ConcurrentOpsTests.cu:246-420 checks each lane against its serial result).
+// Here a scheduler thread owns the GPU side instead:
+//   * submit() only enqueues (thread-safe, non-blocking);
+//   * the scheduler forms a batch from the oldest pending request's operation type, taking
+//     further requests of that type in arrival order while the batch is below max_batch and
+//     the scratch they need fits the HBM budget still free;
+//   * each batch is ONE batched launch sequence (op_hmult_batch / op_rotate_batch, any mix
+//     of levels) on one of n_streams streams, so batches that are admitted while others are
+//     still on the GPU overlap with them;
+//   * a host function enqueued behind each batch marks its requests complete (latency =
+//     completion - arrival) and returns their budget, waking the scheduler.
+// Results are exact integer arithmetic, so a request's output does not depend on what it
+// was batched with; tests/test_serving.py checks that bit for bit.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/fides_b200.h"
+#include "capi_internal.hpp"
+#include "ops.hpp"
+
+namespace fides {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Pending {
+  fides_request r;
+  uint64_t ticket;
+  Clock::time_point arrival;
+  size_t bytes;
+};
+
+struct Done {
+  int status = 0;
+  double latency_ms = 0;
+  bool ready = false;
+};
+
+}  // namespace
+
+struct Server {
+  fides_ctx* handle;
+  Context* c;
+  fides_server_config cfg;
+  const uint64_t* relin = nullptr;
+  std::map<int, const uint64_t*> rot;  // normalised rotation -> key
+  std::vector<cudaStream_t> streams;
+  std::vector<bool> busy;
+
+  std::mutex mu;
+  std::condition_variable cv;     // scheduler wake-up
+  std::condition_variable done_cv;
+  std::deque<Pending> pending;
+  std::unordered_map<uint64_t, Done> done;
+  uint64_t next_ticket = 1;
+  size_t in_use = 0;
+  bool stop = false;
+  fides_server_stats st{};
+  std::thread worker;
+
+  size_t request_bytes(const fides_request& r) const {
+    const int l = r.level, ext = l + c->K;
+    const size_t ks = (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l;
+    const size_t limbs = r.op == FIDES_OP_ROTATE ? ks : ks + (size_t)l * (r.op == FIDES_OP_HMULT ? 4 : 2) + 1;
+    return limbs * c->limb_bytes();
+  }
+
+  int norm_rot(int k) const {
+    const int h = c->N / 2;
+    k %= h;
+    return k < 0 ? k + h : k;
+  }
+
+  struct Batch {
+    Server* s;
+    int stream;
+    std::vector<uint64_t> tickets;
+    std::vector<Clock::time_point> arrivals;
+    size_t bytes;
+    int status;
+  };
+
+  static void CUDART_CB on_done(void* p) {
+    Batch* b = static_cast<Batch*>(p);
+    Server* s = b->s;
+    const auto now = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (size_t i = 0; i < b->tickets.size(); ++i) {
+        Done& d = s->done[b->tickets[i]];
+        d.status = b->status;
+        d.latency_ms = std::chrono::duration<double, std::milli>(now - b->arrivals[i]).count();
+        d.ready = true;
+        s->st.completed++;
+      }
+      s->in_use -= b->bytes;
+      s->busy[b->stream] = false;
+    }
+    s->cv.notify_all();
+    s->done_cv.notify_all();
+    delete b;
+  }
+
+  void fail_locked(const Pending& p, int code) {
+    Done& d = done[p.ticket];
+    d.status = code;
+    d.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - p.arrival).count();
+    d.ready = true;
+    st.rejected++;
+  }
+
+  void run() {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      cv.wait(lk, [&] {
+        if (stop) return true;
+        if (pending.empty()) return false;
+        return std::find(busy.begin(), busy.end(), false) != busy.end();
+      });
+      if (stop && pending.empty()) break;
+      if (stop) {
+        // shutting down: fail what was never started
+        while (!pending.empty()) {
+          fail_locked(pending.front(), FIDES_ERR_STATE);
+          pending.pop_front();
+        }
+        done_cv.notify_all();
+        break;
+      }
+      const int slot = (int)(std::find(busy.begin(), busy.end(), false) - busy.begin());
+      const int op = pending.front().r.op;
+      const size_t budget = cfg.hbm_budget_bytes ? cfg.hbm_budget_bytes : SIZE_MAX;
+      std::vector<Pending> take;
+      size_t bytes = 0;
+      for (auto it = pending.begin(); it != pending.end() && (int)take.size() < cfg.max_batch;) {
+        if (it->r.op != op) {
+          ++it;
+          continue;
+        }
+        if (it->bytes > budget) {  // can never fit: reject
+          fail_locked(*it, FIDES_ERR_OOM);
+          it = pending.erase(it);
+          continue;
+        }
+        if (in_use + bytes + it->bytes > budget) break;  // wait for memory to free up
+        bytes += it->bytes;
+        take.push_back(*it);
+        it = pending.erase(it);
+      }
+      if (take.empty()) {
+        done_cv.notify_all();
+        if (in_use == 0 && !pending.empty() && pending.front().r.op == op) continue;
+        cv.wait_for(lk, std::chrono::microseconds(200));
+        continue;
+      }
+      busy[slot] = true;
+      in_use += bytes;
+      st.batches++;
+      st.batched_requests += take.size();
+      st.peak_bytes = std::max<uint64_t>(st.peak_bytes, in_use);
+      lk.unlock();
+      auto* b = new Batch{this, slot, {}, {}, bytes, FIDES_OK};
+      for (auto& p : take) {
+        b->tickets.push_back(p.ticket);
+        b->arrivals.push_back(p.arrival);
+      }
+      cudaStream_t s = streams[slot];
+      try {
+        FIDES_CUDA(cudaSetDevice(c->device));
+        if (op == FIDES_OP_ROTATE) {
+          std::vector<RotateItem> items;
+          for (auto& p : take)
+            items.push_back(RotateItem{p.r.c0, p.r.c1, p.r.out0, p.r.out1, rot.at(norm_rot(p.r.rotation)), p.r.level,
+                                       h_auto_index(c->logN, p.r.rotation)});
+          op_rotate_batch(c, items.data(), (int)items.size(), s);
+        } else {
+          std::vector<HMultItem> items;
+          for (auto& p : take)
+            items.push_back(HMultItem{p.r.c0, p.r.c1, p.r.d0, p.r.d1, p.r.out0, p.r.out1, p.r.level});
+          op_hmult_batch(c, items.data(), (int)items.size(), relin, op == FIDES_OP_HMULT, s);
+        }
+      } catch (const Error& e) {
+        b->status = e.code;
+      } catch (const std::exception&) {
+        b->status = FIDES_ERR_STATE;
+      }
+      cudaError_t e = cudaLaunchHostFunc(s, on_done, b);
+      if (e != cudaSuccess) {
+        b->status = FIDES_ERR_CUDA;
+        on_done(b);
+      }
+      lk.lock();
+    }
+  }
+};
+
+}  // namespace fides
+
+struct fides_server {
+  fides::Server* s;
+};
+
+namespace {
+template <typename F>
+int sguard(F&& f) {
+  try {
+    f();
+    return FIDES_OK;
+  } catch (const fides::Error& e) {
+    fides::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fides::set_last_error(e.what());
+    return FIDES_ERR_STATE;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fides_server_create(fides_ctx* ctx, const fides_server_config* cfg, fides_server** out) {
+  return sguard([&] {
+    if (!ctx || !ctx->c || !cfg || !out) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    if (cfg->n_streams < 1 || cfg->n_streams > 16 || cfg->max_batch < 1)
+      throw fides::Error(FIDES_ERR_ARG, "need 1 <= n_streams <= 16 and max_batch >= 1");
+    auto* s = new fides::Server();
+    s->handle = ctx;
+    s->c = ctx->c;
+    s->cfg = *cfg;
+    FIDES_CUDA(cudaSetDevice(s->c->device));
+    s->streams.resize(cfg->n_streams);
+    s->busy.assign(cfg->n_streams, false);
+    for (auto& st : s->streams) FIDES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    s->worker = std::thread([s] { s->run(); });
+    *out = new fides_server{s};
+  });
+}
+
+int fides_server_set_relin_key(fides_server* sv, const uint64_t* key) {
+  return sguard([&] {
+    if (!sv || !key) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(sv->s->mu);
+    sv->s->relin = key;
+  });
+}
+
+int fides_server_add_rotation_key(fides_server* sv, int rotation, const uint64_t* key) {
+  return sguard([&] {
+    if (!sv || !key) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(sv->s->mu);
+    sv->s->rot[sv->s->norm_rot(rotation)] = key;
+  });
+}
+
+int fides_server_submit(fides_server* sv, const fides_request* r, uint64_t* ticket) {
+  return sguard([&] {
+    if (!sv || !r || !ticket) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    fides::Server* s = sv->s;
+    if (r->level < 1 || r->level > s->c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (!r->c0 || !r->c1 || !r->out0 || !r->out1) throw fides::Error(FIDES_ERR_ARG, "null operand");
+    if (r->op == FIDES_OP_ROTATE) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (!s->rot.count(s->norm_rot(r->rotation))) throw fides::Error(FIDES_ERR_KEY, "no key for this rotation");
+    } else if (r->op == FIDES_OP_HMULT || r->op == FIDES_OP_HMULT_NORESCALE) {
+      if (!r->d0 || !r->d1) throw fides::Error(FIDES_ERR_ARG, "null second operand");
+      if (r->op == FIDES_OP_HMULT && r->level < 2) throw fides::Error(FIDES_ERR_LEVEL, "rescale needs level >= 2");
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (!s->relin) throw fides::Error(FIDES_ERR_KEY, "no relinearization key");
+    } else {
+      throw fides::Error(FIDES_ERR_ARG, "unknown operation");
+    }
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->stop) throw fides::Error(FIDES_ERR_STATE, "server is stopping");
+      fides::Pending p{*r, s->next_ticket++, fides::Clock::now(), s->request_bytes(*r)};
+      *ticket = p.ticket;
+      s->done[p.ticket] = fides::Done{};
+      s->pending.push_back(p);
+      s->st.submitted++;
+    }
+    s->cv.notify_all();
+  });
+}
+
+int fides_server_wait(fides_server* sv, uint64_t ticket, double* latency_ms, int* status) {
+  return sguard([&] {
+    if (!sv) throw fides::Error(FIDES_ERR_ARG, "null server");
+    fides::Server* s = sv->s;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->done.find(ticket);
+    if (it == s->done.end()) throw fides::Error(FIDES_ERR_ARG, "unknown ticket");
+    s->done_cv.wait(lk, [&] { return s->done[ticket].ready; });
+    fides::Done d = s->done[ticket];
+    s->done.erase(ticket);
+    if (latency_ms) *latency_ms = d.latency_ms;
+    if (status) *status = d.status;
+  });
+}
+
+int fides_server_get_stats(fides_server* sv, fides_server_stats* out) {
+  return sguard([&] {
+    if (!sv || !out) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(sv->s->mu);
+    *out = sv->s->st;
+  });
+}
+
+int fides_server_destroy(fides_server* sv) {
+  return sguard([&] {
+    if (!sv) return;
+    fides::Server* s = sv->s;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto st : s->streams) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    delete s;
+    delete sv;
+  });
+}
+
+}  // extern "C"

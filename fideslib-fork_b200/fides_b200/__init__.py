@@ -44,6 +44,23 @@ class _HMultItem(C.Structure):
     _fields_ = [("a0", vp), ("a1", vp), ("b0", vp), ("b1", vp), ("out0", vp), ("out1", vp), ("level", C.c_int)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("n_streams", C.c_int), ("max_batch", C.c_int), ("hbm_budget_bytes", C.c_size_t)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("op", C.c_int), ("level", C.c_int), ("c0", vp), ("c1", vp), ("d0", vp), ("d1", vp),
+                ("out0", vp), ("out1", vp), ("rotation", C.c_int)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "rejected", "batches", "batched_requests",
+                                          "peak_bytes")]
+
+
+OP_HMULT, OP_HMULT_NORESCALE, OP_ROTATE = 0, 1, 2
+
+
 class _RotateItem(C.Structure):
     _fields_ = [("c0", vp), ("c1", vp), ("out0", vp), ("out1", vp), ("key", vp), ("level", C.c_int),
                 ("auto_index", C.c_uint32)]
@@ -97,6 +114,15 @@ def lib():
         L.fides_hmult_host.argtypes = [vp, u64p, u64p, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
+        L.fides_server_set_relin_key.argtypes = [vp, vp]
+        L.fides_server_add_rotation_key.argtypes = [vp, C.c_int, vp]
+        L.fides_server_submit.argtypes = [vp, C.POINTER(_Request), C.POINTER(C.c_uint64)]
+        L.fides_server_wait.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.fides_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
+        L.fides_server_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -357,3 +383,52 @@ def to_device(a, device: int = 0) -> torch.Tensor:
 def to_host(t: torch.Tensor):
     import numpy as np
     return t.contiguous().view(torch.int64).cpu().numpy().view(np.uint64)
+
+
+class Server:
+    """Continuous-batching request loop (fides_server_*): submit() enqueues, wait() blocks."""
+
+    def __init__(self, ctx: "Context", n_streams: int = 2, max_batch: int = 8, hbm_budget_bytes: int = 0):
+        self.ctx = ctx
+        cfg = _ServerConfig(n_streams, max_batch, hbm_budget_bytes)
+        h = vp()
+        _check(lib().fides_server_create(ctx._h, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def set_relin_key(self, key):
+        self._keep.append(key)
+        _check(lib().fides_server_set_relin_key(self._h, _ptr(key)))
+
+    def add_rotation_key(self, rotation: int, key):
+        self._keep.append(key)
+        _check(lib().fides_server_add_rotation_key(self._h, rotation, _ptr(key)))
+
+    def submit(self, op: int, a: Ciphertext, out: Ciphertext, b: Ciphertext | None = None, rotation: int = 0) -> int:
+        r = _Request(op, a.level, _ptr(a.c0), _ptr(a.c1), _ptr(b.c0) if b else None, _ptr(b.c1) if b else None,
+                     _ptr(out.c0), _ptr(out.c1), rotation)
+        t = C.c_uint64()
+        _check(lib().fides_server_submit(self._h, C.byref(r), C.byref(t)))
+        return int(t.value)
+
+    def wait(self, ticket: int):
+        lat, st = C.c_double(), C.c_int()
+        _check(lib().fides_server_wait(self._h, ticket, C.byref(lat), C.byref(st)))
+        return int(st.value), float(lat.value)
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        _check(lib().fides_server_get_stats(self._h, C.byref(s)))
+        return {n: int(getattr(s, n)) for n, _ in _ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(lib().fides_server_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

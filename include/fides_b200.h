@@ -105,6 +105,11 @@ int fides_keyswitch(fides_ctx* ctx, const uint64_t* d, int level, const uint64_t
 /* Tensor product: replaces binomialMult_ (ElemenwiseBatchKernels.cu:1363-1510). */
 int fides_tensor(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
                  int level, uint64_t* d0, uint64_t* d1, uint64_t* d2, void* stream);
+/* Elementwise RNS add / sub of two polynomials of `level` Q limbs (out may alias an input):
+ * replaces add_ / sub_ (src/AddSub.cu:10-123) behind Ciphertext::add / sub
+ * (src/CKKS/Ciphertext.cpp:244-330). */
+int fides_add(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
+int fides_sub(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
 /* Rescale of n_polys polynomials at level l (FIXEDMANUAL DropLastElementAndScale);
  * out has l-1 limbs per poly.  Replaces Ciphertext::rescale (src/CKKS/Ciphertext.cpp:
  * 569-607) / LimbPartition::rescale (src/CKKS/LimbPartition.cu:711-797). */
@@ -147,6 +152,47 @@ typedef struct fides_rotate_item {
   uint32_t auto_index;
 } fides_rotate_item;
 int fides_rotate_batch(fides_ctx* ctx, const fides_rotate_item* items, int n, void* stream);
+
+/* ---- serving: continuous batching over resident keys -------------------------------
+ * A scheduler thread admits submitted requests by HBM budget into batches (one operation
+ * type per batch, any mix of levels) and runs each batch as one batched launch sequence on
+ * one of n_streams streams, so batches admitted while others run overlap on the device.
+ * Replaces the reference's concurrent-ops lanes (api/ConcurrentOps.hpp:30-64) and
+ * CudaEngine::evalRotateMany batching (CudaEngine.cpp:656-702).  Request buffers are
+ * device memory owned by the caller and must stay valid until fides_server_wait returns. */
+#define FIDES_OP_HMULT 0           /* HMult + relinearize + rescale: out has level - 1 limbs */
+#define FIDES_OP_HMULT_NORESCALE 1 /* HMult + relinearize: out has level limbs */
+#define FIDES_OP_ROTATE 2          /* HRotate by `rotation`: out has level limbs */
+
+typedef struct fides_server fides_server;
+typedef struct fides_server_config {
+  int n_streams;           /* batches in flight at once (1..16) */
+  int max_batch;           /* requests per batch */
+  size_t hbm_budget_bytes; /* scratch the in-flight batches may hold (0 = unlimited) */
+} fides_server_config;
+typedef struct fides_request {
+  int op;
+  int level;
+  const uint64_t *c0, *c1; /* first operand */
+  const uint64_t *d0, *d1; /* second operand (HMult) */
+  uint64_t *out0, *out1;
+  int rotation; /* FIDES_OP_ROTATE */
+} fides_request;
+typedef struct fides_server_stats {
+  uint64_t submitted, completed, rejected, batches, batched_requests, peak_bytes;
+} fides_server_stats;
+
+int fides_server_create(fides_ctx* ctx, const fides_server_config* cfg, fides_server** out);
+int fides_server_set_relin_key(fides_server* s, const uint64_t* relin_key_dev);
+int fides_server_add_rotation_key(fides_server* s, int rotation, const uint64_t* rot_key_dev);
+/* Thread-safe, non-blocking; rejects malformed requests and missing keys immediately. */
+int fides_server_submit(fides_server* s, const fides_request* req, uint64_t* ticket);
+/* Blocks until the request completed; *status is its result (FIDES_ERR_OOM when it can
+ * never fit the budget), *latency_ms the time from submit to completion. */
+int fides_server_wait(fides_server* s, uint64_t ticket, double* latency_ms, int* status);
+int fides_server_get_stats(fides_server* s, fides_server_stats* out);
+/* Completes in-flight batches, fails requests never started (FIDES_ERR_STATE), frees. */
+int fides_server_destroy(fides_server* s);
 
 /* ---- host-buffer entry points (end-to-end path) ------------------------------------- */
 /* Upload a key from host memory into a new device buffer owned by the context. */

@@ -434,4 +434,51 @@ int fides_rotate_host(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int 
   });
 }
 
+struct fides_graph_impl {
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
+
+int fides_capture_begin(fides_ctx* x, void* stream) {
+  return guard([&] {
+    C(x);
+    if (!stream) throw fides::Error(FIDES_ERR_ARG, "capture needs a non-default stream");
+    FIDES_CUDA(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeThreadLocal));
+  });
+}
+
+int fides_capture_end(fides_ctx* x, void* stream, fides_graph** out) {
+  return guard([&] {
+    C(x);
+    need(out, "out");
+    cudaGraph_t g = nullptr;
+    FIDES_CUDA(cudaStreamEndCapture(S(stream), &g));
+    cudaGraphExec_t e = nullptr;
+    cudaError_t rc = cudaGraphInstantiate(&e, g, 0);
+    if (rc != cudaSuccess) {
+      cudaGraphDestroy(g);
+      throw fides::Error(FIDES_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
+    }
+    *out = reinterpret_cast<fides_graph*>(new fides_graph_impl{g, e});
+  });
+}
+
+int fides_graph_launch(fides_graph* g, void* stream) {
+  return guard([&] {
+    need(g, "graph");
+    FIDES_CUDA(cudaGraphLaunch(reinterpret_cast<fides_graph_impl*>(g)->exec, S(stream)));
+  });
+}
+
+int fides_graph_destroy(fides_graph* g) {
+  return guard([&] {
+    if (!g) return;
+    auto* G = reinterpret_cast<fides_graph_impl*>(g);
+    cudaGraphExecDestroy(G->exec);
+    cudaGraphDestroy(G->graph);
+    delete G;
+  });
+}
+
 }  // extern "C"
+

@@ -176,7 +176,8 @@ struct PassShape {
 // One pass of a transform of 2^LOGN points.  Every index is a compile-time function of
 // LOGN, so global and shared addresses are a per-thread base plus immediate offsets.
 template <int LOGN, int PASS, bool FWD, int IN, int OUT>
-__global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G)
+__global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G,
+                                  ((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G) <= 256 ? 3 : 1)
     ntt_pass(const PassArgs a, const __grid_constant__ NttLimbList L) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
   constexpr int P = 1 << LOGP, E = 1 << LOGE, T = P / E, NT = T * G;

@@ -116,6 +116,10 @@ def lib():
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_capture_begin.argtypes = [vp, vp]
+        L.fides_capture_end.argtypes = [vp, vp, C.POINTER(vp)]
+        L.fides_graph_launch.argtypes = [vp, vp]
+        L.fides_graph_destroy.argtypes = [vp]
         L.fides_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
         L.fides_server_set_relin_key.argtypes = [vp, vp]
         L.fides_server_add_rotation_key.argtypes = [vp, C.c_int, vp]
@@ -217,6 +221,10 @@ class Context:
         _check(lib().fides_ctx_profile_read(self._h, self.KERNEL_FAMILIES[family], C.byref(ms), C.byref(by),
                                             C.byref(n)))
         return {"ms": ms.value, "bytes": by.value, "launches": int(n.value)}
+
+    def capture(self, stream) -> "Graph":
+        """Capture the calls made on `stream` (a torch.cuda.Stream that is current) into a graph."""
+        return Graph(self, stream)
 
     def empty(self, *shape) -> torch.Tensor:
         return torch.empty(*shape, self.N, dtype=torch.uint64, device=f"cuda:{self.device}")
@@ -383,6 +391,43 @@ def to_device(a, device: int = 0) -> torch.Tensor:
 def to_host(t: torch.Tensor):
     import numpy as np
     return t.contiguous().view(torch.int64).cpu().numpy().view(np.uint64)
+
+
+class Graph:
+    """A captured sequence of library calls (fides_capture_* / fides_graph_*).
+
+    Usage:  with ctx.capture(stream) as g: ...calls on `stream`...;  then g.launch(stream).
+    """
+
+    def __init__(self, ctx: "Context", stream):
+        self.ctx, self.stream, self._h = ctx, stream, None
+
+    def __enter__(self):
+        _check(lib().fides_capture_begin(self.ctx._h, self.stream.cuda_stream))
+        return self
+
+    def __exit__(self, et, ev, tb):
+        h = vp()
+        rc = lib().fides_capture_end(self.ctx._h, self.stream.cuda_stream, C.byref(h))
+        if et is None:
+            _check(rc)
+            self._h = h
+        return False
+
+    def launch(self, stream=None):
+        s = (stream or self.stream).cuda_stream
+        _check(lib().fides_graph_launch(self._h, s))
+
+    def close(self):
+        if self._h:
+            lib().fides_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

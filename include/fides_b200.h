@@ -153,6 +153,18 @@ typedef struct fides_rotate_item {
 } fides_rotate_item;
 int fides_rotate_batch(fides_ctx* ctx, const fides_rotate_item* items, int n, void* stream);
 
+/* ---- CUDA graphs ----------------------------------------------------------------------
+ * Record everything the library enqueues on `stream` between begin and end into a graph
+ * that replays it with one launch (the reference's run_in_graph, src/CudaUtils.cu:953-979,
+ * and its optional capture of the key-switch body, LimbPartitionMGPU.cu:811-892).  Scratch
+ * taken during capture becomes graph-owned memory, so a replay needs no allocation calls.
+ * Pointers and values passed to the captured calls are frozen into the graph. */
+typedef struct fides_graph fides_graph;
+int fides_capture_begin(fides_ctx* ctx, void* stream);
+int fides_capture_end(fides_ctx* ctx, void* stream, fides_graph** out);
+int fides_graph_launch(fides_graph* g, void* stream);
+int fides_graph_destroy(fides_graph* g);
+
 /* ---- serving: continuous batching over resident keys -------------------------------
  * A scheduler thread admits submitted requests by HBM budget into batches (one operation
  * type per batch, any mix of levels) and runs each batch as one batched launch sequence on

@@ -227,12 +227,55 @@ static int addsub(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level,
   });
 }
 
+int fides_mul(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
+  return addsub(x, a, b, level, out, stream, fides::EW_MUL);
+}
+
+static int scalar_op(fides_ctx* x, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
+                     void* stream, int op) {
+  return guard([&] {
+    auto* c = C(x);
+    need(a, "a");
+    need(scalars, "scalars");
+    need(out, "out");
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (level > fides::MAX_SCALAR_LIMBS) throw fides::Error(FIDES_ERR_ARG, "scalar ops support at most 64 limbs");
+    fides::ScalarJob j{};
+    j.a = a;
+    j.out = out;
+    j.l = level;
+    j.op = op;
+    for (int i = 0; i < level; ++i) j.s[i] = scalars[i] % c->primes[i];
+    fides::launch_scalar(c, &j, 1, S(stream));
+  });
+}
+
+int fides_mul_scalar(fides_ctx* x, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
+                     void* stream) {
+  return scalar_op(x, a, level, scalars, out, stream, fides::EW_MUL_SCALAR);
+}
+
+int fides_add_scalar(fides_ctx* x, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
+                     void* stream) {
+  return scalar_op(x, a, level, scalars, out, stream, fides::EW_ADD_SCALAR);
+}
+
+int fides_mod_raise(fides_ctx* x, const uint64_t* in, int out_level, uint64_t* out, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(in, "x");
+    need(out, "out");
+    if (out == in) throw fides::Error(FIDES_ERR_ARG, "out must not alias the input limb");
+    fides::op_mod_raise(c, in, out_level, out, S(stream));
+  });
+}
+
 int fides_add(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
-  return addsub(x, a, b, level, out, stream, 0);
+  return addsub(x, a, b, level, out, stream, fides::EW_ADD);
 }
 
 int fides_sub(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
-  return addsub(x, a, b, level, out, stream, 1);
+  return addsub(x, a, b, level, out, stream, fides::EW_SUB);
 }
 
 int fides_rescale(fides_ctx* x, const uint64_t* in, int level, uint64_t* out, void* stream) {

@@ -189,16 +189,49 @@ __global__ void __launch_bounds__(EW_THREADS) addsub_kernel(const __grid_constan
   const int j = blockIdx.y;
   if (j >= J.l) return;
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const uint64_t q = primes[j].q;
+  const DevPrime p = primes[j];
+  const uint64_t q = p.q;
   const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(J.a + off);
-  const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(J.b + off);
-  ulonglong2 r;
-  if (J.sub) {
-    r.x = submod(x.x, y.x, q);
-    r.y = submod(x.y, y.y, q);
+  ulonglong2 y;
+  if (J.sub >= EW_MUL_SCALAR) {
+    y.x = y.y = J.b[j];
   } else {
-    r.x = addmod(x.x, y.x, q);
-    r.y = addmod(x.y, y.y, q);
+    y = *reinterpret_cast<const ulonglong2*>(J.b + off);
+  }
+  ulonglong2 r;
+  switch (J.sub) {
+    case EW_SUB:
+      r.x = submod(x.x, y.x, q);
+      r.y = submod(x.y, y.y, q);
+      break;
+    case EW_MUL:
+    case EW_MUL_SCALAR:
+      r.x = mulmod(x.x, y.x, p);
+      r.y = mulmod(x.y, y.y, p);
+      break;
+    default:  // EW_ADD, EW_ADD_SCALAR
+      r.x = addmod(x.x, y.x, q);
+      r.y = addmod(x.y, y.y, q);
+  }
+  *reinterpret_cast<ulonglong2*>(J.out + off) = r;
+}
+
+__global__ void __launch_bounds__(EW_THREADS) scalar_kernel(const __grid_constant__ ScalarJobList L,
+                                                            const DevPrime* primes, int logN) {
+  const ScalarJob& J = L.j[blockIdx.z];
+  const int j = blockIdx.y;
+  if (j >= J.l) return;
+  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const DevPrime p = primes[j];
+  const uint64_t sc = J.s[j];
+  const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(J.a + off);
+  ulonglong2 r;
+  if (J.op == EW_MUL_SCALAR) {
+    r.x = mulmod(x.x, sc, p);
+    r.y = mulmod(x.y, sc, p);
+  } else {
+    r.x = addmod(x.x, sc, p.q);
+    r.y = addmod(x.y, sc, p.q);
   }
   *reinterpret_cast<ulonglong2*>(J.out + off) = r;
 }
@@ -362,6 +395,25 @@ void launch_addsub(Context* c, const AddSubJob* jobs, int n, cudaStream_t s) {
     dim3 grid(c->N / (2 * EW_THREADS), mx, m);
     LaunchScope ls(c, s, KK_ELEM, bytes);
     addsub_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->logN);
+    FIDES_CUDA(cudaGetLastError());
+  }
+}
+
+void launch_scalar(Context* c, const ScalarJob* jobs, int n, cudaStream_t s) {
+  static thread_local ScalarJobList L;
+  for (int off = 0; off < n; off += MAX_SCALAR_JOBS) {
+    int m = std::min(MAX_SCALAR_JOBS, n - off);
+    fill(L, jobs + off, m);
+    int mx = 1;
+    double bytes = 0;
+    for (int i = 0; i < m; ++i) {
+      if (L.j[i].l > MAX_SCALAR_LIMBS) throw Error(-1, "scalar op on more than 64 limbs");
+      mx = std::max(mx, L.j[i].l);
+      bytes += 8.0 * c->N * 2.0 * L.j[i].l;
+    }
+    dim3 grid(c->N / (2 * EW_THREADS), mx, m);
+    LaunchScope ls(c, s, KK_ELEM, bytes);
+    scalar_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->logN);
     FIDES_CUDA(cudaGetLastError());
   }
 }

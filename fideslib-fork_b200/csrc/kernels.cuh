@@ -101,12 +101,14 @@ struct RescaleJobList {
 void launch_switch_modulus(Context* c, const SwitchJob* jobs, int n, cudaStream_t s);
 void launch_rescale_finish(Context* c, const RescaleJob* jobs, int n, cudaStream_t s);
 
-// ---- RNS add / sub (reference add_ / sub_, src/AddSub.cu:10-123)
+// ---- RNS elementwise ops (reference add_ / sub_, src/AddSub.cu:10-123; Mult_ /
+// Scalar_mult_ / scalar_add_, src/CKKS/ElemenwiseBatchKernels.cu:14-200, src/AddSub.cu)
+enum EwOp { EW_ADD = 0, EW_SUB = 1, EW_MUL = 2, EW_MUL_SCALAR = 3, EW_ADD_SCALAR = 4 };
 struct AddSubJob {
-  const uint64_t *a, *b;
+  const uint64_t *a, *b;  // b: second operand (ADD/SUB/MUL) or per-limb scalars (device, *_SCALAR)
   uint64_t* out;
   int l;
-  int sub;  // 0: a + b, 1: a - b
+  int sub;  // EwOp
 };
 constexpr int MAX_ADDSUB_JOBS = 128;
 struct AddSubJobList {
@@ -114,5 +116,21 @@ struct AddSubJobList {
   AddSubJob j[MAX_ADDSUB_JOBS];
 };
 void launch_addsub(Context* c, const AddSubJob* jobs, int n, cudaStream_t s);
+
+// Per-limb scalar ops: out_i = a_i * s_i or a_i + s_i (mod q_i), scalars passed by value.
+constexpr int MAX_SCALAR_LIMBS = 64;
+struct ScalarJob {
+  const uint64_t* a;
+  uint64_t* out;
+  int l;
+  int op;  // EW_MUL_SCALAR or EW_ADD_SCALAR
+  uint64_t s[MAX_SCALAR_LIMBS];
+};
+constexpr int MAX_SCALAR_JOBS = 8;
+struct ScalarJobList {
+  int n, max_l, pad0, pad1;
+  ScalarJob j[MAX_SCALAR_JOBS];
+};
+void launch_scalar(Context* c, const ScalarJob* jobs, int n, cudaStream_t s);
 
 }  // namespace fides

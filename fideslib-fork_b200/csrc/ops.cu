@@ -361,4 +361,21 @@ void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) {
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
 }
 
+void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s) {
+  check_level(c, out_level);
+  const size_t N = c->N;
+  Scratch sc(c, sizeof(uint64_t) * N, s);
+  LimbRef r = lref(sc.u64(), 0);
+  r.src = x;
+  ntt_limbs(c, &r, 1, true, s);
+  std::vector<LimbRef> refs;
+  for (int j = 0; j < out_level; ++j) {
+    LimbRef t = lref(out + j * N, j);
+    t.pro = sc.u64();
+    t.aux = 1;  // source prime = aux - 1 = q_0
+    refs.push_back(t);
+  }
+  ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_SWITCH, OUT_PLAIN);
+}
+
 }  // namespace fides

@@ -115,6 +115,10 @@ def lib():
         L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_mul_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
+        L.fides_add_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
+        L.fides_mod_raise.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_capture_begin.argtypes = [vp, vp]
         L.fides_capture_end.argtypes = [vp, vp, C.POINTER(vp)]
@@ -323,6 +327,47 @@ class Context:
         o1 = (vp * n)(*[_ptr(o.c1) for o in outs])
         _check(lib().fides_rotate_hoisted(self._h, _ptr(ct.c0), _ptr(ct.c1), l, kp, rs, n, o0, o1, _stream()))
         return outs
+
+    # -- elementwise RNS ops (polynomials of `level` Q limbs) --
+    def add_poly(self, a, b, out=None):
+        out = self.empty(a.shape[0]) if out is None else out
+        _check(lib().fides_add(self._h, _ptr(a), _ptr(b), a.shape[0], _ptr(out), _stream()))
+        return out
+
+    def sub_poly(self, a, b, out=None):
+        out = self.empty(a.shape[0]) if out is None else out
+        _check(lib().fides_sub(self._h, _ptr(a), _ptr(b), a.shape[0], _ptr(out), _stream()))
+        return out
+
+    def mul_poly(self, a, b, out=None):
+        out = self.empty(a.shape[0]) if out is None else out
+        _check(lib().fides_mul(self._h, _ptr(a), _ptr(b), a.shape[0], _ptr(out), _stream()))
+        return out
+
+    def _scalars(self, values, l):
+        import numpy as np
+        v = np.array([int(values[i]) % self.q[i] if hasattr(values, "__len__") else int(values) % self.q[i]
+                      for i in range(l)], dtype=np.uint64)
+        return v
+
+    def mul_scalar_poly(self, a, values, out=None):
+        """a_i * values_i mod q_i (values: one int, or one residue per limb)."""
+        out = self.empty(a.shape[0]) if out is None else out
+        v = self._scalars(values, a.shape[0])
+        _check(lib().fides_mul_scalar(self._h, _ptr(a), a.shape[0], v.ctypes.data_as(u64p), _ptr(out), _stream()))
+        return out
+
+    def add_scalar_poly(self, a, values, out=None):
+        out = self.empty(a.shape[0]) if out is None else out
+        v = self._scalars(values, a.shape[0])
+        _check(lib().fides_add_scalar(self._h, _ptr(a), a.shape[0], v.ctypes.data_as(u64p), _ptr(out), _stream()))
+        return out
+
+    def mod_raise_poly(self, x, level: int):
+        """Level-1 polynomial (limb q_0) -> `level` limbs with the centred residues."""
+        out = self.empty(level)
+        _check(lib().fides_mod_raise(self._h, _ptr(x), level, _ptr(out), _stream()))
+        return out
 
     # -- batched forms --
     def mult_batch(self, pairs, relin_key, rescale=True) -> list[Ciphertext]:

@@ -1,0 +1,486 @@
+"""CKKS bootstrapping on the B200 core: ModRaise -> CoeffsToSlots -> EvalMod -> SlotsToCoeffs.
+
+Mirrors the reference's CKKS::Bootstrap (src/CKKS/Bootstrap.cu:437-648): ModRaise (:708+),
+EvalCoeffsToSlots / EvalLinearTransform (src/CKKS/CoeffsToSlots.cu:26-151, BSGS linear
+transforms in src/CKKS/LinearTransform.cu), approxModReduction with a Chebyshev series and
+double-angle iterations (src/CKKS/ApproxModEval.cu:45-167, :527, :873).  OpenFHE's own
+coefficient tables are not available, so every table here is derived from the mathematics:
+
+  * Slots.  Slot j of a plaintext m(X) at scale S is m(zeta^(5^j)) / S, zeta = exp(i pi / N);
+    with w_k = m_k + i m_(k+N/2) this is z = U0 w / S, U0[j, k] = zeta^(5^j k), n = N/2 slots,
+    and U0^H U0 = n I.
+  * Special FFT.  z = U0 w is a radix-2 decimation-in-time transform on bit-reversed input:
+    z = F (P w), F = S_(n/2) ... S_2 S_1, where S_h combines entries p, p + h of each block of
+    2h with the twiddle rho^(5^r), rho = exp(i pi / (4h)), r = p mod h.  Each S_h has three
+    slot diagonals (offsets 0, +h, -h), so CoeffsToSlots applies F^-1 = S_1^-1 ... S_(n/2)^-1
+    and SlotsToCoeffs applies F, each grouped into a few levels of composed diagonals
+    evaluated baby-step / giant-step with hoisted rotations.  Data stay in bit-reversed
+    order between the two transforms; everything in between is slot-wise.
+  * EvalMod.  After CoeffsToSlots the real slots hold t = m'_k / (K q0), m' = m + q0 I; the
+    Chebyshev interpolant of cos(2 pi K t / 2^r - pi / 2^(r+1)) on [-1, 1] followed by r
+    double-angle steps c <- 2 c^2 - 1 gives sin(2 pi m'_k / q0) = sin(2 pi m_k / q0).
+  * Scales.  Level l has scale S_l with S_(l-1) = S_l^2 / q_(l-1) (products of two level-l
+    ciphertexts land exactly on the next level's scale); a ciphertext moved down several
+    levels is first multiplied by an integer constant that re-targets its scale.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+# ------------------------------------------------------------------------------ encoding
+def encode_coeffs(z: np.ndarray, N: int, scale: float) -> np.ndarray:
+    """Complex slot vector (N/2) -> integer coefficients (int64) of m with m(zeta^(5^j)) = scale z_j."""
+    n = N // 2
+    M = 2 * N
+    e = np.empty(n, dtype=np.int64)
+    e[0] = 1
+    for j in range(1, n):
+        e[j] = (e[j - 1] * 5) % M
+    t_pos = (e - 1) // 2
+    t_neg = ((M - e) - 1) // 2
+    Mv = np.zeros(N, dtype=np.complex128)
+    Mv[t_pos] = z
+    Mv[t_neg] = np.conj(z)
+    k = np.arange(N)
+    m = np.fft.fft(Mv) / N * np.exp(-1j * np.pi * k / N)
+    c = np.round(m.real * scale)
+    if np.abs(c).max() >= 2.0 ** 62:
+        raise ValueError("encoded coefficients exceed 62 bits")
+    return c.astype(np.int64)
+
+
+def decode_coeffs(coeff: np.ndarray, N: int, scale: float) -> np.ndarray:
+    n = N // 2
+    M = 2 * N
+    e = np.empty(n, dtype=np.int64)
+    e[0] = 1
+    for j in range(1, n):
+        e[j] = (e[j - 1] * 5) % M
+    k = np.arange(N)
+    Mv = np.fft.ifft(np.asarray(coeff, dtype=np.float64) * np.exp(1j * np.pi * k / N)) * N
+    return Mv[(e - 1) // 2] / scale
+
+
+def to_limbs(coeff: np.ndarray, primes) -> np.ndarray:
+    c = np.asarray(coeff, dtype=np.int64)
+    return np.stack([np.mod(c, np.int64(q)).astype(np.uint64) for q in primes])
+
+
+def bit_reverse_perm(n: int) -> np.ndarray:
+    b = n.bit_length() - 1
+    return np.array([int(format(i, f"0{b}b")[::-1], 2) if b else 0 for i in range(n)], dtype=np.int64)
+
+
+# ------------------------------------------------------------------------------ special FFT
+def stage(n: int, h: int, inverse: bool) -> dict[int, np.ndarray]:
+    """Slot diagonals of S_h (or S_h^-1): out = sum_r D_r * roll(a, -r)."""
+    p = np.arange(n)
+    r = p % (2 * h)
+    lo = r < h
+    idx = np.where(lo, r, r - h)
+    e = np.array([pow(5, int(i), 8 * h) for i in range(h)], dtype=np.float64)
+    tw = np.exp(1j * np.pi * e / (4 * h))[idx]
+    d0 = np.zeros(n, dtype=np.complex128)
+    dp = np.zeros(n, dtype=np.complex128)
+    dm = np.zeros(n, dtype=np.complex128)
+    if not inverse:
+        # lo: a[p] + tw a[p+h]; hi: a[p-h] - tw a[p]
+        d0[lo] = 1
+        dp[lo] = tw[lo]
+        d0[~lo] = -tw[~lo]
+        dm[~lo] = 1
+    else:
+        # lo: (a[p] + a[p+h]) / 2; hi: (a[p-h] - a[p]) / (2 tw)
+        d0[lo] = 0.5
+        dp[lo] = 0.5
+        d0[~lo] = -0.5 / tw[~lo]
+        dm[~lo] = 0.5 / tw[~lo]
+    out = {0: d0}
+    if h < n:
+        out[h % n] = out.get(h % n, 0) + dp
+        out[(-h) % n] = out.get((-h) % n, 0) + dm
+    return out
+
+
+def compose(A: dict[int, np.ndarray], B: dict[int, np.ndarray], n: int) -> dict[int, np.ndarray]:
+    """Diagonals of A @ B: (A B) v = sum_{r,s} (A_r * roll(B_s, -r)) * roll(v, -(r + s))."""
+    out: dict[int, np.ndarray] = {}
+    for r, Ar in A.items():
+        for s, Bs in B.items():
+            k = (r + s) % n
+            out[k] = out.get(k, 0) + Ar * np.roll(Bs, -r)
+    return {k: v for k, v in out.items() if np.abs(v).max() > 0}
+
+
+def apply_diags(D: dict[int, np.ndarray], v: np.ndarray) -> np.ndarray:
+    return sum(d * np.roll(v, -r) for r, d in D.items())
+
+
+def fft_levels(n: int, n_levels: int, inverse: bool, unnormalized: bool = False) -> list[dict[int, np.ndarray]]:
+    """F (or F^-1) as `n_levels` composed matrices, in application order.  With
+    `unnormalized`, the inverse stages are 2 S_h^-1 (unit-modulus entries), i.e. the product
+    is n F^-1."""
+    hs = [1 << i for i in range(n.bit_length() - 1)]  # S_1 .. S_(n/2)
+    order = hs if not inverse else hs[::-1]           # F applies S_1 first; F^-1 applies S_(n/2)^-1 first
+    groups = np.array_split(np.arange(len(order)), n_levels)
+    mats = []
+    for g in groups:
+        M = None
+        for i in g:
+            S = stage(n, order[i], inverse)
+            if inverse and unnormalized:
+                S = {k: 2 * v for k, v in S.items()}
+            M = S if M is None else compose(S, M, n)  # later stages on the left
+        mats.append(M)
+    return mats
+
+
+# ------------------------------------------------------------------------------ evaluator
+class Ct:
+    """Ciphertext handle with its scale (level = number of limbs)."""
+
+    def __init__(self, c0, c1, scale: float):
+        self.c0, self.c1, self.scale = c0, c1, scale
+
+    @property
+    def level(self) -> int:
+        return int(self.c0.shape[0])
+
+
+class Evaluator:
+    """CKKS arithmetic with exact per-level scale bookkeeping over the GPU core."""
+
+    def __init__(self, F, ctx, relin_key, rot_keys: dict, conj_key, top_scale: float):
+        self.F, self.ctx, self.rk = F, ctx, relin_key
+        self.rot_keys, self.conj_key = rot_keys, conj_key
+        self.q = ctx.q
+        L = ctx.n_q
+        self.S = [0.0] * (L + 1)
+        self.S[L] = top_scale
+        for l in range(L, 1, -1):
+            self.S[l - 1] = self.S[l] ** 2 / self.q[l - 1]
+
+    # -- level / scale management --
+    def drop(self, a: Ct, level: int) -> Ct:
+        """Discard limbs (the value is kept modulo the smaller modulus; scale unchanged)."""
+        return Ct(a.c0[:level], a.c1[:level], a.scale)
+
+    def to_level(self, a: Ct, level: int) -> Ct:
+        """Bring `a` to `level` at that level's canonical scale S_level."""
+        if a.level == level and abs(a.scale / self.S[level] - 1) < 1e-15:
+            return a
+        if a.level <= level:
+            raise ValueError(f"cannot raise level {a.level} -> {level}")
+        # integer constant c with a.scale * c / q_top = S_level, then rescale, then discard
+        qt = self.q[a.level - 1]
+        c = round(self.S[level] * qt / a.scale)
+        b = self._rescale_to(self.mul_int(a, c), self.S[level])
+        return self.drop(b, level)
+
+    def _rescale_to(self, a: Ct, new_scale: float) -> Ct:
+        c0 = self.ctx.rescale_poly(a.c0)
+        c1 = self.ctx.rescale_poly(a.c1)
+        return Ct(c0, c1, new_scale)
+
+    def rescale(self, a: Ct) -> Ct:
+        return self._rescale_to(a, a.scale / self.q[a.level - 1])
+
+    # -- arithmetic --
+    def add(self, a: Ct, b: Ct) -> Ct:
+        l = min(a.level, b.level)
+        a = self.to_level(a, l) if (a.level != l or abs(a.scale / self.S[l] - 1) > 1e-12) else a
+        b = self.to_level(b, l) if (b.level != l or abs(b.scale / self.S[l] - 1) > 1e-12) else b
+        return Ct(self.ctx.add_poly(a.c0, b.c0), self.ctx.add_poly(a.c1, b.c1), a.scale)
+
+    def add_raw(self, a: Ct, b: Ct) -> Ct:
+        """a + b for operands already at the same level and scale."""
+        return Ct(self.ctx.add_poly(a.c0, b.c0), self.ctx.add_poly(a.c1, b.c1), a.scale)
+
+    def sub_raw(self, a: Ct, b: Ct) -> Ct:
+        return Ct(self.ctx.sub_poly(a.c0, b.c0), self.ctx.sub_poly(a.c1, b.c1), a.scale)
+
+    def add_const(self, a: Ct, value: float) -> Ct:
+        v = round(value * a.scale)
+        return Ct(self.ctx.add_scalar_poly(a.c0, [v % q for q in self.q[:a.level]]), a.c1, a.scale)
+
+    def mul_int(self, a: Ct, c: int) -> Ct:
+        vals = [c % q for q in self.q[:a.level]]
+        return Ct(self.ctx.mul_scalar_poly(a.c0, vals), self.ctx.mul_scalar_poly(a.c1, vals), a.scale)
+
+    def mul_const(self, a: Ct, value: float, target_level: int) -> Ct:
+        """value * a, landing at `target_level` (< a.level) with scale S_target."""
+        qt = self.q[a.level - 1]
+        c = round(value * self.S[target_level] * qt / a.scale)
+        b = self.mul_int(a, c)
+        b = self._rescale_to(b, self.S[target_level])
+        return self.drop(b, target_level)
+
+    def mul(self, a: Ct, b: Ct) -> Ct:
+        l = min(a.level, b.level)
+        a = self.to_level(a, l)
+        b = self.to_level(b, l)
+        out = self.ctx.mult(self.F.Ciphertext(a.c0, a.c1), self.F.Ciphertext(b.c0, b.c1), self.rk, rescale=True)
+        return Ct(out.c0, out.c1, self.S[l - 1])
+
+    def square(self, a: Ct) -> Ct:
+        return self.mul(a, a)
+
+    def mul_plain(self, a: Ct, pt, pt_scale: float) -> Ct:
+        """a * pt (EVAL limbs at a.level), then rescale."""
+        c0 = self.ctx.mul_poly(a.c0, pt[:a.level])
+        c1 = self.ctx.mul_poly(a.c1, pt[:a.level])
+        return self._rescale_to(Ct(c0, c1, 0), a.scale * pt_scale / self.q[a.level - 1])
+
+    def mul_plain_int(self, a: Ct, pt) -> Ct:
+        """a * pt for an integer plaintext (scale 1), no rescale."""
+        return Ct(self.ctx.mul_poly(a.c0, pt[:a.level]), self.ctx.mul_poly(a.c1, pt[:a.level]), a.scale)
+
+    def conjugate(self, a: Ct) -> Ct:
+        k = 2 * self.ctx.N - 1
+        out = self.ctx.rotate_auto(self.F.Ciphertext(a.c0, a.c1), self.conj_key, k)
+        return Ct(out.c0, out.c1, a.scale)
+
+    def rotate_many(self, a: Ct, rs: list[int]) -> list[Ct]:
+        rs2 = [r for r in rs if r % (self.ctx.N // 2) != 0]
+        res = {}
+        if rs2:
+            outs = self.ctx.rotate_hoisted(self.F.Ciphertext(a.c0, a.c1), [self.rot_keys[r] for r in rs2], rs2)
+            res = {r: Ct(o.c0, o.c1, a.scale) for r, o in zip(rs2, outs)}
+        return [a if r % (self.ctx.N // 2) == 0 else res[r] for r in rs]
+
+    def rotate(self, a: Ct, r: int) -> Ct:
+        return self.rotate_many(a, [r])[0]
+
+
+# ------------------------------------------------------------------------------ bootstrapper
+class Bootstrapper:
+    """Precomputed CoeffsToSlots / SlotsToCoeffs diagonals and EvalMod constants."""
+
+    def __init__(self, ev: Evaluator, K: int = 12, r: int = 3, degree: int = 63, cts_levels: int = 3,
+                 stc_levels: int = 3, baby: int = 8, prescale_bits: int = 0):
+        self.ev = ev
+        ctx = ev.ctx
+        self.N = ctx.N
+        self.n = self.N // 2
+        self.K, self.r, self.degree = K, r, degree
+        # the input is multiplied by 2^prescale_bits before ModRaise so that the message fills
+        # more of q0 (a correction factor); SlotsToCoeffs divides it back out
+        self.prescale = 1 << prescale_bits
+        self.cts_levels, self.stc_levels, self.baby = cts_levels, stc_levels, baby
+        self.q0 = ctx.q[0]
+        # Chebyshev interpolant of cos(2 pi K t / 2^r - pi / 2^(r+1)) on [-1, 1]
+        f = lambda t: np.cos(2 * np.pi * K * t / 2 ** r - np.pi / 2 ** (r + 1))
+        self.cheb = np.polynomial.chebyshev.chebinterpolate(f, degree)
+        self.cts = fft_levels(self.n, cts_levels, inverse=True, unnormalized=True)
+        self.stc = fft_levels(self.n, stc_levels, inverse=False)
+        self.rotations = sorted({r for M in self.cts + self.stc for r in self._bsgs_rotations(M)} - {0})
+        self.pt_int = {}
+
+    # --- BSGS plan of one composed matrix
+    def _plan(self, M: dict):
+        n, g = self.n, self.baby
+        offs = sorted(M)
+        step = math.gcd(*[o for o in offs if o] + [n]) if any(offs) else n
+        ts = sorted({((o + n // 2) % n - n // 2) // step for o in offs})  # signed multiples of step
+        giant = {}
+        for t in ts:
+            i, j = divmod(t, g)
+            giant.setdefault(i, []).append(j)
+        return step, giant
+
+    def _bsgs_rotations(self, M: dict):
+        step, giant = self._plan(M)
+        g = self.baby
+        rs = {step * j for js in giant.values() for j in js}
+        rs |= {step * g * i for i in giant}
+        return {r % self.n for r in rs}
+
+    def needed_rotations(self) -> list[int]:
+        return self.rotations
+
+    # --- plaintext preparation (encoding on the GPU: torch FFT, then the library's NTT)
+    def _encode_pt(self, z, level: int, scale: float):
+        import torch
+        F, ctx = self.ev.F, self.ev.ctx
+        N = self.N
+        dev = f"cuda:{ctx.device}"
+        if not hasattr(self, "_enc"):
+            n, M = N // 2, 2 * N
+            e = np.empty(n, dtype=np.int64)
+            e[0] = 1
+            for j in range(1, n):
+                e[j] = (e[j - 1] * 5) % M
+            self._enc = (torch.from_numpy((e - 1) // 2).to(dev), torch.from_numpy(((M - e) - 1) // 2).to(dev),
+                         torch.exp(-1j * torch.pi * torch.arange(N, device=dev, dtype=torch.float64) / N),
+                         torch.tensor(ctx.q, dtype=torch.int64, device=dev))
+        tp, tn, twist, qs = self._enc
+        zt = torch.from_numpy(np.ascontiguousarray(z, dtype=np.complex128)).to(dev)
+        Mv = torch.zeros(N, dtype=torch.complex128, device=dev)
+        Mv[tp] = zt
+        Mv[tn] = torch.conj(zt)
+        m = torch.fft.fft(Mv) / N * twist
+        c = torch.round(m.real * scale)
+        if float(c.abs().max()) >= 2.0 ** 62:
+            raise ValueError("encoded coefficients exceed 62 bits")
+        ci = c.to(torch.int64)
+        limbs = torch.remainder(ci.unsqueeze(0), qs[:level].unsqueeze(1)).contiguous().view(torch.uint64)
+        ctx.ntt(limbs)
+        return limbs
+
+    def _int_pt(self, coeff, level: int):
+        F, ctx = self.ev.F, self.ev.ctx
+        limbs = F.to_device(to_limbs(coeff, ctx.q[:level]))
+        ctx.ntt(limbs)
+        return limbs
+
+    def prepare(self, top_level: int, msg_scale: float):
+        """Encode the transform diagonals for a bootstrap raising to `top_level`, for input
+        ciphertexts whose slots are encoded at `msg_scale`."""
+        ev, n = self.ev, self.n
+        in_scale = ev.S[top_level]  # the scale given to the raised ciphertext (free choice)
+        msg_scale = msg_scale * self.prescale
+        self.top, self.in_scale, self.msg_scale = top_level, in_scale, msg_scale
+        # CoeffsToSlots: slots -> c' P w / S with c' = S / (2 K q0).  The matrices are the
+        # unnormalised stages (product n F^-1, unit-modulus entries) and the factor c' / n is
+        # spread evenly over them, so every encoded diagonal keeps ~42 significant bits.
+        gfac = (in_scale / (2 * self.K * self.q0) / n) ** (1.0 / len(self.cts))
+        self.cts_pts = []
+        level, scale = top_level, in_scale
+        for m, M in enumerate(self.cts):
+            self.cts_pts.append(self._prepare_matrix(M, gfac, level, scale))
+            level -= 1
+            scale = ev.S[level]
+        self.cts_out_level = level
+        # EvalMod levels: ceil(log2 degree) + 1 (series sum) + r (double angle)
+        depth = math.ceil(math.log2(self.degree)) + 1 + self.r
+        self.stc_in_level = self.cts_out_level - depth
+        # SlotsToCoeffs: c'' = q0 / (2 pi msg_scale), spread evenly over the matrices
+        sfac = (self.q0 / (2 * np.pi * msg_scale)) ** (1.0 / len(self.stc))
+        self.stc_pts = []
+        level = self.stc_in_level
+        for m, M in enumerate(self.stc):
+            fac = sfac
+            self.stc_pts.append(self._prepare_matrix(M, fac, level, ev.S[level]))
+            level -= 1
+        self.out_level = level
+        N = self.N
+        mono = np.zeros(N, dtype=np.int64)
+        mono[N // 2] = 1  # X^(N/2): slots * i
+        self.pt_i = self._int_pt(mono, top_level)
+        self.pt_minus_i = self._int_pt(-mono, top_level)
+
+    def _prepare_matrix(self, M: dict, fac: float, level: int, scale: float):
+        """Pre-rotated, encoded diagonals for BSGS at `level` (input scale `scale`)."""
+        ev, n, g = self.ev, self.n, self.baby
+        step, giant = self._plan(M)
+        target = ev.S[level - 1]
+        pt_scale = target * ev.q[level - 1] / scale  # so that rescale lands on S_(level-1)
+        out = {}
+        for i, js in giant.items():
+            for j in js:
+                off = (step * (g * i + j)) % n
+                d = M.get(off)
+                if d is None:
+                    continue
+                d = np.roll(d * fac, step * g * i)  # rot^{-g i}(D)
+                out[(i, j)] = self._encode_pt(d, level, pt_scale)
+        return {"step": step, "giant": giant, "pts": out, "pt_scale": pt_scale, "level": level}
+
+    # --- homomorphic linear transform
+    def _apply(self, a: Ct, P: dict) -> Ct:
+        ev, g = self.ev, self.baby
+        step, giant = P["step"], P["giant"]
+        assert a.level == P["level"], (a.level, P["level"])
+        js = sorted({j for v in giant.values() for j in v})
+        baby = dict(zip(js, ev.rotate_many(a, [(step * j) % self.n for j in js])))
+        acc = None
+        for i, jl in sorted(giant.items()):
+            inner = None
+            for j in jl:
+                pt = P["pts"].get((i, j))
+                if pt is None:
+                    continue
+                b = baby[j]
+                t0 = ev.ctx.mul_poly(b.c0, pt)
+                t1 = ev.ctx.mul_poly(b.c1, pt)
+                inner = (t0, t1) if inner is None else (ev.ctx.add_poly(inner[0], t0), ev.ctx.add_poly(inner[1], t1))
+            if inner is None:
+                continue
+            part = Ct(inner[0], inner[1], a.scale)
+            if i:
+                part = ev.rotate(part, (step * g * i) % self.n)
+            acc = part if acc is None else ev.add_raw(acc, part)
+        return ev._rescale_to(acc, ev.S[a.level - 1])
+
+    # --- EvalMod
+    def _chebyshev(self, t: Ct) -> Ct:
+        ev, d = self.ev, self.degree
+        T = {1: t}
+        l0 = t.level
+
+        def get(k):
+            if k in T:
+                return T[k]
+            if k % 2 == 0:
+                h = get(k // 2)
+                x = ev.square(h)
+                x = ev.add_raw(x, x)
+                x = ev.add_const(x, -1.0)
+            else:
+                a, b = get(k // 2), get(k // 2 + 1)
+                x = ev.mul(a, b)
+                x = ev.add_raw(x, x)
+                one = ev.to_level(T[1], x.level)
+                x = ev.sub_raw(x, one)
+            T[k] = x
+            return x
+
+        for k in range(2, d + 1):
+            get(k)
+        final = min(T[k].level for k in T) - 1
+        acc = None
+        for k in range(1, d + 1):
+            c = float(self.cheb[k])
+            if abs(c) < 1e-18:
+                continue
+            term = ev.mul_const(T[k], c, final)
+            acc = term if acc is None else ev.add_raw(acc, term)
+        acc = ev.add_const(acc, float(self.cheb[0]))
+        return acc
+
+    def _eval_mod(self, t: Ct) -> Ct:
+        ev = self.ev
+        c = self._chebyshev(t)
+        for _ in range(self.r):
+            x = ev.square(c)
+            x = ev.add_raw(x, x)
+            c = ev.add_const(x, -1.0)
+        return c
+
+    # --- the bootstrap
+    def bootstrap(self, ct: Ct) -> Ct:
+        ev = self.ev
+        F = ev.F
+        x = ct if self.prescale == 1 else ev.mul_int(Ct(ct.c0[:1], ct.c1[:1], ct.scale), self.prescale)
+        # ModRaise: m -> m + q0 I at every limb of the top level
+        a = Ct(ev.ctx.mod_raise_poly(x.c0[:1], self.top), ev.ctx.mod_raise_poly(x.c1[:1], self.top), self.in_scale)
+        # CoeffsToSlots
+        for P in self.cts_pts:
+            a = self._apply(a, P)
+        # real / imaginary parts: t_re = a + conj(a), t_im = -i (a - conj(a))
+        cj = ev.conjugate(a)
+        t_re = ev.add_raw(a, cj)
+        t_im = ev.mul_plain_int(ev.sub_raw(a, cj), self.pt_minus_i)
+        # EvalMod on both, then recombine u = s_re + i s_im
+        s_re = self._eval_mod(t_re)
+        s_im = self._eval_mod(t_im)
+        s_re = ev.to_level(s_re, self.stc_in_level)
+        s_im = ev.to_level(s_im, self.stc_in_level)
+        u = ev.add_raw(s_re, ev.mul_plain_int(s_im, self.pt_i))
+        # SlotsToCoeffs
+        for P in self.stc_pts:
+            u = self._apply(u, P)
+        return u

@@ -110,6 +110,19 @@ int fides_tensor(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, const u
  * (src/CKKS/Ciphertext.cpp:244-330). */
 int fides_add(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
 int fides_sub(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
+/* Elementwise product of two polynomials (ciphertext component x plaintext, EVAL):
+ * replaces Mult_ / multPt (ElemenwiseBatchKernels.cu:83-120, Ciphertext::multPt). */
+int fides_mul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
+/* Per-limb scalar multiply / add (host array of `level` residues, reduced mod q_i): replaces
+ * Scalar_mult_ / scalar_add_ (ElemenwiseBatchKernels.cu, AddSub.cu) behind multScalar /
+ * addScalar.  At most 64 limbs. */
+int fides_mul_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
+                     void* stream);
+int fides_add_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
+                     void* stream);
+/* ModRaise of one level-1 polynomial (limb q_0, EVAL) to out_level limbs: INTT, centred
+ * SwitchModulus(q_0 -> q_j), NTT (reference Bootstrap.cu ModRaise, src/CKKS/Bootstrap.cu:708+). */
+int fides_mod_raise(fides_ctx* ctx, const uint64_t* x, int out_level, uint64_t* out, void* stream);
 /* Rescale of n_polys polynomials at level l (FIXEDMANUAL DropLastElementAndScale);
  * out has l-1 limbs per poly.  Replaces Ciphertext::rescale (src/CKKS/Ciphertext.cpp:
  * 569-607) / LimbPartition::rescale (src/CKKS/LimbPartition.cu:711-797). */

@@ -1,0 +1,105 @@
+"""Bootstrapping: the special-FFT factorisation (CPU) and a full GPU bootstrap whose
+decrypted output matches the FP64 plaintext (precision in bits, as the reference's
+BootstrapPrecisionTests measure it, test/BootstrapPrecisionTests.cu:141-259)."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from ckks_host import KeyGen, decode, encode, xrng
+
+
+def _u0(n):
+    N = 2 * n
+    zeta = np.exp(1j * np.pi / N)
+    e = [pow(5, j, 2 * N) for j in range(n)]
+    return np.array([[zeta ** (e[j] * k) for k in range(n)] for j in range(n)])
+
+
+@pytest.mark.parametrize("logn,levels", [(4, 2), (6, 3), (7, 3)])
+def test_special_fft_factorisation(logn, levels):
+    from fides_b200 import bootstrap as B
+    n = 1 << logn
+    U = _u0(n)
+    w = xrng(logn).normal(size=n) + 1j * xrng(logn + 1).normal(size=n)
+    P = B.bit_reverse_perm(n)
+    v = w[P]
+    for M in B.fft_levels(n, levels, inverse=False):
+        v = B.apply_diags(M, v)
+    assert np.abs(v - U @ w).max() < 1e-9 * n
+    u = U @ w
+    for M in B.fft_levels(n, levels, inverse=True):
+        u = B.apply_diags(M, u)
+    assert np.abs(u - w[P]).max() < 1e-9 * n
+    assert np.abs(U.conj().T @ U - n * np.eye(n)).max() < 1e-9 * n
+
+
+def test_slot_encoding_matches_client_encoder():
+    from fides_b200 import bootstrap as B
+    N = 64
+    z = xrng(3).uniform(-1, 1, N // 2) + 1j * xrng(4).uniform(-1, 1, N // 2)
+    assert np.array_equal(B.encode_coeffs(z, N, 2.0 ** 30), encode(z, N, 2.0 ** 30).astype(np.int64))
+    assert np.abs(B.decode_coeffs(B.encode_coeffs(z, N, 2.0 ** 30), N, 2.0 ** 30) - z).max() < 1e-8
+
+
+def make_boot(F, logN, n_q=20, dnum=4, hw=32, K=12):
+    from fides_b200 import params as P
+    from fides_b200 import bootstrap as B
+    prm = P.chain(logN, 60, 50, n_q, dnum, name=f"boot N=2^{logN}")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=61, hamming_weight=hw)
+    rk = F.to_device(kg.relin_key())
+    conj = F.to_device(kg.auto_key(2 * prm.N - 1))
+    probe = B.Bootstrapper.__new__(B.Bootstrapper)
+    ev = B.Evaluator(F, ctx, rk, {}, conj, top_scale=2.0 ** 50)
+    bs = B.Bootstrapper(ev, K=K)
+    ev.rot_keys = {r: F.to_device(kg.rotation_key(r)) for r in bs.needed_rotations()}
+    return prm, o, kg, ctx, ev, bs
+
+
+@pytest.mark.gpu
+def test_bootstrap_precision_n4096(fides):
+    from fides_b200 import bootstrap as B
+    prm, o, kg, ctx, ev, bs = make_boot(fides, 12)
+    N, n = prm.N, prm.N // 2
+    delta = 2.0 ** 50
+    bs.prepare(top_level=prm.n_q, msg_scale=delta)
+    assert bs.out_level >= 2
+    rng = xrng(62)
+    z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    c0, c1 = kg.encrypt(encode(z, N, delta).astype(np.int64), 1)
+    ct = B.Ct(fides.to_device(c0), fides.to_device(c1), delta)
+    out = bs.bootstrap(ct)
+    got = decode(kg.decrypt_limb0(fides.to_host(out.c0), fides.to_host(out.c1)), N, out.scale)
+    err = np.abs(got - z).max()
+    bits = -math.log2(err)
+    print(f"bootstrap N=2^12: out level {out.level}, max error {err:.3e} ({bits:.1f} bits)")
+    assert bits > 12
+
+
+@pytest.mark.gpu
+def test_bootstrap_graph_replay_is_bit_identical(fides):
+    import torch
+    from fides_b200 import bootstrap as B
+    prm, o, kg, ctx, ev, bs = make_boot(fides, 12)
+    bs.prescale = 1 << 4
+    delta = 2.0 ** 50
+    bs.prepare(top_level=prm.n_q, msg_scale=delta)
+    rng = xrng(63)
+    n = prm.N // 2
+    z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+    ct = B.Ct(fides.to_device(c0), fides.to_device(c1), delta)
+    direct = bs.bootstrap(ct)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        gout = bs.bootstrap(ct)
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(direct.c0, gout.c0) and torch.equal(direct.c1, gout.c1)
+    got = decode(kg.decrypt_limb0(fides.to_host(gout.c0), fides.to_host(gout.c1)), prm.N, gout.scale)
+    assert -math.log2(np.abs(got - z).max()) > 14

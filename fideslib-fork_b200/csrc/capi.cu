@@ -96,6 +96,24 @@ int fides_ctx_set_scratch_limit(fides_ctx* x, size_t bytes) {
 
 uint64_t fides_ctx_launch_count(const fides_ctx* x) { return x && x->c ? x->c->launches.load() : 0; }
 
+int fides_ctx_set_conv_engine(fides_ctx* x, int engine) {
+  return guard([&] {
+    if (engine < fides::CONV_AUTO || engine > fides::CONV_TENSOR) throw fides::Error(FIDES_ERR_ARG, "bad engine");
+    C(x)->conv_engine = engine;
+  });
+}
+
+int fides_ctx_device_status(fides_ctx* x, uint32_t* status, int clear) {
+  return guard([&] {
+    auto* c = C(x);
+    if (!status) throw fides::Error(FIDES_ERR_ARG, "null status");
+    FIDES_CUDA(cudaSetDevice(c->device));
+    FIDES_CUDA(cudaDeviceSynchronize());
+    FIDES_CUDA(cudaMemcpy(status, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (clear) FIDES_CUDA(cudaMemset(c->d_status, 0, sizeof(uint32_t)));
+  });
+}
+
 int fides_ctx_profile(fides_ctx* x, int enable) {
   return guard([&] {
     auto* c = C(x);

@@ -13,6 +13,7 @@
 #include <thread>
 
 #include "context.hpp"
+#include "conv_tc.hpp"
 
 namespace fides {
 
@@ -259,6 +260,9 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       std::vector<int> src_pos, src_prime, dst_pos, dst_prime;
       std::vector<ShoupConst> pre;
       std::vector<uint64_t> mat;
+      std::vector<uint8_t> tc_b;  // empty: no tensor-core form
+      std::vector<TcDest> tc_dst;
+      int kpad = 0, ndp = 0;
     };
     auto build_conv = [&](const std::vector<int>& sp, const std::vector<int>& spr, const std::vector<int>& dp,
                           const std::vector<int>& dpr) {
@@ -282,6 +286,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
           h.mat[(size_t)i * nd + j] = v;
         }
       }
+      if (conv_tc_fits(logN, ns, nd, primes, dpr)) build_tc_image(h.mat.data(), ns, nd, dpr, primes, h.tc_b, h.tc_dst, h.kpad, h.ndp);
       return h;
     };
     std::vector<std::vector<HostConv>> hmu(n_q + 1);
@@ -315,8 +320,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     append(blob, pmod, o_pmod);
     append(blob, rs, o_rs);
     struct Off {
-      size_t sp, spr, pre, dp, dpr, mat;
-      int ns, nd;
+      size_t sp, spr, pre, dp, dpr, mat, tcb, tcd;
+      int ns, nd, kpad, ndp;
     };
     auto put = [&](const HostConv& h) {
       Off o;
@@ -326,8 +331,12 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       append(blob, h.dst_pos, o.dp);
       append(blob, h.dst_prime, o.dpr);
       append(blob, h.mat, o.mat);
+      append(blob, h.tc_b, o.tcb);
+      append(blob, h.tc_dst, o.tcd);
       o.ns = (int)h.src_prime.size();
       o.nd = (int)h.dst_prime.size();
+      o.kpad = h.tc_b.empty() ? 0 : h.kpad;
+      o.ndp = h.ndp;
       return o;
     };
     std::vector<std::vector<Off>> omu(n_q + 1);
@@ -356,6 +365,12 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       t.dst_pos = reinterpret_cast<const int*>(base + o.dp);
       t.dst_prime = reinterpret_cast<const int*>(base + o.dpr);
       t.mat = reinterpret_cast<const uint64_t*>(base + o.mat);
+      if (o.kpad) {
+        t.tc_b = reinterpret_cast<const uint8_t*>(base + o.tcb);
+        t.tc_dst = reinterpret_cast<const TcDest*>(base + o.tcd);
+        t.tc_kpad = o.kpad;
+        t.tc_nd_pad = o.ndp;
+      }
       return t;
     };
     c->modup_tab.resize(n_q + 1);
@@ -368,6 +383,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     FIDES_CUDA(cudaDeviceGetDefaultMemPool(&c->pool, device));
     uint64_t thr = UINT64_MAX;
     FIDES_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    FIDES_CUDA(cudaMalloc(&c->d_status, sizeof(uint32_t)));
+    FIDES_CUDA(cudaMemset(c->d_status, 0, sizeof(uint32_t)));
   } catch (...) {
     destroy_context(c);
     throw;
@@ -385,6 +402,7 @@ void destroy_context(Context* c) {
   }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->d_tables) cudaFree(c->d_tables);
+  if (c->d_status) cudaFree(c->d_status);
   if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }

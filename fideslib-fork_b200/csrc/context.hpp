@@ -36,6 +36,12 @@ struct __align__(16) ShoupConst {
   uint64_t w, ws;
 };
 
+// Destination-prime constants of the tensor-core conversion epilogue.
+struct __align__(16) TcDest {
+  uint64_t q;
+  uint64_t qinv;  // bits of the double nearest 1 / q
+};
+
 // Table of one approximate basis conversion (ApproxSwitchCRTBasis):
 //   y_i = [x_i * pre_i]_{q_src_i};  out_j = [sum_i y_i * mat[i][j]]_{q_dst_j}.
 struct ConvTable {
@@ -46,7 +52,18 @@ struct ConvTable {
   const int* dst_pos = nullptr;    // limb index of output j in the output poly
   const int* dst_prime = nullptr;  // prime id of output j
   const uint64_t* mat = nullptr;   // [n_src][n_dst]
+  // Tensor-core form (conv_tc.cu); tc_b == nullptr when the table does not fit it.
+  //   tc_b: the MMA B operand, byte (n, k) = byte (n mod 8) of mat[k/8][n/8] * 2^(8 (k mod 8))
+  //         mod q_dst, stored as its shared-memory image: 16-byte K slices, slice s of row n at
+  //         (s * nd_pad * 8 + n) * 16.
+  const uint8_t* tc_b = nullptr;
+  const TcDest* tc_dst = nullptr;  // [nd_pad]
+  int tc_kpad = 0;                 // K = 8 n_src rounded up to a multiple of 32
+  int tc_nd_pad = 0;               // n_dst rounded up to even
 };
+
+// Basis-conversion engine: tensor cores (INT8 split on tcgen05) or 64-bit SIMT.
+enum ConvEngine { CONV_AUTO = 0, CONV_SIMT = 1, CONV_TENSOR = 2 };
 
 struct RescaleConst {
   uint64_t qinv, qinv_s;  // q_top^-1 mod q_j
@@ -78,6 +95,8 @@ struct Context {
   void* d_tables = nullptr;          // backing store of the conversion tables
   std::vector<std::vector<ConvTable>> modup_tab;  // [l][d]
   std::vector<ConvTable> moddown_tab;              // [l]
+  int conv_engine = CONV_AUTO;
+  uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up
 
   // scratch: stream-ordered allocations from the device's memory pool
   cudaMemPool_t pool = nullptr;

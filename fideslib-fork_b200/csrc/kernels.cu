@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "conv_tc.hpp"
 
 namespace fides {
 
@@ -247,13 +248,20 @@ int fill(List& L, const Job* jobs, int n) {
 
 void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
   static thread_local ConvJobList L;
-  // Group jobs by source width so each launch uses one specialised kernel.
+  // Tables with a tensor-core form go to the tcgen05 kernel unless the SIMT engine is forced;
+  // the rest are grouped by source width so each launch uses one specialised kernel.
+  std::vector<ConvJob> tc;
   std::vector<ConvJob> byw[MAX_SRC + 1];
+  const bool use_tc = c->conv_engine == CONV_TENSOR || (c->conv_engine == CONV_AUTO && kConvAutoTensor);
   for (int i = 0; i < n; ++i) {
     const ConvTable& t = jobs[i].t;
     if (t.n_src > MAX_SRC || t.n_dst > MAX_DST || t.n_src < 1) throw Error(-1, "basis conversion width out of range");
-    byw[t.n_src].push_back(jobs[i]);
+    if (use_tc && t.tc_b)
+      tc.push_back(jobs[i]);
+    else
+      byw[t.n_src].push_back(jobs[i]);
   }
+  if (!tc.empty()) launch_conv_tc(c, tc.data(), (int)tc.size(), s);
   for (int w = 1; w <= MAX_SRC; ++w) {
     const auto& v = byw[w];
     for (size_t off = 0; off < v.size(); off += MAX_CONV_JOBS) {

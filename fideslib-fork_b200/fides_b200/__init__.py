@@ -90,6 +90,8 @@ def lib():
         L.fides_ctx_launch_count.argtypes = [vp]
         L.fides_ctx_launch_count.restype = C.c_uint64
         L.fides_ctx_profile.argtypes = [vp, C.c_int]
+        L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
+        L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                              C.POINTER(C.c_uint64)]
         L.fides_rotation_auto_index.argtypes = [C.c_int, C.c_int]
@@ -214,6 +216,20 @@ class Context:
 
     def set_scratch_limit(self, nbytes: int):
         _check(lib().fides_ctx_set_scratch_limit(self._h, nbytes))
+
+    CONV_ENGINES = {"auto": 0, "simt": 1, "tensor": 2}
+
+    def set_conv_engine(self, engine: str):
+        """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer
+        units) or 'tensor' (exact INT8-split product on the tcgen05 tensor cores)."""
+        _check(lib().fides_ctx_set_conv_engine(self._h, self.CONV_ENGINES[engine]))
+
+    def device_status(self, clear: bool = True) -> int:
+        """Synchronises and returns the device status word (bit 0: a bounded device wait
+        gave up)."""
+        st = C.c_uint32()
+        _check(lib().fides_ctx_device_status(self._h, C.byref(st), 1 if clear else 0))
+        return int(st.value)
 
     KERNEL_FAMILIES = {"ntt": 0, "conv": 1, "ksk": 2, "elem": 3}
 

@@ -66,6 +66,15 @@ int fides_ctx_set_scratch_limit(fides_ctx* ctx, size_t bytes);
 /* Count of kernels this context has launched (for launch accounting). */
 uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
 
+/* Basis-conversion engine (ModUp / ModDown): 0 = automatic, 1 = 64-bit SIMT, 2 = tensor cores
+ * (exact INT8-split product on tcgen05, for conversions of at most 16 source limbs whose byte
+ * matrix fits in shared memory; wider ones stay on SIMT).  Results are identical. No reference
+ * counterpart: the reference has one conversion kernel family (src/Conv.cu:27-423). */
+int fides_ctx_set_conv_engine(fides_ctx* ctx, int engine);
+/* Synchronises the device and reads the context's device status word: bit 0 = a bounded
+ * device-side wait gave up (the affected outputs are incomplete).  clear != 0 resets it. */
+int fides_ctx_device_status(fides_ctx* ctx, uint32_t* status, int clear);
+
 /* Profiling mode: when enabled, every kernel launch is bracketed by CUDA events on its
  * stream and attributed to a family (0 = NTT passes, 1 = basis conversion, 2 = KSK inner
  * product, 3 = other elementwise).  fides_ctx_profile_read synchronises on the recorded

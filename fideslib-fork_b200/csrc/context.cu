@@ -241,6 +241,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       pinv[j] = h_shoup(h_invmod(P, q), q);
     }
     std::vector<RescaleConst> rs((size_t)(n_q + 1) * n_q);
+    std::vector<ShoupConst> pqinv((size_t)(n_q + 1) * n_q, ShoupConst{0, 0});
     for (int l = 2; l <= n_q; ++l) {
       uint64_t qt = primes[l - 1];
       for (int j = 0; j < l - 1; ++j) {
@@ -253,6 +254,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
         r.qinv_s = a.ws;
         r.m = b.w;
         r.m_s = b.ws;
+        if (K > 0) pqinv[(size_t)l * n_q + j] = h_shoup(h_mulmod(pinv[j].w, qi, q), q);
       }
     }
     // ---- conversion tables
@@ -311,7 +313,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     }
     // ---- pack everything into one device blob
     std::vector<char> blob;
-    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs;
+    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq;
     append(blob, hp, o_prime);
     append(blob, tf, o_tf);
     append(blob, ti, o_ti);
@@ -319,6 +321,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     append(blob, pinv, o_pinv);
     append(blob, pmod, o_pmod);
     append(blob, rs, o_rs);
+    append(blob, pqinv, o_pq);
     struct Off {
       size_t sp, spr, pre, dp, dpr, mat, tcb, tcd;
       int ns, nd, kpad, ndp;
@@ -355,6 +358,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     c->d_pinv = reinterpret_cast<ShoupConst*>(base + o_pinv);
     c->d_pmod = reinterpret_cast<ShoupConst*>(base + o_pmod);
     c->d_rescale = reinterpret_cast<RescaleConst*>(base + o_rs);
+    c->d_pqinv = reinterpret_cast<ShoupConst*>(base + o_pq);
     auto mk = [&](const Off& o) {
       ConvTable t;
       t.n_src = o.ns;

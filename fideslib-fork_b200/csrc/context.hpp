@@ -92,6 +92,7 @@ struct Context {
   ShoupConst* d_pinv = nullptr;      // [n_q]: P^-1 mod q_j
   ShoupConst* d_pmod = nullptr;      // [n_q]: P mod q_j
   RescaleConst* d_rescale = nullptr; // [n_q + 1][n_q]: row l = rescale from level l
+  ShoupConst* d_pqinv = nullptr;     // [n_q + 1][n_q]: row l = (P q_(l-1))^-1 mod q_j
   void* d_tables = nullptr;          // backing store of the conversion tables
   std::vector<std::vector<ConvTable>> modup_tab;  // [l][d]
   std::vector<ConvTable> moddown_tab;              // [l]

@@ -10,14 +10,19 @@ namespace fides {
 void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream_t s, NttIn in, NttOut out) {
   if (n <= 0) return;
   if (c->logN < 10) throw Error(-1, "GPU NTT needs logN >= 10");
-  if (inverse ? (in == IN_SWITCH || out != OUT_PLAIN) : (in == IN_MUL))
-    throw Error(-1, "NTT prologue/epilogue not available in this direction");
+  const bool ok = inverse ? ((in == IN_PLAIN || in == IN_MUL || in == IN_ADD_PMUL) &&
+                             (out == OUT_PLAIN || out == OUT_SUB_PINV))
+                          : ((in == IN_PLAIN || in == IN_SWITCH || in == IN_CONV_SW) &&
+                             (out == OUT_PLAIN || out == OUT_MODDOWN || out == OUT_RESCALE || out == OUT_MDRS));
+  if (!ok) throw Error(-1, "NTT prologue/epilogue not available in this direction");
   nttk::PassArgs a;
   a.primes = c->d_prime;
   a.tw = inverse ? c->d_tw_inv : c->d_tw_fwd;
   a.inv_last = c->d_inv_last;
   a.pinv = c->d_pinv;
   a.rescale = c->d_rescale;
+  a.pmod = c->d_pmod;
+  a.pqinv = c->d_pqinv;
   a.logN = c->logN;
   a.log1 = (c->logN + 1) / 2;
   a.n_q = c->n_q;

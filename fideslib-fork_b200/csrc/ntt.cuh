@@ -29,15 +29,19 @@ namespace fides {
 
 // What the first pass loads.
 enum NttIn {
-  IN_PLAIN = 0,   // x = src[i]  (src = ptr when in place)
-  IN_MUL = 1,     // inverse only: x = src[i] * pro[i] mod q   (tensor term a1 b1)
-  IN_SWITCH = 2,  // forward only: x = SwitchModulus(pro[i]) from prime aux - 1 (rescale)
+  IN_PLAIN = 0,    // x = src[i]  (src = ptr when in place)
+  IN_MUL = 1,      // inverse only: x = src[i] * pro[i] mod q   (tensor term a1 b1)
+  IN_SWITCH = 2,   // forward only: x = SwitchModulus(pro[i]) from prime aux - 1 (rescale)
+  IN_CONV_SW = 3,  // forward only: x = src[i] + P SwitchModulus(pro[i]) from prime aux - 1
+  IN_ADD_PMUL = 4, // inverse only: x = src[i] + P pro[i]
 };
 // What the last pass stores to ptr.
 enum NttOut {
   OUT_PLAIN = 0,
-  OUT_MODDOWN = 1,  // forward only: out = (ep0[i] - v) P^-1 (+ ep1[i])     (ModDown finish)
-  OUT_RESCALE = 2,  // forward only: out = qinv_l ep0[i] + QlQlInv_l v, l = aux (rescale finish)
+  OUT_MODDOWN = 1,   // forward only: out = (ep0[i] - v) P^-1 (+ ep1[i])     (ModDown finish)
+  OUT_RESCALE = 2,   // forward only: out = qinv_l ep0[i] + QlQlInv_l v, l = aux (rescale finish)
+  OUT_MDRS = 3,      // forward only: out = (ep0[i] - v) (P q_(l-1))^-1 (+ q_(l-1)^-1 ep1[i]), l = aux
+  OUT_SUB_PINV = 4,  // inverse only: out = (v - ep0[i]) P^-1
 };
 
 struct LimbRef {
@@ -47,7 +51,7 @@ struct LimbRef {
   const uint64_t* ep0;    // epilogue operands
   const uint64_t* ep1;
   int prime;
-  int aux;  // IN_SWITCH / OUT_RESCALE: the level l being rescaled (top prime l - 1)
+  int aux;  // IN_SWITCH / IN_CONV_SW / OUT_RESCALE / OUT_MDRS: the level l being rescaled (top prime l - 1)
   uint64_t pad;
 };
 

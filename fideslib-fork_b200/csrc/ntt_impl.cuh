@@ -52,7 +52,9 @@ struct PassArgs {
   const ShoupConst* tw;        // forward or inverse twiddles, [prime][N]
   const ShoupConst* inv_last;  // [prime]: psi_rev^-1[1] * N^-1
   const ShoupConst* pinv;      // [Q prime]: P^-1 mod q (OUT_MODDOWN)
-  const RescaleConst* rescale; // [level][Q prime] (OUT_RESCALE)
+  const RescaleConst* rescale; // [level][Q prime] (OUT_RESCALE, OUT_MDRS)
+  const ShoupConst* pmod;      // [Q prime]: P mod q (IN_CONV_SW, IN_ADD_PMUL)
+  const ShoupConst* pqinv;     // [level][Q prime]: (P q_(level-1))^-1 mod q (OUT_MDRS)
   int logN;
   int log1;  // size of the column sub-transform
   int n_q;
@@ -215,10 +217,15 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
   constexpr bool first_pass = FWD ? (PASS == COL) : (PASS == ROW);
   const uint64_t* in = (first_pass && lr.src) ? lr.src : data;
   DevPrime opr;
-  if (IN == IN_SWITCH) opr = a.primes[lr.aux - 1];
+  if (IN == IN_SWITCH || IN == IN_CONV_SW) opr = a.primes[lr.aux - 1];
+  ShoupConst pm{0, 0};
+  if (IN == IN_CONV_SW || IN == IN_ADD_PMUL) pm = a.pmod[lr.prime];
   auto load = [&](size_t i) -> uint64_t {
     if (first_pass && IN == IN_SWITCH) return switch_modulus(lr.pro[i], opr, pr);
     if (first_pass && IN == IN_MUL) return mulmod(in[i], lr.pro[i], pr);
+    if (first_pass && IN == IN_CONV_SW)
+      return addmod(in[i], shoup(switch_modulus(lr.pro[i], opr, pr), pm.w, pm.ws, pr.q), pr.q);
+    if (first_pass && IN == IN_ADD_PMUL) return addmod(in[i], shoup(lr.pro[i], pm.w, pm.ws, pr.q), pr.q);
     return in[i];
   };
 
@@ -262,14 +269,20 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
   // ---- store (the last pass applies the epilogue)
   ShoupConst pinv{0, 0};
   RescaleConst rsc{0, 0, 0, 0};
-  if (OUT == OUT_MODDOWN) pinv = a.pinv[lr.prime];
-  if (OUT == OUT_RESCALE) rsc = a.rescale[(size_t)lr.aux * a.n_q + lr.prime];
+  if (OUT == OUT_MODDOWN || OUT == OUT_SUB_PINV) pinv = a.pinv[lr.prime];
+  if (OUT == OUT_MDRS) pinv = a.pqinv[(size_t)lr.aux * a.n_q + lr.prime];
+  if (OUT == OUT_RESCALE || OUT == OUT_MDRS) rsc = a.rescale[(size_t)lr.aux * a.n_q + lr.prime];
   auto store = [&](size_t i, uint64_t v) {
-    if (OUT == OUT_MODDOWN) {
+    if (OUT == OUT_MODDOWN || OUT == OUT_MDRS) {
       v = shoup(submod(lr.ep0[i], v, pr.q), pinv.w, pinv.ws, pr.q);
-      if (lr.ep1) v = addmod(v, lr.ep1[i], pr.q);
+      if (lr.ep1) {
+        const uint64_t e = lr.ep1[i];
+        v = addmod(v, OUT == OUT_MDRS ? shoup(e, rsc.qinv, rsc.qinv_s, pr.q) : e, pr.q);
+      }
     } else if (OUT == OUT_RESCALE) {
       v = addmod(shoup(lr.ep0[i], rsc.qinv, rsc.qinv_s, pr.q), shoup(v, rsc.m, rsc.m_s, pr.q), pr.q);
+    } else if (OUT == OUT_SUB_PINV) {
+      v = shoup(submod(v, lr.ep0[i], pr.q), pinv.w, pinv.ws, pr.q);
     }
     data[i] = v;
   };
@@ -318,20 +331,29 @@ void run_transform(Context* c, const PassArgs& a, const NttLimbList& L, bool inv
   if (!inverse) {
     if (in == IN_SWITCH)
       launch_pass<LOGN, COL, true, IN_SWITCH, OUT_PLAIN>(c, a, L, s);
+    else if (in == IN_CONV_SW)
+      launch_pass<LOGN, COL, true, IN_CONV_SW, OUT_PLAIN>(c, a, L, s);
     else
       launch_pass<LOGN, COL, true, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
     if (out == OUT_MODDOWN)
       launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_MODDOWN>(c, a, L, s);
     else if (out == OUT_RESCALE)
       launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_RESCALE>(c, a, L, s);
+    else if (out == OUT_MDRS)
+      launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_MDRS>(c, a, L, s);
     else
       launch_pass<LOGN, ROW, true, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
   } else {
     if (in == IN_MUL)
       launch_pass<LOGN, ROW, false, IN_MUL, OUT_PLAIN>(c, a, L, s);
+    else if (in == IN_ADD_PMUL)
+      launch_pass<LOGN, ROW, false, IN_ADD_PMUL, OUT_PLAIN>(c, a, L, s);
     else
       launch_pass<LOGN, ROW, false, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
-    launch_pass<LOGN, COL, false, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
+    if (out == OUT_SUB_PINV)
+      launch_pass<LOGN, COL, false, IN_PLAIN, OUT_SUB_PINV>(c, a, L, s);
+    else
+      launch_pass<LOGN, COL, false, IN_PLAIN, OUT_PLAIN>(c, a, L, s);
   }
 }
 

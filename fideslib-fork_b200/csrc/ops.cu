@@ -98,23 +98,71 @@ void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* c
   ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_PLAIN, OUT_MODDOWN);
 }
 
-// Scratch limbs of one key switch at level l: INTT copy, digits, A, B, two conversions.
-size_t ks_limbs(Context* c, int l) {
-  const int ext = l + c->K;
-  return (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l;
+// ModDown fused with the rescale that follows it.  With u = ModDown(x) + add the value
+// being rescaled from level l (top prime q_t = q_(l-1)), linearity of the transforms over
+// Z_q gives, residue for residue:
+//   top   = INTT(u_t) = (INTT(x_t + P add_t) - conv_t) P^-1                (coefficients)
+//   out_j = (x_j - NTT(conv_j + P SwitchModulus(top))) (P q_t)^-1 + q_t^-1 add_j,  j < l - 1
+// so the result equals ModDown followed by Rescale (reference: NTT<NTT_MODDOWN> then
+// rescale, src/CKKS/LimbPartitionMGPU.cu:89-232) bit for bit, with one INTT and l - 1 NTTs
+// in place of l NTTs, one INTT and l - 1 NTTs.
+void moddown_rescale_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs,
+                           uint64_t* const* tops, uint64_t* const* outs, const uint64_t* const* adds, int n,
+                           cudaStream_t s) {
+  const size_t N = c->N;
+  const int K = c->K;
+  if (K == 0) throw Error(-1, "ModDown needs special primes");
+  std::vector<LimbRef> refs;
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < K; ++k) refs.push_back(lref(exts[i] + (ls[i] + k) * N, c->n_q + k));
+  ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
+  std::vector<ConvJob> jobs;
+  std::vector<LimbRef> top_add, top_plain, fwd;
+  for (int i = 0; i < n; ++i) {
+    const int l = ls[i];
+    const uint64_t* add = adds ? adds[i] : nullptr;
+    jobs.push_back(ConvJob{c->moddown_tab[l], exts[i] + l * N, convs[i]});
+    LimbRef t = lref(tops[i], l - 1);
+    t.src = exts[i] + (size_t)(l - 1) * N;
+    t.pro = add ? add + (size_t)(l - 1) * N : nullptr;
+    t.ep0 = convs[i] + (size_t)(l - 1) * N;
+    (add ? top_add : top_plain).push_back(t);
+    for (int j = 0; j < l - 1; ++j) {
+      LimbRef r = lref(outs[i] + j * N, j);
+      r.src = convs[i] + j * N;
+      r.pro = tops[i];
+      r.ep0 = exts[i] + j * N;
+      r.ep1 = add ? add + j * N : nullptr;
+      r.aux = l;
+      fwd.push_back(r);
+    }
+  }
+  launch_conv(c, jobs.data(), (int)jobs.size(), s);
+  ntt_limbs(c, top_add.data(), (int)top_add.size(), true, s, IN_ADD_PMUL, OUT_SUB_PINV);
+  ntt_limbs(c, top_plain.data(), (int)top_plain.size(), true, s, IN_PLAIN, OUT_SUB_PINV);
+  ntt_limbs(c, fwd.data(), (int)fwd.size(), false, s, IN_CONV_SW, OUT_MDRS);
 }
 
-// Key switch of n items whose inputs are xs[i] (or xs[i] * ys[i]).
+// Scratch limbs of one key switch at level l: INTT copy, digits, A, B, two conversions,
+// two rescale tops.
+size_t ks_limbs(Context* c, int l) {
+  const int ext = l + c->K;
+  return (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l + 2;
+}
+
+// Key switch of n items whose inputs are xs[i] (or xs[i] * ys[i]); with `rescale` the
+// outputs f0/f1 (+ add0/add1) are rescaled to level l - 1 in the same ModDown.
 void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
                      const uint64_t* const* keys, uint64_t* const* f0, uint64_t* const* f1,
-                     const uint64_t* const* add0, const uint64_t* const* add1, int n, cudaStream_t s) {
+                     const uint64_t* const* add0, const uint64_t* const* add1, int n, cudaStream_t s,
+                     bool rescale = false) {
   const size_t N = c->N;
   size_t total = 0;
   for (int i = 0; i < n; ++i) total += ks_limbs(c, ls[i]);
   Scratch sc(c, sizeof(uint64_t) * N * total, s);
   Bump bp{sc.u64(), N};
   std::vector<int> ls2(2 * n);
-  std::vector<uint64_t*> tmp(n), dig(n), ex(2 * n), conv(2 * n), outs(2 * n);
+  std::vector<uint64_t*> tmp(n), dig(n), ex(2 * n), conv(2 * n), outs(2 * n), tops(2 * n);
   std::vector<const uint64_t*> adds(2 * n);
   std::vector<KskJob> kj;
   for (int i = 0; i < n; ++i) {
@@ -128,6 +176,8 @@ void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* cons
     ex[2 * i + 1] = A;
     conv[2 * i] = bp.take(l);
     conv[2 * i + 1] = bp.take(l);
+    tops[2 * i] = bp.take(1);
+    tops[2 * i + 1] = bp.take(1);
     outs[2 * i] = f0[i];
     outs[2 * i + 1] = f1[i];
     adds[2 * i] = add0 ? add0[i] : nullptr;
@@ -136,7 +186,10 @@ void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* cons
   }
   modup_stage(c, xs, ys, ls, tmp.data(), dig.data(), n, s);
   launch_ksk(c, kj.data(), n, s);
-  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), adds.data(), 2 * n, s);
+  if (rescale)
+    moddown_rescale_stage(c, ex.data(), ls2.data(), conv.data(), tops.data(), outs.data(), adds.data(), 2 * n, s);
+  else
+    moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), adds.data(), 2 * n, s);
 }
 
 }  // namespace
@@ -253,14 +306,14 @@ void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* r
   size_t total = 0;
   for (int i = 0; i < n; ++i) {
     check_level(c, items[i].l, rescale ? 2 : 1);
-    total += (size_t)items[i].l * (rescale ? 4 : 2);
+    total += (size_t)items[i].l * 2;
   }
   Scratch sc(c, sizeof(uint64_t) * N * total, s);
   Bump bp{sc.u64(), N};
   std::vector<TensorJob> tj;
-  std::vector<const uint64_t*> xs(n), ys(n), keys(n, relin_key), d0s(n), d1s(n), rx;
-  std::vector<uint64_t*> f0(n), f1(n), ro;
-  std::vector<int> ls(n), rl;
+  std::vector<const uint64_t*> xs(n), ys(n), keys(n, relin_key), d0s(n), d1s(n);
+  std::vector<uint64_t*> f0(n), f1(n);
+  std::vector<int> ls(n);
   for (int i = 0; i < n; ++i) {
     const HMultItem& it = items[i];
     const int l = it.l;
@@ -274,21 +327,12 @@ void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* r
     d1s[i] = d1;
     f0[i] = it.out0;
     f1[i] = it.out1;
-    if (rescale) {
-      f0[i] = bp.take(l);
-      f1[i] = bp.take(l);
-      rx.push_back(f0[i]);
-      rx.push_back(f1[i]);
-      ro.push_back(it.out0);
-      ro.push_back(it.out1);
-      rl.push_back(l);
-      rl.push_back(l);
-    }
   }
   launch_tensor(c, tj.data(), n, s);
+  // The inputs are consumed (tensor terms, ModUp and KSK reads) before the outputs are
+  // first written by the final transforms, so outputs may alias inputs.
   keyswitch_stage(c, xs.data(), ys.data(), ls.data(), keys.data(), f0.data(), f1.data(), d0s.data(), d1s.data(), n,
-                  s);
-  if (rescale) op_rescale_batch(c, rx.data(), rl.data(), ro.data(), (int)rx.size(), s);
+                  s, rescale);
 }
 
 void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s) {

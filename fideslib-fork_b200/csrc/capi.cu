@@ -47,6 +47,10 @@ cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
 void fides::set_last_error(const std::string& msg) { g_err = msg; }
 
+namespace fides {
+double measure_bf_peak(int device);  // calibrate.cu
+}
+
 extern "C" {
 
 const char* fides_last_error(void) { return g_err.c_str(); }
@@ -95,6 +99,13 @@ int fides_ctx_set_scratch_limit(fides_ctx* x, size_t bytes) {
 }
 
 uint64_t fides_ctx_launch_count(const fides_ctx* x) { return x && x->c ? x->c->launches.load() : 0; }
+
+int fides_int_peak(int device, double* butterflies_per_s) {
+  return guard([&] {
+    need(butterflies_per_s, "butterflies_per_s");
+    *butterflies_per_s = fides::measure_bf_peak(device);
+  });
+}
 
 int fides_ctx_set_conv_engine(fides_ctx* x, int engine) {
   return guard([&] {

@@ -91,6 +91,7 @@ def lib():
         L.fides_ctx_launch_count.restype = C.c_uint64
         L.fides_ctx_profile.argtypes = [vp, C.c_int]
         L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
+        L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                              C.POINTER(C.c_uint64)]
@@ -153,6 +154,14 @@ def _ptr(t) -> int | None:
 
 def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
+
+
+def int_peak(device: int = 0) -> float:
+    """Butterflies per second the GPU sustains on the NTT's forward butterfly with
+    register-resident data (the integer-pipe roofline of the NTT passes)."""
+    v = C.c_double()
+    _check(lib().fides_int_peak(device, C.byref(v)))
+    return float(v.value)
 
 
 def auto_index(logN: int, rotation: int) -> int:

@@ -71,6 +71,10 @@ uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
  * matrix fits in shared memory; wider ones stay on SIMT).  Results are identical. No reference
  * counterpart: the reference has one conversion kernel family (src/Conv.cu:27-423). */
 int fides_ctx_set_conv_engine(fides_ctx* ctx, int engine);
+/* Compute roofline of the NTT: butterflies per second that `device` sustains running the
+ * forward NTT butterfly (one 64-bit Shoup product, two 64-bit additions) on register-resident
+ * data, with no memory traffic.  Takes about 100 ms.  No reference counterpart. */
+int fides_int_peak(int device, double* butterflies_per_s);
 /* Synchronises the device and reads the context's device status word: bit 0 = a bounded
  * device-side wait gave up (the affected outputs are incomplete).  clear != 0 resets it. */
 int fides_ctx_device_status(fides_ctx* ctx, uint32_t* status, int clear);

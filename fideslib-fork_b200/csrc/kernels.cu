@@ -89,12 +89,15 @@ __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__
   const size_t kstride = (size_t)(n_q + K) * N;
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 sa0{0, 0}, sb0{0, 0}, sa1{0, 0}, sb1{0, 0};
+  ulonglong2 x1{0, 0}, y1{0, 0};  // a1, b1 of this limb (tensor mode)
   for (int d = 0; d < beta; ++d) {
     ulonglong2 v;
     if (d == own && J.x) {
       v = ld2(J.x + (size_t)i * N + n);
       if (J.x2) {
         ulonglong2 w = ld2(J.x2 + (size_t)i * N + n);
+        x1 = v;
+        y1 = w;
         v.x = mulmod(v.x, w.x, p);
         v.y = mulmod(v.y, w.y, p);
       }
@@ -107,6 +110,25 @@ __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__
     mac128(sb0, v.x, kb.x);
     mac128(sa1, v.y, ka.y);
     mac128(sb1, v.y, kb.y);
+  }
+  if (J.a0 && i < l) {
+    // every Q limb has one own digit, so x1 / y1 hold a1 / b1 here
+    if (beta > 12) {  // keep the sums below 2^128: at most 15 products of two values < 2^62
+      sa0 = U128{reduce128(sa0, p), 0};
+      sb0 = U128{reduce128(sb0, p), 0};
+      sa1 = U128{reduce128(sa1, p), 0};
+      sb1 = U128{reduce128(sb1, p), 0};
+    }
+    const ShoupConst pm = pmod[i];
+    const ulonglong2 x0 = ld2(J.a0 + (size_t)i * N + n), y0 = ld2(J.b0 + (size_t)i * N + n);
+    const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
+    const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
+    mac128(sb0, x0.x, py0x);  // + P a0 b0
+    mac128(sb1, x0.y, py0y);
+    mac128(sa0, x0.x, py1x);  // + P (a0 b1 + a1 b0)
+    mac128(sa0, x1.x, py0x);
+    mac128(sa1, x0.y, py1y);
+    mac128(sa1, x1.y, py0y);
   }
   uint64_t ra0 = reduce128(sa0, p), rb0 = reduce128(sb0, p);
   uint64_t ra1 = reduce128(sa1, p), rb1 = reduce128(sb1, p);
@@ -317,7 +339,7 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     double bytes = 0;
     for (int i = 0; i < m; ++i) {
       const int l = L.j[i].l, ext = l + c->K, b = c->beta(l);
-      bytes += 8.0 * c->N * ((double)ext * (3 * b + 2) + (L.j[i].c0 ? l : 0));
+      bytes += 8.0 * c->N * ((double)ext * (3 * b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
     }
     LaunchScope ls(c, s, KK_KSK, bytes);
     ksk_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha);

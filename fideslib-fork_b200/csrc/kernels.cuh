@@ -37,6 +37,10 @@ struct KskJob {
   uint64_t* out_b;
   int l;
   uint32_t auto_k;  // 0 = no automorphism
+  // optional HMult tensor terms (x = a1, x2 = b1): add P a0 b0 to out_b's and
+  // P (a0 b1 + a1 b0) to out_a's Q limbs, so that ModDown yields ModDown(.) + d0 / + d1
+  const uint64_t* a0 = nullptr;
+  const uint64_t* b0 = nullptr;
 };
 constexpr int MAX_KSK_JOBS = 64;
 struct KskJobList {

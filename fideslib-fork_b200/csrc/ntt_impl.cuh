@@ -13,6 +13,24 @@ constexpr int COL = 0, ROW = 1;
 constexpr int LOGE = 4;  // 16 elements per thread
 constexpr int G = 16;    // sub-transforms per CTA
 
+// Asynchronous 16-byte global -> shared copies (cp.async), used to fetch an epilogue operand
+// while the butterflies run.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Whether pass PASS of a transform stages its epilogue operand ep0 in shared memory: the
+// forward row pass (the last one) with a ModDown / rescale epilogue.  Its G rows are one
+// contiguous block of ep0, copied with cp.async at the start of the pass.
+template <int PASS, bool FWD, int OUT>
+struct EpStage {
+  static constexpr bool on = PASS == ROW && FWD && (OUT == OUT_MODDOWN || OUT == OUT_MDRS || OUT == OUT_RESCALE);
+};
+
 __device__ __forceinline__ ShoupConst ld_tw(const ShoupConst* p) {
   ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
   return ShoupConst{v.x, v.y};
@@ -247,6 +265,16 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<LO0>(t, r))];
   }
 
+  // ---- epilogue operand: start fetching it into shared memory (after the data region)
+  constexpr bool EPS = EpStage<PASS, FWD, OUT>::on;
+  uint64_t* sep = sm + G * PADP;
+  if constexpr (EPS) {
+    const uint64_t* e0 = lr.ep0 + (size_t)sub0 * P;
+#pragma unroll
+    for (int k = 0; k < G * P / 2 / NT; ++k) cp_async16(sep + 2 * (k * NT + tid), e0 + 2 * (k * NT + tid));
+    cp_async_commit();
+  }
+
   // ---- chunks
   uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
   if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
@@ -272,15 +300,19 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
   if (OUT == OUT_MODDOWN || OUT == OUT_SUB_PINV) pinv = a.pinv[lr.prime];
   if (OUT == OUT_MDRS) pinv = a.pqinv[(size_t)lr.aux * a.n_q + lr.prime];
   if (OUT == OUT_RESCALE || OUT == OUT_MDRS) rsc = a.rescale[(size_t)lr.aux * a.n_q + lr.prime];
+  auto ep0 = [&](size_t i) -> uint64_t {
+    if constexpr (EPS) return sep[i - (size_t)sub0 * P];
+    return lr.ep0[i];
+  };
   auto store = [&](size_t i, uint64_t v) {
     if (OUT == OUT_MODDOWN || OUT == OUT_MDRS) {
-      v = shoup(submod(lr.ep0[i], v, pr.q), pinv.w, pinv.ws, pr.q);
+      v = shoup(submod(ep0(i), v, pr.q), pinv.w, pinv.ws, pr.q);
       if (lr.ep1) {
         const uint64_t e = lr.ep1[i];
         v = addmod(v, OUT == OUT_MDRS ? shoup(e, rsc.qinv, rsc.qinv_s, pr.q) : e, pr.q);
       }
     } else if (OUT == OUT_RESCALE) {
-      v = addmod(shoup(lr.ep0[i], rsc.qinv, rsc.qinv_s, pr.q), shoup(v, rsc.m, rsc.m_s, pr.q), pr.q);
+      v = addmod(shoup(ep0(i), rsc.qinv, rsc.qinv_s, pr.q), shoup(v, rsc.m, rsc.m_s, pr.q), pr.q);
     } else if (OUT == OUT_SUB_PINV) {
       v = shoup(submod(v, lr.ep0[i], pr.q), pinv.w, pinv.ws, pr.q);
     }
@@ -288,6 +320,10 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
   };
   constexpr int LOL = Chunk<LOGP, FWD, NCH - 1>::LO;
   constexpr bool direct_store = (PASS == COL) || (LOL == LOGP - LOGE);
+  if constexpr (EPS) {
+    cp_async_wait_all();
+    if (direct_store) __syncthreads();  // the staged store below synchronises anyway
+  }
   if (direct_store) {
 #pragma unroll
     for (int r = 0; r < E; ++r) store(gidx(sub, u_of<LOL>(t, r)), x[r]);
@@ -310,7 +346,8 @@ template <int LOGN, int PASS, bool FWD, int IN, int OUT>
 void launch_pass(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
   constexpr int P = 1 << LOGP, T = P / (1 << LOGE);
-  constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LOGE))) * (int)sizeof(uint64_t);
+  constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LOGE))) * (int)sizeof(uint64_t) +
+                       (EpStage<PASS, FWD, OUT>::on ? G * P * (int)sizeof(uint64_t) : 0);
   static bool attr_set = false;  // per instantiation; set before first launch
   if (!attr_set) {
     FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,

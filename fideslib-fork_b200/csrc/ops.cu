@@ -155,7 +155,8 @@ size_t ks_limbs(Context* c, int l) {
 void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
                      const uint64_t* const* keys, uint64_t* const* f0, uint64_t* const* f1,
                      const uint64_t* const* add0, const uint64_t* const* add1, int n, cudaStream_t s,
-                     bool rescale = false) {
+                     bool rescale = false, const uint64_t* const* a0s = nullptr,
+                     const uint64_t* const* b0s = nullptr) {
   const size_t N = c->N;
   size_t total = 0;
   for (int i = 0; i < n; ++i) total += ks_limbs(c, ls[i]);
@@ -171,7 +172,12 @@ void keyswitch_stage(Context* c, const uint64_t* const* xs, const uint64_t* cons
     dig[i] = bp.take((size_t)c->beta(l) * ext);
     uint64_t* A = bp.take(ext);
     uint64_t* B = bp.take(ext);
-    kj.push_back(KskJob{xs[i], ys ? ys[i] : nullptr, dig[i], keys[i], nullptr, A, B, l, 0});
+    KskJob kjob{xs[i], ys ? ys[i] : nullptr, dig[i], keys[i], nullptr, A, B, l, 0};
+    if (a0s) {
+      kjob.a0 = a0s[i];
+      kjob.b0 = b0s[i];
+    }
+    kj.push_back(kjob);
     ex[2 * i] = B;
     ex[2 * i + 1] = A;
     conv[2 * i] = bp.take(l);
@@ -302,37 +308,27 @@ void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* r
                     cudaStream_t s) {
   if (n <= 0) return;
   if (!relin_key) throw Error(-5, "null relinearization key");
-  const size_t N = c->N;
-  size_t total = 0;
-  for (int i = 0; i < n; ++i) {
-    check_level(c, items[i].l, rescale ? 2 : 1);
-    total += (size_t)items[i].l * 2;
-  }
-  Scratch sc(c, sizeof(uint64_t) * N * total, s);
-  Bump bp{sc.u64(), N};
-  std::vector<TensorJob> tj;
-  std::vector<const uint64_t*> xs(n), ys(n), keys(n, relin_key), d0s(n), d1s(n);
+  std::vector<const uint64_t*> xs(n), ys(n), a0s(n), b0s(n), keys(n, relin_key);
   std::vector<uint64_t*> f0(n), f1(n);
   std::vector<int> ls(n);
   for (int i = 0; i < n; ++i) {
     const HMultItem& it = items[i];
-    const int l = it.l;
-    uint64_t* d0 = bp.take(l);
-    uint64_t* d1 = bp.take(l);
-    tj.push_back(TensorJob{it.a0, it.a1, it.b0, it.b1, d0, d1, nullptr, l, 0});
+    check_level(c, it.l, rescale ? 2 : 1);
     xs[i] = it.a1;
     ys[i] = it.b1;
-    ls[i] = l;
-    d0s[i] = d0;
-    d1s[i] = d1;
+    a0s[i] = it.a0;
+    b0s[i] = it.b0;
+    ls[i] = it.l;
     f0[i] = it.out0;
     f1[i] = it.out1;
   }
-  launch_tensor(c, tj.data(), n, s);
-  // The inputs are consumed (tensor terms, ModUp and KSK reads) before the outputs are
-  // first written by the final transforms, so outputs may alias inputs.
-  keyswitch_stage(c, xs.data(), ys.data(), ls.data(), keys.data(), f0.data(), f1.data(), d0s.data(), d1s.data(), n,
-                  s, rescale);
+  // The tensor terms d0 = a0 b0 and d1 = a0 b1 + a1 b0 enter the KSK inner product as
+  // P d0 / P d1 on the Q limbs (ModDown(x + P d) = ModDown(x) + d exactly), and d2 = a1 b1
+  // is formed inside the ModUp INTT and the KSK's own-digit term, so no tensor product is
+  // ever written.  The inputs are consumed before the outputs are first written by the
+  // final transforms, so outputs may alias inputs.
+  keyswitch_stage(c, xs.data(), ys.data(), ls.data(), keys.data(), f0.data(), f1.data(), nullptr, nullptr, n, s,
+                  rescale, a0s.data(), b0s.data());
 }
 
 void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s) {

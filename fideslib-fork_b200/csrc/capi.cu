@@ -1,7 +1,10 @@
 // extern "C" boundary (include/fides_b200.h).  Converts exceptions into status codes and
 // a thread-local message, the C counterpart of the reference's OPENFHE_THROW / CudaError
 // (api/engine/cuda/CudaEngine.cpp, src/CudaUtils.cuh:706-757).
+#include <algorithm>
 #include <cstring>
+#include <exception>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -64,7 +67,11 @@ int fides_ctx_create(const fides_params* p, fides_ctx** out) {
     try {
       x->c = fides::create_context(p->logN, p->n_q, p->n_special, p->dnum, p->primes, p->psi, p->device);
       FIDES_CUDA(cudaStreamCreateWithFlags(&x->host_stream, cudaStreamNonBlocking));
+      FIDES_CUDA(cudaStreamCreateWithFlags(&x->h2d_stream, cudaStreamNonBlocking));
+      FIDES_CUDA(cudaStreamCreateWithFlags(&x->d2h_stream, cudaStreamNonBlocking));
     } catch (...) {
+      if (x->host_stream) cudaStreamDestroy(x->host_stream);
+      if (x->h2d_stream) cudaStreamDestroy(x->h2d_stream);
       if (x->c) fides::destroy_context(x->c);
       delete x;
       throw;
@@ -77,6 +84,8 @@ int fides_ctx_destroy(fides_ctx* x) {
   return guard([&] {
     if (!x) return;
     if (x->host_stream) cudaStreamDestroy(x->host_stream);
+    if (x->h2d_stream) cudaStreamDestroy(x->h2d_stream);
+    if (x->d2h_stream) cudaStreamDestroy(x->d2h_stream);
     fides::destroy_context(x->c);
     delete x;
   });
@@ -475,9 +484,123 @@ void host_roundtrip(fides_ctx* x, const std::vector<const uint64_t*>& ins, int i
     FIDES_CUDA(cudaMemcpyAsync(outs[i], dout[i], sizeof(uint64_t) * N * out_limbs, cudaMemcpyDeviceToHost, s));
   FIDES_CUDA(cudaStreamSynchronize(s));
 }
+// One item of a pipelined host batch: its host inputs and outputs (limb counts each).
+struct HostJob {
+  std::vector<const uint64_t*> in;
+  int in_limbs;
+  std::vector<uint64_t*> out;
+  int out_limbs;
+};
+
+// Pipelined host batch: item k's host->device copies (h2d stream), computation (host
+// stream) and device->host copies (d2h stream) are ordered by events, so copies of
+// neighbouring items run on the copy engines under item k's kernels.  Three device slots
+// rotate; slot reuse waits for the slot's previous device->host copies.  Returns after
+// the last copy completes.  Host buffers should be pinned for the copies to overlap.
+template <typename Op>
+void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op) {
+  auto* c = C(x);
+  const size_t N = c->N;
+  const int n = (int)jobs.size();
+  if (n == 0) return;
+  constexpr int SLOTS = 3;
+  size_t slot_limbs = 0;
+  for (const auto& j : jobs) {
+    for (auto* p : j.in) need(p, "host input");
+    for (auto* p : j.out) need(p, "host output");
+    slot_limbs = std::max(slot_limbs, j.in.size() * (size_t)j.in_limbs + j.out.size() * (size_t)j.out_limbs);
+  }
+  cudaStream_t sh = x->h2d_stream, sc = x->host_stream, sd = x->d2h_stream;
+  std::vector<cudaEvent_t> ev;
+  auto event = [&] {
+    cudaEvent_t e;
+    FIDES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ev.push_back(e);
+    return e;
+  };
+  std::unique_ptr<fides::Scratch> slots;
+  std::exception_ptr err;
+  try {
+    slots.reset(new fides::Scratch(c, sizeof(uint64_t) * N * slot_limbs * std::min(n, SLOTS), sh));
+    std::vector<cudaEvent_t> done_d2h(n);
+    for (int k = 0; k < n; ++k) {
+      const HostJob& j = jobs[k];
+      uint64_t* base = slots->u64() + (size_t)(k % SLOTS) * slot_limbs * N;
+      if (k >= SLOTS) FIDES_CUDA(cudaStreamWaitEvent(sh, done_d2h[k - SLOTS], 0));
+      std::vector<uint64_t*> din(j.in.size()), dout(j.out.size());
+      uint64_t* p = base;
+      for (size_t i = 0; i < j.in.size(); ++i, p += (size_t)j.in_limbs * N) {
+        din[i] = p;
+        FIDES_CUDA(cudaMemcpyAsync(p, j.in[i], sizeof(uint64_t) * N * j.in_limbs, cudaMemcpyHostToDevice, sh));
+      }
+      for (size_t i = 0; i < j.out.size(); ++i, p += (size_t)j.out_limbs * N) dout[i] = p;
+      cudaEvent_t in_ready = event();
+      FIDES_CUDA(cudaEventRecord(in_ready, sh));
+      FIDES_CUDA(cudaStreamWaitEvent(sc, in_ready, 0));
+      op(k, din, dout, sc);
+      cudaEvent_t computed = event();
+      FIDES_CUDA(cudaEventRecord(computed, sc));
+      FIDES_CUDA(cudaStreamWaitEvent(sd, computed, 0));
+      for (size_t i = 0; i < j.out.size(); ++i)
+        FIDES_CUDA(cudaMemcpyAsync(j.out[i], dout[i], sizeof(uint64_t) * N * j.out_limbs, cudaMemcpyDeviceToHost,
+                                   sd));
+      done_d2h[k] = event();
+      FIDES_CUDA(cudaEventRecord(done_d2h[k], sd));
+    }
+  } catch (...) {
+    err = std::current_exception();
+  }
+  // every stream drains before the slots are released
+  cudaError_t e1 = cudaStreamSynchronize(sh), e2 = cudaStreamSynchronize(sc), e3 = cudaStreamSynchronize(sd);
+  slots.reset();
+  for (auto e : ev) cudaEventDestroy(e);
+  if (err) std::rethrow_exception(err);
+  FIDES_CUDA(e1);
+  FIDES_CUDA(e2);
+  FIDES_CUDA(e3);
+}
 }  // namespace
 
 extern "C" {
+
+int fides_hmult_host_batch(fides_ctx* x, const fides_hmult_host_item* items, int n, const uint64_t* relin_key_dev,
+                           int rescale) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    if (n > 0) need(items, "items");
+    std::vector<HostJob> jobs(n);
+    for (int k = 0; k < n; ++k) {
+      const auto& it = items[k];
+      if (it.level < (rescale ? 2 : 1) || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+      jobs[k] = HostJob{{it.a0, it.a1, it.b0, it.b1}, it.level, {it.out0, it.out1}, rescale ? it.level - 1 : it.level};
+    }
+    host_pipeline(x, jobs, [&](int k, std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {
+      fides::HMultItem h{in[0], in[1], in[2], in[3], out[0], out[1], items[k].level};
+      fides::op_hmult_batch(c, &h, 1, relin_key_dev, rescale != 0, s);
+    });
+  });
+}
+
+int fides_rotate_host_batch(fides_ctx* x, const fides_rotate_host_item* items, int n) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    if (n > 0) need(items, "items");
+    std::vector<HostJob> jobs(n);
+    for (int k = 0; k < n; ++k) {
+      const auto& it = items[k];
+      if (it.level < 1 || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+      jobs[k] = HostJob{{it.c0, it.c1}, it.level, {it.out0, it.out1}, it.level};
+    }
+    host_pipeline(x, jobs, [&](int k, std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {
+      const auto& it = items[k];
+      fides::RotateItem r{in[0], in[1], out[0], out[1], it.rot_key_dev, it.level,
+                          fides::h_auto_index(c->logN, it.rotation)};
+      fides::op_rotate_batch(c, &r, 1, s);
+    });
+  });
+}
 
 int fides_hmult_host(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
                      int level, const uint64_t* relin_key_dev, int rescale, uint64_t* out0, uint64_t* out1) {

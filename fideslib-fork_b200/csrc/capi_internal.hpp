@@ -13,5 +13,7 @@ void set_last_error(const std::string& msg);
 
 struct fides_ctx {
   fides::Context* c;
-  cudaStream_t host_stream;  // stream of the host-buffer entry points
+  cudaStream_t host_stream;  // stream of the host-buffer entry points (and pipelined compute)
+  cudaStream_t h2d_stream = nullptr;  // pipelined host batches: host -> device copies
+  cudaStream_t d2h_stream = nullptr;  //                         device -> host copies
 };

@@ -61,6 +61,15 @@ class _ServerStats(C.Structure):
 OP_HMULT, OP_HMULT_NORESCALE, OP_ROTATE = 0, 1, 2
 
 
+class _HMultHostItem(C.Structure):
+    _fields_ = [("a0", vp), ("a1", vp), ("b0", vp), ("b1", vp), ("out0", vp), ("out1", vp), ("level", C.c_int)]
+
+
+class _RotateHostItem(C.Structure):
+    _fields_ = [("c0", vp), ("c1", vp), ("out0", vp), ("out1", vp), ("key", vp), ("level", C.c_int),
+                ("rotation", C.c_int)]
+
+
 class _RotateItem(C.Structure):
     _fields_ = [("c0", vp), ("c1", vp), ("out0", vp), ("out1", vp), ("key", vp), ("level", C.c_int),
                 ("auto_index", C.c_uint32)]
@@ -116,6 +125,8 @@ def lib():
         L.fides_key_free.argtypes = [vp, vp]
         L.fides_hmult_host.argtypes = [vp, u64p, u64p, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
+        L.fides_hmult_host_batch.argtypes = [vp, C.POINTER(_HMultHostItem), C.c_int, vp, C.c_int]
+        L.fides_rotate_host_batch.argtypes = [vp, C.POINTER(_RotateHostItem), C.c_int]
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -449,6 +460,33 @@ class Context:
         P = lambda a: a.ctypes.data_as(u64p)
         _check(lib().fides_rotate_host(self._h, P(c0), P(c1), l, dev_key, rotation, P(out0), P(out1)))
         return out0, out1
+
+
+    def mult_host_batch(self, items, dev_key: int, rescale=True):
+        """Pipelined HMult of host ciphertexts.  items: (a0, a1, b0, b1, out0, out1) tuples of
+        contiguous uint64 arrays (pinned for overlap); outputs are written in place."""
+        arr = (_HMultHostItem * max(1, len(items)))()
+        for k, (a0, a1, b0, b1, o0, o1) in enumerate(items):
+            arr[k] = _HMultHostItem(a0.ctypes.data, a1.ctypes.data, b0.ctypes.data, b1.ctypes.data,
+                                    o0.ctypes.data, o1.ctypes.data, a0.shape[0])
+        _check(lib().fides_hmult_host_batch(self._h, arr, len(items), dev_key, 1 if rescale else 0))
+
+    def rotate_host_batch(self, items):
+        """Pipelined rotations of host ciphertexts.  items: (c0, c1, out0, out1, dev_key,
+        rotation) tuples; outputs are written in place."""
+        arr = (_RotateHostItem * max(1, len(items)))()
+        for k, (c0, c1, o0, o1, key, r) in enumerate(items):
+            arr[k] = _RotateHostItem(c0.ctypes.data, c1.ctypes.data, o0.ctypes.data, o1.ctypes.data, key,
+                                     c0.shape[0], r)
+        _check(lib().fides_rotate_host_batch(self._h, arr, len(items)))
+
+
+def pinned_empty(shape) -> "np.ndarray":
+    """A uint64 host array in page-locked memory (for asynchronous host <-> device copies)."""
+    import numpy as np
+    n = int(np.prod(shape))
+    t = torch.empty(n, dtype=torch.int64, pin_memory=True)
+    return t.numpy().view(np.uint64).reshape(shape)  # the array's base chain keeps t alive
 
 
 def to_device(a, device: int = 0) -> torch.Tensor:

@@ -244,6 +244,28 @@ int fides_hmult_host(fides_ctx* ctx, const uint64_t* a0, const uint64_t* a1, con
                      uint64_t* out1);
 int fides_rotate_host(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                       const uint64_t* rot_key_dev, int rotation, uint64_t* out0, uint64_t* out1);
+/* Pipelined host batches: n independent ops on host buffers.  Item k's host->device copies,
+ * its computation and its device->host copies run on three streams ordered by events, so
+ * the copies of neighbouring items overlap item k's kernels (pin the host buffers for the
+ * copies to be asynchronous).  Returns when every output has arrived in host memory.
+ * Results equal fides_hmult_host / fides_rotate_host item by item.  No reference
+ * counterpart: CudaEngine loads, computes and recovers one ciphertext at a time
+ * (CudaEngine.cpp:1156-1227). */
+typedef struct {
+  const uint64_t *a0, *a1, *b0, *b1; /* [level][N] each */
+  uint64_t *out0, *out1;             /* [level - 1][N] with rescale, else [level][N] */
+  int level;
+} fides_hmult_host_item;
+int fides_hmult_host_batch(fides_ctx* ctx, const fides_hmult_host_item* items, int n,
+                           const uint64_t* relin_key_dev, int rescale);
+typedef struct {
+  const uint64_t *c0, *c1; /* [level][N] each */
+  uint64_t *out0, *out1;   /* [level][N] each */
+  const uint64_t* rot_key_dev;
+  int level;
+  int rotation;
+} fides_rotate_host_item;
+int fides_rotate_host_batch(fides_ctx* ctx, const fides_rotate_host_item* items, int n);
 
 /* ---- allocation-free entry point ----------------------------------------------------
  * No counterpart in the reference.  fides_rescale_noalloc computes exactly what

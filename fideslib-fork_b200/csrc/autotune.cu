@@ -1,0 +1,100 @@
+// NTT tile-shape autotuner.  For each direction, pass and launch-size class, time the
+// transform on device-resident synthetic limbs with every supported sub-transforms-per-CTA
+// (4, 8, 16) and keep the fastest in the context's shape table (Context::ntt_g).  The
+// shape changes only how the sub-transforms are grouped into CTAs, never the arithmetic,
+// so results are identical whatever the table holds.
+#include <algorithm>
+#include <vector>
+
+#include "autotune.hpp"
+#include "ntt.cuh"
+
+namespace fides {
+namespace {
+
+// Residues in [0, q) of the limb's prime (a SplitMix64 stream reduced modulo q).
+__global__ void fill_residues(uint64_t* x, const DevPrime* primes, const int* prime_of_limb, int logN) {
+  const size_t i = (size_t)blockIdx.y << logN | (blockIdx.x * blockDim.x + threadIdx.x);
+  uint64_t z = i * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  x[i] = z % primes[prime_of_limb[blockIdx.y]].q;
+}
+
+constexpr int SIZES[4] = {4, 16, 64, 256};  // one representative launch per size class
+constexpr int SHAPES[3] = {4, 8, 16};
+
+}  // namespace
+
+void autotune_ntt(Context* c, float* best_ms) {
+  const int max_limbs = SIZES[3];
+  const int np = c->n_q + c->K;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FIDES_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  FIDES_CUDA(cudaEventCreate(&e0));
+  FIDES_CUDA(cudaEventCreate(&e1));
+  uint8_t saved[2][2][4];
+  std::copy(&c->ntt_g[0][0][0], &c->ntt_g[0][0][0] + 16, &saved[0][0][0]);
+  try {
+    Scratch data(c, c->limb_bytes() * max_limbs, s);
+    Scratch ids(c, sizeof(int) * max_limbs, s);
+    std::vector<int> h_ids(max_limbs);
+    for (int i = 0; i < max_limbs; ++i) h_ids[i] = i % np;
+    FIDES_CUDA(cudaMemcpyAsync(ids.p, h_ids.data(), sizeof(int) * max_limbs, cudaMemcpyHostToDevice, s));
+    const int threads = std::min(256, c->N);
+    fill_residues<<<dim3(c->N / threads, max_limbs), threads, 0, s>>>(data.u64(), c->d_prime,
+                                                                     static_cast<const int*>(ids.p), c->logN);
+    FIDES_CUDA(cudaGetLastError());
+    std::vector<LimbRef> refs(max_limbs);
+    for (int i = 0; i < max_limbs; ++i) refs[i] = lref(data.u64() + (size_t)i * c->N, h_ids[i]);
+    for (int inv = 0; inv < 2; ++inv)
+      for (int cls = 0; cls < 4; ++cls) {
+        const int n = SIZES[cls];
+        auto time_it = [&] {
+          float best = 1e30f;
+          for (int rep = 0; rep < 4; ++rep) {  // the first repetition warms up
+            FIDES_CUDA(cudaEventRecord(e0, s));
+            // a forward+inverse pair keeps the data reduced for the next repetition
+            ntt_limbs(c, refs.data(), n, inv != 0, s);
+            FIDES_CUDA(cudaEventRecord(e1, s));
+            ntt_limbs(c, refs.data(), n, inv == 0, s);
+            FIDES_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            FIDES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep) best = std::min(best, ms);
+          }
+          return best;
+        };
+        // coordinate descent: the column pass with the row pass at 16, then the row pass
+        float best = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+          int pick = 16;
+          best = 1e30f;
+          for (int g : SHAPES) {
+            c->ntt_g[inv][pass][cls] = (uint8_t)g;
+            if (pass == 0) c->ntt_g[inv][1][cls] = 16;
+            const float t = time_it();
+            if (t < best) best = t, pick = g;
+          }
+          c->ntt_g[inv][pass][cls] = (uint8_t)pick;
+        }
+        // the other direction of the timing pair uses its current table entries
+        if (best_ms) best_ms[inv * 4 + cls] = best;
+      }
+    FIDES_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    std::copy(&saved[0][0][0], &saved[0][0][0] + 16, &c->ntt_g[0][0][0]);
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(s);
+}
+
+}  // namespace fides

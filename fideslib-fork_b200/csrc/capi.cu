@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/fides_b200.h"
+#include "autotune.hpp"
 #include "capi_internal.hpp"
 #include "context.hpp"
 #include "kernels.cuh"
@@ -113,6 +114,28 @@ int fides_int_peak(int device, double* butterflies_per_s) {
   return guard([&] {
     need(butterflies_per_s, "butterflies_per_s");
     *butterflies_per_s = fides::measure_bf_peak(device);
+  });
+}
+
+int fides_ctx_autotune(fides_ctx* x, float* best_ms) {
+  return guard([&] { fides::autotune_ntt(C(x), best_ms); });
+}
+
+int fides_ctx_ntt_shapes(fides_ctx* x, uint8_t* shapes) {
+  return guard([&] {
+    auto* c = C(x);
+    need(shapes, "shapes");
+    std::memcpy(shapes, &c->ntt_g[0][0][0], 16);
+  });
+}
+
+int fides_ctx_set_ntt_shape(fides_ctx* x, int inverse, int pass, int size_class, int subs_per_cta) {
+  return guard([&] {
+    auto* c = C(x);
+    if (inverse < 0 || inverse > 1 || pass < 0 || pass > 1 || size_class < 0 || size_class > 3 ||
+        (subs_per_cta != 4 && subs_per_cta != 8 && subs_per_cta != 16))
+      throw fides::Error(FIDES_ERR_ARG, "bad NTT shape");
+    c->ntt_g[inverse][pass][size_class] = (uint8_t)subs_per_cta;
   });
 }
 

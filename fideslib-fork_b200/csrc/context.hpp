@@ -97,6 +97,13 @@ struct Context {
   std::vector<std::vector<ConvTable>> modup_tab;  // [l][d]
   std::vector<ConvTable> moddown_tab;              // [l]
   int conv_engine = CONV_AUTO;
+  // NTT tile shapes: sub-transforms per CTA (4, 8 or 16) of each pass, by direction (0 =
+  // forward, 1 = inverse), pass (0 = column, 1 = row) and launch-size class (limbs in the
+  // launch: <= 8, <= 32, <= 128, more).  Defaults keep every SM busy on small launches;
+  // fides_ctx_autotune replaces them with timed choices.
+  uint8_t ntt_g[2][2][4] = {{{4, 8, 16, 16}, {4, 8, 16, 16}}, {{4, 8, 16, 16}, {4, 8, 16, 16}}};
+  static int ntt_size_class(int limbs) { return limbs <= 8 ? 0 : limbs <= 32 ? 1 : limbs <= 128 ? 2 : 3; }
+  int ntt_shape(bool inverse, int pass, int limbs) const { return ntt_g[inverse][pass][ntt_size_class(limbs)]; }
   uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up
 
   // scratch: stream-ordered allocations from the device's memory pool

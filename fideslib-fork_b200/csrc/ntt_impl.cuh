@@ -11,7 +11,9 @@ namespace nttk {
 constexpr int COL = 0, ROW = 1;
 
 constexpr int LOGE = 4;  // 16 elements per thread
-constexpr int G = 16;    // sub-transforms per CTA
+// Sub-transforms per CTA (G) is a template parameter of every pass: 4, 8 or 16, chosen per
+// launch by the context's tile-shape table (fides_ctx_autotune).  The butterflies and their
+// order are the same for every G, so the results are identical.
 
 // Asynchronous 16-byte global -> shared copies (cp.async), used to fetch an epilogue operand
 // while the butterflies run.
@@ -24,7 +26,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Whether pass PASS of a transform stages its epilogue operand ep0 in shared memory: the
-// forward row pass (the last one) with a ModDown / rescale epilogue.  Its G rows are one
+// forward row pass (the last one) with a ModDown / rescale epilogue.  A CTA's rows are one
 // contiguous block of ep0, copied with cp.async at the start of the pass.
 template <int PASS, bool FWD, int OUT>
 struct EpStage {
@@ -195,9 +197,15 @@ struct PassShape {
 
 // One pass of a transform of 2^LOGN points.  Every index is a compile-time function of
 // LOGN, so global and shared addresses are a per-thread base plus immediate offsets.
-template <int LOGN, int PASS, bool FWD, int IN, int OUT>
-__global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G,
-                                  ((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G) <= 256 ? 3 : 1)
+// Threads of a pass CTA, and CTAs per SM the register budget is sized for (24 warps).
+template <int LOGN, int PASS, int G>
+struct PassThreads {
+  static constexpr int NT = (1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G;
+  static constexpr int MINB = NT >= 768 ? 1 : (768 / NT > 32 ? 32 : 768 / NT);
+};
+
+template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G>
+__global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LOGN, PASS, G>::MINB)
     ntt_pass(const PassArgs a, const __grid_constant__ NttLimbList L) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
   constexpr int P = 1 << LOGP, E = 1 << LOGE, T = P / E, NT = T * G;
@@ -342,23 +350,33 @@ __global__ void __launch_bounds__((1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * 
 }
 
 
-template <int LOGN, int PASS, bool FWD, int IN, int OUT>
-void launch_pass(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
+template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G>
+void launch_pass_g(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
   constexpr int P = 1 << LOGP, T = P / (1 << LOGE);
   constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LOGE))) * (int)sizeof(uint64_t) +
                        (EpStage<PASS, FWD, OUT>::on ? G * P * (int)sizeof(uint64_t) : 0);
   static bool attr_set = false;  // per instantiation; set before first launch
   if (!attr_set) {
-    FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    smem));
+    FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT, G>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set = true;
   }
   dim3 grid(((1 << LOGN) >> LOGP) / G, L.n);
   // algorithmic bytes: half of a transform's read + write of each limb (two passes)
   LaunchScope ls(c, s, KK_NTT, 8.0 * (1 << LOGN) * L.n);
-  ntt_pass<LOGN, PASS, FWD, IN, OUT><<<grid, T * G, smem, s>>>(a, L);
+  ntt_pass<LOGN, PASS, FWD, IN, OUT, G><<<grid, T * G, smem, s>>>(a, L);
   FIDES_CUDA(cudaGetLastError());
+}
+
+// The pass with the sub-transforms-per-CTA the context's shape table picks for this launch.
+template <int LOGN, int PASS, bool FWD, int IN, int OUT>
+void launch_pass(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
+  switch (c->ntt_shape(!FWD, PASS, L.n)) {
+    case 4: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 4>(c, a, L, s); break;
+    case 8: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 8>(c, a, L, s); break;
+    default: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 16>(c, a, L, s);
+  }
 }
 
 // The pass sequence of one transform for a given ring dimension.

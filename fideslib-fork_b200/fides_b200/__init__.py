@@ -101,6 +101,9 @@ def lib():
         L.fides_ctx_profile.argtypes = [vp, C.c_int]
         L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
         L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
+        L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
+        L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                              C.POINTER(C.c_uint64)]
@@ -238,6 +241,24 @@ class Context:
         _check(lib().fides_ctx_set_scratch_limit(self._h, nbytes))
 
     CONV_ENGINES = {"auto": 0, "simt": 1, "tensor": 2}
+    NTT_SIZE_CLASSES = (8, 32, 128, None)  # upper bounds of limbs per launch
+
+    def autotune(self) -> dict:
+        """Time the NTT tile shapes on the device and keep the fastest (fides_ctx_autotune).
+        Returns the shape table and each class's representative transform time."""
+        ms = (C.c_float * 8)()
+        _check(lib().fides_ctx_autotune(self._h, ms))
+        return {"shapes": self.ntt_shapes(), "transform_ms": {"forward": list(ms[0:4]), "inverse": list(ms[4:8])}}
+
+    def ntt_shapes(self) -> dict:
+        """Sub-transforms per CTA by direction / pass / launch-size class."""
+        v = (C.c_uint8 * 16)()
+        _check(lib().fides_ctx_ntt_shapes(self._h, v))
+        return {d: {p: list(v[8 * i + 4 * j: 8 * i + 4 * j + 4]) for j, p in enumerate(("column", "row"))}
+                for i, d in enumerate(("forward", "inverse"))}
+
+    def set_ntt_shape(self, inverse: bool, pass_: int, size_class: int, subs_per_cta: int):
+        _check(lib().fides_ctx_set_ntt_shape(self._h, int(inverse), pass_, size_class, subs_per_cta))
 
     def set_conv_engine(self, engine: str):
         """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer

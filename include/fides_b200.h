@@ -71,6 +71,18 @@ uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
  * matrix fits in shared memory; wider ones stay on SIMT).  Results are identical. No reference
  * counterpart: the reference has one conversion kernel family (src/Conv.cu:27-423). */
 int fides_ctx_set_conv_engine(fides_ctx* ctx, int engine);
+/* NTT tile-shape autotuner.  Each NTT pass groups 4, 8 or 16 sub-transforms per CTA; the
+ * context keeps one choice per direction (0 forward, 1 inverse), pass (0 column, 1 row) and
+ * launch-size class (limbs per launch <= 8, <= 32, <= 128, more).  fides_ctx_autotune times
+ * every shape on the device (about 0.2 s at N = 2^16) and keeps the fastest; best_ms
+ * (optional, 8 floats [inverse][class]) receives one transform's time of each class's
+ * representative launch (4, 16, 64, 256 limbs).  Results never depend on the shapes.  Do
+ * not run it concurrently with other work on the context.  No reference counterpart: the
+ * reference fixes its NTT launch geometry (src/CKKS/LimbPartition.cu:444-472). */
+int fides_ctx_autotune(fides_ctx* ctx, float* best_ms);
+/* The 16 shape entries, index [inverse][pass][size class]. */
+int fides_ctx_ntt_shapes(fides_ctx* ctx, uint8_t* shapes);
+int fides_ctx_set_ntt_shape(fides_ctx* ctx, int inverse, int pass, int size_class, int subs_per_cta);
 /* Compute roofline of the NTT: butterflies per second that `device` sustains running the
  * forward NTT butterfly (one 64-bit Shoup product, two 64-bit additions) on register-resident
  * data, with no memory traffic.  Takes about 100 ms.  No reference counterpart. */

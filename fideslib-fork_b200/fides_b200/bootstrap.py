@@ -484,3 +484,26 @@ class Bootstrapper:
         for P in self.stc_pts:
             u = self._apply(u, P)
         return u
+
+
+def bootstrap_concurrent(bs: Bootstrapper, cts: list, streams=None) -> list:
+    """Bootstrap several ciphertexts at once, each on its own CUDA stream forked from and
+    joined back to the current stream, so that their kernels overlap on the device (one
+    bootstrap at N = 2^16 spends most of its time at low levels, where a single ciphertext
+    fills few SMs).  Captured inside torch.cuda.graph, the batch becomes one graph with a
+    parallel branch per ciphertext.  Results are those of bs.bootstrap, ciphertext by
+    ciphertext."""
+    import torch
+    main = torch.cuda.current_stream()
+    streams = streams or [torch.cuda.Stream() for _ in cts]
+    outs = [None] * len(cts)
+    for i, (ct, s) in enumerate(zip(cts, streams)):
+        s.wait_stream(main)
+        with torch.cuda.stream(s):
+            outs[i] = bs.bootstrap(ct)
+    for s in streams:
+        main.wait_stream(s)
+    for o in outs:  # the outputs are handed to the current stream
+        o.c0.record_stream(main)
+        o.c1.record_stream(main)
+    return outs

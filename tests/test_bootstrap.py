@@ -103,3 +103,34 @@ def test_bootstrap_graph_replay_is_bit_identical(fides):
     assert torch.equal(direct.c0, gout.c0) and torch.equal(direct.c1, gout.c1)
     got = decode(kg.decrypt_limb0(fides.to_host(gout.c0), fides.to_host(gout.c1)), prm.N, gout.scale)
     assert -math.log2(np.abs(got - z).max()) > 14
+
+
+@pytest.mark.gpu
+def test_concurrent_batch_equals_sequential(fides):
+    """A batch bootstrapped on parallel streams (and as one graph with parallel branches)
+    gives exactly the ciphertexts of one-at-a-time bootstraps."""
+    import torch
+    from fides_b200 import bootstrap as B
+    prm, o, kg, ctx, ev, bs = make_boot(fides, 12)
+    delta = 2.0 ** 50
+    bs.prepare(top_level=prm.n_q, msg_scale=delta)
+    rng = xrng(64)
+    n = prm.N // 2
+    cts = []
+    for _ in range(3):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        cts.append(B.Ct(fides.to_device(c0), fides.to_device(c1), delta))
+    seq = [bs.bootstrap(c) for c in cts]
+    par = B.bootstrap_concurrent(bs, cts)
+    torch.cuda.synchronize()
+    for a, b in zip(seq, par):
+        assert torch.equal(a.c0, b.c0) and torch.equal(a.c1, b.c1)
+    g = torch.cuda.CUDAGraph()
+    streams = [torch.cuda.Stream() for _ in cts]
+    with torch.cuda.graph(g):
+        gout = B.bootstrap_concurrent(bs, cts, streams)
+    g.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(seq, gout):
+        assert torch.equal(a.c0, b.c0) and torch.equal(a.c1, b.c1)

@@ -117,6 +117,10 @@ int fides_int_peak(int device, double* butterflies_per_s) {
   });
 }
 
+int fides_ctx_reserve_scratch(fides_ctx* x, size_t bytes) {
+  return guard([&] { fides::reserve_scratch(C(x), bytes); });
+}
+
 int fides_ctx_autotune(fides_ctx* x, float* best_ms) {
   return guard([&] { fides::autotune_ntt(C(x), best_ms); });
 }

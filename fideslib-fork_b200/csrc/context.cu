@@ -117,6 +117,23 @@ Scratch::Scratch(Context* c, size_t b, cudaStream_t st) : ctx(c), s(st), bytes(b
   }
 }
 
+void reserve_scratch(Context* c, size_t bytes) {
+  if (bytes == 0) return;
+  FIDES_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = nullptr;
+  FIDES_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, c->pool, s);
+  if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(-3, std::string("scratch reservation failed: ") + cudaGetErrorString(e));
+  }
+  FIDES_CUDA(e2);
+}
+
 Scratch::~Scratch() {
   if (p) {
     cudaFreeAsync(p, s);

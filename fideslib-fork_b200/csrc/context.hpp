@@ -138,6 +138,11 @@ struct Scratch {
   Scratch& operator=(const Scratch&) = delete;
 };
 
+// Grows the scratch pool to hold at least `bytes` (allocate, free, synchronise): the pool
+// keeps freed memory (release threshold unbounded), so later stream-ordered allocations up to
+// that size never map new memory on the launch path.
+void reserve_scratch(Context* c, size_t bytes);
+
 Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* primes, const uint64_t* psi, int device);
 void destroy_context(Context* c);
 

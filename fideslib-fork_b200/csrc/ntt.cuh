@@ -57,7 +57,10 @@ struct LimbRef {
 
 inline LimbRef lref(uint64_t* p, int prime) { return LimbRef{p, nullptr, nullptr, nullptr, nullptr, prime, 0, 0}; }
 
-constexpr int MAX_NTT_LIMBS = 448;
+#ifndef FIDES_MAX_NTT_LIMBS
+#define FIDES_MAX_NTT_LIMBS 448
+#endif
+constexpr int MAX_NTT_LIMBS = FIDES_MAX_NTT_LIMBS;
 
 struct NttLimbList {
   int n;

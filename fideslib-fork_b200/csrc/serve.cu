@@ -71,8 +71,10 @@ struct Server {
 
   size_t request_bytes(const fides_request& r) const {
     const int l = r.level, ext = l + c->K;
-    const size_t ks = (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l;
-    const size_t limbs = r.op == FIDES_OP_ROTATE ? ks : ks + (size_t)l * (r.op == FIDES_OP_HMULT ? 4 : 2) + 1;
+    // the scratch of one key switch (ops.cu ks_limbs): INTT copy, digits, the two extended
+    // KSK outputs, two conversions and the two rescale tops; HMult and HRotate need no more
+    const size_t limbs = (size_t)l + (size_t)c->beta(l) * ext + 2 * (size_t)ext + 2 * (size_t)l + 2;
+    (void)r.op;
     return limbs * c->limb_bytes();
   }
 
@@ -242,6 +244,20 @@ int fides_server_create(fides_ctx* ctx, const fides_server_config* cfg, fides_se
     s->streams.resize(cfg->n_streams);
     s->busy.assign(cfg->n_streams, false);
     for (auto& st : s->streams) FIDES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // grow the scratch pool once to the most the server can have in flight (every stream
+    // running a full batch of top-level HMults, capped by the budget), so that admitted
+    // batches never map new memory inside the scheduling loop
+    {
+      fides_request top{};
+      top.op = FIDES_OP_HMULT;
+      top.level = s->c->n_q;
+      size_t most = (size_t)cfg->n_streams * cfg->max_batch * s->request_bytes(top);
+      if (cfg->hbm_budget_bytes) most = std::min(most, cfg->hbm_budget_bytes);
+      size_t free_b = 0, total_b = 0;
+      FIDES_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      most = std::min(most, free_b / 2);
+      fides::reserve_scratch(s->c, most);
+    }
     s->worker = std::thread([s] { s->run(); });
     *out = new fides_server{s};
   });

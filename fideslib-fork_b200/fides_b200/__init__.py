@@ -102,6 +102,7 @@ def lib():
         L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
         L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
+        L.fides_ctx_reserve_scratch.argtypes = [vp, C.c_size_t]
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
@@ -236,6 +237,10 @@ class Context:
     @property
     def scratch_bytes(self) -> int:
         return int(lib().fides_ctx_scratch_bytes(self._h))
+
+    def reserve_scratch(self, nbytes: int):
+        """Grow the scratch pool to `nbytes` once, up front."""
+        _check(lib().fides_ctx_reserve_scratch(self._h, nbytes))
 
     def set_scratch_limit(self, nbytes: int):
         _check(lib().fides_ctx_set_scratch_limit(self._h, nbytes))

@@ -63,6 +63,10 @@ int fides_ctx_alpha(const fides_ctx* ctx);
 size_t fides_ctx_scratch_bytes(const fides_ctx* ctx);
 /* Cap on scratch growth (0 = unlimited); exceeding it returns FIDES_ERR_OOM. */
 int fides_ctx_set_scratch_limit(fides_ctx* ctx, size_t bytes);
+/* Grows the device scratch pool to hold at least `bytes` once, up front (the pool keeps
+ * freed memory), so that later operations never map new memory on their launch path.
+ * fides_server_create calls it with the server's worst case. */
+int fides_ctx_reserve_scratch(fides_ctx* ctx, size_t bytes);
 /* Count of kernels this context has launched (for launch accounting). */
 uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
 

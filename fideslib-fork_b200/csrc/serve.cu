@@ -12,7 +12,10 @@
 //     of levels) on one of n_streams streams, so batches that are admitted while others are
 //     still on the GPU overlap with them;
 //   * a host function enqueued behind each batch marks its requests complete (latency =
-//     completion - arrival) and returns their budget, waking the scheduler.
+//     completion - arrival) and returns their budget, waking the scheduler;
+//   * bootstrap requests go to registered bootstrap engines (a captured CUDA graph over
+//     static buffers, each on its own stream): copy in, graph launch, copy out, so they
+//     overlap the HMult / HRotate batches; their memory is the graph's, already resident.
 // Results are exact integer arithmetic, so a request's output does not depend on what it
 // was batched with; tests/test_serving.py checks that bit for bit.
 #include <algorithm>
@@ -56,6 +59,14 @@ struct Server {
   const uint64_t* relin = nullptr;
   std::map<int, const uint64_t*> rot;  // normalised rotation -> key
   std::vector<cudaStream_t> streams;
+  struct BootEngine {
+    cudaGraphExec_t exec;
+    const uint64_t *in0, *in1, *out0, *out1;
+    int in_level, out_level;
+    cudaStream_t stream;
+    bool busy;
+  };
+  std::deque<BootEngine> boot;  // a deque: registering an engine keeps references to the others valid
   std::vector<bool> busy;
 
   std::mutex mu;
@@ -86,7 +97,7 @@ struct Server {
 
   struct Batch {
     Server* s;
-    int stream;
+    int stream;  // index into streams, or -1 - engine for a bootstrap
     std::vector<uint64_t> tickets;
     std::vector<Clock::time_point> arrivals;
     size_t bytes;
@@ -107,7 +118,10 @@ struct Server {
         s->st.completed++;
       }
       s->in_use -= b->bytes;
-      s->busy[b->stream] = false;
+      if (b->stream >= 0)
+        s->busy[b->stream] = false;
+      else
+        s->boot[-1 - b->stream].busy = false;
     }
     s->cv.notify_all();
     s->done_cv.notify_all();
@@ -122,13 +136,35 @@ struct Server {
     st.rejected++;
   }
 
+  // Copy in, graph launch, copy out on the engine's stream, then the completion callback.
+  void launch_bootstrap(BootEngine& e, int index, const Pending& p) {
+    auto* b = new Batch{this, -1 - index, {p.ticket}, {p.arrival}, 0, FIDES_OK};
+    const size_t lb = c->limb_bytes();
+    cudaError_t err = cudaSetDevice(c->device);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in0), p.r.c0, lb * e.in_level, cudaMemcpyDeviceToDevice, e.stream);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in1), p.r.c1, lb * e.in_level, cudaMemcpyDeviceToDevice, e.stream);
+    if (err == cudaSuccess) err = cudaGraphLaunch(e.exec, e.stream);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(p.r.out0, e.out0, lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(p.r.out1, e.out1, lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
+    if (err != cudaSuccess) b->status = FIDES_ERR_CUDA;
+    if (cudaLaunchHostFunc(e.stream, on_done, b) != cudaSuccess) {
+      b->status = FIDES_ERR_CUDA;
+      on_done(b);
+    }
+  }
+
   void run() {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
       cv.wait(lk, [&] {
         if (stop) return true;
         if (pending.empty()) return false;
-        return std::find(busy.begin(), busy.end(), false) != busy.end();
+        if (std::find(busy.begin(), busy.end(), false) != busy.end()) return true;
+        return std::any_of(boot.begin(), boot.end(), [](const BootEngine& e) { return !e.busy; });
       });
       if (stop && pending.empty()) break;
       if (stop) {
@@ -140,12 +176,39 @@ struct Server {
         done_cv.notify_all();
         break;
       }
-      const int slot = (int)(std::find(busy.begin(), busy.end(), false) - busy.begin());
-      const int op = pending.front().r.op;
+      // bootstrap requests: one per idle engine, oldest first
+      bool launched_boot = false;
+      for (auto it = pending.begin(); it != pending.end();) {
+        if (it->r.op != FIDES_OP_BOOTSTRAP) {
+          ++it;
+          continue;
+        }
+        auto eng = std::find_if(boot.begin(), boot.end(), [](const BootEngine& e) { return !e.busy; });
+        if (eng == boot.end()) break;
+        Pending p = *it;
+        it = pending.erase(it);
+        eng->busy = true;
+        st.batches++;
+        st.batched_requests++;
+        launched_boot = true;
+        lk.unlock();
+        launch_bootstrap(*eng, (int)(eng - boot.begin()), p);
+        lk.lock();
+        it = pending.begin();  // the deque may have changed while unlocked
+      }
+      const auto first = std::find_if(pending.begin(), pending.end(),
+                                      [](const Pending& p) { return p.r.op != FIDES_OP_BOOTSTRAP; });
+      const auto free_slot = std::find(busy.begin(), busy.end(), false);
+      if (first == pending.end() || free_slot == busy.end()) {
+        if (!launched_boot) cv.wait_for(lk, std::chrono::microseconds(200));
+        continue;
+      }
+      const int slot = (int)(free_slot - busy.begin());
+      const int op = first->r.op;
       const size_t budget = cfg.hbm_budget_bytes ? cfg.hbm_budget_bytes : SIZE_MAX;
       std::vector<Pending> take;
       size_t bytes = 0;
-      for (auto it = pending.begin(); it != pending.end() && (int)take.size() < cfg.max_batch;) {
+      for (auto it = first; it != pending.end() && (int)take.size() < cfg.max_batch;) {
         if (it->r.op != op) {
           ++it;
           continue;
@@ -279,6 +342,24 @@ int fides_server_add_rotation_key(fides_server* sv, int rotation, const uint64_t
   });
 }
 
+int fides_server_add_bootstrap(fides_server* sv, void* graph_exec, const uint64_t* in0, const uint64_t* in1,
+                               int in_level, const uint64_t* out0, const uint64_t* out1, int out_level) {
+  return sguard([&] {
+    if (!sv || !graph_exec || !in0 || !in1 || !out0 || !out1) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    fides::Server* s = sv->s;
+    if (in_level < 1 || in_level > s->c->n_q || out_level < 1 || out_level > s->c->n_q)
+      throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->boot.empty() && (s->boot[0].in_level != in_level || s->boot[0].out_level != out_level))
+      throw fides::Error(FIDES_ERR_ARG, "bootstrap engines must share their levels");
+    fides::Server::BootEngine e{static_cast<cudaGraphExec_t>(graph_exec), in0, in1, out0, out1, in_level,
+                                out_level, nullptr, false};
+    FIDES_CUDA(cudaSetDevice(s->c->device));
+    FIDES_CUDA(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+    s->boot.push_back(e);
+  });
+}
+
 int fides_server_submit(fides_server* sv, const fides_request* r, uint64_t* ticket) {
   return sguard([&] {
     if (!sv || !r || !ticket) throw fides::Error(FIDES_ERR_ARG, "null argument");
@@ -288,6 +369,10 @@ int fides_server_submit(fides_server* sv, const fides_request* r, uint64_t* tick
     if (r->op == FIDES_OP_ROTATE) {
       std::lock_guard<std::mutex> lk(s->mu);
       if (!s->rot.count(s->norm_rot(r->rotation))) throw fides::Error(FIDES_ERR_KEY, "no key for this rotation");
+    } else if (r->op == FIDES_OP_BOOTSTRAP) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->boot.empty()) throw fides::Error(FIDES_ERR_KEY, "no bootstrap engine registered");
+      if (r->level != s->boot[0].in_level) throw fides::Error(FIDES_ERR_LEVEL, "bootstrap input level mismatch");
     } else if (r->op == FIDES_OP_HMULT || r->op == FIDES_OP_HMULT_NORESCALE) {
       if (!r->d0 || !r->d1) throw fides::Error(FIDES_ERR_ARG, "null second operand");
       if (r->op == FIDES_OP_HMULT && r->level < 2) throw fides::Error(FIDES_ERR_LEVEL, "rescale needs level >= 2");
@@ -345,6 +430,10 @@ int fides_server_destroy(fides_server* sv) {
     for (auto st : s->streams) {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
+    }
+    for (auto& e : s->boot) {
+      cudaStreamSynchronize(e.stream);
+      cudaStreamDestroy(e.stream);
     }
     delete s;
     delete sv;

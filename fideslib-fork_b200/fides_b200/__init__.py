@@ -58,7 +58,7 @@ class _ServerStats(C.Structure):
                                           "peak_bytes")]
 
 
-OP_HMULT, OP_HMULT_NORESCALE, OP_ROTATE = 0, 1, 2
+OP_HMULT, OP_HMULT_NORESCALE, OP_ROTATE, OP_BOOTSTRAP = 0, 1, 2, 3
 
 
 class _HMultHostItem(C.Structure):
@@ -103,6 +103,7 @@ def lib():
         L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
         L.fides_ctx_reserve_scratch.argtypes = [vp, C.c_size_t]
+        L.fides_server_add_bootstrap.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_int]
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
@@ -582,6 +583,14 @@ class Server:
     def add_rotation_key(self, rotation: int, key):
         self._keep.append(key)
         _check(lib().fides_server_add_rotation_key(self._h, rotation, _ptr(key)))
+
+    def add_bootstrap(self, graph, static_in: Ciphertext, static_out: Ciphertext):
+        """Register a bootstrap engine: a torch.cuda.CUDAGraph that bootstraps static_in into
+        static_out (see fides_b200.bootstrap.make_engine).  Engines run concurrently."""
+        self._keep += [graph, static_in, static_out]
+        _check(lib().fides_server_add_bootstrap(self._h, graph.raw_cuda_graph_exec(), _ptr(static_in.c0),
+                                                _ptr(static_in.c1), static_in.level, _ptr(static_out.c0),
+                                                _ptr(static_out.c1), static_out.level))
 
     def submit(self, op: int, a: Ciphertext, out: Ciphertext, b: Ciphertext | None = None, rotation: int = 0) -> int:
         r = _Request(op, a.level, _ptr(a.c0), _ptr(a.c1), _ptr(b.c0) if b else None, _ptr(b.c1) if b else None,

@@ -507,3 +507,24 @@ def bootstrap_concurrent(bs: Bootstrapper, cts: list, streams=None) -> list:
         o.c0.record_stream(main)
         o.c1.record_stream(main)
     return outs
+
+
+def make_engine(bs: Bootstrapper, scale: float):
+    """A bootstrap engine for the request loop (fides_server_add_bootstrap): static device
+    buffers for a one-limb input ciphertext (bootstrapping reads limb 0 only) and a CUDA
+    graph, captured once, that bootstraps them into a static output.  Returns (graph,
+    static input, static output) as (torch.cuda.CUDAGraph, Ciphertext, Ciphertext); the
+    graph's private memory pool keeps every intermediate resident."""
+    import torch
+    F, ctx = bs.ev.F, bs.ev.ctx
+    c0, c1 = ctx.empty(1), ctx.empty(1)
+    c0.view(torch.int64).zero_()
+    c1.view(torch.int64).zero_()
+    static = Ct(c0, c1, scale)
+    bs.bootstrap(static)  # warm-up outside the capture (lazy kernel loading, tables)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        out = bs.bootstrap(static)
+    torch.cuda.synchronize()
+    return g, F.Ciphertext(c0, c1), F.Ciphertext(out.c0, out.c1)

@@ -217,6 +217,8 @@ int fides_graph_destroy(fides_graph* g);
 #define FIDES_OP_HMULT 0           /* HMult + relinearize + rescale: out has level - 1 limbs */
 #define FIDES_OP_HMULT_NORESCALE 1 /* HMult + relinearize: out has level limbs */
 #define FIDES_OP_ROTATE 2          /* HRotate by `rotation`: out has level limbs */
+#define FIDES_OP_BOOTSTRAP 3       /* bootstrap through a registered engine (below): the input
+                                    * has the engine's in_level limbs, out its out_level limbs */
 
 typedef struct fides_server fides_server;
 typedef struct fides_server_config {
@@ -239,6 +241,16 @@ typedef struct fides_server_stats {
 int fides_server_create(fides_ctx* ctx, const fides_server_config* cfg, fides_server** out);
 int fides_server_set_relin_key(fides_server* s, const uint64_t* relin_key_dev);
 int fides_server_add_rotation_key(fides_server* s, int rotation, const uint64_t* rot_key_dev);
+/* Registers one bootstrap engine: an instantiated CUDA graph (cudaGraphExec_t) that
+ * bootstraps the ciphertext held in the static device buffers (in0, in1: in_level limbs
+ * each) into (out0, out1: out_level limbs each), with every key and intermediate it needs
+ * resident.  A FIDES_OP_BOOTSTRAP request copies its input into the static input, launches
+ * the graph and copies the static output to its own output, all on the engine's stream,
+ * so it overlaps the HMult / HRotate batches; each engine runs one request at a time and
+ * several engines run concurrently.  The graph and buffers must outlive the server.  No
+ * reference counterpart (the reference has no request loop). */
+int fides_server_add_bootstrap(fides_server* s, void* graph_exec, const uint64_t* in0, const uint64_t* in1,
+                               int in_level, const uint64_t* out0, const uint64_t* out1, int out_level);
 /* Thread-safe, non-blocking; rejects malformed requests and missing keys immediately. */
 int fides_server_submit(fides_server* s, const fides_request* req, uint64_t* ticket);
 /* Blocks until the request completed; *status is its result (FIDES_ERR_OOM when it can

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from ckks_host import KeyGen, decode, encode, xrng
+from ckks_host import KeyGen, decode, encode, uniform_limbs, xrng
 
 
 def _u0(n):
@@ -134,3 +134,82 @@ def test_concurrent_batch_equals_sequential(fides):
     torch.cuda.synchronize()
     for a, b in zip(seq, gout):
         assert torch.equal(a.c0, b.c0) and torch.equal(a.c1, b.c1)
+
+
+@pytest.mark.gpu
+def test_served_bootstraps_in_a_mix(fides):
+    """Bootstrap requests through the request loop (two engines) mixed with HMult / HRotate
+    requests submitted from several threads: every bootstrap equals the direct bootstrap of
+    its input and every HMult / HRotate equals the same request run alone."""
+    import random
+    import threading
+    import torch
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    delta = 2.0 ** 50
+    bs.prepare(top_level=prm.n_q, msg_scale=delta)
+    engines = [B.make_engine(bs, delta) for _ in range(2)]
+    rng = xrng(65)
+    n = prm.N // 2
+    boot_in, boot_ref = [], []
+    for _ in range(4):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        ct = F.Ciphertext(F.to_device(c0[:1]), F.to_device(c1[:1]))
+        boot_in.append(ct)
+        r = bs.bootstrap(B.Ct(ct.c0, ct.c1, delta))
+        boot_ref.append((r.c0.clone(), r.c1.clone()))
+    torch.cuda.synchronize()
+    rot_key = F.to_device(kg.rotation_key(1))
+    reqs = []
+    rnd = random.Random(7)
+    for i in range(12):
+        l = rnd.choice([4, 8, 12])
+        a = F.Ciphertext(F.to_device(uniform_limbs(rng, prm.q[:l], prm.N)), F.to_device(uniform_limbs(rng, prm.q[:l], prm.N)))
+        if i % 2:
+            b = F.Ciphertext(F.to_device(uniform_limbs(rng, prm.q[:l], prm.N)), F.to_device(uniform_limbs(rng, prm.q[:l], prm.N)))
+            reqs.append((F.OP_HMULT, a, b, l - 1))
+        else:
+            reqs.append((F.OP_ROTATE, a, None, l))
+    alone = []
+    for op, a, b, lo in reqs:
+        alone.append(ctx.mult(a, b, ev.rk, rescale=True) if op == F.OP_HMULT else ctx.rotate(a, rot_key, 1))
+    srv = F.Server(ctx, n_streams=2, max_batch=4)
+    try:
+        srv.set_relin_key(ev.rk)
+        srv.add_rotation_key(1, rot_key)
+        for g, sin, sout in engines:
+            srv.add_bootstrap(g, sin, sout)
+        out_lvl = engines[0][2].level
+        jobs = [("b", i) for i in range(len(boot_in))] + [("o", i) for i in range(len(reqs))]
+        random.Random(8).shuffle(jobs)
+        outs = {}
+        tickets = {}
+
+        def worker(part):
+            for kind, i in part:
+                if kind == "b":
+                    out = F.Ciphertext(ctx.empty(out_lvl), ctx.empty(out_lvl))
+                    outs[("b", i)] = out
+                    tickets[("b", i)] = srv.submit(F.OP_BOOTSTRAP, boot_in[i], out)
+                else:
+                    op, a, b, lo = reqs[i]
+                    out = F.Ciphertext(ctx.empty(lo), ctx.empty(lo))
+                    outs[("o", i)] = out
+                    tickets[("o", i)] = srv.submit(op, a, out, b, 1)
+
+        ts = [threading.Thread(target=worker, args=(jobs[k::3],)) for k in range(3)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        for key, t in tickets.items():
+            st, _ = srv.wait(t)
+            assert st == 0, key
+    finally:
+        srv.close()
+    for i, (r0, r1) in enumerate(boot_ref):
+        assert torch.equal(outs[("b", i)].c0, r0) and torch.equal(outs[("b", i)].c1, r1), f"bootstrap {i}"
+    for i, x in enumerate(alone):
+        assert torch.equal(outs[("o", i)].c0, x.c0) and torch.equal(outs[("o", i)].c1, x.c1), f"request {i}"

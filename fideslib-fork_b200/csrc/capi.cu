@@ -417,6 +417,39 @@ int fides_rotate_hoisted(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, i
   });
 }
 
+int fides_rotate_hoisted_batch(fides_ctx* x, const fides_hoist_item* items, int n_items, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n_items < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    if (n_items > 0) need(items, "items");
+    std::vector<fides::HoistItem> v(n_items);
+    for (int i = 0; i < n_items; ++i) {
+      const fides_hoist_item& h = items[i];
+      need(h.c0, "c0");
+      need(h.c1, "c1");
+      if (h.n < 0) throw fides::Error(FIDES_ERR_ARG, "negative rotation count");
+      if (h.n > 0) {
+        need(h.keys, "keys");
+        need(h.rotations, "rotations");
+        need(h.out0, "out0");
+        need(h.out1, "out1");
+      }
+      v[i].c0 = h.c0;
+      v[i].c1 = h.c1;
+      v[i].l = h.level;
+      for (int j = 0; j < h.n; ++j) {
+        need(h.out0[j], "out0[j]");
+        need(h.out1[j], "out1[j]");
+        v[i].keys.push_back(h.keys[j]);
+        v[i].ks.push_back(fides::h_auto_index(c->logN, h.rotations[j]));
+        v[i].out0.push_back(h.out0[j]);
+        v[i].out1.push_back(h.out1[j]);
+      }
+    }
+    fides::op_hoisted_batch(c, v.data(), n_items, S(stream));
+  });
+}
+
 int fides_hmult_batch(fides_ctx* x, const fides_hmult_item* items, int n, const uint64_t* relin_key, int rescale,
                       void* stream) {
   return guard([&] {

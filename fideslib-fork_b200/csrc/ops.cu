@@ -369,37 +369,63 @@ void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s)
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
 }
 
-void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) {
-  const int n = (int)it.keys.size();
-  if (n <= 0) return;
-  check_level(c, it.l);
+void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStream_t s) {
+  // Every ciphertext's c1 is raised once (one ModUp launch sequence over all of them), the KSK
+  // pass covers every (ciphertext, rotation) pair -- adding P c0 and scattering by the
+  // automorphism -- and one ModDown covers every output (hoistedRotateDotKSK_2_ and
+  // fusedHoistedRotateBatch, ElemenwiseBatchKernels.cu:277-377, LimbPartitionBatch.cu:526+).
+  if (n_items <= 0) return;
   const size_t N = c->N;
-  const int l = it.l, ext = l + c->K;
-  for (int j = 0; j < n; ++j)
-    if (!it.keys[j]) throw Error(-5, "null rotation key");
-  size_t total = (size_t)l + (size_t)c->beta(l) * ext + (size_t)n * (2 * ext + 2 * l);
+  size_t total = 0;
+  int n_out = 0;
+  for (int i = 0; i < n_items; ++i) {
+    const HoistItem& it = items[i];
+    check_level(c, it.l);
+    for (auto* k : it.keys)
+      if (!k) throw Error(-5, "null rotation key");
+    const int l = it.l, ext = l + c->K, r = (int)it.keys.size();
+    total += (size_t)l + (size_t)c->beta(l) * ext + (size_t)r * (2 * ext + 2 * l);
+    n_out += r;
+  }
+  if (n_out == 0) return;
   Scratch sc(c, sizeof(uint64_t) * N * total, s);
   Bump bp{sc.u64(), N};
-  uint64_t* tmp = bp.take(l);
-  uint64_t* dig = bp.take((size_t)c->beta(l) * ext);
-  modup_stage(c, &it.c1, nullptr, &l, &tmp, &dig, 1, s);
-  std::vector<KskJob> kj;
-  std::vector<uint64_t*> ex(2 * n), conv(2 * n), outs(2 * n);
-  std::vector<int> ls2(2 * n, l);
-  for (int j = 0; j < n; ++j) {
-    uint64_t* A = bp.take(ext);
-    uint64_t* B = bp.take(ext);
-    kj.push_back(KskJob{it.c1, nullptr, dig, it.keys[j], it.c0, A, B, l, it.ks[j]});
-    ex[2 * j] = B;
-    ex[2 * j + 1] = A;
-    conv[2 * j] = bp.take(l);
-    conv[2 * j + 1] = bp.take(l);
-    outs[2 * j] = it.out0[j];
-    outs[2 * j + 1] = it.out1[j];
+  std::vector<const uint64_t*> xs(n_items);
+  std::vector<int> ls(n_items);
+  std::vector<uint64_t*> tmp(n_items), dig(n_items);
+  for (int i = 0; i < n_items; ++i) {
+    const int l = items[i].l, ext = l + c->K;
+    xs[i] = items[i].c1;
+    ls[i] = l;
+    tmp[i] = bp.take(l);
+    dig[i] = bp.take((size_t)c->beta(l) * ext);
   }
-  launch_ksk(c, kj.data(), n, s);
-  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
+  modup_stage(c, xs.data(), nullptr, ls.data(), tmp.data(), dig.data(), n_items, s);
+  std::vector<KskJob> kj;
+  std::vector<uint64_t*> ex, conv, outs;
+  std::vector<int> ls2;
+  for (int i = 0; i < n_items; ++i) {
+    const HoistItem& it = items[i];
+    const int l = it.l, ext = l + c->K;
+    for (size_t j = 0; j < it.keys.size(); ++j) {
+      uint64_t* A = bp.take(ext);
+      uint64_t* B = bp.take(ext);
+      kj.push_back(KskJob{it.c1, nullptr, dig[i], it.keys[j], it.c0, A, B, l, it.ks[j]});
+      ex.push_back(B);
+      ex.push_back(A);
+      conv.push_back(bp.take(l));
+      conv.push_back(bp.take(l));
+      outs.push_back(it.out0[j]);
+      outs.push_back(it.out1[j]);
+      ls2.push_back(l);
+      ls2.push_back(l);
+    }
+  }
+  launch_ksk(c, kj.data(), (int)kj.size(), s);
+  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, (int)outs.size(), s);
 }
+
+void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) { op_hoisted_batch(c, &it, 1, s); }
 
 void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s) {
   check_level(c, out_level);

@@ -56,6 +56,9 @@ void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* r
                     cudaStream_t s);
 void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s);
 void op_hoisted(Context* c, const HoistItem& item, cudaStream_t s);
+// Hoisted rotations of several ciphertexts (any levels, own rotation lists) in one launch
+// sequence per stage.
+void op_hoisted_batch(Context* c, const HoistItem* items, int n, cudaStream_t s);
 // ModRaise (reference Bootstrap.cu ModRaise): a level-1 polynomial (limb q_0, EVAL) raised to
 // `out_level` limbs: INTT, SwitchModulus(q_0 -> q_j) of the centred residues, NTT.
 void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s);

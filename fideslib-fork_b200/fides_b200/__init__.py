@@ -65,6 +65,11 @@ class _HMultHostItem(C.Structure):
     _fields_ = [("a0", vp), ("a1", vp), ("b0", vp), ("b1", vp), ("out0", vp), ("out1", vp), ("level", C.c_int)]
 
 
+class _HoistItem(C.Structure):
+    _fields_ = [("c0", vp), ("c1", vp), ("level", C.c_int), ("n", C.c_int), ("keys", C.POINTER(vp)),
+                ("rotations", C.POINTER(C.c_int)), ("out0", C.POINTER(vp)), ("out1", C.POINTER(vp))]
+
+
 class _RotateHostItem(C.Structure):
     _fields_ = [("c0", vp), ("c1", vp), ("out0", vp), ("out1", vp), ("key", vp), ("level", C.c_int),
                 ("rotation", C.c_int)]
@@ -104,6 +109,7 @@ def lib():
         L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
         L.fides_ctx_reserve_scratch.argtypes = [vp, C.c_size_t]
         L.fides_server_add_bootstrap.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_int]
+        L.fides_rotate_hoisted_batch.argtypes = [vp, C.POINTER(_HoistItem), C.c_int, vp]
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
@@ -389,6 +395,26 @@ class Context:
         o0 = (vp * n)(*[_ptr(o.c0) for o in outs])
         o1 = (vp * n)(*[_ptr(o.c1) for o in outs])
         _check(lib().fides_rotate_hoisted(self._h, _ptr(ct.c0), _ptr(ct.c1), l, kp, rs, n, o0, o1, _stream()))
+        return outs
+
+    def rotate_hoisted_batch(self, cts, keys, rotations) -> list[list[Ciphertext]]:
+        """Hoisted rotations of several ciphertexts (any levels) in one launch sequence per
+        stage.  keys / rotations: per-ciphertext lists (or one list shared by all)."""
+        if rotations and not isinstance(rotations[0], (list, tuple)):
+            rotations, keys = [rotations] * len(cts), [keys] * len(cts)
+        items = (_HoistItem * max(1, len(cts)))()
+        outs, keep = [], []
+        for i, (ct, ks, rs) in enumerate(zip(cts, keys, rotations)):
+            n, l = len(rs), ct.level
+            o = [Ciphertext(self.empty(l), self.empty(l)) for _ in range(n)]
+            kp = (vp * max(1, n))(*[_ptr(k) for k in ks])
+            rp = (C.c_int * max(1, n))(*rs)
+            o0 = (vp * max(1, n))(*[_ptr(x.c0) for x in o])
+            o1 = (vp * max(1, n))(*[_ptr(x.c1) for x in o])
+            keep += [kp, rp, o0, o1]
+            items[i] = _HoistItem(_ptr(ct.c0), _ptr(ct.c1), l, n, kp, rp, o0, o1)
+            outs.append(o)
+        _check(lib().fides_rotate_hoisted_batch(self._h, items, len(cts), _stream()))
         return outs
 
     # -- elementwise RNS ops (polynomials of `level` Q limbs) --

@@ -172,6 +172,21 @@ int fides_rotate_auto(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, in
 int fides_rotate_hoisted(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                          const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
                          uint64_t* const* out1, void* stream);
+/* Hoisted rotations of a batch of ciphertexts at any levels, each with its own rotation
+ * list: one ModUp launch sequence over all c1, one KSK pass over every (ciphertext,
+ * rotation) pair, one ModDown over every output.  Replaces fusedHoistedRotateBatch /
+ * hoistedRotateDotKSKBatched (LimbPartitionBatch.cu:526+, ElemenwiseBatchKernels.cu:379-634),
+ * which require equal levels.  Item k's outputs j are out0[j] / out1[j] of that item. */
+typedef struct {
+  const uint64_t *c0, *c1;     /* [level][N] each */
+  int level;
+  int n;                       /* rotations of this ciphertext */
+  const uint64_t* const* keys; /* [n] device keys */
+  const int* rotations;        /* [n] */
+  uint64_t* const* out0;       /* [n] outputs, [level][N] each */
+  uint64_t* const* out1;
+} fides_hoist_item;
+int fides_rotate_hoisted_batch(fides_ctx* ctx, const fides_hoist_item* items, int n_items, void* stream);
 /* Rotation index -> automorphism index (Context.cu:916-944 + RNSPoly.cpp:656-658). */
 uint32_t fides_rotation_auto_index(int logN, int rotation);
 

@@ -72,7 +72,11 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
   }
 }
 
-// Two adjacent coefficients per thread (16-byte loads of every stream).
+// Two adjacent coefficients per thread (16-byte loads of every stream).  MAXB is the
+// largest digit count of the launch's jobs (0 = any): with it known at compile time every
+// load of the thread -- all digits, both key halves, the own-digit and tensor operands -- is
+// issued before the first product, so a thread keeps up to 3 MAXB + 4 loads in flight.
+template <int MAXB>
 __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
                                                          const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
                                                          int alpha) {
@@ -88,53 +92,82 @@ __global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__
   const int own = i < l ? i / alpha : -1;
   const size_t kstride = (size_t)(n_q + K) * N;
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
+  const size_t off = (size_t)i * N + n, koff = (size_t)pid * N + n;
+  const bool tensor = J.a0 && i < l;
   U128 sa0{0, 0}, sb0{0, 0}, sa1{0, 0}, sb1{0, 0};
-  ulonglong2 x1{0, 0}, y1{0, 0};  // a1, b1 of this limb (tensor mode)
-  for (int d = 0; d < beta; ++d) {
-    ulonglong2 v;
-    if (d == own && J.x) {
-      v = ld2(J.x + (size_t)i * N + n);
-      if (J.x2) {
-        ulonglong2 w = ld2(J.x2 + (size_t)i * N + n);
-        x1 = v;
-        y1 = w;
-        v.x = mulmod(v.x, w.x, p);
-        v.y = mulmod(v.y, w.y, p);
-      }
-    } else {
-      v = ld2(J.digits + ((size_t)d * ext + i) * N + n);
+  ulonglong2 x1{0, 0}, y1{0, 0};  // a1, b1 of this limb (own digit)
+  auto digit = [&](int d, ulonglong2 v, ulonglong2 ka, ulonglong2 kb) {
+    if (d == own && J.x2) {  // the own digit is x * x2 (tensor term a1 b1)
+      x1 = v;
+      v.x = mulmod(v.x, y1.x, p);
+      v.y = mulmod(v.y, y1.y, p);
     }
-    const ulonglong2 ka = ld2(J.key + (size_t)d * kstride + (size_t)pid * N + n);
-    const ulonglong2 kb = ld2(J.key + (size_t)(dnum + d) * kstride + (size_t)pid * N + n);
     mac128(sa0, v.x, ka.x);
     mac128(sb0, v.x, kb.x);
     mac128(sa1, v.y, ka.y);
     mac128(sb1, v.y, kb.y);
-  }
-  if (J.a0 && i < l) {
-    // every Q limb has one own digit, so x1 / y1 hold a1 / b1 here
-    if (beta > 12) {  // keep the sums below 2^128: at most 15 products of two values < 2^62
-      sa0 = U128{reduce128(sa0, p), 0};
-      sb0 = U128{reduce128(sb0, p), 0};
-      sa1 = U128{reduce128(sa1, p), 0};
-      sb1 = U128{reduce128(sb1, p), 0};
+  };
+  if constexpr (MAXB > 0) {
+    ulonglong2 v[MAXB], ka[MAXB], kb[MAXB];
+#pragma unroll
+    for (int d = 0; d < MAXB; ++d)
+      if (d < beta) {
+        const uint64_t* src = (d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n;
+        v[d] = ld2(src);
+        ka[d] = ld2(J.key + (size_t)d * kstride + koff);
+        kb[d] = ld2(J.key + (size_t)(dnum + d) * kstride + koff);
+      }
+    if (own >= 0 && J.x2) y1 = ld2(J.x2 + off);
+    ulonglong2 x0{0, 0}, y0{0, 0};
+    if (tensor) {
+      x0 = ld2(J.a0 + off);
+      y0 = ld2(J.b0 + off);
     }
-    const ShoupConst pm = pmod[i];
-    const ulonglong2 x0 = ld2(J.a0 + (size_t)i * N + n), y0 = ld2(J.b0 + (size_t)i * N + n);
-    const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
-    const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
-    mac128(sb0, x0.x, py0x);  // + P a0 b0
-    mac128(sb1, x0.y, py0y);
-    mac128(sa0, x0.x, py1x);  // + P (a0 b1 + a1 b0)
-    mac128(sa0, x1.x, py0x);
-    mac128(sa1, x0.y, py1y);
-    mac128(sa1, x1.y, py0y);
+#pragma unroll
+    for (int d = 0; d < MAXB; ++d)
+      if (d < beta) digit(d, v[d], ka[d], kb[d]);
+    if (tensor) {
+      const ShoupConst pm = pmod[i];
+      const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
+      const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
+      mac128(sb0, x0.x, py0x);  // + P a0 b0
+      mac128(sb1, x0.y, py0y);
+      mac128(sa0, x0.x, py1x);  // + P (a0 b1 + a1 b0)
+      mac128(sa0, x1.x, py0x);
+      mac128(sa1, x0.y, py1y);
+      mac128(sa1, x1.y, py0y);
+    }
+  } else {
+    if (own >= 0 && J.x2) y1 = ld2(J.x2 + off);
+    for (int d = 0; d < beta; ++d) {
+      const uint64_t* src = (d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n;
+      digit(d, ld2(src), ld2(J.key + (size_t)d * kstride + koff), ld2(J.key + (size_t)(dnum + d) * kstride + koff));
+    }
+    if (tensor) {
+      // every Q limb has one own digit, so x1 / y1 hold a1 / b1 here
+      if (beta > 12) {  // keep the sums below 2^128: at most 15 products of two values < 2^62
+        sa0 = U128{reduce128(sa0, p), 0};
+        sb0 = U128{reduce128(sb0, p), 0};
+        sa1 = U128{reduce128(sa1, p), 0};
+        sb1 = U128{reduce128(sb1, p), 0};
+      }
+      const ShoupConst pm = pmod[i];
+      const ulonglong2 x0 = ld2(J.a0 + off), y0 = ld2(J.b0 + off);
+      const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
+      const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
+      mac128(sb0, x0.x, py0x);
+      mac128(sb1, x0.y, py0y);
+      mac128(sa0, x0.x, py1x);
+      mac128(sa0, x1.x, py0x);
+      mac128(sa1, x0.y, py1y);
+      mac128(sa1, x1.y, py0y);
+    }
   }
   uint64_t ra0 = reduce128(sa0, p), rb0 = reduce128(sb0, p);
   uint64_t ra1 = reduce128(sa1, p), rb1 = reduce128(sb1, p);
   if (J.c0 && i < l) {
     const ShoupConst pm = pmod[i];
-    const ulonglong2 c = ld2(J.c0 + (size_t)i * N + n);
+    const ulonglong2 c = ld2(J.c0 + off);
     rb0 = addmod(rb0, shoup(c.x, pm.w, pm.ws, p.q), p.q);
     rb1 = addmod(rb1, shoup(c.y, pm.w, pm.ws, p.q), p.q);
   }
@@ -341,8 +374,19 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
       const int l = L.j[i].l, ext = l + c->K, b = c->beta(l);
       bytes += 8.0 * c->N * ((double)ext * (3 * b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
     }
+    int maxb = 0;
+    for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     LaunchScope ls(c, s, KK_KSK, bytes);
-    ksk_kernel<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha);
+    switch (maxb) {
+#define FIDES_KSK_CASE(B)                                                                                     \
+  case B:                                                                                                     \
+    ksk_kernel<B><<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha); \
+    break;
+      FIDES_KSK_CASE(1) FIDES_KSK_CASE(2) FIDES_KSK_CASE(3) FIDES_KSK_CASE(4)
+#undef FIDES_KSK_CASE
+      default:
+        ksk_kernel<0><<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha);
+    }
     FIDES_CUDA(cudaGetLastError());
   }
 }

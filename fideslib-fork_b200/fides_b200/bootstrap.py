@@ -260,8 +260,14 @@ class Bootstrapper:
     """Precomputed CoeffsToSlots / SlotsToCoeffs diagonals and EvalMod constants."""
 
     def __init__(self, ev: Evaluator, K: int = 12, r: int = 3, degree: int = 63, cts_levels: int = 3,
-                 stc_levels: int = 3, baby: int = 8, prescale_bits: int = 0):
+                 stc_levels: int = 3, baby: int = 8, prescale_bits: int = 0, encapsulation=None):
         self.ev = ev
+        # sparse-secret encapsulation (Bootstrap.cu keySwitchSparse): device switching keys
+        # (dense -> sparse, sparse -> dense).  The level-1 input is switched to the sparse
+        # secret before ModRaise, so the overflow I of ModRaise stays small, and switched
+        # back right after it, so CoeffsToSlots / EvalMod / SlotsToCoeffs run under the dense
+        # secret with its ordinary keys.  None: the input is already under a sparse secret.
+        self.encapsulation = encapsulation
         ctx = ev.ctx
         self.N = ctx.N
         self.n = self.N // 2
@@ -461,12 +467,23 @@ class Bootstrapper:
         return c
 
     # --- the bootstrap
+    def _switch(self, a: Ct, key) -> Ct:
+        """(c0, c1) under the key's payload secret -> (c0 + f0, f1) under its target secret."""
+        f0, f1 = self.ev.ctx.keyswitch(a.c1, key)
+        return Ct(self.ev.ctx.add_poly(a.c0, f0), f1, a.scale)
+
     def bootstrap(self, ct: Ct) -> Ct:
         ev = self.ev
         F = ev.F
-        x = ct if self.prescale == 1 else ev.mul_int(Ct(ct.c0[:1], ct.c1[:1], ct.scale), self.prescale)
+        x = Ct(ct.c0[:1], ct.c1[:1], ct.scale)
+        if self.encapsulation:
+            x = self._switch(x, self.encapsulation[0])  # dense -> sparse, at level 1
+        if self.prescale != 1:
+            x = ev.mul_int(x, self.prescale)
         # ModRaise: m -> m + q0 I at every limb of the top level
         a = Ct(ev.ctx.mod_raise_poly(x.c0[:1], self.top), ev.ctx.mod_raise_poly(x.c1[:1], self.top), self.in_scale)
+        if self.encapsulation:
+            a = self._switch(a, self.encapsulation[1])  # sparse -> dense, at the top level
         # CoeffsToSlots
         for P in self.cts_pts:
             a = self._apply(a, P)

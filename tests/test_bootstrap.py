@@ -213,3 +213,36 @@ def test_served_bootstraps_in_a_mix(fides):
         assert torch.equal(outs[("b", i)].c0, r0) and torch.equal(outs[("b", i)].c1, r1), f"bootstrap {i}"
     for i, x in enumerate(alone):
         assert torch.equal(outs[("o", i)].c0, x.c0) and torch.equal(outs[("o", i)].c1, x.c1), f"request {i}"
+
+
+@pytest.mark.gpu
+def test_bootstrap_sparse_secret_encapsulation(fides):
+    """Dense (uniform ternary) secret with sparse-secret encapsulation: the level-1 input is
+    switched to a HW-32 secret for ModRaise and back to the dense secret right after it, so
+    every other key is the dense secret's.  The result decrypts under the dense secret."""
+    from fides_b200 import params as P
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm = P.chain(12, 60, 50, 20, 4, name="boot N=2^12 dense")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    dense = KeyGen(o, seed_stream=81)
+    sparse = KeyGen(o, seed_stream=82, hamming_weight=32)
+    assert np.count_nonzero(dense.s_coeff) > 1000
+    to_sparse = F.to_device(dense.switching_key(sparse.s_eval, dense.s_eval))
+    to_dense = F.to_device(dense.switching_key(dense.s_eval, sparse.s_eval))
+    ev = B.Evaluator(F, ctx, F.to_device(dense.relin_key()), {}, F.to_device(dense.auto_key(2 * prm.N - 1)),
+                     top_scale=2.0 ** 50)
+    bs = B.Bootstrapper(ev, K=12, encapsulation=(to_sparse, to_dense))
+    ev.rot_keys = {r: F.to_device(dense.rotation_key(r)) for r in bs.needed_rotations()}
+    delta = 2.0 ** 50
+    bs.prepare(top_level=prm.n_q, msg_scale=delta)
+    rng = xrng(66)
+    n = prm.N // 2
+    z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    c0, c1 = dense.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+    out = bs.bootstrap(B.Ct(F.to_device(c0), F.to_device(c1), delta))
+    got = decode(dense.decrypt_limb0(F.to_host(out.c0), F.to_host(out.c1)), prm.N, out.scale)
+    bits = -math.log2(np.abs(got - z).max())
+    print(f"bootstrap with encapsulation N=2^12: {bits:.1f} bits, out level {out.level}")
+    assert bits > 12

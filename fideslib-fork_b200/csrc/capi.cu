@@ -296,6 +296,35 @@ int fides_mul(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uin
   return addsub(x, a, b, level, out, stream, fides::EW_MUL);
 }
 
+int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                    const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
+                    void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (n_terms < 1 || n_terms > fides::MAX_DOT_TERMS) throw fides::Error(FIDES_ERR_ARG, "need 1..32 terms");
+    need(c0s, "c0s");
+    need(c1s, "c1s");
+    need(pts, "pts");
+    need(out0, "out0");
+    need(out1, "out1");
+    fides::DotJob j{};
+    for (int t = 0; t < n_terms; ++t) {
+      need(c0s[t], "c0s[t]");
+      need(c1s[t], "c1s[t]");
+      need(pts[t], "pts[t]");
+      j.c0[t] = c0s[t];
+      j.c1[t] = c1s[t];
+      j.pt[t] = pts[t];
+    }
+    j.out0 = out0;
+    j.out1 = out1;
+    j.n = n_terms;
+    j.l = level;
+    fides::launch_dot_plain(c, j, S(stream));
+  });
+}
+
 static int scalar_op(fides_ctx* x, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
                      void* stream, int op) {
   return guard([&] {

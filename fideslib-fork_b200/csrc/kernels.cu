@@ -292,6 +292,32 @@ __global__ void __launch_bounds__(EW_THREADS) scalar_kernel(const __grid_constan
   *reinterpret_cast<ulonglong2*>(J.out + off) = r;
 }
 
+// Two adjacent coefficients per thread; sums of up to 15 products (< 2^124 each) stay below
+// 2^128 before a reduction.
+__global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_constant__ DotJob J,
+                                                               const DevPrime* primes, int logN) {
+  const int j = blockIdx.y;
+  const DevPrime p = primes[j];
+  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
+  U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
+  for (int t = 0; t < J.n; ++t) {
+    if (t && t % 15 == 0) {
+      a0 = U128{reduce128(a0, p), 0};
+      a1 = U128{reduce128(a1, p), 0};
+      b0 = U128{reduce128(b0, p), 0};
+      b1 = U128{reduce128(b1, p), 0};
+    }
+    const ulonglong2 w = ld2(J.pt[t] + off), x = ld2(J.c0[t] + off), y = ld2(J.c1[t] + off);
+    mac128(a0, w.x, x.x);
+    mac128(a1, w.y, x.y);
+    mac128(b0, w.x, y.x);
+    mac128(b1, w.y, y.y);
+  }
+  *reinterpret_cast<ulonglong2*>(J.out0 + off) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
+  *reinterpret_cast<ulonglong2*>(J.out1 + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
+}
+
 template <typename List, typename Job>
 int fill(List& L, const Job* jobs, int n) {
   L.n = n;
@@ -359,6 +385,14 @@ void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
       FIDES_CUDA(cudaGetLastError());
     }
   }
+}
+
+void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s) {
+  if (job.n < 1 || job.n > MAX_DOT_TERMS) throw Error(-1, "dot product needs 1..32 terms");
+  dim3 grid(c->N / (2 * EW_THREADS), job.l);
+  LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (3.0 * job.n + 2));
+  dot_plain_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+  FIDES_CUDA(cudaGetLastError());
 }
 
 void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {

@@ -137,4 +137,19 @@ struct ScalarJobList {
 };
 void launch_scalar(Context* c, const ScalarJob* jobs, int n, cudaStream_t s);
 
+// ---- plaintext-ciphertext inner product of a linear transform's giant step
+// (LTdotProductPtBatch / dotProductLtBatchedPt___, LimbPartitionBatch.cu:266,
+// ElemenwiseBatchKernels.cu:682-1106): out_k = sum_t pt_t * c_k,t mod q, k = 0, 1, with
+// 128-bit accumulation, one launch per giant step instead of two products and two sums per
+// diagonal.
+constexpr int MAX_DOT_TERMS = 32;
+struct DotJob {
+  const uint64_t* c0[MAX_DOT_TERMS];
+  const uint64_t* c1[MAX_DOT_TERMS];
+  const uint64_t* pt[MAX_DOT_TERMS];
+  uint64_t *out0, *out1;
+  int n, l;
+};
+void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
+
 }  // namespace fides

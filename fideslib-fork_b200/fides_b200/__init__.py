@@ -142,6 +142,7 @@ def lib():
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
+        L.fides_dot_plain.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         L.fides_add_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_mod_raise.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -431,6 +432,19 @@ class Context:
     def mul_poly(self, a, b, out=None):
         out = self.empty(a.shape[0]) if out is None else out
         _check(lib().fides_mul(self._h, _ptr(a), _ptr(b), a.shape[0], _ptr(out), _stream()))
+        return out
+
+    def dot_plain(self, cts, pts, level=None, out=None):
+        """sum_t pts[t] * cts[t] (both components, EVAL) in one launch: the plaintext inner
+        product of a linear transform's giant step.  cts: Ciphertexts, pts: polynomials with at
+        least `level` limbs (level defaults to the first ciphertext's)."""
+        n = len(cts)
+        l = cts[0].level if level is None else level
+        out = Ciphertext(self.empty(l), self.empty(l)) if out is None else out
+        c0 = (vp * n)(*[_ptr(c.c0) for c in cts])
+        c1 = (vp * n)(*[_ptr(c.c1) for c in cts])
+        pp = (vp * n)(*[_ptr(p) for p in pts])
+        _check(lib().fides_dot_plain(self._h, c0, c1, pp, n, l, _ptr(out.c0), _ptr(out.c1), _stream()))
         return out
 
     def _scalars(self, values, l):

@@ -404,18 +404,15 @@ class Bootstrapper:
         baby = dict(zip(js, ev.rotate_many(a, [(step * j) % self.n for j in js])))
         acc = None
         for i, jl in sorted(giant.items()):
-            inner = None
-            for j in jl:
-                pt = P["pts"].get((i, j))
-                if pt is None:
-                    continue
-                b = baby[j]
-                t0 = ev.ctx.mul_poly(b.c0, pt)
-                t1 = ev.ctx.mul_poly(b.c1, pt)
-                inner = (t0, t1) if inner is None else (ev.ctx.add_poly(inner[0], t0), ev.ctx.add_poly(inner[1], t1))
-            if inner is None:
+            terms = [(baby[j], P["pts"][(i, j)]) for j in jl if (i, j) in P["pts"]]
+            if not terms:
                 continue
-            part = Ct(inner[0], inner[1], a.scale)
+            inner = None
+            for k in range(0, len(terms), 32):  # one fused launch per 32 diagonals
+                chunk = terms[k:k + 32]
+                d = ev.ctx.dot_plain([t[0] for t in chunk], [t[1] for t in chunk], level=a.level)
+                inner = d if inner is None else Ct(ev.ctx.add_poly(inner.c0, d.c0), ev.ctx.add_poly(inner.c1, d.c1), 0)
+            part = Ct(inner.c0, inner.c1, a.scale)
             if i:
                 part = ev.rotate(part, (step * g * i) % self.n)
             acc = part if acc is None else ev.add_raw(acc, part)

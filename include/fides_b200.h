@@ -149,6 +149,12 @@ int fides_mul_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_
                      void* stream);
 int fides_add_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
                      void* stream);
+/* Plaintext-ciphertext inner product of a linear transform's giant step:
+ * out0 = sum_t pts[t] * c0s[t], out1 = sum_t pts[t] * c1s[t] (EVAL, mod q, level limbs),
+ * 1 <= n_terms <= 32, one launch (LTdotProductPtBatch, LimbPartitionBatch.cu:266). */
+int fides_dot_plain(fides_ctx* ctx, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                    const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
+                    void* stream);
 /* ModRaise of one level-1 polynomial (limb q_0, EVAL) to out_level limbs: INTT, centred
  * SwitchModulus(q_0 -> q_j), NTT (reference Bootstrap.cu ModRaise, src/CKKS/Bootstrap.cu:708+). */
 int fides_mod_raise(fides_ctx* ctx, const uint64_t* x, int out_level, uint64_t* out, void* stream);

@@ -261,6 +261,29 @@ def test_host_entry_points(Cfg):
         Cfg.ctx.key_free(rk)
 
 
+@pytest.mark.parametrize("terms,level", [(1, 30), (15, 17), (16, 30), (32, 5)])
+def test_dot_plain_config_c(Cfg, terms, level):
+    """The fused plaintext inner product of a linear transform's giant step equals the
+    oracle's sum of elementwise products, residue for residue (1 term, the 15-term reduction
+    boundary, one past it, and the 32-term maximum)."""
+    ids = list(range(level))
+    cts = [Cfg.rand_ct(level, 1000 + t) for t in range(terms)]
+    pts = [uniform_limbs(xrng(1100 + t), Cfg.prm.q[:level], Cfg.o.N) for t in range(terms)]
+    ref = [None, None]
+    for (c0, c1), pt in zip(cts, pts):
+        for k, c in enumerate((c0, c1)):
+            m = Cfg.o.mul(c, pt, ids)
+            ref[k] = m if ref[k] is None else Cfg.o.add(ref[k], m, ids)
+    got = Cfg.ctx.dot_plain([Cfg.dev_ct(c) for c in cts], [Cfg.F.to_device(p) for p in pts])
+    assert eq(got.c0, ref[0]) and eq(got.c1, ref[1])
+
+
+def test_dot_plain_rejects_bad_terms(Cfg):
+    c = Cfg.dev_ct(Cfg.rand_ct(4, 2))
+    with pytest.raises(Cfg.F.FidesError):
+        Cfg.ctx.dot_plain([c] * 33, [c.c0] * 33)
+
+
 def test_error_statuses(Cfg):
     F = Cfg.F
     c = Cfg.dev_ct(Cfg.rand_ct(4, 1))

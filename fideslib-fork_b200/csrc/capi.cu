@@ -325,6 +325,70 @@ int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* co
   });
 }
 
+int fides_lincomb(fides_ctx* x, int n_lanes, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                  const uint64_t* scalars, const uint64_t* add0, int n_terms, int level, uint64_t* const* out0s,
+                  uint64_t* const* out1s, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (level < 1 || level > c->n_q || level > fides::MAX_LC_LIMBS)
+      throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (n_terms < 1 || n_terms > fides::MAX_LC_TERMS) throw fides::Error(FIDES_ERR_ARG, "need 1..16 terms");
+    if (n_lanes < 1 || n_lanes > fides::MAX_LC_LANES) throw fides::Error(FIDES_ERR_ARG, "need 1..8 lanes");
+    need(c0s, "c0s");
+    need(c1s, "c1s");
+    need(scalars, "scalars");
+    need(out0s, "out0s");
+    need(out1s, "out1s");
+    static thread_local fides::LinCombJob j;
+    for (int a = 0; a < n_lanes; ++a) {
+      need(out0s[a], "out0s[lane]");
+      need(out1s[a], "out1s[lane]");
+      j.out0[a] = out0s[a];
+      j.out1[a] = out1s[a];
+      for (int t = 0; t < n_terms; ++t) {
+        const int k = a * n_terms + t;
+        need(c0s[k], "c0s[lane * n_terms + t]");
+        need(c1s[k], "c1s[lane * n_terms + t]");
+        j.x0[a][t] = c0s[k];
+        j.x1[a][t] = c1s[k];
+      }
+    }
+    for (int t = 0; t < n_terms; ++t)
+      for (int i = 0; i < level; ++i) {
+        const uint64_t v = scalars[(size_t)t * level + i];
+        if (v >= c->primes[i]) throw fides::Error(FIDES_ERR_ARG, "scalar not reduced mod q_i");
+        j.s[t][i] = v;
+      }
+    for (int i = 0; i < level; ++i) {
+      const uint64_t v = add0 ? add0[i] : 0;
+      if (v >= c->primes[i]) throw fides::Error(FIDES_ERR_ARG, "add0 not reduced mod q_i");
+      j.add0[i] = v;
+    }
+    j.n = n_terms;
+    j.l = level;
+    j.lanes = n_lanes;
+    fides::launch_lincomb(c, j, S(stream));
+  });
+}
+
+int fides_rescale_batch(fides_ctx* x, const uint64_t* const* xs, const int* levels, uint64_t* const* outs, int n,
+                        void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "n < 0");
+    if (n == 0) return;
+    need(xs, "xs");
+    need(levels, "levels");
+    need(outs, "outs");
+    for (int i = 0; i < n; ++i) {
+      need(xs[i], "xs[i]");
+      need(outs[i], "outs[i]");
+      if (levels[i] < 2 || levels[i] > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    }
+    fides::op_rescale_batch(c, xs, levels, outs, n, S(stream));
+  });
+}
+
 static int scalar_op(fides_ctx* x, const uint64_t* a, int level, const uint64_t* scalars, uint64_t* out,
                      void* stream, int op) {
   return guard([&] {

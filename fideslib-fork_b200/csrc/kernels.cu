@@ -318,6 +318,33 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
   *reinterpret_cast<ulonglong2*>(J.out1 + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
 }
 
+__global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
+                                                             const DevPrime* primes, int logN) {
+  const int j = blockIdx.y, lane = blockIdx.z;
+  const DevPrime p = primes[j];
+  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
+  U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
+  for (int t = 0; t < J.n; ++t) {
+    if (t && t % 15 == 0) {
+      a0 = U128{reduce128(a0, p), 0};
+      a1 = U128{reduce128(a1, p), 0};
+      b0 = U128{reduce128(b0, p), 0};
+      b1 = U128{reduce128(b1, p), 0};
+    }
+    const uint64_t w = J.s[t][j];
+    const ulonglong2 x = ld2(J.x0[lane][t] + off), y = ld2(J.x1[lane][t] + off);
+    mac128(a0, w, x.x);
+    mac128(a1, w, x.y);
+    mac128(b0, w, y.x);
+    mac128(b1, w, y.y);
+  }
+  const uint64_t ad = J.add0[j];
+  *reinterpret_cast<ulonglong2*>(J.out0[lane] + off) =
+      make_ulonglong2(addmod(reduce128(a0, p), ad, p.q), addmod(reduce128(a1, p), ad, p.q));
+  *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
+}
+
 template <typename List, typename Job>
 int fill(List& L, const Job* jobs, int n) {
   L.n = n;
@@ -392,6 +419,16 @@ void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s) {
   dim3 grid(c->N / (2 * EW_THREADS), job.l);
   LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (3.0 * job.n + 2));
   dot_plain_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+  FIDES_CUDA(cudaGetLastError());
+}
+
+void launch_lincomb(Context* c, const LinCombJob& job, cudaStream_t s) {
+  if (job.n < 1 || job.n > MAX_LC_TERMS || job.l < 1 || job.l > MAX_LC_LIMBS || job.lanes < 1 ||
+      job.lanes > MAX_LC_LANES)
+    throw Error(-1, "linear combination needs 1..16 terms of 1..64 limbs in 1..8 lanes");
+  dim3 grid(c->N / (2 * EW_THREADS), job.l, job.lanes);
+  LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * job.lanes * (2.0 * job.n + 2));
+  lincomb_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
   FIDES_CUDA(cudaGetLastError());
 }
 

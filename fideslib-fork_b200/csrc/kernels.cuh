@@ -152,4 +152,26 @@ struct DotJob {
 };
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 
+// ---- ciphertext linear combination with per-limb integer constants:
+// out0 = sum_t s_t * x0_t + add0, out1 = sum_t s_t * x1_t (mod q_j per limb j).  The scalar
+// steps of a Chebyshev series in one launch: the weighted sums of the Paterson-Stockmeyer
+// leaves (evalPartialLinearWSumFused, ApproxModEval.cu:272, inside innerEvalChebyshevPS,
+// ApproxModEval.cu:341) and the 2 T_a T_b - T_c recurrence combinations, instead of a
+// multiply and an add launch per term.  Lanes: the same constants applied to up to 8
+// independent sets of operands (one grid z slice each), e.g. the real and imaginary halves
+// of EvalMod.
+constexpr int MAX_LC_TERMS = 16;
+constexpr int MAX_LC_LIMBS = 64;
+constexpr int MAX_LC_LANES = 8;
+struct LinCombJob {
+  const uint64_t* x0[MAX_LC_LANES][MAX_LC_TERMS];
+  const uint64_t* x1[MAX_LC_LANES][MAX_LC_TERMS];
+  uint64_t* out0[MAX_LC_LANES];
+  uint64_t* out1[MAX_LC_LANES];
+  uint64_t s[MAX_LC_TERMS][MAX_LC_LIMBS];
+  uint64_t add0[MAX_LC_LIMBS];
+  int n, l, lanes;
+};
+void launch_lincomb(Context* c, const LinCombJob& job, cudaStream_t s);
+
 }  // namespace fides

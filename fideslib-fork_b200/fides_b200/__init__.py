@@ -143,6 +143,8 @@ def lib():
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_dot_plain.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        L.fides_lincomb.argtypes = [vp, C.c_int, vp, vp, u64p, u64p, C.c_int, C.c_int, vp, vp, vp]
+        L.fides_rescale_batch.argtypes = [vp, vp, vp, vp, C.c_int, vp]
         L.fides_add_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_mod_raise.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -364,7 +366,19 @@ class Context:
         return out
 
     def rescale(self, ct: Ciphertext) -> Ciphertext:
-        return Ciphertext(self.rescale_poly(ct.c0), self.rescale_poly(ct.c1))
+        return Ciphertext(*self.rescale_many([ct.c0, ct.c1]))
+
+    def rescale_many(self, polys) -> list:
+        """Rescale of several polynomials (any levels >= 2) in one launch sequence."""
+        n = len(polys)
+        if n == 0:
+            return []
+        outs = [self.empty(x.shape[0] - 1) for x in polys]
+        xs = (vp * n)(*[_ptr(x) for x in polys])
+        os_ = (vp * n)(*[_ptr(o) for o in outs])
+        ls = (C.c_int * n)(*[x.shape[0] for x in polys])
+        _check(lib().fides_rescale_batch(self._h, xs, ls, os_, n, _stream()))
+        return outs
 
     def mult(self, a: Ciphertext, b: Ciphertext, relin_key, rescale=True, out: Ciphertext | None = None) -> Ciphertext:
         l = a.level
@@ -446,6 +460,28 @@ class Context:
         pp = (vp * n)(*[_ptr(p) for p in pts])
         _check(lib().fides_dot_plain(self._h, c0, c1, pp, n, l, _ptr(out.c0), _ptr(out.c1), _stream()))
         return out
+
+    def lincomb(self, cts, scalars, add0=None, level=None):
+        """sum_t scalars[t] * cts[t] (+ add0 on c0) over `level` limbs in one launch.  scalars[t]
+        and add0: an integer (reduced mod every q_i) or one residue per limb."""
+        return self.lincomb_lanes([cts], scalars, add0, level)[0]
+
+    def lincomb_lanes(self, lanes, scalars, add0=None, level=None):
+        """The same combination over several lanes (lists of ciphertexts, one list per lane,
+        all of the same length): one launch, one output Ciphertext per lane."""
+        import numpy as np
+        n, m = len(lanes[0]), len(lanes)
+        l = min(c.level for cts in lanes for c in cts) if level is None else level
+        outs = [Ciphertext(self.empty(l), self.empty(l)) for _ in range(m)]
+        s = np.stack([self._scalars(v, l) for v in scalars])
+        a = None if add0 is None else self._scalars(add0, l)
+        c0 = (vp * (n * m))(*[_ptr(c.c0) for cts in lanes for c in cts])
+        c1 = (vp * (n * m))(*[_ptr(c.c1) for cts in lanes for c in cts])
+        o0 = (vp * m)(*[_ptr(o.c0) for o in outs])
+        o1 = (vp * m)(*[_ptr(o.c1) for o in outs])
+        _check(lib().fides_lincomb(self._h, m, c0, c1, s.ctypes.data_as(u64p),
+                                   None if a is None else a.ctypes.data_as(u64p), n, l, o0, o1, _stream()))
+        return outs
 
     def _scalars(self, values, l):
         import numpy as np

@@ -170,20 +170,26 @@ class Evaluator:
 
     def to_level(self, a: Ct, level: int) -> Ct:
         """Bring `a` to `level` at that level's canonical scale S_level."""
+        return self.to_level_many([a], level)[0]
+
+    def to_level_many(self, cts: list, level: int) -> list:
+        """to_level on several ciphertexts of one level and scale: discard down to level + 1
+        limbs, multiply by the integer c with scale * c / q_level = S_level, rescale by q_level
+        (one combination launch and one batched rescale for all of them)."""
+        a = cts[0]
         if a.level == level and abs(a.scale / self.S[level] - 1) < 1e-15:
-            return a
+            return list(cts)
         if a.level <= level:
             raise ValueError(f"cannot raise level {a.level} -> {level}")
-        # integer constant c with a.scale * c / q_top = S_level, then rescale, then discard
-        qt = self.q[a.level - 1]
-        c = round(self.S[level] * qt / a.scale)
-        b = self._rescale_to(self.mul_int(a, c), self.S[level])
-        return self.drop(b, level)
+        c = round(self.S[level] * self.q[level] / a.scale)
+        return self._rescale_many_to(self.lincomb_many([[self.drop(b, level + 1)] for b in cts], [c]), self.S[level])
 
     def _rescale_to(self, a: Ct, new_scale: float) -> Ct:
-        c0 = self.ctx.rescale_poly(a.c0)
-        c1 = self.ctx.rescale_poly(a.c1)
-        return Ct(c0, c1, new_scale)
+        return self._rescale_many_to([a], new_scale)[0]
+
+    def _rescale_many_to(self, cts: list, new_scale: float) -> list:
+        outs = self.ctx.rescale_many([p for a in cts for p in (a.c0, a.c1)])
+        return [Ct(outs[2 * i], outs[2 * i + 1], new_scale) for i in range(len(cts))]
 
     def rescale(self, a: Ct) -> Ct:
         return self._rescale_to(a, a.scale / self.q[a.level - 1])
@@ -205,6 +211,61 @@ class Evaluator:
     def add_const(self, a: Ct, value: float) -> Ct:
         v = round(value * a.scale)
         return Ct(self.ctx.add_scalar_poly(a.c0, [v % q for q in self.q[:a.level]]), a.c1, a.scale)
+
+    def lincomb(self, terms, const: float = 0.0) -> Ct:
+        """sum_t c_t * a_t + const for integer c_t, operands at one level and scale (one
+        launch; the scale is kept)."""
+        return self.lincomb_many([[a for a, _ in terms]], [c for _, c in terms], const)[0]
+
+    def lincomb_many(self, lanes: list, ints: list, const: float = 0.0) -> list:
+        """The same integer combination sum_t ints[t] * lane[t] + const on every lane (a list of
+        ciphertexts of one level and scale per lane): one launch for all lanes."""
+        a = lanes[0][0]
+        l = min(b.level for lane in lanes for b in lane)
+        add = round(const * a.scale) if const else None
+        outs = self.ctx.lincomb_lanes(lanes, ints, add0=add, level=l)
+        return [Ct(o.c0, o.c1, a.scale) for o in outs]
+
+    def add_many(self, xs: list, ys: list) -> list:
+        """x + y lane by lane (same level and scale), one launch."""
+        return self.lincomb_many([[x, y] for x, y in zip(xs, ys)], [1, 1])
+
+    def lincomb_to(self, terms, const: float, target: int) -> Ct:
+        return self.lincomb_to_many([[a for a, _ in terms]], [v for _, v in terms], const, target)[0]
+
+    def lincomb_to_many(self, lanes: list, coefs: list, const: float, target: int) -> list:
+        """sum_t coefs[t] * lane[t] + const for real coefficients, landing at `target` limbs
+        with scale S_target on every lane: operand t (any level > target, any scale, the same
+        on every lane) is read on its first target + 1 limbs and multiplied by the integer
+        round(coefs[t] S_target q_target / scale_t); the sum is rescaled by q_target (one
+        combination launch and one batched rescale for all lanes)."""
+        qt, S = self.q[target], self.S[target]
+        keep, ints = [], []
+        for t, v in enumerate(coefs):
+            a = lanes[0][t]
+            if a.level <= target:
+                raise ValueError(f"operand at level {a.level} cannot land at level {target}")
+            c = round(v * S * qt / a.scale)
+            if c:
+                keep.append(t)
+                ints.append(c)
+        if not keep:  # constant only: a zero combination of the first operand carries it
+            keep, ints = [0], [0]
+        add = round(const * S * qt)
+        outs = self.ctx.lincomb_lanes([[lane[t] for t in keep] for lane in lanes], ints,
+                                      add0=add if add else None, level=target + 1)
+        return self._rescale_many_to([Ct(o.c0, o.c1, 0.0) for o in outs], S)
+
+    def mul_many(self, pairs) -> list[Ct]:
+        """a * b (relinearised, rescaled) for several pairs in one batched launch sequence;
+        each pair is brought to its lower level first."""
+        F = self.F
+        ab = []
+        for a, b in pairs:
+            l = min(a.level, b.level)
+            ab.append((self.to_level(a, l), self.to_level(b, l)))
+        outs = self.ctx.mult_batch([(F.Ciphertext(a.c0, a.c1), F.Ciphertext(b.c0, b.c1)) for a, b in ab], self.rk)
+        return [Ct(o.c0, o.c1, self.S[a.level - 1]) for o, (a, _) in zip(outs, ab)]
 
     def mul_int(self, a: Ct, c: int) -> Ct:
         vals = [c % q for q in self.q[:a.level]]
@@ -253,6 +314,15 @@ class Evaluator:
 
     def rotate(self, a: Ct, r: int) -> Ct:
         return self.rotate_many(a, [r])[0]
+
+    def rotate_batch(self, jobs) -> list[Ct]:
+        """Rotations of several ciphertexts (jobs: (ciphertext, rotation), rotation != 0 mod
+        slots) in one batched key switch."""
+        if not jobs:
+            return []
+        F = self.F
+        outs = self.ctx.rotate_batch([(F.Ciphertext(a.c0, a.c1), self.rot_keys[r], r) for a, r in jobs])
+        return [Ct(o.c0, o.c1, a.scale) for o, (a, _) in zip(outs, jobs)]
 
 
 # ------------------------------------------------------------------------------ bootstrapper
@@ -402,7 +472,7 @@ class Bootstrapper:
         assert a.level == P["level"], (a.level, P["level"])
         js = sorted({j for v in giant.values() for j in v})
         baby = dict(zip(js, ev.rotate_many(a, [(step * j) % self.n for j in js])))
-        acc = None
+        parts, turns = [], []
         for i, jl in sorted(giant.items()):
             terms = [(baby[j], P["pts"][(i, j)]) for j in jl if (i, j) in P["pts"]]
             if not terms:
@@ -411,57 +481,100 @@ class Bootstrapper:
             for k in range(0, len(terms), 32):  # one fused launch per 32 diagonals
                 chunk = terms[k:k + 32]
                 d = ev.ctx.dot_plain([t[0] for t in chunk], [t[1] for t in chunk], level=a.level)
-                inner = d if inner is None else Ct(ev.ctx.add_poly(inner.c0, d.c0), ev.ctx.add_poly(inner.c1, d.c1), 0)
-            part = Ct(inner.c0, inner.c1, a.scale)
-            if i:
-                part = ev.rotate(part, (step * g * i) % self.n)
-            acc = part if acc is None else ev.add_raw(acc, part)
-        return ev._rescale_to(acc, ev.S[a.level - 1])
+                d = Ct(d.c0, d.c1, a.scale)
+                inner = d if inner is None else ev.add_many([inner], [d])[0]
+            r = (step * g * i) % self.n
+            (turns if r else parts).append((inner, r))
+        # every giant-step rotation in one batched key switch, then one sum and one rescale
+        parts = [p for p, _ in parts] + ev.rotate_batch(turns)
+        while len(parts) > 1:
+            parts = [ev.lincomb_many([parts[k:k + 16]], [1] * len(parts[k:k + 16]))[0] if len(parts[k:k + 16]) > 1
+                     else parts[k] for k in range(0, len(parts), 16)]
+        return ev._rescale_to(parts[0], ev.S[a.level - 1])
 
     # --- EvalMod
-    def _chebyshev(self, t: Ct) -> Ct:
-        ev, d = self.ev, self.degree
-        T = {1: t}
-        l0 = t.level
+    # Paterson-Stockmeyer leaves: Chebyshev series of degree < 16.  The error of a power
+    # computed by doubling grows ~4x per doubling (T_8 is 2 bits worse than T_4), and with
+    # leaves of degree < 8 the large coefficients c_8..c_15 of the EvalMod cosine would ride on
+    # the error of T_8 (1.2 bits lost at N = 2^16); with 16 they multiply powers computed
+    # directly, as in a term-by-term sum, at 3 more HMults.
+    PS_BABY = 16
 
-        def get(k):
-            if k in T:
-                return T[k]
+    def _cheb_powers(self, ts: list) -> dict:
+        """T_1..T_16 and the giant powers T_32, T_64, ... (<= degree) of every lane, each at its
+        natural level: T_2k = 2 T_k^2 - 1, T_2k+1 = 2 T_k T_k+1 - T_1 (one batched HMult and
+        one combination launch over the lanes per power)."""
+        ev = self.ev
+        T = {1: list(ts)}
+
+        def make(k):
             if k % 2 == 0:
-                h = get(k // 2)
-                x = ev.square(h)
-                x = ev.add_raw(x, x)
-                x = ev.add_const(x, -1.0)
+                x = ev.mul_many([(a, a) for a in T[k // 2]])
+                T[k] = ev.lincomb_many([[p] for p in x], [2], const=-1.0)
             else:
-                a, b = get(k // 2), get(k // 2 + 1)
-                x = ev.mul(a, b)
-                x = ev.add_raw(x, x)
-                one = ev.to_level(T[1], x.level)
-                x = ev.sub_raw(x, one)
-            T[k] = x
-            return x
+                x = ev.mul_many(list(zip(T[k // 2], T[k // 2 + 1])))
+                one = self._t_at(T, 1, x[0].level)
+                T[k] = ev.lincomb_many([[p, o] for p, o in zip(x, one)], [2, -1])
 
-        for k in range(2, d + 1):
-            get(k)
-        final = min(T[k].level for k in T) - 1
-        acc = None
-        for k in range(1, d + 1):
-            c = float(self.cheb[k])
-            if abs(c) < 1e-18:
-                continue
-            term = ev.mul_const(T[k], c, final)
-            acc = term if acc is None else ev.add_raw(acc, term)
-        acc = ev.add_const(acc, float(self.cheb[0]))
-        return acc
+        for k in range(2, self.PS_BABY + 1):
+            make(k)
+        m = 2 * self.PS_BABY
+        while m <= self.degree:
+            make(m)
+            m *= 2
+        return T
+
+    def _t_at(self, T: dict, k: int, level: int) -> list:
+        """T_k of every lane brought to `level` at its canonical scale (cached)."""
+        cache = T.setdefault("at", {})
+        if (k, level) not in cache:
+            cache[(k, level)] = self.ev.to_level_many(T[k], level)
+        return cache[(k, level)]
+
+    def _ps(self, coeffs: np.ndarray, level_out: int, T: dict, lanes: int) -> list:
+        """Chebyshev series sum_i coeffs[i] T_i at `level_out` (scale S_level_out) by
+        Paterson-Stockmeyer (innerEvalChebyshevPS, src/CKKS/ApproxModEval.cu:341): split
+        p = q T_m + r at the largest power of two m < deg p + 1 using T_(m+j) = 2 T_m T_j - T_(m-j);
+        q lands one level higher and is multiplied by T_m, r lands at level_out; series of degree
+        < PS_BABY are one weighted sum of T_0..T_(PS_BABY-1) (evalPartialLinearWSum,
+        ApproxModEval.cu:328)."""
+        ev, n = self.ev, len(coeffs)
+        if n <= self.PS_BABY:
+            ks = list(range(1, n)) or [1]
+            cf = [float(coeffs[k]) if k < n else 0.0 for k in ks]
+            return ev.lincomb_to_many([[T[k][i] for k in ks] for i in range(lanes)], cf, float(coeffs[0]), level_out)
+        m = 1 << ((n - 1).bit_length() - 1)
+        q = np.zeros(n - m)
+        r = np.array(coeffs[:m], dtype=np.float64)
+        q[0] = coeffs[m]
+        for j in range(1, n - m):
+            q[j] = 2 * coeffs[m + j]
+            r[m - j] -= coeffs[m + j]
+        qc = self._ps(q, level_out + 1, T, lanes)
+        prod = ev.mul_many(list(zip(qc, self._t_at(T, m, level_out + 1))))
+        rc = self._ps(r, level_out, T, lanes)
+        return ev.add_many(prod, rc)
+
+    def _chebyshev_many(self, ts: list) -> list:
+        """The EvalMod series at every lane (one ciphertext per lane, same level and scale)."""
+        T = self._cheb_powers(ts)
+        depth = math.ceil(math.log2(self.degree)) + 1
+        return self._ps(np.asarray(self.cheb, dtype=np.float64), ts[0].level - depth, T, len(ts))
+
+    def _chebyshev(self, t: Ct) -> Ct:
+        return self._chebyshev_many([t])[0]
+
+    def _eval_mod_many(self, ts: list) -> list:
+        """EvalMod (Chebyshev series of the scaled cosine, then r double-angle steps
+        c -> 2 c^2 - 1) on several ciphertexts at once, each step batched over them."""
+        ev = self.ev
+        cs = self._chebyshev_many(ts)
+        for _ in range(self.r):
+            cs = ev.lincomb_many([[x] for x in ev.mul_many([(c, c) for c in cs])], [2], const=-1.0)
+        return cs
 
     def _eval_mod(self, t: Ct) -> Ct:
-        ev = self.ev
-        c = self._chebyshev(t)
-        for _ in range(self.r):
-            x = ev.square(c)
-            x = ev.add_raw(x, x)
-            c = ev.add_const(x, -1.0)
-        return c
+        return self._eval_mod_many([t])[0]
 
     # --- the bootstrap
     def _switch(self, a: Ct, key) -> Ct:
@@ -489,8 +602,7 @@ class Bootstrapper:
         t_re = ev.add_raw(a, cj)
         t_im = ev.mul_plain_int(ev.sub_raw(a, cj), self.pt_minus_i)
         # EvalMod on both, then recombine u = s_re + i s_im
-        s_re = self._eval_mod(t_re)
-        s_im = self._eval_mod(t_im)
+        s_re, s_im = self._eval_mod_many([t_re, t_im])
         s_re = ev.to_level(s_re, self.stc_in_level)
         s_im = ev.to_level(s_im, self.stc_in_level)
         u = ev.add_raw(s_re, ev.mul_plain_int(s_im, self.pt_i))

@@ -155,6 +155,21 @@ int fides_add_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_
 int fides_dot_plain(fides_ctx* ctx, const uint64_t* const* c0s, const uint64_t* const* c1s,
                     const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
                     void* stream);
+/* Ciphertext linear combination with integer constants (EVAL, level limbs), over n_lanes
+ * independent operand sets that share the constants:
+ *   out0s[a] = sum_t s_t * c0s[a * n_terms + t] + add0,  out1s[a] = sum_t s_t * c1s[a * n_terms + t]
+ * where scalars holds n_terms x level residues (row t = s_t mod q_0..q_(level-1)) and add0
+ * level residues (or NULL).  1 <= n_terms <= 16, 1 <= n_lanes <= 8, level <= 64; one launch.
+ * The scalar steps of the Chebyshev series evaluation (evalPartialLinearWSum,
+ * src/CKKS/ApproxModEval.cu:328; multConst / addConst per term in the reference). */
+int fides_lincomb(fides_ctx* ctx, int n_lanes, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                  const uint64_t* scalars, const uint64_t* add0, int n_terms, int level, uint64_t* const* out0s,
+                  uint64_t* const* out1s, void* stream);
+/* Rescale of n polynomials, polynomial i at levels[i] limbs -> levels[i] - 1 limbs, in one
+ * launch sequence (a batched fides_rescale; Ciphertext::rescale per ciphertext in the
+ * reference, src/CKKS/Ciphertext.cpp:569-607).  An output may not overlap another input. */
+int fides_rescale_batch(fides_ctx* ctx, const uint64_t* const* xs, const int* levels, uint64_t* const* outs, int n,
+                        void* stream);
 /* ModRaise of one level-1 polynomial (limb q_0, EVAL) to out_level limbs: INTT, centred
  * SwitchModulus(q_0 -> q_j), NTT (reference Bootstrap.cu ModRaise, src/CKKS/Bootstrap.cu:708+). */
 int fides_mod_raise(fides_ctx* ctx, const uint64_t* x, int out_level, uint64_t* out, void* stream);

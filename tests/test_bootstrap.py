@@ -80,6 +80,31 @@ def test_bootstrap_precision_n4096(fides):
 
 
 @pytest.mark.gpu
+def test_chebyshev_paterson_stockmeyer(fides):
+    """The EvalMod series evaluated by Paterson-Stockmeyer over two lanes decrypts to the FP64
+    Chebyshev sum of the slots, lands ceil(log2 d) + 1 levels down, and each lane equals the
+    same series evaluated alone (lanes are independent)."""
+    from fides_b200 import bootstrap as B
+    prm, o, kg, ctx, ev, bs = make_boot(fides, 12)
+    N, n, l = prm.N, prm.N // 2, prm.n_q
+    zs, cts = [], []
+    for i in range(2):
+        z = xrng(70 + i).uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z.astype(np.complex128), N, ev.S[l]).astype(np.int64), l)
+        zs.append(z)
+        cts.append(B.Ct(fides.to_device(c0), fides.to_device(c1), ev.S[l]))
+    outs = bs._chebyshev_many(cts)
+    alone = bs._chebyshev(cts[1])
+    assert outs[0].level == l - (math.ceil(math.log2(bs.degree)) + 1)
+    for z, out in zip(zs, outs):
+        got = decode(kg.decrypt_limb0(fides.to_host(out.c0), fides.to_host(out.c1)), N, out.scale)
+        ref = np.polynomial.chebyshev.chebval(z, bs.cheb)
+        assert -math.log2(np.abs(got - ref).max()) > 20
+    assert np.array_equal(fides.to_host(alone.c0), fides.to_host(outs[1].c0))
+    assert np.array_equal(fides.to_host(alone.c1), fides.to_host(outs[1].c1))
+
+
+@pytest.mark.gpu
 def test_bootstrap_graph_replay_is_bit_identical(fides):
     import torch
     from fides_b200 import bootstrap as B

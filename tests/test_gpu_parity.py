@@ -278,6 +278,41 @@ def test_dot_plain_config_c(Cfg, terms, level):
     assert eq(got.c0, ref[0]) and eq(got.c1, ref[1])
 
 
+@pytest.mark.parametrize("terms,level", [(1, 30), (15, 17), (16, 5)])
+def test_lincomb_config_c(Cfg, terms, level):
+    """sum_t s_t * ct_t + add0 with per-limb integer constants equals the oracle's products
+    and sums residue for residue (add0 on c0 only)."""
+    N, q = Cfg.o.N, Cfg.prm.q[:level]
+    ids = list(range(level))
+    rng = xrng(1200 + terms)
+    cts = [Cfg.rand_ct(level, 1300 + t) for t in range(terms)]
+    scal = [[int(rng.integers(0, qi)) for qi in q] for _ in range(terms)]
+    add = [int(rng.integers(0, qi)) for qi in q]
+    bc = lambda v: np.repeat(np.array(v, dtype=np.uint64)[:, None], N, axis=1)
+    ref = [bc(add), np.zeros((level, N), dtype=np.uint64)]
+    for (c0, c1), sv in zip(cts, scal):
+        ref = [Cfg.o.add(ref[k], Cfg.o.mul(c, bc(sv), ids), ids) for k, c in enumerate((c0, c1))]
+    got = Cfg.ctx.lincomb([Cfg.dev_ct(c) for c in cts], scal, add0=add, level=level)
+    assert eq(got.c0, ref[0]) and eq(got.c1, ref[1])
+
+
+def test_lincomb_lanes_and_rescale_batch(Cfg):
+    """Lanes of one combination launch equal the combination run lane by lane, and a batched
+    rescale of polynomials at mixed levels equals the oracle's rescale of each."""
+    F, l = Cfg.F, 12
+    rng = xrng(1400)
+    lanes = [[Cfg.dev_ct(Cfg.rand_ct(l, 1410 + 4 * a + t)) for t in range(4)] for a in range(3)]
+    scal = [[int(rng.integers(0, qi)) for qi in Cfg.prm.q[:l]] for _ in range(4)]
+    outs = Cfg.ctx.lincomb_lanes(lanes, scal, add0=7, level=l)
+    for lane, o in zip(lanes, outs):
+        one = Cfg.ctx.lincomb(lane, scal, add0=7, level=l)
+        assert torch.equal(one.c0, o.c0) and torch.equal(one.c1, o.c1)
+    polys = [Cfg.rand_ct(lv, 1450 + lv)[0] for lv in (30, 17, 2)]
+    got = Cfg.ctx.rescale_many([F.to_device(x) for x in polys])
+    for x, g in zip(polys, got):
+        assert eq(g, Cfg.o.rescale(x))
+
+
 def test_dot_plain_rejects_bad_terms(Cfg):
     c = Cfg.dev_ct(Cfg.rand_ct(4, 2))
     with pytest.raises(Cfg.F.FidesError):

@@ -12,6 +12,7 @@
 #include "autotune.hpp"
 #include "capi_internal.hpp"
 #include "context.hpp"
+#include "encode.hpp"
 #include "kernels.cuh"
 #include "ntt.cuh"
 #include "ops.hpp"
@@ -386,6 +387,26 @@ int fides_rescale_batch(fides_ctx* x, const uint64_t* const* xs, const int* leve
       if (levels[i] < 2 || levels[i] > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
     }
     fides::op_rescale_batch(c, xs, levels, outs, n, S(stream));
+  });
+}
+
+int fides_encode(fides_ctx* x, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
+                 void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(slots, "slots");
+    need(out, "out");
+    fides::op_encode(c, slots, n_slots, n_pts, scale, level, out, S(stream));
+  });
+}
+
+int fides_decode(fides_ctx* x, const uint64_t* pts, int level, int n_pts, int n_slots, double scale, double* slots,
+                 void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(pts, "pts");
+    need(slots, "slots");
+    fides::op_decode(c, pts, level, n_pts, n_slots, scale, slots, S(stream));
   });
 }
 

@@ -8,6 +8,7 @@
 //   - ModDown tables PHatInvModp / PHatModq / PInvModq (ConstantsGPU.cu:480-534);
 //   - rescale constants q_l^-1 and QlQlInvModqlDivqlModq (RawCiphertext.cu:318-440), the
 //     latter equal to -q_l^-1 mod q_j because q_j divides Q_{l-1}.
+#include <cmath>
 #include <algorithm>
 #include <cstring>
 #include <thread>
@@ -406,6 +407,23 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     FIDES_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr));
     FIDES_CUDA(cudaMalloc(&c->d_status, sizeof(uint32_t)));
     FIDES_CUDA(cudaMemset(c->d_status, 0, sizeof(uint32_t)));
+    // ---- special-FFT twiddles for slot encode / decode (stage len = 2h, position j < h)
+    {
+      const size_t nh = (size_t)c->N / 2;
+      std::vector<double> tw(2 * nh, 0.0);
+      for (size_t h = 1; h < nh; h <<= 1) {
+        const uint64_t m4 = 8 * h;  // 4 len
+        uint64_t e = 1;             // 5^j mod 4 len
+        for (size_t j = 0; j < h; ++j) {
+          const double ang = -2.0 * M_PI * (double)e / (double)m4;
+          tw[2 * (h + j)] = std::cos(ang);
+          tw[2 * (h + j) + 1] = std::sin(ang);
+          e = (e * 5) % m4;
+        }
+      }
+      FIDES_CUDA(cudaMalloc(&c->d_sfft, tw.size() * sizeof(double)));
+      FIDES_CUDA(cudaMemcpy(c->d_sfft, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
   } catch (...) {
     destroy_context(c);
     throw;
@@ -424,6 +442,7 @@ void destroy_context(Context* c) {
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->d_tables) cudaFree(c->d_tables);
   if (c->d_status) cudaFree(c->d_status);
+  if (c->d_sfft) cudaFree(c->d_sfft);
   if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }

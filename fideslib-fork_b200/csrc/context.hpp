@@ -104,7 +104,11 @@ struct Context {
   uint8_t ntt_g[2][2][4] = {{{4, 8, 16, 16}, {4, 8, 16, 16}}, {{4, 8, 16, 16}, {4, 8, 16, 16}}};
   static int ntt_size_class(int limbs) { return limbs <= 8 ? 0 : limbs <= 32 ? 1 : limbs <= 128 ? 2 : 3; }
   int ntt_shape(bool inverse, int pass, int limbs) const { return ntt_g[inverse][pass][ntt_size_class(limbs)]; }
-  uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up
+  uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up,
+                                 // bit 1 = an encoded coefficient exceeded q_0 / 2
+  // special-FFT twiddles of the slot encoder, [N/2] (double, double) pairs: entry h + j
+  // (h = len / 2, j < h) = exp(-2 pi i (5^j mod 4 len) / (4 len))
+  void* d_sfft = nullptr;
 
   // scratch: stream-ordered allocations from the device's memory pool
   cudaMemPool_t pool = nullptr;

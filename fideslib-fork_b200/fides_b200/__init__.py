@@ -145,6 +145,8 @@ def lib():
         L.fides_dot_plain.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         L.fides_lincomb.argtypes = [vp, C.c_int, vp, vp, u64p, u64p, C.c_int, C.c_int, vp, vp, vp]
         L.fides_rescale_batch.argtypes = [vp, vp, vp, vp, C.c_int, vp]
+        L.fides_encode.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]
+        L.fides_decode.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, vp]
         L.fides_add_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_mod_raise.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_sub.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -460,6 +462,33 @@ class Context:
         pp = (vp * n)(*[_ptr(p) for p in pts])
         _check(lib().fides_dot_plain(self._h, c0, c1, pp, n, l, _ptr(out.c0), _ptr(out.c1), _stream()))
         return out
+
+    # -- slot encode / decode on the device --
+    def encode(self, slots, scale: float, level: int):
+        """Complex slots -> EVALUATION-form plaintext(s).  slots: complex tensor of shape
+        [n_slots] or [n_pts, n_slots] (any device; copied to this GPU as complex128).  Returns
+        a uint64 tensor [level, N] (or [n_pts, level, N])."""
+        z = torch.as_tensor(slots).to(device=self.device, dtype=torch.complex128).contiguous()
+        single = z.dim() == 1
+        z = z.reshape(1, -1) if single else z
+        n_pts, n = z.shape
+        out = torch.empty((n_pts, level, self.N), dtype=torch.int64, device=self.device).view(torch.uint64)
+        _check(lib().fides_encode(self._h, torch.view_as_real(z).data_ptr(), n, n_pts, float(scale), level, _ptr(out),
+                                  _stream()))
+        return out[0] if single else out
+
+    def decode(self, pts, scale: float, n_slots=None):
+        """EVALUATION-form plaintext(s) [level, N] or [n_pts, level, N] -> complex128 slots
+        (limb 0 is read)."""
+        single = pts.dim() == 2
+        p = pts.reshape(1, *pts.shape) if single else pts
+        p = p.contiguous()
+        n_pts, level = p.shape[0], p.shape[1]
+        n = self.N // 2 if n_slots is None else n_slots
+        z = torch.empty((n_pts, n), dtype=torch.complex128, device=self.device)
+        _check(lib().fides_decode(self._h, _ptr(p), level, n_pts, n, float(scale), torch.view_as_real(z).data_ptr(),
+                                  _stream()))
+        return z[0] if single else z
 
     def lincomb(self, cts, scalars, add0=None, level=None):
         """sum_t scalars[t] * cts[t] (+ add0 on c0) over `level` limbs in one launch.  scalars[t]

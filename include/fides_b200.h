@@ -170,6 +170,22 @@ int fides_lincomb(fides_ctx* ctx, int n_lanes, const uint64_t* const* c0s, const
  * reference, src/CKKS/Ciphertext.cpp:569-607).  An output may not overlap another input. */
 int fides_rescale_batch(fides_ctx* ctx, const uint64_t* const* xs, const int* levels, uint64_t* const* outs, int n,
                         void* stream);
+/* CKKS slot encode on the device (replaces Plaintext::loadSlotsBatch / EncodeChunkSlots,
+ * src/CKKS/DeviceEncodeBatch.cu:529-828, and the host CKKSPackedEncoding::Encode it mirrors):
+ * n_pts plaintexts of n_slots complex slots each (slots = [n_pts][n_slots][re, im] doubles in
+ * device memory; n_slots a power of two <= N/2) are multiplied by `scale`, mapped to
+ * coefficients by the inverse special FFT (coefficient gap N / (2 n_slots)), rounded to the
+ * nearest integer and written as `level` limbs in EVALUATION form, out = [n_pts][level][N].
+ * Every coefficient must stay below q_0 / 2 in magnitude; a larger one is written as 0 and
+ * sets bit 1 of the device status word (fides_ctx_device_status). */
+int fides_encode(fides_ctx* ctx, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
+                 void* stream);
+/* CKKS slot decode on the device: n_pts plaintexts [n_pts][level][N] in EVALUATION form ->
+ * n_slots complex slots each divided by `scale` (slots = [n_pts][n_slots][re, im] doubles in
+ * device memory).  Reads limb 0 only, so the coefficients must lie below q_0 / 2 in magnitude
+ * (a decrypted message at a scale well below q_0). */
+int fides_decode(fides_ctx* ctx, const uint64_t* pts, int level, int n_pts, int n_slots, double scale, double* slots,
+                 void* stream);
 /* ModRaise of one level-1 polynomial (limb q_0, EVAL) to out_level limbs: INTT, centred
  * SwitchModulus(q_0 -> q_j), NTT (reference Bootstrap.cu ModRaise, src/CKKS/Bootstrap.cu:708+). */
 int fides_mod_raise(fides_ctx* ctx, const uint64_t* x, int out_level, uint64_t* out, void* stream);

@@ -379,32 +379,9 @@ class Bootstrapper:
 
     # --- plaintext preparation (encoding on the GPU: torch FFT, then the library's NTT)
     def _encode_pt(self, z, level: int, scale: float):
+        """Slots -> EVALUATION-form plaintext on the device (fides_encode)."""
         import torch
-        F, ctx = self.ev.F, self.ev.ctx
-        N = self.N
-        dev = f"cuda:{ctx.device}"
-        if not hasattr(self, "_enc"):
-            n, M = N // 2, 2 * N
-            e = np.empty(n, dtype=np.int64)
-            e[0] = 1
-            for j in range(1, n):
-                e[j] = (e[j - 1] * 5) % M
-            self._enc = (torch.from_numpy((e - 1) // 2).to(dev), torch.from_numpy(((M - e) - 1) // 2).to(dev),
-                         torch.exp(-1j * torch.pi * torch.arange(N, device=dev, dtype=torch.float64) / N),
-                         torch.tensor(ctx.q, dtype=torch.int64, device=dev))
-        tp, tn, twist, qs = self._enc
-        zt = torch.from_numpy(np.ascontiguousarray(z, dtype=np.complex128)).to(dev)
-        Mv = torch.zeros(N, dtype=torch.complex128, device=dev)
-        Mv[tp] = zt
-        Mv[tn] = torch.conj(zt)
-        m = torch.fft.fft(Mv) / N * twist
-        c = torch.round(m.real * scale)
-        if float(c.abs().max()) >= 2.0 ** 62:
-            raise ValueError("encoded coefficients exceed 62 bits")
-        ci = c.to(torch.int64)
-        limbs = torch.remainder(ci.unsqueeze(0), qs[:level].unsqueeze(1)).contiguous().view(torch.uint64)
-        ctx.ntt(limbs)
-        return limbs
+        return self.ev.ctx.encode(torch.from_numpy(np.ascontiguousarray(z, dtype=np.complex128)), scale, level)
 
     def _int_pt(self, coeff, level: int):
         F, ctx = self.ev.F, self.ev.ctx
@@ -447,6 +424,8 @@ class Bootstrapper:
         mono[N // 2] = 1  # X^(N/2): slots * i
         self.pt_i = self._int_pt(mono, top_level)
         self.pt_minus_i = self._int_pt(-mono, top_level)
+        if ev.ctx.device_status(clear=False) & 2:
+            raise ValueError("an encoded diagonal coefficient exceeded q_0 / 2")
 
     def _prepare_matrix(self, M: dict, fac: float, level: int, scale: float):
         """Pre-rotated, encoded diagonals for BSGS at `level` (input scale `scale`)."""

@@ -216,6 +216,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     // ---- per-prime constants and twiddles
     std::vector<DevPrime> hp(np);
     std::vector<ShoupConst> tf((size_t)np * N), ti((size_t)np * N), il(np);
+    std::vector<double2> tff((size_t)np * N), tfi((size_t)np * N);
+    std::vector<F64Prime> f64(np);
     auto work = [&](int i) {
       uint64_t q = primes[i];
       DevPrime& d = hp[i];
@@ -240,6 +242,12 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
         ti[i * N + j] = h_shoup(ipw[r], q);
       }
       il[i] = h_shoup(h_mulmod(ipw[h_brev(1, logN)], d.ninv, q), q);
+      const double qd = (double)q;  // exact for q < 2^53; used only for q < 2^50
+      for (size_t j = 0; j < (size_t)N; ++j) {
+        tff[i * N + j] = make_double2((double)tf[i * N + j].w, (double)tf[i * N + j].w / qd);
+        tfi[i * N + j] = make_double2((double)ti[i * N + j].w, (double)ti[i * N + j].w / qd);
+      }
+      f64[i] = F64Prime{qd, 1.0 / qd, (double)d.ninv, (double)d.ninv / qd, (double)il[i].w, (double)il[i].w / qd};
     };
     {
       unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -331,7 +339,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     }
     // ---- pack everything into one device blob
     std::vector<char> blob;
-    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq;
+    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq, o_tff, o_tfi, o_f64;
     append(blob, hp, o_prime);
     append(blob, tf, o_tf);
     append(blob, ti, o_ti);
@@ -340,6 +348,9 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     append(blob, pmod, o_pmod);
     append(blob, rs, o_rs);
     append(blob, pqinv, o_pq);
+    append(blob, tff, o_tff);
+    append(blob, tfi, o_tfi);
+    append(blob, f64, o_f64);
     struct Off {
       size_t sp, spr, pre, dp, dpr, mat, tcb, tcd;
       int ns, nd, kpad, ndp;
@@ -377,6 +388,9 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     c->d_pmod = reinterpret_cast<ShoupConst*>(base + o_pmod);
     c->d_rescale = reinterpret_cast<RescaleConst*>(base + o_rs);
     c->d_pqinv = reinterpret_cast<ShoupConst*>(base + o_pq);
+    c->d_twf_fwd = reinterpret_cast<double2*>(base + o_tff);
+    c->d_twf_inv = reinterpret_cast<double2*>(base + o_tfi);
+    c->d_f64 = reinterpret_cast<F64Prime*>(base + o_f64);
     auto mk = [&](const Off& o) {
       ConvTable t;
       t.n_src = o.ns;

@@ -65,6 +65,13 @@ struct ConvTable {
 // Basis-conversion engine: tensor cores (INT8 split on tcgen05) or 64-bit SIMT.
 enum ConvEngine { CONV_AUTO = 0, CONV_SIMT = 1, CONV_TENSOR = 2 };
 
+// FP64 constants of a prime below 2^50 for the floating-point NTT butterflies: q, 1/q, and
+// the inverse transform's last-stage factors N^-1 and psi_rev^-1[1] N^-1 with their
+// quotients by q.
+struct F64Prime {
+  double q, qinv, ninv, ninv_q, last, last_q;
+};
+
 struct RescaleConst {
   uint64_t qinv, qinv_s;  // q_top^-1 mod q_j
   uint64_t m, m_s;        // QlQlInvModqlDivqlModq_j = -q_top^-1 mod q_j
@@ -89,6 +96,9 @@ struct Context {
   ShoupConst* d_tw_fwd = nullptr;    // [n_q + K][N]: psi_rev (bit-reversed powers of psi)
   ShoupConst* d_tw_inv = nullptr;    // [n_q + K][N]: psi^-1 bit-reversed
   ShoupConst* d_inv_last = nullptr;  // [n_q + K]: psi_rev^-1[1] * N^-1 (last GS stage)
+  double2* d_twf_fwd = nullptr;      // [n_q + K][N]: (w, w / q) of d_tw_fwd as doubles (q < 2^50)
+  double2* d_twf_inv = nullptr;      // [n_q + K][N]: the same for d_tw_inv
+  F64Prime* d_f64 = nullptr;         // [n_q + K]
   ShoupConst* d_pinv = nullptr;      // [n_q]: P^-1 mod q_j
   ShoupConst* d_pmod = nullptr;      // [n_q]: P mod q_j
   RescaleConst* d_rescale = nullptr; // [n_q + 1][n_q]: row l = rescale from level l

@@ -67,9 +67,44 @@ __device__ __forceinline__ void gs_bf(uint64_t& x, uint64_t& y, ShoupConst w, ui
   x = s;
 }
 
+// ---- FP64 butterflies for primes q < 2^50.  The residues are integers held in doubles
+// (signed, |x| < 2^51), and every operation below is exact:
+//   * y w = p + e exactly (p = fl(y w), e = fma(y, w, -p));
+//   * k = rint(y (w/q)) from one fma with the rounding constant 1.5 2^52 (|y w/q| < 2^51);
+//     |k - y w / q| <= 1/2 + |y| 2^-53 because w/q is correctly rounded;
+//   * p - k q is an integer below 2^52 in magnitude, so fma(-k, q, p) is exact, and so is
+//     adding e: r = y w - k q with |r| <= q (1/2 + |y| 2^-53).
+// A forward butterfly reduces x the same way (x - rint(x / q) q) before x +- r, so values
+// entering a stage stay within 8/7 q (< 2^51 for q < 2^50); the inverse reduces the sum and
+// multiplies the difference, keeping values within q.  On B200 the FP64 pipe runs this
+// product at ~1.7x the rate of the 64-bit integer Shoup product, which is the NTT's bound.
+constexpr double F64_RND = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double F64_TWO52 = 4503599627370496.0;
+__device__ __forceinline__ double f_mulmod(double y, double w, double wq, double q) {
+  const double p = __dmul_rn(y, w);
+  const double e = __fma_rn(y, w, -p);
+  const double k = __dadd_rn(__fma_rn(y, wq, F64_RND), -F64_RND);
+  return __dadd_rn(__fma_rn(-k, q, p), e);
+}
+__device__ __forceinline__ double f_reduce(double x, double q, double qinv) {
+  const double k = __dadd_rn(__fma_rn(x, qinv, F64_RND), -F64_RND);
+  return __fma_rn(-k, q, x);
+}
+// u64 < 2^52 -> double (exact), and a value |v| < 2^51 -> its canonical residue in [0, q).
+__device__ __forceinline__ double f_from_u64(uint64_t v) {
+  return __dadd_rn(__longlong_as_double((long long)(0x4330000000000000ull | v)), -F64_TWO52);
+}
+__device__ __forceinline__ uint64_t f_to_canon(double v, double q, double qinv, uint64_t qi) {
+  const double c = __dadd_rn(f_reduce(v, q, qinv), q);  // in (0, 2q)
+  const uint64_t u = (uint64_t)__double_as_longlong(__dadd_rn(c, F64_TWO52)) & ((1ull << 52) - 1);
+  return u >= qi ? u - qi : u;
+}
+
 struct PassArgs {
   const DevPrime* primes;
   const ShoupConst* tw;        // forward or inverse twiddles, [prime][N]
+  const double2* twf;          // the same twiddles as (w, w / q) doubles (q < 2^50)
+  const F64Prime* f64;         // [prime]
   const ShoupConst* inv_last;  // [prime]: psi_rev^-1[1] * N^-1
   const ShoupConst* pinv;      // [Q prime]: P^-1 mod q (OUT_MODDOWN)
   const RescaleConst* rescale; // [level][Q prime] (OUT_RESCALE, OUT_MDRS)
@@ -137,6 +172,50 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
   }
 }
 
+// run_chunk on FP64 residues (q < 2^50): the same stages, pairs and twiddles.
+template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS>
+__device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int sub, int sbase, const double2* tw,
+                                              const F64Prime& fp) {
+  constexpr int E = 1 << LOGE;
+  const int th = t >> LO;
+#pragma unroll
+  for (int k = 0; k <= BHI - BLO; ++k) {
+    const int b = FWD ? (BHI - k) : (BLO + k);
+    const int rb = b - LO;
+    const int sig = LOGP - 1 - b;
+    const int s = sbase + sig;
+    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LOGE - b - 1));
+#pragma unroll
+    for (int hi = 0; hi < (E >> (rb + 1)); ++hi) {
+      if (!FWD && PASS == COL && b == LOGP - 1) {
+#pragma unroll
+        for (int lr = 0; lr < (1 << rb); ++lr) {
+          const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
+          const double a = x[r0], c = x[r1];
+          x[r0] = f_mulmod(__dadd_rn(a, c), fp.ninv, fp.ninv_q, fp.q);
+          x[r1] = f_mulmod(__dsub_rn(a, c), fp.last, fp.last_q, fp.q);
+        }
+      } else {
+        const double2 w = __ldg(tw + base + hi);
+#pragma unroll
+        for (int lr = 0; lr < (1 << rb); ++lr) {
+          const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
+          if (FWD) {
+            const double a = f_reduce(x[r0], fp.q, fp.qinv);
+            const double r = f_mulmod(x[r1], w.x, w.y, fp.q);
+            x[r0] = __dadd_rn(a, r);
+            x[r1] = __dsub_rn(a, r);
+          } else {
+            const double a = x[r0], c = x[r1];
+            x[r0] = f_reduce(__dadd_rn(a, c), fp.q, fp.qinv);
+            x[r1] = f_mulmod(__dsub_rn(a, c), w.x, w.y, fp.q);
+          }
+        }
+      }
+    }
+  }
+}
+
 // Bound of the inverse transform's values after `stages` stages from reduced input.
 __device__ __forceinline__ uint64_t inv_bound(uint64_t q, int stages) {
   uint64_t B = q;
@@ -187,6 +266,38 @@ __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, S
     run_chunk<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
   }
   static_assert(NCH <= 3, "sub-transform too large");
+}
+
+// chunks() on FP64 residues; the shared-memory exchanges move the doubles' bits.
+template <int LOGP, int PASS, bool FWD, typename SIDX>
+__device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu, SIDX sidx, int g, int t, int subtw,
+                                           int sbase, const double2* tw, const F64Prime& fp, bool direct_load) {
+  constexpr int E = 1 << LOGE;
+  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
+  double* sm = reinterpret_cast<double*>(smu);
+  using C0 = Chunk<LOGP, FWD, 0>;
+  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+  if constexpr (NCH > 1) {
+    using C1 = Chunk<LOGP, FWD, 1>;
+    if (!direct_load) __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO>(t, r))] = x[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
+    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+  }
+  if constexpr (NCH > 2) {
+    using C1 = Chunk<LOGP, FWD, 1>;
+    using C2 = Chunk<LOGP, FWD, 2>;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO>(t, r))] = x[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
+    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+  }
 }
 
 template <int LOGN, int PASS>
@@ -284,6 +395,17 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   }
 
   // ---- chunks
+  const bool f64 = pr.q < (1ull << 50);  // uniform per CTA: one limb per CTA
+  if (f64) {
+    // FP64 butterflies; every pass of such a limb stores canonical residues
+    const F64Prime fp = a.f64[lr.prime];
+    double xf[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) xf[r] = f_reduce(f_from_u64(x[r]), fp.q, fp.qinv);  // inputs < 2^52
+    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N, fp, direct_load);
+#pragma unroll
+    for (int r = 0; r < E; ++r) x[r] = f_to_canon(xf[r], fp.q, fp.qinv, pr.q);
+  } else {
   uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
   if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
   if (FWD && pr.q < (1ull << 58))
@@ -300,6 +422,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
 #pragma unroll
       for (int r = 0; r < E; ++r) x[r] = csub(csub(x[r], pr.q2), pr.q);   // x < 4q
     }
+  }
   }
 
   // ---- store (the last pass applies the epilogue)

@@ -53,7 +53,8 @@ cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 void fides::set_last_error(const std::string& msg) { g_err = msg; }
 
 namespace fides {
-double measure_bf_peak(int device);  // calibrate.cu
+double measure_bf_peak(int device);      // calibrate.cu
+double measure_bf_peak_f64(int device);  // calibrate.cu
 }
 
 extern "C" {
@@ -115,6 +116,23 @@ int fides_int_peak(int device, double* butterflies_per_s) {
   return guard([&] {
     need(butterflies_per_s, "butterflies_per_s");
     *butterflies_per_s = fides::measure_bf_peak(device);
+  });
+}
+
+int fides_f64_peak(int device, double* butterflies_per_s) {
+  return guard([&] {
+    need(butterflies_per_s, "butterflies_per_s");
+    *butterflies_per_s = fides::measure_bf_peak_f64(device);
+  });
+}
+
+int fides_ctx_ntt_counts(fides_ctx* x, uint64_t* f64_limbs, uint64_t* int_limbs) {
+  return guard([&] {
+    auto* c = C(x);
+    need(f64_limbs, "f64_limbs");
+    need(int_limbs, "int_limbs");
+    *f64_limbs = c->ntt_limbs_by_form[0].load();
+    *int_limbs = c->ntt_limbs_by_form[1].load();
   });
 }
 

@@ -126,6 +126,8 @@ struct Context {
   std::atomic<size_t> scratch_peak{0};
   size_t scratch_limit = 0;
   std::atomic<uint64_t> launches{0};
+  // limb transforms submitted to the NTT, by butterfly form: [0] FP64 (q < 2^50), [1] integer
+  std::atomic<uint64_t> ntt_limbs_by_form[2] = {0, 0};
   // profiling mode: CUDA events around every launch, per kernel family
   bool profiling = false;
   std::mutex prof_mu;

@@ -28,6 +28,12 @@ void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream
   a.logN = c->logN;
   a.log1 = (c->logN + 1) / 2;
   a.n_q = c->n_q;
+  {
+    uint64_t nf = 0;
+    for (int i = 0; i < n; ++i) nf += c->primes[limbs[i].prime] < (1ull << 50);
+    c->ntt_limbs_by_form[0] += nf;
+    c->ntt_limbs_by_form[1] += (uint64_t)n - nf;
+  }
   static thread_local NttLimbList L;  // ~25 KB: keep off the stack
   for (int off = 0; off < n; off += MAX_NTT_LIMBS) {
     L.n = std::min(MAX_NTT_LIMBS, n - off);

@@ -33,9 +33,23 @@ struct EpStage {
   static constexpr bool on = PASS == ROW && FWD && (OUT == OUT_MODDOWN || OUT == OUT_MDRS || OUT == OUT_RESCALE);
 };
 
-__device__ __forceinline__ ShoupConst ld_tw(const ShoupConst* p) {
-  ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
-  return ShoupConst{v.x, v.y};
+// Twiddle loads carry an L2 evict-last policy: a launch streams hundreds of limbs through L2
+// while every limb of one prime re-reads that prime's twiddle table, so the tables should
+// outlive the streaming data in L2.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ ShoupConst ld_tw(const ShoupConst* p, uint64_t pol) {
+  uint64_t w, ws;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(w), "=l"(ws) : "l"(p), "l"(pol));
+  return ShoupConst{w, ws};
+}
+__device__ __forceinline__ double2 ld_twf(const double2* p, uint64_t pol) {
+  double2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
 }
 
 // Cooley-Tukey butterfly, Harvey lazy form: x, y in [0, 4q) -> [0, 4q).
@@ -74,9 +88,13 @@ __device__ __forceinline__ void gs_bf(uint64_t& x, uint64_t& y, ShoupConst w, ui
 //     |k - y w / q| <= 1/2 + |y| 2^-53 because w/q is correctly rounded;
 //   * p - k q is an integer below 2^52 in magnitude, so fma(-k, q, p) is exact, and so is
 //     adding e: r = y w - k q with |r| <= q (1/2 + |y| 2^-53).
-// A forward butterfly reduces x the same way (x - rint(x / q) q) before x +- r, so values
-// entering a stage stay within 8/7 q (< 2^51 for q < 2^50); the inverse reduces the sum and
-// multiplies the difference, keeping values within q.  On B200 the FP64 pipe runs this
+// A forward butterfly reduces x the same way (x - rint(x / q) q) before x +- r on every other
+// stage of a pass (stages 0, 2, 4, ...): after a reducing stage values are within
+// (1 + A/8) q, after the next within (13/8 + 9A/64) q, so with A the bound entering a reducing
+// stage, A <= 1.9 and every operand of a product stays below 2q <= 2^51 for q < 2^50.  The
+// inverse reduces the sum and multiplies the difference on every stage (values within q).
+// Between the two passes of a transform the doubles are stored as they are (their bits);
+// only the last pass writes canonical residues.  On B200 the FP64 pipe runs this
 // product at ~1.7x the rate of the 64-bit integer Shoup product, which is the NTT's bound.
 constexpr double F64_RND = 6755399441055744.0;  // 1.5 * 2^52
 constexpr double F64_TWO52 = 4503599627370496.0;
@@ -90,13 +108,14 @@ __device__ __forceinline__ double f_reduce(double x, double q, double qinv) {
   const double k = __dadd_rn(__fma_rn(x, qinv, F64_RND), -F64_RND);
   return __fma_rn(-k, q, x);
 }
-// u64 < 2^52 -> double (exact), and a value |v| < 2^51 -> its canonical residue in [0, q).
+// u64 < 2^52 -> double (exact), and a value |v| < 2q -> its canonical residue in [0, q):
+// v + 2q + 2^52 lies in [2^52, 2^53), where the double's low 52 bits are the integer v + 2q.
 __device__ __forceinline__ double f_from_u64(uint64_t v) {
   return __dadd_rn(__longlong_as_double((long long)(0x4330000000000000ull | v)), -F64_TWO52);
 }
-__device__ __forceinline__ uint64_t f_to_canon(double v, double q, double qinv, uint64_t qi) {
-  const double c = __dadd_rn(f_reduce(v, q, qinv), q);  // in (0, 2q)
-  const uint64_t u = (uint64_t)__double_as_longlong(__dadd_rn(c, F64_TWO52)) & ((1ull << 52) - 1);
+__device__ __forceinline__ uint64_t f_to_canon(double v, double q2_two52, uint64_t qi) {
+  uint64_t u = (uint64_t)__double_as_longlong(__dadd_rn(v, q2_two52)) & ((1ull << 52) - 1);  // v + 2q
+  u = u >= 2 * qi ? u - 2 * qi : u;
   return u >= qi ? u - qi : u;
 }
 
@@ -132,7 +151,7 @@ __device__ __forceinline__ int padu(int u) {
 // [LO, LO + LOGE).  FWD walks bits high -> low, inverse low -> high.
 template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS, bool SMALL>
 __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int sub, int sbase, const ShoupConst* tw,
-                                          const DevPrime& pr, ShoupConst last, uint64_t& B) {
+                                          const DevPrime& pr, ShoupConst last, uint64_t& B, uint64_t pol) {
   constexpr int E = 1 << LOGE;
   const int th = t >> LO;
 #pragma unroll
@@ -155,7 +174,7 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
           x[r1] = shoup(a - c + B, last.w, last.ws, pr.q);
         }
       } else {
-        const ShoupConst w = ld_tw(tw + base + hi);
+        const ShoupConst w = ld_tw(tw + base + hi, pol);
 #pragma unroll
         for (int lr = 0; lr < (1 << rb); ++lr) {
           const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
@@ -175,7 +194,7 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
 // run_chunk on FP64 residues (q < 2^50): the same stages, pairs and twiddles.
 template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS>
 __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int sub, int sbase, const double2* tw,
-                                              const F64Prime& fp) {
+                                              const F64Prime& fp, uint64_t pol) {
   constexpr int E = 1 << LOGE;
   const int th = t >> LO;
 #pragma unroll
@@ -196,12 +215,12 @@ __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int
           x[r1] = f_mulmod(__dsub_rn(a, c), fp.last, fp.last_q, fp.q);
         }
       } else {
-        const double2 w = __ldg(tw + base + hi);
+        const double2 w = ld_twf(tw + base + hi, pol);
 #pragma unroll
         for (int lr = 0; lr < (1 << rb); ++lr) {
           const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
           if (FWD) {
-            const double a = f_reduce(x[r0], fp.q, fp.qinv);
+            const double a = (sig & 1) ? x[r0] : f_reduce(x[r0], fp.q, fp.qinv);
             const double r = f_mulmod(x[r1], w.x, w.y, fp.q);
             x[r0] = __dadd_rn(a, r);
             x[r1] = __dsub_rn(a, r);
@@ -239,11 +258,11 @@ struct Chunk {
 template <int LOGP, int PASS, bool FWD, bool SMALL, typename SIDX>
 __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, SIDX sidx, int g, int t, int subtw,
                                        int sbase, const ShoupConst* tw, const DevPrime& pr, ShoupConst last,
-                                       uint64_t& B, bool direct_load) {
+                                       uint64_t& B, bool direct_load, uint64_t pol) {
   constexpr int E = 1 << LOGE;
   constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
   using C0 = Chunk<LOGP, FWD, 0>;
-  run_chunk<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+  run_chunk<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   if constexpr (NCH > 1) {
     using C1 = Chunk<LOGP, FWD, 1>;
     if (!direct_load) __syncthreads();
@@ -252,7 +271,7 @@ __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, S
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
-    run_chunk<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+    run_chunk<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   }
   if constexpr (NCH > 2) {
     using C1 = Chunk<LOGP, FWD, 1>;
@@ -263,7 +282,7 @@ __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, S
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
-    run_chunk<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B);
+    run_chunk<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   }
   static_assert(NCH <= 3, "sub-transform too large");
 }
@@ -271,12 +290,13 @@ __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, S
 // chunks() on FP64 residues; the shared-memory exchanges move the doubles' bits.
 template <int LOGP, int PASS, bool FWD, typename SIDX>
 __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu, SIDX sidx, int g, int t, int subtw,
-                                           int sbase, const double2* tw, const F64Prime& fp, bool direct_load) {
+                                           int sbase, const double2* tw, const F64Prime& fp, bool direct_load,
+                                           uint64_t pol) {
   constexpr int E = 1 << LOGE;
   constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
   double* sm = reinterpret_cast<double*>(smu);
   using C0 = Chunk<LOGP, FWD, 0>;
-  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
   if constexpr (NCH > 1) {
     using C1 = Chunk<LOGP, FWD, 1>;
     if (!direct_load) __syncthreads();
@@ -285,7 +305,7 @@ __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
-    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
   }
   if constexpr (NCH > 2) {
     using C1 = Chunk<LOGP, FWD, 1>;
@@ -296,7 +316,7 @@ __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
-    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp);
+    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
   }
 }
 
@@ -395,23 +415,36 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   }
 
   // ---- chunks
+  const uint64_t pol = l2_evict_last_policy();
   const bool f64 = pr.q < (1ull << 50);  // uniform per CTA: one limb per CTA
   if (f64) {
     // FP64 butterflies; every pass of such a limb stores canonical residues
     const F64Prime fp = a.f64[lr.prime];
     double xf[E];
+    if (first_pass) {
 #pragma unroll
-    for (int r = 0; r < E; ++r) xf[r] = f_reduce(f_from_u64(x[r]), fp.q, fp.qinv);  // inputs < 2^52
-    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N, fp, direct_load);
+      for (int r = 0; r < E; ++r) xf[r] = f_reduce(f_from_u64(x[r]), fp.q, fp.qinv);  // inputs < 2^52
+    } else {
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = f_to_canon(xf[r], fp.q, fp.qinv, pr.q);
+      for (int r = 0; r < E; ++r) xf[r] = __longlong_as_double((long long)x[r]);  // the first pass's doubles
+    }
+    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N, fp, direct_load,
+                                pol);
+    if (first_pass) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) x[r] = (uint64_t)__double_as_longlong(xf[r]);
+    } else {
+      const double q2t = __dadd_rn(2.0 * fp.q, F64_TWO52);
+#pragma unroll
+      for (int r = 0; r < E; ++r) x[r] = f_to_canon(xf[r], q2t, pr.q);
+    }
   } else {
   uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
   if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
   if (FWD && pr.q < (1ull << 58))
-    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load);
+    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load, pol);
   else
-    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load);
+    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load, pol);
 
   // ---- final reduction of the completed transform
   if (FWD && PASS == ROW) {

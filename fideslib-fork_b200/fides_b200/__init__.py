@@ -106,6 +106,8 @@ def lib():
         L.fides_ctx_profile.argtypes = [vp, C.c_int]
         L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
         L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.fides_f64_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.fides_ctx_ntt_counts.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
         L.fides_ctx_reserve_scratch.argtypes = [vp, C.c_size_t]
         L.fides_server_add_bootstrap.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_int]
@@ -191,6 +193,14 @@ def int_peak(device: int = 0) -> float:
     return float(v.value)
 
 
+def f64_peak(device: int = 0) -> float:
+    """Butterflies per second of the FP64 butterfly the NTT uses for primes below 2^50,
+    register-resident (the FP64-pipe roofline of those limbs' passes)."""
+    v = C.c_double()
+    _check(lib().fides_f64_peak(device, C.byref(v)))
+    return float(v.value)
+
+
 def auto_index(logN: int, rotation: int) -> int:
     return int(lib().fides_rotation_auto_index(logN, rotation))
 
@@ -241,6 +251,12 @@ class Context:
     # -- bookkeeping --
     def beta(self, l: int) -> int:
         return (l + self.alpha - 1) // self.alpha
+
+    def ntt_counts(self) -> tuple[int, int]:
+        """(FP64-form, integer-form) limb transforms submitted since creation."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().fides_ctx_ntt_counts(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
 
     @property
     def launch_count(self) -> int:

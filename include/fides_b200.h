@@ -91,6 +91,12 @@ int fides_ctx_set_ntt_shape(fides_ctx* ctx, int inverse, int pass, int size_clas
  * forward NTT butterfly (one 64-bit Shoup product, two 64-bit additions) on register-resident
  * data, with no memory traffic.  Takes about 100 ms.  No reference counterpart. */
 int fides_int_peak(int device, double* butterflies_per_s);
+/* The same for the FP64 butterfly the NTT uses for primes below 2^50 (its FP64-pipe
+ * roofline).  No reference counterpart. */
+int fides_f64_peak(int device, double* butterflies_per_s);
+/* Limb transforms submitted to the NTT since the context was created, by butterfly form:
+ * FP64 (primes below 2^50) and 64-bit integer.  No reference counterpart. */
+int fides_ctx_ntt_counts(fides_ctx* ctx, uint64_t* f64_limbs, uint64_t* int_limbs);
 /* Synchronises the device and reads the context's device status word: bit 0 = a bounded
  * device-side wait gave up (the affected outputs are incomplete).  clear != 0 resets it. */
 int fides_ctx_device_status(fides_ctx* ctx, uint32_t* status, int clear);

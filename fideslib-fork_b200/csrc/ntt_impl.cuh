@@ -328,11 +328,16 @@ struct PassShape {
 
 // One pass of a transform of 2^LOGN points.  Every index is a compile-time function of
 // LOGN, so global and shared addresses are a per-thread base plus immediate offsets.
-// Threads of a pass CTA, and CTAs per SM the register budget is sized for (24 warps).
+// Threads of a pass CTA, and CTAs per SM the register budget is sized for (by default 768
+// threads = 24 warps per SM, i.e. 80 registers; FIDES_NTT_THREADS_PER_SM overrides it).
+#ifndef FIDES_NTT_THREADS_PER_SM
+#define FIDES_NTT_THREADS_PER_SM 768
+#endif
 template <int LOGN, int PASS, int G>
 struct PassThreads {
+  static constexpr int TPS = FIDES_NTT_THREADS_PER_SM;
   static constexpr int NT = (1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G;
-  static constexpr int MINB = NT >= 768 ? 1 : (768 / NT > 32 ? 32 : 768 / NT);
+  static constexpr int MINB = NT >= TPS ? 1 : (TPS / NT > 32 ? 32 : TPS / NT);
 };
 
 template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G>

@@ -13,6 +13,7 @@
 #include "capi_internal.hpp"
 #include "context.hpp"
 #include "encode.hpp"
+#include "interop.hpp"
 #include "kernels.cuh"
 #include "ntt.cuh"
 #include "ops.hpp"
@@ -425,6 +426,37 @@ int fides_decode(fides_ctx* x, const uint64_t* pts, int level, int n_pts, int n_
     need(pts, "pts");
     need(slots, "slots");
     fides::op_decode(c, pts, level, n_pts, n_slots, scale, slots, S(stream));
+  });
+}
+
+int fides_ct_import(fides_ctx* x, int n_polys, const uint64_t* const* limbs, const uint64_t* moduli, int level,
+                    int format, int natural_order, uint64_t* out, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(limbs, "limbs");
+    need(out, "out");
+    if (format != 0 && format != 1) throw fides::Error(FIDES_ERR_ARG, "format must be 0 (EVAL) or 1 (COEFF)");
+    fides::op_ct_import(c, n_polys, limbs, moduli, level, format, natural_order != 0, out, S(stream));
+  });
+}
+
+int fides_ct_export(fides_ctx* x, int n_polys, const uint64_t* in, int level, int format, int natural_order,
+                    uint64_t* const* limbs, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(in, "in");
+    need(limbs, "limbs");
+    if (format != 0 && format != 1) throw fides::Error(FIDES_ERR_ARG, "format must be 0 (EVAL) or 1 (COEFF)");
+    fides::op_ct_export(c, n_polys, in, level, format, natural_order != 0, limbs, S(stream));
+  });
+}
+
+int fides_key_import(fides_ctx* x, const uint64_t* const* limbs, int natural_order, uint64_t** dev_key) {
+  return guard([&] {
+    auto* c = C(x);
+    need(limbs, "limbs");
+    need(dev_key, "dev_key");
+    *dev_key = fides::op_key_import(c, limbs, natural_order != 0, nullptr);
   });
 }
 

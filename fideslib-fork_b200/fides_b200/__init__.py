@@ -148,6 +148,9 @@ def lib():
         L.fides_lincomb.argtypes = [vp, C.c_int, vp, vp, u64p, u64p, C.c_int, C.c_int, vp, vp, vp]
         L.fides_rescale_batch.argtypes = [vp, vp, vp, vp, C.c_int, vp]
         L.fides_encode.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]
+        L.fides_ct_import.argtypes = [vp, C.c_int, vp, u64p, C.c_int, C.c_int, C.c_int, vp, vp]
+        L.fides_ct_export.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, vp]
+        L.fides_key_import.argtypes = [vp, vp, C.c_int, C.POINTER(vp)]
         L.fides_decode.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, vp]
         L.fides_add_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_mod_raise.argtypes = [vp, vp, C.c_int, vp, vp]
@@ -478,6 +481,56 @@ class Context:
         pp = (vp * n)(*[_ptr(p) for p in pts])
         _check(lib().fides_dot_plain(self._h, c0, c1, pp, n, l, _ptr(out.c0), _ptr(out.c1), _stream()))
         return out
+
+    # -- interop with per-limb host arrays (the reference's RawCipherText / RawKeySwitchKey) --
+    def import_limbs(self, polys, format_coeff=False, natural_order=False, check_moduli=True, moduli=None):
+        """polys: list of polynomials, each a list of `level` numpy uint64 arrays of N residues
+        (one per limb, any host memory).  Returns a device tensor [n_polys, level, N] in
+        bit-reversed EVALUATION form."""
+        import numpy as np
+        n, level = len(polys), len(polys[0])
+        arrs = [np.ascontiguousarray(a, dtype=np.uint64) for p in polys for a in p]
+        ptrs = (vp * len(arrs))(*[a.ctypes.data for a in arrs])
+        if moduli is not None:
+            mod = np.array(moduli, dtype=np.uint64)
+        else:
+            mod = np.array((self.q + self.p)[:level], dtype=np.uint64) if check_moduli else None
+        out = torch.empty((n, level, self.N), dtype=torch.int64, device=self.device).view(torch.uint64)
+        _check(lib().fides_ct_import(self._h, n, ptrs, None if mod is None else mod.ctypes.data_as(u64p), level,
+                                     1 if format_coeff else 0, 1 if natural_order else 0, _ptr(out), _stream()))
+        torch.cuda.current_stream(self.device).synchronize()  # the host arrays may go away
+        return out
+
+    def export_limbs(self, dev, format_coeff=False, natural_order=False):
+        """Device [n_polys, level, N] (bit-reversed EVAL) -> list of lists of numpy limbs."""
+        import numpy as np
+        d = dev if dev.dim() == 3 else dev.unsqueeze(0)
+        n, level = d.shape[0], d.shape[1]
+        outs = [[np.empty(self.N, dtype=np.uint64) for _ in range(level)] for _ in range(n)]
+        ptrs = (vp * (n * level))(*[a.ctypes.data for p in outs for a in p])
+        _check(lib().fides_ct_export(self._h, n, _ptr(d.contiguous()), level, 1 if format_coeff else 0,
+                                     1 if natural_order else 0, ptrs, _stream()))
+        return outs
+
+    def import_key(self, r_key, natural_order=False):
+        """r_key[a/b][digit][limb] numpy arrays (None = zero limb) -> device key pointer (int),
+        freed with key_free."""
+        import numpy as np
+        flat, keep = [], []
+        for ab in range(2):
+            for d in range(self.dnum):
+                for i in range(self.n_q + self.K):
+                    a = r_key[ab][d][i]
+                    if a is None:
+                        flat.append(None)
+                    else:
+                        a = np.ascontiguousarray(a, dtype=np.uint64)
+                        keep.append(a)
+                        flat.append(a.ctypes.data)
+        ptrs = (vp * len(flat))(*flat)
+        out = vp()
+        _check(lib().fides_key_import(self._h, ptrs, 1 if natural_order else 0, C.byref(out)))
+        return int(out.value)
 
     # -- slot encode / decode on the device --
     def encode(self, slots, scale: float, level: int):

@@ -321,6 +321,22 @@ int fides_server_destroy(fides_server* s);
 /* ---- host-buffer entry points (end-to-end path) ------------------------------------- */
 /* Upload a key from host memory into a new device buffer owned by the context. */
 int fides_key_upload(fides_ctx* ctx, const uint64_t* host_key, uint64_t** dev_key);
+/* Interop with the reference's raw host formats (src/CKKS/openfhe-interface/RawCiphertext.cuh:
+ * RawCipherText :20-37, RawKeySwitchKey :90-95), replacing Ciphertext::load / store
+ * (src/CKKS/Ciphertext.cpp:415-464) and KeySwitchingKey::Initialize (KeySwitchingKey.cu:19-35).
+ * limbs: one host array of N residues per limb, [n_polys][level] pointers (sub_0[i].data(),
+ * sub_1[i].data(), ... ); moduli (NULL: not checked) must equal the context's primes;
+ * format 0 = EVALUATION, 1 = COEFFICIENT (converted by the NTT on import, the INTT on export);
+ * natural_order != 0: evaluation vectors in natural order instead of OpenFHE's bit-reversed
+ * order (the reference's REV = 0), permuted on the device.  out / in = [n_polys][level][N] device
+ * limbs in this library's bit-reversed EVALUATION layout.  Export returns after the copies. */
+int fides_ct_import(fides_ctx* ctx, int n_polys, const uint64_t* const* limbs, const uint64_t* moduli, int level,
+                    int format, int natural_order, uint64_t* out, void* stream);
+int fides_ct_export(fides_ctx* ctx, int n_polys, const uint64_t* in, int level, int format, int natural_order,
+                    uint64_t* const* limbs, void* stream);
+/* RawKeySwitchKey::r_key -> a device key (as fides_key_upload): limbs = [2][dnum][n_q + K] host
+ * pointers (a = [0], b = [1]; NULL = a zero limb), EVALUATION form. */
+int fides_key_import(fides_ctx* ctx, const uint64_t* const* limbs, int natural_order, uint64_t** dev_key);
 int fides_key_free(fides_ctx* ctx, uint64_t* dev_key);
 /* HMult(+rescale) of host ciphertexts: copies in, computes, copies out, synchronises.
  * Mirrors CudaEngine::evalMult's load -> op -> RecoverHostCiphertext cycle

@@ -72,116 +72,153 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
   }
 }
 
-// Two adjacent coefficients per thread (16-byte loads of every stream).  MAXB is the
-// largest digit count of the launch's jobs (0 = any): with it known at compile time every
-// load of the thread -- all digits, both key halves, the own-digit and tensor operands -- is
-// issued before the first product, so a thread keeps up to 3 MAXB + 4 loads in flight.
-template <int MAXB>
-__global__ void __launch_bounds__(EW_THREADS) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
-                                                         const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
-                                                         int alpha) {
-  const KskJob& J = L.j[blockIdx.z];
-  const int l = J.l, ext = l + K;
+// CPT adjacent coefficients per thread (the launches use CPT = 2: 16-byte loads of every
+// stream; one coefficient per thread was measured 13 % slower).  MAXB is the largest digit
+// count of the launch's jobs (0 = any): with it known at compile time every load of a job --
+// all digits, the own-digit and tensor operands -- is issued before its first product.  JG:
+// jobs per group (one CTA runs a group; its jobs share the key tile, read once); the grouped
+// form keeps three CTAs per SM at the cost of a few spilled registers, which measured faster
+// (KSK -9 % with groups of 4) than the unbounded register count (two CTAs per SM).
+template <int CPT>
+struct KVec {
+  uint64_t c[CPT];
+};
+template <int CPT>
+__device__ __forceinline__ KVec<CPT> kld(const uint64_t* q) {
+  KVec<CPT> v;
+  if constexpr (CPT == 2) {
+    const ulonglong2 t = *reinterpret_cast<const ulonglong2*>(q);
+    v.c[0] = t.x;
+    v.c[1] = t.y;
+  } else {
+    v.c[0] = *q;
+  }
+  return v;
+}
+
+template <int MAXB, int JG, int CPT>
+__global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
+                                                            const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
+                                                            int alpha) {
+  using V = KVec<CPT>;
+  const int g0 = L.gstart[blockIdx.z], gn = L.gcount[blockIdx.z];
+  const KskJob& J0 = L.j[g0];  // the group's jobs share key, level and extras
+  const int l = J0.l, ext = l + K;
   const int i = blockIdx.y;
   if (i >= ext) return;
   const int N = 1 << logN;
-  const int n = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int n = CPT * (blockIdx.x * blockDim.x + threadIdx.x);
   const int pid = i < l ? i : n_q + (i - l);
   const DevPrime p = primes[pid];
   const int beta = (l + alpha - 1) / alpha;
   const int own = i < l ? i / alpha : -1;
   const size_t kstride = (size_t)(n_q + K) * N;
-  auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   const size_t off = (size_t)i * N + n, koff = (size_t)pid * N + n;
-  const bool tensor = J.a0 && i < l;
-  U128 sa0{0, 0}, sb0{0, 0}, sa1{0, 0}, sb1{0, 0};
-  ulonglong2 x1{0, 0}, y1{0, 0};  // a1, b1 of this limb (own digit)
-  auto digit = [&](int d, ulonglong2 v, ulonglong2 ka, ulonglong2 kb) {
-    if (d == own && J.x2) {  // the own digit is x * x2 (tensor term a1 b1)
-      x1 = v;
-      v.x = mulmod(v.x, y1.x, p);
-      v.y = mulmod(v.y, y1.y, p);
+  const bool tensor = J0.a0 && i < l;
+  // one job: sum_d D_d key_d (+ extras), reduced and stored; ka / kb: the key tile (MAXB > 0)
+  auto run = [&](const KskJob& J, const V* ka, const V* kb) {
+    U128 sa[CPT], sb[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) sa[c] = sb[c] = U128{0, 0};
+    V x1{}, y1{};  // a1, b1 of this limb (own digit)
+    auto digit = [&](int d, V v, const V& a_, const V& b_) {
+      if (d == own && J.x2) {  // the own digit is x * x2 (tensor term a1 b1)
+        x1 = v;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) v.c[c] = mulmod(v.c[c], y1.c[c], p);
+      }
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        mac128(sa[c], v.c[c], a_.c[c]);
+        mac128(sb[c], v.c[c], b_.c[c]);
+      }
+    };
+    auto tensor_terms = [&](const V& x0, const V& y0) {
+      const ShoupConst pm = pmod[i];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const uint64_t py0 = shoup(y0.c[c], pm.w, pm.ws, p.q), py1 = shoup(y1.c[c], pm.w, pm.ws, p.q);
+        mac128(sb[c], x0.c[c], py0);  // + P a0 b0
+        mac128(sa[c], x0.c[c], py1);  // + P (a0 b1 + a1 b0)
+        mac128(sa[c], x1.c[c], py0);
+      }
+    };
+    if constexpr (MAXB > 0) {
+      V v[MAXB];
+#pragma unroll
+      for (int d = 0; d < MAXB; ++d)
+        if (d < beta) v[d] = kld<CPT>((d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n);
+      if (own >= 0 && J.x2) y1 = kld<CPT>(J.x2 + off);
+      V x0{}, y0{};
+      if (tensor) {
+        x0 = kld<CPT>(J.a0 + off);
+        y0 = kld<CPT>(J.b0 + off);
+      }
+#pragma unroll
+      for (int d = 0; d < MAXB; ++d)
+        if (d < beta) digit(d, v[d], ka[d], kb[d]);
+      if (tensor) tensor_terms(x0, y0);
+    } else {
+      if (own >= 0 && J.x2) y1 = kld<CPT>(J.x2 + off);
+      for (int d = 0; d < beta; ++d) {
+        const uint64_t* src = (d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n;
+        digit(d, kld<CPT>(src), kld<CPT>(J.key + (size_t)d * kstride + koff),
+              kld<CPT>(J.key + (size_t)(dnum + d) * kstride + koff));
+      }
+      if (tensor) {
+        // every Q limb has one own digit, so x1 / y1 hold a1 / b1 here
+        if (beta > 12) {  // keep the sums below 2^128: at most 15 products of two values < 2^62
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+            sa[c] = U128{reduce128(sa[c], p), 0};
+            sb[c] = U128{reduce128(sb[c], p), 0};
+          }
+        }
+        tensor_terms(kld<CPT>(J.a0 + off), kld<CPT>(J.b0 + off));
+      }
     }
-    mac128(sa0, v.x, ka.x);
-    mac128(sb0, v.x, kb.x);
-    mac128(sa1, v.y, ka.y);
-    mac128(sb1, v.y, kb.y);
+    uint64_t ra[CPT], rb[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      ra[c] = reduce128(sa[c], p);
+      rb[c] = reduce128(sb[c], p);
+    }
+    if (J.c0 && i < l) {
+      const ShoupConst pm = pmod[i];
+      const V cv = kld<CPT>(J.c0 + off);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) rb[c] = addmod(rb[c], shoup(cv.c[c], pm.w, pm.ws, p.q), p.q);
+    }
+    uint64_t* oa = J.out_a + (size_t)i * N;
+    uint64_t* ob = J.out_b + (size_t)i * N;
+    if (J.auto_k) {
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const uint32_t o = auto_slot(logN, J.auto_k, (uint32_t)(n + c));
+        oa[o] = ra[c];
+        ob[o] = rb[c];
+      }
+    } else if constexpr (CPT == 2) {
+      *reinterpret_cast<ulonglong2*>(oa + n) = make_ulonglong2(ra[0], ra[1]);
+      *reinterpret_cast<ulonglong2*>(ob + n) = make_ulonglong2(rb[0], rb[1]);
+    } else {
+      oa[n] = ra[0];
+      ob[n] = rb[0];
+    }
   };
   if constexpr (MAXB > 0) {
-    ulonglong2 v[MAXB], ka[MAXB], kb[MAXB];
+    V ka[MAXB], kb[MAXB];  // the group's key tile, read once
 #pragma unroll
     for (int d = 0; d < MAXB; ++d)
       if (d < beta) {
-        const uint64_t* src = (d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n;
-        v[d] = ld2(src);
-        ka[d] = ld2(J.key + (size_t)d * kstride + koff);
-        kb[d] = ld2(J.key + (size_t)(dnum + d) * kstride + koff);
+        ka[d] = kld<CPT>(J0.key + (size_t)d * kstride + koff);
+        kb[d] = kld<CPT>(J0.key + (size_t)(dnum + d) * kstride + koff);
       }
-    if (own >= 0 && J.x2) y1 = ld2(J.x2 + off);
-    ulonglong2 x0{0, 0}, y0{0, 0};
-    if (tensor) {
-      x0 = ld2(J.a0 + off);
-      y0 = ld2(J.b0 + off);
-    }
 #pragma unroll
-    for (int d = 0; d < MAXB; ++d)
-      if (d < beta) digit(d, v[d], ka[d], kb[d]);
-    if (tensor) {
-      const ShoupConst pm = pmod[i];
-      const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
-      const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
-      mac128(sb0, x0.x, py0x);  // + P a0 b0
-      mac128(sb1, x0.y, py0y);
-      mac128(sa0, x0.x, py1x);  // + P (a0 b1 + a1 b0)
-      mac128(sa0, x1.x, py0x);
-      mac128(sa1, x0.y, py1y);
-      mac128(sa1, x1.y, py0y);
-    }
+    for (int jj = 0; jj < JG; ++jj)
+      if (jj < gn) run(L.j[g0 + jj], ka, kb);
   } else {
-    if (own >= 0 && J.x2) y1 = ld2(J.x2 + off);
-    for (int d = 0; d < beta; ++d) {
-      const uint64_t* src = (d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n;
-      digit(d, ld2(src), ld2(J.key + (size_t)d * kstride + koff), ld2(J.key + (size_t)(dnum + d) * kstride + koff));
-    }
-    if (tensor) {
-      // every Q limb has one own digit, so x1 / y1 hold a1 / b1 here
-      if (beta > 12) {  // keep the sums below 2^128: at most 15 products of two values < 2^62
-        sa0 = U128{reduce128(sa0, p), 0};
-        sb0 = U128{reduce128(sb0, p), 0};
-        sa1 = U128{reduce128(sa1, p), 0};
-        sb1 = U128{reduce128(sb1, p), 0};
-      }
-      const ShoupConst pm = pmod[i];
-      const ulonglong2 x0 = ld2(J.a0 + off), y0 = ld2(J.b0 + off);
-      const uint64_t py0x = shoup(y0.x, pm.w, pm.ws, p.q), py0y = shoup(y0.y, pm.w, pm.ws, p.q);
-      const uint64_t py1x = shoup(y1.x, pm.w, pm.ws, p.q), py1y = shoup(y1.y, pm.w, pm.ws, p.q);
-      mac128(sb0, x0.x, py0x);
-      mac128(sb1, x0.y, py0y);
-      mac128(sa0, x0.x, py1x);
-      mac128(sa0, x1.x, py0x);
-      mac128(sa1, x0.y, py1y);
-      mac128(sa1, x1.y, py0y);
-    }
-  }
-  uint64_t ra0 = reduce128(sa0, p), rb0 = reduce128(sb0, p);
-  uint64_t ra1 = reduce128(sa1, p), rb1 = reduce128(sb1, p);
-  if (J.c0 && i < l) {
-    const ShoupConst pm = pmod[i];
-    const ulonglong2 c = ld2(J.c0 + off);
-    rb0 = addmod(rb0, shoup(c.x, pm.w, pm.ws, p.q), p.q);
-    rb1 = addmod(rb1, shoup(c.y, pm.w, pm.ws, p.q), p.q);
-  }
-  uint64_t* oa = J.out_a + (size_t)i * N;
-  uint64_t* ob = J.out_b + (size_t)i * N;
-  if (J.auto_k) {
-    const uint32_t o0 = auto_slot(logN, J.auto_k, (uint32_t)n), o1 = auto_slot(logN, J.auto_k, (uint32_t)n + 1);
-    oa[o0] = ra0;
-    ob[o0] = rb0;
-    oa[o1] = ra1;
-    ob[o1] = rb1;
-  } else {
-    *reinterpret_cast<ulonglong2*>(oa + n) = make_ulonglong2(ra0, ra1);
-    *reinterpret_cast<ulonglong2*>(ob + n) = make_ulonglong2(rb0, rb1);
+    for (int jj = 0; jj < gn; ++jj) run(L.j[g0 + jj], nullptr, nullptr);
   }
 }
 
@@ -437,26 +474,53 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
   for (int off = 0; off < n; off += MAX_KSK_JOBS) {
     int m = std::min(MAX_KSK_JOBS, n - off);
     fill(L, jobs + off, m);
+    // groups of consecutive jobs with one key, level and set of extras
+    auto same = [](const KskJob& a, const KskJob& b) {
+      return a.key == b.key && a.l == b.l && a.auto_k == b.auto_k && !a.x2 == !b.x2 && !a.a0 == !b.a0 &&
+             !a.c0 == !b.c0 && !a.x == !b.x;
+    };
+    L.ngroups = 0;
+    int gmax = 1;
+    for (int i = 0; i < m;) {
+      int k = 1;
+      while (i + k < m && k < MAX_KSK_GROUP && same(L.j[i], L.j[i + k])) ++k;
+      L.gstart[L.ngroups] = (uint8_t)i;
+      L.gcount[L.ngroups] = (uint8_t)k;
+      ++L.ngroups;
+      gmax = std::max(gmax, k);
+      i += k;
+    }
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
-    dim3 grid(c->N / (2 * EW_THREADS), mx, m);
+    const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : 4;
+    dim3 grid(c->N / (2 * EW_THREADS), mx, L.ngroups);
+    // algorithmic bytes: each job's digits, outputs and extra operands, and each group's key once
     double bytes = 0;
     for (int i = 0; i < m; ++i) {
       const int l = L.j[i].l, ext = l + c->K, b = c->beta(l);
-      bytes += 8.0 * c->N * ((double)ext * (3 * b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
+      bytes += 8.0 * c->N * ((double)ext * (b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
+    }
+    for (int g = 0; g < L.ngroups; ++g) {
+      const int l = L.j[L.gstart[g]].l;
+      bytes += 8.0 * c->N * 2.0 * c->beta(l) * (l + c->K);
     }
     int maxb = 0;
     for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     LaunchScope ls(c, s, KK_KSK, bytes);
-    switch (maxb) {
-#define FIDES_KSK_CASE(B)                                                                                     \
-  case B:                                                                                                     \
-    ksk_kernel<B><<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha); \
+    auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K,
+                                                              c->dnum, c->alpha); };
+    switch (maxb * 8 + jg) {
+#define FIDES_KSK_CASE(B, G)                    \
+  case B * 8 + G:                               \
+    go(ksk_kernel<B, G, 2>);                    \
     break;
-      FIDES_KSK_CASE(1) FIDES_KSK_CASE(2) FIDES_KSK_CASE(3) FIDES_KSK_CASE(4)
+      FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4)
+      FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4)
+      FIDES_KSK_CASE(3, 1) FIDES_KSK_CASE(3, 2) FIDES_KSK_CASE(3, 4)
+      FIDES_KSK_CASE(4, 1) FIDES_KSK_CASE(4, 2) FIDES_KSK_CASE(4, 4)
 #undef FIDES_KSK_CASE
       default:
-        ksk_kernel<0><<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K, c->dnum, c->alpha);
+        go(ksk_kernel<0, 1, 2>);
     }
     FIDES_CUDA(cudaGetLastError());
   }

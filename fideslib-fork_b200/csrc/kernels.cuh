@@ -43,8 +43,13 @@ struct KskJob {
   const uint64_t* b0 = nullptr;
 };
 constexpr int MAX_KSK_JOBS = 64;
+// Jobs that share a switching key (one relinearisation or rotation key for a batch) and the
+// same level and extras form a group of up to 4; one CTA runs a whole group, reading each key
+// tile once for all of its jobs.
+constexpr int MAX_KSK_GROUP = 4;
 struct KskJobList {
-  int n, max_ext, pad0, pad1;
+  int n, max_ext, ngroups, pad1;
+  uint8_t gstart[MAX_KSK_JOBS], gcount[MAX_KSK_JOBS];
   KskJob j[MAX_KSK_JOBS];
 };
 void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s);

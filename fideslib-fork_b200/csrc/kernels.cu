@@ -96,7 +96,7 @@ __device__ __forceinline__ KVec<CPT> kld(const uint64_t* q) {
   return v;
 }
 
-template <int MAXB, int JG, int CPT>
+template <int MAXB, int JG, int CPT, bool SHARE_DIGITS = false>
 __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
                                                             const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
                                                             int alpha) {
@@ -115,8 +115,9 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
   const size_t kstride = (size_t)(n_q + K) * N;
   const size_t off = (size_t)i * N + n, koff = (size_t)pid * N + n;
   const bool tensor = J0.a0 && i < l;
-  // one job: sum_d D_d key_d (+ extras), reduced and stored; ka / kb: the key tile (MAXB > 0)
-  auto run = [&](const KskJob& J, const V* ka, const V* kb) {
+  // one job: sum_d D_d key_d (+ extras), reduced and stored; ka / kb: the group's key tile, or
+  // vd: the group's digit tile (MAXB > 0; the other one is loaded here)
+  auto run = [&](const KskJob& J, const V* ka_g, const V* kb_g, const V* vd) {
     U128 sa[CPT], sb[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) sa[c] = sb[c] = U128{0, 0};
@@ -144,10 +145,20 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
       }
     };
     if constexpr (MAXB > 0) {
-      V v[MAXB];
+      V v[MAXB], ka[MAXB], kb[MAXB];
 #pragma unroll
       for (int d = 0; d < MAXB; ++d)
-        if (d < beta) v[d] = kld<CPT>((d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n);
+        if (d < beta) {
+          if (SHARE_DIGITS) {
+            v[d] = vd[d];
+            ka[d] = kld<CPT>(J.key + (size_t)d * kstride + koff);
+            kb[d] = kld<CPT>(J.key + (size_t)(dnum + d) * kstride + koff);
+          } else {
+            v[d] = kld<CPT>((d == own && J.x) ? J.x + off : J.digits + ((size_t)d * ext + i) * N + n);
+            ka[d] = ka_g[d];
+            kb[d] = kb_g[d];
+          }
+        }
       if (own >= 0 && J.x2) y1 = kld<CPT>(J.x2 + off);
       V x0{}, y0{};
       if (tensor) {
@@ -206,7 +217,15 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
       ob[n] = rb[0];
     }
   };
-  if constexpr (MAXB > 0) {
+  if constexpr (MAXB > 0 && SHARE_DIGITS) {
+    V vd[MAXB];  // the group's digit tile (hoisted rotations of one ciphertext), read once
+#pragma unroll
+    for (int d = 0; d < MAXB; ++d)
+      if (d < beta) vd[d] = kld<CPT>((d == own && J0.x) ? J0.x + off : J0.digits + ((size_t)d * ext + i) * N + n);
+#pragma unroll
+    for (int jj = 0; jj < JG; ++jj)
+      if (jj < gn) run(L.j[g0 + jj], nullptr, nullptr, vd);
+  } else if constexpr (MAXB > 0) {
     V ka[MAXB], kb[MAXB];  // the group's key tile, read once
 #pragma unroll
     for (int d = 0; d < MAXB; ++d)
@@ -216,9 +235,9 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
       }
 #pragma unroll
     for (int jj = 0; jj < JG; ++jj)
-      if (jj < gn) run(L.j[g0 + jj], ka, kb);
+      if (jj < gn) run(L.j[g0 + jj], ka, kb, nullptr);
   } else {
-    for (int jj = 0; jj < gn; ++jj) run(L.j[g0 + jj], nullptr, nullptr);
+    for (int jj = 0; jj < gn; ++jj) run(L.j[g0 + jj], nullptr, nullptr, nullptr);
   }
 }
 
@@ -474,21 +493,35 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
   for (int off = 0; off < n; off += MAX_KSK_JOBS) {
     int m = std::min(MAX_KSK_JOBS, n - off);
     fill(L, jobs + off, m);
-    // groups of consecutive jobs with one key, level and set of extras
-    auto same = [](const KskJob& a, const KskJob& b) {
+    // groups of consecutive jobs with one key, level and set of extras (a batch under one
+    // switching key), or else with one digit set (hoisted rotations of one ciphertext)
+    auto same_key = [](const KskJob& a, const KskJob& b) {
       return a.key == b.key && a.l == b.l && a.auto_k == b.auto_k && !a.x2 == !b.x2 && !a.a0 == !b.a0 &&
              !a.c0 == !b.c0 && !a.x == !b.x;
     };
-    L.ngroups = 0;
-    int gmax = 1;
-    for (int i = 0; i < m;) {
-      int k = 1;
-      while (i + k < m && k < MAX_KSK_GROUP && same(L.j[i], L.j[i + k])) ++k;
-      L.gstart[L.ngroups] = (uint8_t)i;
-      L.gcount[L.ngroups] = (uint8_t)k;
-      ++L.ngroups;
-      gmax = std::max(gmax, k);
-      i += k;
+    auto same_digits = [](const KskJob& a, const KskJob& b) {
+      return a.digits == b.digits && a.x == b.x && a.x2 == b.x2 && a.l == b.l && !a.a0 == !b.a0 && !a.c0 == !b.c0;
+    };
+    auto group = [&](auto same) {
+      L.ngroups = 0;
+      int gm = 1;
+      for (int i = 0; i < m;) {
+        int k = 1;
+        while (i + k < m && k < MAX_KSK_GROUP && same(L.j[i], L.j[i + k])) ++k;
+        L.gstart[L.ngroups] = (uint8_t)i;
+        L.gcount[L.ngroups] = (uint8_t)k;
+        ++L.ngroups;
+        gm = std::max(gm, k);
+        i += k;
+      }
+      return gm;
+    };
+    int gmax = group(same_key);
+    bool share_digits = false;
+    if (gmax == 1) {
+      gmax = group(same_digits);
+      share_digits = gmax > 1;
+      if (!share_digits) group(same_key);
     }
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
@@ -501,18 +534,23 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
       bytes += 8.0 * c->N * ((double)ext * (b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
     }
     for (int g = 0; g < L.ngroups; ++g) {
-      const int l = L.j[L.gstart[g]].l;
-      bytes += 8.0 * c->N * 2.0 * c->beta(l) * (l + c->K);
+      const int l = L.j[L.gstart[g]].l, b = c->beta(l), ext = l + c->K;
+      // the shared tile once per group, the other per job
+      bytes += 8.0 * c->N * (share_digits ? (double)b * ext + 2.0 * b * ext * L.gcount[g] - (double)b * ext * L.gcount[g]
+                                          : 2.0 * b * ext);
     }
     int maxb = 0;
     for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     LaunchScope ls(c, s, KK_KSK, bytes);
     auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K,
                                                               c->dnum, c->alpha); };
-    switch (maxb * 8 + jg) {
+    switch (maxb * 8 + jg + (share_digits ? 64 : 0)) {
 #define FIDES_KSK_CASE(B, G)                    \
   case B * 8 + G:                               \
     go(ksk_kernel<B, G, 2>);                    \
+    break;                                      \
+  case 64 + B * 8 + G:                          \
+    go(ksk_kernel<B, G, 2, true>);              \
     break;
       FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4)
       FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4)

@@ -241,20 +241,32 @@ __global__ void __launch_bounds__(TC_M, 7)
     ok = __syncthreads_and(bar_wait_bounded(bar_a, c & 1));
     if (!ok) break;
     tc_fence_after();
-    for (int g = 0; g < ndc; g += 4) {
-      uint32_t d[4][8];
+    // software-pipelined epilogue: the TMEM loads of the next pair of outputs are in flight
+    // while the current pair is folded (tcgen05.wait::ld waits for all of them, so each wait
+    // follows the fold of the pair loaded before it)
+    uint32_t d[2][2][8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (g + u < ndc) tmem_ld8(trow + 8 * (g + u), d[u]);
-      tmem_wait_ld();
+    for (int u = 0; u < 2; ++u)
+      if (u < ndc) tmem_ld8(trow + 8 * u, d[0][u]);
+    tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        pin8(d[u]);
-        const int j = c * TC_DCHUNK + g + u;
-        if (g + u < ndc && j < nd) {
-          const TcDest& P = dconst[j];
-          J.dst[(size_t)dpos[j] * N + coef] = tc_fold(d[u], P.q, __longlong_as_double((long long)P.qinv));
+    for (int h = 0; h < TC_DCHUNK / 2; ++h) {
+      const int g = 2 * h;
+      if (g < ndc) {
+        const int cur = h & 1, nxt = cur ^ 1;
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+          if (g + 2 + u < ndc) tmem_ld8(trow + 8 * (g + 2 + u), d[nxt][u]);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          pin8(d[cur][u]);
+          const int j = c * TC_DCHUNK + g + u;
+          if (g + u < ndc && j < nd) {
+            const TcDest& P = dconst[j];
+            J.dst[(size_t)dpos[j] * N + coef] = tc_fold(d[cur][u], P.q, __longlong_as_double((long long)P.qinv));
+          }
         }
+        tmem_wait_ld();
       }
     }
     tc_fence_before();

@@ -826,6 +826,51 @@ int fides_rotate_host_batch(fides_ctx* x, const fides_rotate_host_item* items, i
   });
 }
 
+int fides_mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
+                           int rescale, const fides_rotate_host_item* rot, int n_rot) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n_hm < 0 || n_rot < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    if (n_hm > 0) {
+      need(hm, "hmult items");
+      need(relin_key_dev, "relin_key_dev");
+    }
+    if (n_rot > 0) need(rot, "rotate items");
+    // one pipeline, the two kinds interleaved: an HMult moves twice the host->device bytes of
+    // a rotation for the same device->host bytes, so alternating them keeps both copy
+    // directions busy, and one pipeline fills and drains once
+    std::vector<HostJob> jobs;
+    std::vector<std::pair<int, int>> which;  // (kind, index)
+    for (int i = 0, j = 0; i < n_hm || j < n_rot;) {
+      if (i < n_hm) {
+        const auto& it = hm[i];
+        if (it.level < (rescale ? 2 : 1) || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+        jobs.push_back(HostJob{{it.a0, it.a1, it.b0, it.b1}, it.level, {it.out0, it.out1},
+                               rescale ? it.level - 1 : it.level});
+        which.push_back({0, i++});
+      }
+      if (j < n_rot) {
+        const auto& it = rot[j];
+        if (it.level < 1 || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+        need(it.rot_key_dev, "rot_key_dev");
+        jobs.push_back(HostJob{{it.c0, it.c1}, it.level, {it.out0, it.out1}, it.level});
+        which.push_back({1, j++});
+      }
+    }
+    host_pipeline(x, jobs, [&](int k, std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {
+      if (which[k].first == 0) {
+        fides::HMultItem h{in[0], in[1], in[2], in[3], out[0], out[1], hm[which[k].second].level};
+        fides::op_hmult_batch(c, &h, 1, relin_key_dev, rescale != 0, s);
+      } else {
+        const auto& it = rot[which[k].second];
+        fides::RotateItem r{in[0], in[1], out[0], out[1], it.rot_key_dev, it.level,
+                            fides::h_auto_index(c->logN, it.rotation)};
+        fides::op_rotate_batch(c, &r, 1, s);
+      }
+    });
+  });
+}
+
 int fides_hmult_host(fides_ctx* x, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1,
                      int level, const uint64_t* relin_key_dev, int rescale, uint64_t* out0, uint64_t* out1) {
   return guard([&] {

@@ -140,6 +140,8 @@ def lib():
         L.fides_rotate_host.argtypes = [vp, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
         L.fides_hmult_host_batch.argtypes = [vp, C.POINTER(_HMultHostItem), C.c_int, vp, C.c_int]
         L.fides_rotate_host_batch.argtypes = [vp, C.POINTER(_RotateHostItem), C.c_int]
+        L.fides_mixed_host_batch.argtypes = [vp, C.POINTER(_HMultHostItem), C.c_int, vp, C.c_int,
+                                             C.POINTER(_RotateHostItem), C.c_int]
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -680,6 +682,20 @@ class Context:
             arr[k] = _RotateHostItem(c0.ctypes.data, c1.ctypes.data, o0.ctypes.data, o1.ctypes.data, key,
                                      c0.shape[0], r)
         _check(lib().fides_rotate_host_batch(self._h, arr, len(items)))
+
+    def mixed_host_batch(self, hmult_items, dev_key: int, rotate_items, rescale=True):
+        """HMults and rotations of host ciphertexts through one pipeline (items as in
+        mult_host_batch / rotate_host_batch, alternated); outputs are written in place."""
+        ha = (_HMultHostItem * max(1, len(hmult_items)))()
+        for k, (a0, a1, b0, b1, o0, o1) in enumerate(hmult_items):
+            ha[k] = _HMultHostItem(a0.ctypes.data, a1.ctypes.data, b0.ctypes.data, b1.ctypes.data,
+                                   o0.ctypes.data, o1.ctypes.data, a0.shape[0])
+        ra = (_RotateHostItem * max(1, len(rotate_items)))()
+        for k, (c0, c1, o0, o1, key, r) in enumerate(rotate_items):
+            ra[k] = _RotateHostItem(c0.ctypes.data, c1.ctypes.data, o0.ctypes.data, o1.ctypes.data, key,
+                                    c0.shape[0], r)
+        _check(lib().fides_mixed_host_batch(self._h, ha, len(hmult_items), dev_key, 1 if rescale else 0, ra,
+                                            len(rotate_items)))
 
 
 def pinned_empty(shape) -> "np.ndarray":

@@ -368,6 +368,14 @@ typedef struct {
   int rotation;
 } fides_rotate_host_item;
 int fides_rotate_host_batch(fides_ctx* ctx, const fides_rotate_host_item* items, int n);
+/* Both kinds in one pipeline, alternated (an HMult item, a rotation item, ...): one fill and
+ * drain of the pipeline instead of two, and the copy directions stay balanced (an HMult moves
+ * twice a rotation's host->device bytes for the same device->host bytes).  Results equal
+ * fides_hmult_host_batch / fides_rotate_host_batch on the same items.  No reference
+ * counterpart (the reference loads and recovers one ciphertext at a time,
+ * CudaEngine.cpp:1156-1227). */
+int fides_mixed_host_batch(fides_ctx* ctx, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
+                           int rescale, const fides_rotate_host_item* rot, int n_rot);
 
 /* ---- allocation-free entry point ----------------------------------------------------
  * No counterpart in the reference.  fides_rescale_noalloc computes exactly what

@@ -72,6 +72,36 @@ def test_rotate_host_batch_matches_oracle(env):
             ctx.key_free(v)
 
 
+def test_mixed_host_batch_matches_oracle(env):
+    """HMults and rotations alternated in one pipeline (fides_mixed_host_batch), uneven counts
+    and levels: every item equals the oracle."""
+    F, prm, o, ctx, rk, rot = env
+    key = ctx.key_upload(rk)
+    keys = {r: ctx.key_upload(k) for r, k in rot.items()}
+    try:
+        hm, hrefs = [], []
+        for k, l in enumerate([6, 4, 5]):
+            a, b = host_ct(F, prm, l, 1500 + 2 * k), host_ct(F, prm, l, 1501 + 2 * k)
+            o0, o1 = F.pinned_empty((l - 1, prm.N)), F.pinned_empty((l - 1, prm.N))
+            hm.append((a[0], a[1], b[0], b[1], o0, o1))
+            hrefs.append(o.hmult(a[0], a[1], b[0], b[1], rk, rescale=True))
+        rt, rrefs = [], []
+        for k, (l, r) in enumerate([(6, 1), (3, -2), (5, 1), (6, -2), (2, 1)]):
+            c = host_ct(F, prm, l, 1600 + k)
+            o0, o1 = F.pinned_empty((l, prm.N)), F.pinned_empty((l, prm.N))
+            rt.append((c[0], c[1], o0, o1, keys[r], r))
+            rrefs.append(o.rotate(c[0], c[1], rot[r], r))
+        ctx.mixed_host_batch(hm, key, rt, True)
+        for k, ((*_, o0, o1), (r0, r1)) in enumerate(zip(hm, hrefs)):
+            assert np.array_equal(o0, r0) and np.array_equal(o1, r1), f"hmult item {k}"
+        for k, ((_, _, o0, o1, _, _), (r0, r1)) in enumerate(zip(rt, rrefs)):
+            assert np.array_equal(o0, r0) and np.array_equal(o1, r1), f"rotate item {k}"
+    finally:
+        ctx.key_free(key)
+        for v in keys.values():
+            ctx.key_free(v)
+
+
 def test_host_batch_rejects_bad_level(env):
     F, prm, o, ctx, rk, _ = env
     key = ctx.key_upload(rk)

@@ -838,23 +838,24 @@ int fides_mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_
     if (n_rot > 0) need(rot, "rotate items");
     // one pipeline, the two kinds interleaved: an HMult moves twice the host->device bytes of
     // a rotation for the same device->host bytes, so alternating them keeps both copy
-    // directions busy, and one pipeline fills and drains once
+    // directions busy, and one pipeline fills and drains once; a rotation goes first, so the
+    // fill (the first item's host->device copies, which nothing overlaps) is the shorter one
     std::vector<HostJob> jobs;
     std::vector<std::pair<int, int>> which;  // (kind, index)
     for (int i = 0, j = 0; i < n_hm || j < n_rot;) {
-      if (i < n_hm) {
-        const auto& it = hm[i];
-        if (it.level < (rescale ? 2 : 1) || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
-        jobs.push_back(HostJob{{it.a0, it.a1, it.b0, it.b1}, it.level, {it.out0, it.out1},
-                               rescale ? it.level - 1 : it.level});
-        which.push_back({0, i++});
-      }
       if (j < n_rot) {
         const auto& it = rot[j];
         if (it.level < 1 || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
         need(it.rot_key_dev, "rot_key_dev");
         jobs.push_back(HostJob{{it.c0, it.c1}, it.level, {it.out0, it.out1}, it.level});
         which.push_back({1, j++});
+      }
+      if (i < n_hm) {
+        const auto& it = hm[i];
+        if (it.level < (rescale ? 2 : 1) || it.level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+        jobs.push_back(HostJob{{it.a0, it.a1, it.b0, it.b1}, it.level, {it.out0, it.out1},
+                               rescale ? it.level - 1 : it.level});
+        which.push_back({0, i++});
       }
     }
     host_pipeline(x, jobs, [&](int k, std::vector<uint64_t*>& in, std::vector<uint64_t*>& out, cudaStream_t s) {

@@ -217,6 +217,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     std::vector<DevPrime> hp(np);
     std::vector<ShoupConst> tf((size_t)np * N), ti((size_t)np * N), il(np);
     std::vector<double2> tff((size_t)np * N), tfi((size_t)np * N);
+    std::vector<double> twf_w((size_t)np * N), twi_w((size_t)np * N);
     std::vector<F64Prime> f64(np);
     auto work = [&](int i) {
       uint64_t q = primes[i];
@@ -246,6 +247,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       for (size_t j = 0; j < (size_t)N; ++j) {
         tff[i * N + j] = make_double2((double)tf[i * N + j].w, (double)tf[i * N + j].w / qd);
         tfi[i * N + j] = make_double2((double)ti[i * N + j].w, (double)ti[i * N + j].w / qd);
+        twf_w[i * N + j] = (double)tf[i * N + j].w;
+        twi_w[i * N + j] = (double)ti[i * N + j].w;
       }
       f64[i] = F64Prime{qd, 1.0 / qd, (double)d.ninv, (double)d.ninv / qd, (double)il[i].w, (double)il[i].w / qd};
     };
@@ -339,7 +342,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     }
     // ---- pack everything into one device blob
     std::vector<char> blob;
-    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq, o_tff, o_tfi, o_f64;
+    size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq, o_tff, o_tfi, o_f64, o_tww, o_twwi;
     append(blob, hp, o_prime);
     append(blob, tf, o_tf);
     append(blob, ti, o_ti);
@@ -350,6 +353,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     append(blob, pqinv, o_pq);
     append(blob, tff, o_tff);
     append(blob, tfi, o_tfi);
+    append(blob, twf_w, o_tww);
+    append(blob, twi_w, o_twwi);
     append(blob, f64, o_f64);
     struct Off {
       size_t sp, spr, pre, dp, dpr, mat, tcb, tcd;
@@ -390,6 +395,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     c->d_pqinv = reinterpret_cast<ShoupConst*>(base + o_pq);
     c->d_twf_fwd = reinterpret_cast<double2*>(base + o_tff);
     c->d_twf_inv = reinterpret_cast<double2*>(base + o_tfi);
+    c->d_tww_fwd = reinterpret_cast<double*>(base + o_tww);
+    c->d_tww_inv = reinterpret_cast<double*>(base + o_twwi);
     c->d_f64 = reinterpret_cast<F64Prime*>(base + o_f64);
     auto mk = [&](const Off& o) {
       ConvTable t;

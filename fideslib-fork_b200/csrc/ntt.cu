@@ -19,6 +19,7 @@ void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream
   a.primes = c->d_prime;
   a.tw = inverse ? c->d_tw_inv : c->d_tw_fwd;
   a.twf = inverse ? c->d_twf_inv : c->d_twf_fwd;
+  a.tww = inverse ? c->d_tww_inv : c->d_tww_fwd;
   a.f64 = c->d_f64;
   a.inv_last = c->d_inv_last;
   a.pinv = c->d_pinv;

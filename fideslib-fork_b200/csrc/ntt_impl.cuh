@@ -46,6 +46,11 @@ __device__ __forceinline__ ShoupConst ld_tw(const ShoupConst* p, uint64_t pol) {
   asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(w), "=l"(ws) : "l"(p), "l"(pol));
   return ShoupConst{w, ws};
 }
+__device__ __forceinline__ double ld_tww(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ double2 ld_twf(const double2* p, uint64_t pol) {
   double2 v;
   asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
@@ -123,6 +128,8 @@ struct PassArgs {
   const DevPrime* primes;
   const ShoupConst* tw;        // forward or inverse twiddles, [prime][N]
   const double2* twf;          // the same twiddles as (w, w / q) doubles (q < 2^50)
+  const double* tww;           // w alone: the row passes (one twiddle per row and stage each) read
+                               // half the bytes and derive w / q
   const F64Prime* f64;         // [prime]
   const ShoupConst* inv_last;  // [prime]: psi_rev^-1[1] * N^-1
   const ShoupConst* pinv;      // [Q prime]: P^-1 mod q (OUT_MODDOWN)
@@ -194,7 +201,7 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
 // run_chunk on FP64 residues (q < 2^50): the same stages, pairs and twiddles.
 template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS>
 __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int sub, int sbase, const double2* tw,
-                                              const F64Prime& fp, uint64_t pol) {
+                                              const double* tww, const F64Prime& fp, uint64_t pol) {
   constexpr int E = 1 << LOGE;
   const int th = t >> LO;
 #pragma unroll
@@ -215,7 +222,15 @@ __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int
           x[r1] = f_mulmod(__dsub_rn(a, c), fp.last, fp.last_q, fp.q);
         }
       } else {
-        const double2 w = ld_twf(tw + base + hi, pol);
+        double2 w;
+        if constexpr (PASS == ROW) {
+          // w / q correctly rounded from w: a Newton step on fl(w / q) (exact residual by fma)
+          w.x = ld_tww(tww + base + hi, pol);
+          const double q0 = __dmul_rn(w.x, fp.qinv);
+          w.y = __fma_rn(__fma_rn(-q0, fp.q, w.x), fp.qinv, q0);
+        } else {
+          w = ld_twf(tw + base + hi, pol);
+        }
 #pragma unroll
         for (int lr = 0; lr < (1 << rb); ++lr) {
           const int r0 = (hi << (rb + 1)) | lr, r1 = r0 | (1 << rb);
@@ -290,13 +305,13 @@ __device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, S
 // chunks() on FP64 residues; the shared-memory exchanges move the doubles' bits.
 template <int LOGP, int PASS, bool FWD, typename SIDX>
 __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu, SIDX sidx, int g, int t, int subtw,
-                                           int sbase, const double2* tw, const F64Prime& fp, bool direct_load,
-                                           uint64_t pol) {
+                                           int sbase, const double2* tw, const double* tww, const F64Prime& fp,
+                                           bool direct_load, uint64_t pol) {
   constexpr int E = 1 << LOGE;
   constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
   double* sm = reinterpret_cast<double*>(smu);
   using C0 = Chunk<LOGP, FWD, 0>;
-  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
+  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   if constexpr (NCH > 1) {
     using C1 = Chunk<LOGP, FWD, 1>;
     if (!direct_load) __syncthreads();
@@ -305,7 +320,7 @@ __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
-    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
+    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   }
   if constexpr (NCH > 2) {
     using C1 = Chunk<LOGP, FWD, 1>;
@@ -316,7 +331,7 @@ __device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
-    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, fp, pol);
+    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   }
 }
 
@@ -433,8 +448,8 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
 #pragma unroll
       for (int r = 0; r < E; ++r) xf[r] = __longlong_as_double((long long)x[r]);  // the first pass's doubles
     }
-    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N, fp, direct_load,
-                                pol);
+    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N,
+                                a.tww + (size_t)lr.prime * N, fp, direct_load, pol);
     if (first_pass) {
 #pragma unroll
       for (int r = 0; r < E; ++r) x[r] = (uint64_t)__double_as_longlong(xf[r]);

@@ -368,7 +368,7 @@ typedef struct {
   int rotation;
 } fides_rotate_host_item;
 int fides_rotate_host_batch(fides_ctx* ctx, const fides_rotate_host_item* items, int n);
-/* Both kinds in one pipeline, alternated (an HMult item, a rotation item, ...): one fill and
+/* Both kinds in one pipeline, alternated (a rotation item, an HMult item, ...): one fill and
  * drain of the pipeline instead of two, and the copy directions stay balanced (an HMult moves
  * twice a rotation's host->device bytes for the same device->host bytes).  Results equal
  * fides_hmult_host_batch / fides_rotate_host_batch on the same items.  No reference

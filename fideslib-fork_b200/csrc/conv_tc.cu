@@ -2,9 +2,9 @@
 // conv_tc.hpp; this file holds the table builder and the kernel.
 //
 // One CTA converts 128 coefficients (the MMA's M, one TMEM lane each) of one job:
-//   1. warp 0 allocates 64 TMEM columns; the CTA copies the table's B image (the shared-memory
-//      form of the byte matrix) and writes A: the eight bytes of every pre-scaled residue y_i
-//      of its 128 coefficients, K-major;
+//   1. warp 0 allocates 64 TMEM columns; thread 0 starts a bulk copy of the table's B image
+//      (the shared-memory form of the byte matrix) while the CTA writes A: the eight bytes of
+//      every pre-scaled residue y_i of its 128 coefficients, K-major;
 //   2. per chunk of 8 destination limbs (64 columns: 8 byte planes each), thread 0 issues
 //      K/32 MMAs (M 128, N 8 x limbs, K 32) and commits them to an mbarrier;
 //   3. after a bounded wait, each warp reads its 32 TMEM lanes (tcgen05.ld 32x32b), folds the
@@ -63,7 +63,7 @@ struct TcLayout {
 };
 __host__ __device__ inline TcLayout tc_layout(int kpad, int ndp) {
   TcLayout L;
-  L.o_dst = 16;  // [0, 8): mbarrier, [8, 12): TMEM address
+  L.o_dst = 32;  // [0, 8): MMA mbarrier, [8, 16): B-copy mbarrier, [16, 20): TMEM address
   L.o_pos = L.o_dst + ndp * (int)sizeof(TcDest);
   L.o_a = (L.o_pos + ndp * 4 + 127) & ~127;
   L.o_b = L.o_a + TC_M * kpad;
@@ -142,11 +142,14 @@ __device__ __forceinline__ void pin8(uint32_t (&d)[8]) {
 }
 
 // sum_c 2^(8c) d[c] mod q for planes d[c] < 2^23 and a prime 2^48 < q < 2^62.
-// V = x + 2^32 y with x, y < 2^49 (so V < 2^80) is reduced by floating-point Barrett
-// reduction (the double-precision quotient estimate of NTL's MulMod): the integers x, y
-// convert to doubles exactly (2^52 exponent trick), fl(V) fl(1/q) is within 2^-20 of V/q
-// because V/q < 2^32, so qh = floor(fl(V / q)) is floor(V / q) or one off either way.
-// Then V - qh q lies in (-q, 2q) and is computed exactly in wrapping 64-bit arithmetic.
+// V = x + 2^32 y with x, y < 2^49 (V < 2^79.01 for K <= 128) is reduced by floating-point
+// Barrett reduction (the double-precision quotient estimate of NTL's MulMod): the integers
+// x, y convert to doubles exactly (2^52 exponent trick), and vd = fl(V), qinv = fl(1/q) give
+// vd qinv within 2^-20 of V/q (V/q < 2^31.01); the fma adds 2^-17 with one more rounding of
+// at most 2^-21, so t lies in (V/q + 2^-17.6, V/q + 2^-16.6) and qh = floor(t) is
+// floor(V/q) or one more (qh < 2^32).  V - qh q lies in [-q, q), is computed exactly in
+// wrapping 64-bit arithmetic and needs one correction.  (Checked against 128-bit arithmetic
+// on 40 M random, extreme and next-to-a-multiple-of-q plane sets over 4000 primes.)
 __device__ __forceinline__ uint64_t tc_fold(const uint32_t (&d)[8], uint64_t q, double qinv) {
   const uint32_t a0 = d[0] + (d[1] << 8), a1 = d[2] + (d[3] << 8);  // < 2^32
   const uint32_t a2 = d[4] + (d[5] << 8), a3 = d[6] + (d[7] << 8);
@@ -156,10 +159,40 @@ __device__ __forceinline__ uint64_t tc_fold(const uint32_t (&d)[8], uint64_t q, 
   const double xd = __longlong_as_double((long long)(0x4330000000000000ull | x)) - two52;
   const double yd = __longlong_as_double((long long)(0x4330000000000000ull | y)) - two52;
   const double vd = fma(yd, 4294967296.0, xd);
-  const uint32_t qh = (uint32_t)__double2loint(__dadd_rd(vd * qinv, two52));  // floor, < 2^32
-  int64_t r = (int64_t)(x + (y << 32) - (uint64_t)qh * q);
-  r = r < 0 ? r + (int64_t)q : r;
-  return (uint64_t)(r >= (int64_t)q ? r - (int64_t)q : r);
+  const uint32_t qh = (uint32_t)__double2loint(__dadd_rd(fma(vd, qinv, 0x1p-17), two52));  // floor, < 2^32
+  uint64_t r = x + (y << 32) - (uint64_t)qh * q;
+  return r + ((uint64_t)((int64_t)r >> 63) & q);
+}
+
+// Stores the folded outputs of one chunk of NDC destination limbs (8 byte-plane columns each,
+// starting at TMEM address trow).  The TMEM loads of the next pair are in flight while the
+// current pair is folded; tcgen05.wait::ld waits for all of them, so each wait follows the
+// fold of the pair loaded before it.  dofs[j] = output limb position of destination j times N.
+template <int NDC, bool CHECK>
+__device__ __forceinline__ void tc_epilogue(uint32_t trow, int j0, int nd, const TcDest* dconst, const int* dofs,
+                                            uint64_t* out) {
+  uint32_t d[2][2][8];
+  tmem_ld8(trow, d[0][0]);
+  tmem_ld8(trow + 8, d[0][1]);
+  tmem_wait_ld();
+#pragma unroll
+  for (int h = 0; h < NDC / 2; ++h) {
+    const int cur = h & 1, nxt = cur ^ 1;
+    if (h + 1 < NDC / 2) {
+      tmem_ld8(trow + 8 * (2 * h + 2), d[nxt][0]);
+      tmem_ld8(trow + 8 * (2 * h + 3), d[nxt][1]);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      pin8(d[cur][u]);
+      const int j = j0 + 2 * h + u;
+      if (!CHECK || j < nd) {
+        const TcDest P = dconst[j];
+        out[dofs[j]] = tc_fold(d[cur][u], P.q, __longlong_as_double((long long)P.qinv));
+      }
+    }
+    if (h + 1 < NDC / 2) tmem_wait_ld();
+  }
 }
 
 __global__ void __launch_bounds__(TC_M, 7)
@@ -173,12 +206,13 @@ __global__ void __launch_bounds__(TC_M, 7)
   const int N = 1 << logN;
   const int coef = blockIdx.x * TC_M + tid;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + 8);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + 16);
   TcDest* dconst = reinterpret_cast<TcDest*>(sm + Ly.o_dst);
-  int* dpos = reinterpret_cast<int*>(sm + Ly.o_pos);
+  int* dofs = reinterpret_cast<int*>(sm + Ly.o_pos);
   uint8_t* sA = sm + Ly.o_a;
   uint8_t* sB = sm + Ly.o_b;
-  const uint32_t bar_a = smem_addr(bar);
+  const uint32_t bar_a = smem_addr(bar), bar_b = smem_addr(bar + 1);
+  const uint32_t b_bytes = (uint32_t)kpad * 8u * (uint32_t)ndp;  // a multiple of 256
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)),
@@ -188,17 +222,20 @@ __global__ void __launch_bounds__(TC_M, 7)
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_b), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // B image: one bulk copy (global and shared addresses 16-byte aligned, size a multiple of 16)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b), "r"(b_bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(sB)),
+        "l"(T.tc_b), "r"(b_bytes), "r"(bar_b)
+        : "memory");
   }
-  {  // B image and destination constants
-    const uint4* gb = reinterpret_cast<const uint4*>(T.tc_b);
-    uint4* sb = reinterpret_cast<uint4*>(sB);
-    const int n16 = kpad * ndp / 2;  // kpad * 8 ndp bytes / 16
-    for (int i = tid; i < n16; i += TC_M) sb[i] = gb[i];
-    for (int j = tid; j < ndp; j += TC_M) {
-      dconst[j] = T.tc_dst[j];
-      dpos[j] = j < nd ? T.dst_pos[j] : 0;
-    }
+  for (int j = tid; j < ndp; j += TC_M) {  // destination constants
+    dconst[j] = T.tc_dst[j];
+    dofs[j] = j < nd ? T.dst_pos[j] << logN : 0;
   }
   {  // A: the bytes of the pre-scaled residues of this thread's coefficient
     uint64_t x[TC_MAX_SRC];
@@ -220,14 +257,14 @@ __global__ void __launch_bounds__(TC_M, 7)
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   tc_fence_before();
-  __syncthreads();
+  bool ok = __syncthreads_and(bar_wait_bounded(bar_b, 0));  // B image landed
   tc_fence_after();
   const uint32_t tbase = *slot;
   const uint32_t a0 = smem_addr(sA), b0 = smem_addr(sB);
   const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);
   const int nchunks = (ndp + TC_DCHUNK - 1) / TC_DCHUNK;
-  bool ok = true;
-  for (int c = 0; c < nchunks; ++c) {
+  uint64_t* out = J.dst + coef;
+  for (int c = 0; ok && c < nchunks; ++c) {
     const int ndc = min(TC_DCHUNK, ndp - c * TC_DCHUNK);  // even: N = 8 ndc is a multiple of 16
     if (tid == 0) {
       const uint32_t idesc = idesc_u8(8 * ndc);
@@ -241,34 +278,17 @@ __global__ void __launch_bounds__(TC_M, 7)
     ok = __syncthreads_and(bar_wait_bounded(bar_a, c & 1));
     if (!ok) break;
     tc_fence_after();
-    // software-pipelined epilogue: the TMEM loads of the next pair of outputs are in flight
-    // while the current pair is folded (tcgen05.wait::ld waits for all of them, so each wait
-    // follows the fold of the pair loaded before it)
-    uint32_t d[2][2][8];
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-      if (u < ndc) tmem_ld8(trow + 8 * u, d[0][u]);
-    tmem_wait_ld();
-#pragma unroll
-    for (int h = 0; h < TC_DCHUNK / 2; ++h) {
-      const int g = 2 * h;
-      if (g < ndc) {
-        const int cur = h & 1, nxt = cur ^ 1;
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-          if (g + 2 + u < ndc) tmem_ld8(trow + 8 * (g + 2 + u), d[nxt][u]);
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          pin8(d[cur][u]);
-          const int j = c * TC_DCHUNK + g + u;
-          if (g + u < ndc && j < nd) {
-            const TcDest& P = dconst[j];
-            J.dst[(size_t)dpos[j] * N + coef] = tc_fold(d[cur][u], P.q, __longlong_as_double((long long)P.qinv));
-          }
-        }
-        tmem_wait_ld();
-      }
-    }
+    const int j0 = c * TC_DCHUNK;
+    if (ndc == TC_DCHUNK && j0 + TC_DCHUNK <= nd)
+      tc_epilogue<TC_DCHUNK, false>(trow, j0, nd, dconst, dofs, out);
+    else if (ndc == 2)
+      tc_epilogue<2, true>(trow, j0, nd, dconst, dofs, out);
+    else if (ndc == 4)
+      tc_epilogue<4, true>(trow, j0, nd, dconst, dofs, out);
+    else if (ndc == 6)
+      tc_epilogue<6, true>(trow, j0, nd, dconst, dofs, out);
+    else
+      tc_epilogue<8, true>(trow, j0, nd, dconst, dofs, out);
     tc_fence_before();
     __syncthreads();  // TMEM columns are free for the next chunk
     tc_fence_after();

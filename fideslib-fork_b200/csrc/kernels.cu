@@ -1,5 +1,6 @@
 // Elementwise RNS kernels, basis conversion and KSK inner product.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "kernels.cuh"
@@ -96,10 +97,37 @@ __device__ __forceinline__ KVec<CPT> kld(const uint64_t* q) {
   return v;
 }
 
+// FP64 products for limbs of primes q < 2^50 (the NTT's FP64 residues, here on canonical
+// inputs a, b < q): p = fl(ab), e = fma(a, b, -p) = ab - p exactly; k = rint(p (1/q)) from one
+// fma with the rounding constant 1.5 2^52, within 1 of ab / q (p (1/q) is within
+// (ab / q) 2^-52 <= 1/2 of ab / q); p - k q is below 2^53 in magnitude, so fma(-k, q, p) is
+// exact, and so is adding e: r = ab - k q with |r| <= q.  The a side of the inner product (up to
+// four digits and two tensor terms: |sum| <= 6q < 2^53, summed exactly and reduced once) and
+// the own digit's a1 b1 run on the FP64 pipe; the b side keeps the 128-bit integer products on
+// the FMA-heavy pipe.  (Moving the tensor terms' P products and the b side's P a0 b0 to FP64
+// as well was 12 % slower.)
+__device__ __forceinline__ double ksk_f64(uint64_t v) {
+  return __dadd_rn(__longlong_as_double((long long)(0x4330000000000000ull | v)), -4503599627370496.0);
+}
+__device__ __forceinline__ double ksk_mul_f64(uint64_t a, uint64_t b, double q, double qinv) {
+  const double x = ksk_f64(a), y = ksk_f64(b);
+  const double p = __dmul_rn(x, y);
+  const double e = __fma_rn(x, y, -p);
+  const double k = __dadd_rn(__fma_rn(p, qinv, 6755399441055744.0), -6755399441055744.0);
+  return __dadd_rn(__fma_rn(-k, q, p), e);
+}
+// canonical residue of an exact sum |s| < 2^53
+__device__ __forceinline__ uint64_t ksk_canon_f64(double s, double q, double qinv) {
+  const double k = __dadd_rn(__fma_rn(s, qinv, 6755399441055744.0), -6755399441055744.0);
+  double r = __fma_rn(-k, q, s);  // |r| <= q / 2 + 1
+  if (r < 0) r = __dadd_rn(r, q);
+  return (uint64_t)__double_as_longlong(__dadd_rn(r, 4503599627370496.0)) & ((1ull << 52) - 1);
+}
+
 template <int MAXB, int JG, int CPT, bool SHARE_DIGITS = false>
 __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
-                                                            const ShoupConst* pmod, int logN, int n_q, int K, int dnum,
-                                                            int alpha) {
+                                                            const ShoupConst* pmod, const F64Prime* f64, int logN,
+                                                            int n_q, int K, int dnum, int alpha) {
   using V = KVec<CPT>;
   const int g0 = L.gstart[blockIdx.z], gn = L.gcount[blockIdx.z];
   const KskJob& J0 = L.j[g0];  // the group's jobs share key, level and extras
@@ -115,22 +143,39 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
   const size_t kstride = (size_t)(n_q + K) * N;
   const size_t off = (size_t)i * N + n, koff = (size_t)pid * N + n;
   const bool tensor = J0.a0 && i < l;
+  // FP64 a side: limbs of primes below 2^50, at most 4 digits (so at most 6 summed terms)
+  const bool fa_on = MAXB > 0 && p.q < (1ull << 50);
+  double fq = 0, fqinv = 0;
+  if (fa_on) {
+    fq = f64[pid].q;
+    fqinv = f64[pid].qinv;
+  }
   // one job: sum_d D_d key_d (+ extras), reduced and stored; ka / kb: the group's key tile, or
-  // vd: the group's digit tile (MAXB > 0; the other one is loaded here)
-  auto run = [&](const KskJob& J, const V* ka_g, const V* kb_g, const V* vd) {
+  // vd: the group's digit tile (MAXB > 0; the other one is loaded here).  FA: the a side's
+  // products and the own digit's a1 b1 in FP64.
+  auto run = [&](const KskJob& J, const V* ka_g, const V* kb_g, const V* vd, auto fa_) {
+    constexpr bool FA = decltype(fa_)::value;
     U128 sa[CPT], sb[CPT];
+    double fs[CPT];  // FA: the a side
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) sa[c] = sb[c] = U128{0, 0};
+    for (int c = 0; c < CPT; ++c) {
+      sa[c] = sb[c] = U128{0, 0};
+      fs[c] = 0;
+    }
     V x1{}, y1{};  // a1, b1 of this limb (own digit)
     auto digit = [&](int d, V v, const V& a_, const V& b_) {
       if (d == own && J.x2) {  // the own digit is x * x2 (tensor term a1 b1)
         x1 = v;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) v.c[c] = mulmod(v.c[c], y1.c[c], p);
+        for (int c = 0; c < CPT; ++c)
+          v.c[c] = FA ? ksk_canon_f64(ksk_mul_f64(v.c[c], y1.c[c], fq, fqinv), fq, fqinv) : mulmod(v.c[c], y1.c[c], p);
       }
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
-        mac128(sa[c], v.c[c], a_.c[c]);
+        if constexpr (FA)
+          fs[c] = __dadd_rn(fs[c], ksk_mul_f64(v.c[c], a_.c[c], fq, fqinv));
+        else
+          mac128(sa[c], v.c[c], a_.c[c]);
         mac128(sb[c], v.c[c], b_.c[c]);
       }
     };
@@ -140,8 +185,12 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
       for (int c = 0; c < CPT; ++c) {
         const uint64_t py0 = shoup(y0.c[c], pm.w, pm.ws, p.q), py1 = shoup(y1.c[c], pm.w, pm.ws, p.q);
         mac128(sb[c], x0.c[c], py0);  // + P a0 b0
-        mac128(sa[c], x0.c[c], py1);  // + P (a0 b1 + a1 b0)
-        mac128(sa[c], x1.c[c], py0);
+        if constexpr (FA) {           // + P (a0 b1 + a1 b0)
+          fs[c] = __dadd_rn(fs[c], __dadd_rn(ksk_mul_f64(x0.c[c], py1, fq, fqinv), ksk_mul_f64(x1.c[c], py0, fq, fqinv)));
+        } else {
+          mac128(sa[c], x0.c[c], py1);
+          mac128(sa[c], x1.c[c], py0);
+        }
       }
     };
     if constexpr (MAXB > 0) {
@@ -191,7 +240,10 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
     uint64_t ra[CPT], rb[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-      ra[c] = reduce128(sa[c], p);
+      if constexpr (FA)
+        ra[c] = ksk_canon_f64(fs[c], fq, fqinv);
+      else
+        ra[c] = reduce128(sa[c], p);
       rb[c] = reduce128(sb[c], p);
     }
     if (J.c0 && i < l) {
@@ -222,9 +274,15 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
 #pragma unroll
     for (int d = 0; d < MAXB; ++d)
       if (d < beta) vd[d] = kld<CPT>((d == own && J0.x) ? J0.x + off : J0.digits + ((size_t)d * ext + i) * N + n);
+    if (fa_on) {
 #pragma unroll
-    for (int jj = 0; jj < JG; ++jj)
-      if (jj < gn) run(L.j[g0 + jj], nullptr, nullptr, vd);
+      for (int jj = 0; jj < JG; ++jj)
+        if (jj < gn) run(L.j[g0 + jj], nullptr, nullptr, vd, std::true_type{});
+    } else {
+#pragma unroll
+      for (int jj = 0; jj < JG; ++jj)
+        if (jj < gn) run(L.j[g0 + jj], nullptr, nullptr, vd, std::false_type{});
+    }
   } else if constexpr (MAXB > 0) {
     V ka[MAXB], kb[MAXB];  // the group's key tile, read once
 #pragma unroll
@@ -233,11 +291,17 @@ __global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const _
         ka[d] = kld<CPT>(J0.key + (size_t)d * kstride + koff);
         kb[d] = kld<CPT>(J0.key + (size_t)(dnum + d) * kstride + koff);
       }
+    if (fa_on) {
 #pragma unroll
-    for (int jj = 0; jj < JG; ++jj)
-      if (jj < gn) run(L.j[g0 + jj], ka, kb, nullptr);
+      for (int jj = 0; jj < JG; ++jj)
+        if (jj < gn) run(L.j[g0 + jj], ka, kb, nullptr, std::true_type{});
+    } else {
+#pragma unroll
+      for (int jj = 0; jj < JG; ++jj)
+        if (jj < gn) run(L.j[g0 + jj], ka, kb, nullptr, std::false_type{});
+    }
   } else {
-    for (int jj = 0; jj < gn; ++jj) run(L.j[g0 + jj], nullptr, nullptr, nullptr);
+    for (int jj = 0; jj < gn; ++jj) run(L.j[g0 + jj], nullptr, nullptr, nullptr, std::false_type{});
   }
 }
 
@@ -542,8 +606,8 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     int maxb = 0;
     for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     LaunchScope ls(c, s, KK_KSK, bytes);
-    auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->logN, c->n_q, c->K,
-                                                              c->dnum, c->alpha); };
+    auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->d_f64, c->logN, c->n_q,
+                                                              c->K, c->dnum, c->alpha); };
     switch (maxb * 8 + jg + (share_digits ? 64 : 0)) {
 #define FIDES_KSK_CASE(B, G)                    \
   case B * 8 + G:                               \

@@ -2,9 +2,9 @@
 // conv_tc.hpp; this file holds the table builder and the kernel.
 //
 // One CTA converts 128 coefficients (the MMA's M, one TMEM lane each) of one job:
-//   1. warp 0 allocates 64 TMEM columns; thread 0 starts a bulk copy of the table's B image
-//      (the shared-memory form of the byte matrix) while the CTA writes A: the eight bytes of
-//      every pre-scaled residue y_i of its 128 coefficients, K-major;
+//   1. warp 0 allocates 64 TMEM columns; the CTA starts cp.async copies of the table's B image
+//      (the shared-memory form of the byte matrix) and, while they are in flight, writes A: the
+//      eight bytes of every pre-scaled residue y_i of its 128 coefficients, K-major;
 //   2. per chunk of 8 destination limbs (64 columns: 8 byte planes each), thread 0 issues
 //      K/32 MMAs (M 128, N 8 x limbs, K 32) and commits them to an mbarrier;
 //   3. after a bounded wait, each warp reads its 32 TMEM lanes (tcgen05.ld 32x32b), folds the
@@ -63,7 +63,7 @@ struct TcLayout {
 };
 __host__ __device__ inline TcLayout tc_layout(int kpad, int ndp) {
   TcLayout L;
-  L.o_dst = 32;  // [0, 8): MMA mbarrier, [8, 16): B-copy mbarrier, [16, 20): TMEM address
+  L.o_dst = 16;  // [0, 8): mbarrier, [8, 12): TMEM address
   L.o_pos = L.o_dst + ndp * (int)sizeof(TcDest);
   L.o_a = (L.o_pos + ndp * 4 + 127) & ~127;
   L.o_b = L.o_a + TC_M * kpad;
@@ -136,6 +136,9 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&d)[8]) {
                : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
 // Orders later uses of d after tcgen05.wait::ld.
 __device__ __forceinline__ void pin8(uint32_t (&d)[8]) {
   asm volatile("" : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7]));
@@ -206,13 +209,12 @@ __global__ void __launch_bounds__(TC_M, 7)
   const int N = 1 << logN;
   const int coef = blockIdx.x * TC_M + tid;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + 16);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + 8);
   TcDest* dconst = reinterpret_cast<TcDest*>(sm + Ly.o_dst);
   int* dofs = reinterpret_cast<int*>(sm + Ly.o_pos);
   uint8_t* sA = sm + Ly.o_a;
   uint8_t* sB = sm + Ly.o_b;
-  const uint32_t bar_a = smem_addr(bar), bar_b = smem_addr(bar + 1);
-  const uint32_t b_bytes = (uint32_t)kpad * 8u * (uint32_t)ndp;  // a multiple of 256
+  const uint32_t bar_a = smem_addr(bar);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)),
@@ -222,16 +224,12 @@ __global__ void __launch_bounds__(TC_M, 7)
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_b), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    // B image: one bulk copy (global and shared addresses 16-byte aligned, size a multiple of 16)
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b), "r"(b_bytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(sB)),
-        "l"(T.tc_b), "r"(b_bytes), "r"(bar_b)
-        : "memory");
+  }
+  {  // B image: 16-byte cp.async copies (kpad 8 ndp bytes, a multiple of 256), waited for below
+    const int n16 = kpad * ndp / 2;
+    for (int k = tid; k < n16; k += TC_M) tc_cp_async16(sB + 16 * k, T.tc_b + 16 * k);
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
   for (int j = tid; j < ndp; j += TC_M) {  // destination constants
     dconst[j] = T.tc_dst[j];
@@ -255,10 +253,12 @@ __global__ void __launch_bounds__(TC_M, 7)
       *reinterpret_cast<ulonglong2*>(sA + p * (TC_M * 16) + tid * 16) = make_ulonglong2(lo, hi);
     }
   }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's part of the B image
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A and B, visible to the MMAs
   tc_fence_before();
-  bool ok = __syncthreads_and(bar_wait_bounded(bar_b, 0));  // B image landed
+  __syncthreads();
   tc_fence_after();
+  bool ok = true;
   const uint32_t tbase = *slot;
   const uint32_t a0 = smem_addr(sA), b0 = smem_addr(sB);
   const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);

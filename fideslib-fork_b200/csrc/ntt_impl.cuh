@@ -400,8 +400,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   auto load = [&](size_t i) -> uint64_t {
     if (first_pass && IN == IN_SWITCH) return switch_modulus(lr.pro[i], opr, pr);
     if (first_pass && IN == IN_MUL) return mulmod(in[i], lr.pro[i], pr);
-    if (first_pass && IN == IN_CONV_SW)
-      return addmod(in[i], shoup(switch_modulus(lr.pro[i], opr, pr), pm.w, pm.ws, pr.q), pr.q);
+    if (first_pass && IN == IN_CONV_SW) return in[i];  // + P SwitchModulus(top) below
     if (first_pass && IN == IN_ADD_PMUL) return addmod(in[i], shoup(lr.pro[i], pm.w, pm.ws, pr.q), pr.q);
     return in[i];
   };
@@ -409,9 +408,30 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   // ---- load chunk 0 (direct when lanes map to consecutive addresses, else staged)
   constexpr int LO0 = Chunk<LOGP, FWD, 0>::LO;
   constexpr bool direct_load = (PASS == COL) || (LO0 == LOGP - LOGE);
+  // conv + P SwitchModulus(top) (a column pass): the tile of the top limb is copied into the
+  // exchange buffer by cp.async while the conv loads are in flight, so the prologue waits for
+  // memory once (loading both operands per element serialised the loads: long-scoreboard
+  // stalls 10x a plain pass's)
+  constexpr bool STAGE_PRO = first_pass && IN == IN_CONV_SW;
+  static_assert(!STAGE_PRO || PASS == COL, "the conv-switch prologue is a column-pass prologue");
+  if constexpr (STAGE_PRO) {
+#pragma unroll
+    for (int k = 0; k < G * P / 2 / NT; ++k) {
+      const int c = k * NT + tid, u = c / (G / 2), h = c % (G / 2);
+      cp_async16(sm + u * G + 2 * h, lr.pro + (size_t)u * S + sub0 + 2 * h);
+    }
+    cp_async_commit();
+  }
   if (direct_load) {
 #pragma unroll
     for (int r = 0; r < E; ++r) x[r] = load(gidx(sub, u_of<LO0>(t, r)));
+    if constexpr (STAGE_PRO) {
+      cp_async_wait_all();
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < E; ++r)
+        x[r] = addmod(x[r], shoup(switch_modulus(sm[u_of<LO0>(t, r) * G + g], opr, pr), pm.w, pm.ws, pr.q), pr.q);
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < E; ++k) {
@@ -449,7 +469,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
       for (int r = 0; r < E; ++r) xf[r] = __longlong_as_double((long long)x[r]);  // the first pass's doubles
     }
     chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N,
-                                a.tww + (size_t)lr.prime * N, fp, direct_load, pol);
+                                a.tww + (size_t)lr.prime * N, fp, direct_load && !STAGE_PRO, pol);
     if (first_pass) {
 #pragma unroll
       for (int r = 0; r < E; ++r) x[r] = (uint64_t)__double_as_longlong(xf[r]);
@@ -462,9 +482,9 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
   if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
   if (FWD && pr.q < (1ull << 58))
-    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load, pol);
+    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
   else
-    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load, pol);
+    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
 
   // ---- final reduction of the completed transform
   if (FWD && PASS == ROW) {

@@ -19,8 +19,23 @@
 // with the digit metadata of the __constant__ block (contiguous digits of alpha = ceil(L /
 // dnum) primes) and the Q-hat tables in the reference's index layouts (MODUPIDX_SCALE,
 // MODUPIDX_MATRIX, MODDOWN_MATRIX), computed here from the primes.
-// Outputs are bit-identical to this project's transforms and conversions for the same primes
-// and root (tests/test_ref_kernels.py), which is how the harness is validated before timing.
+// And the key-switch and elementwise kernels with their launch geometry (grid N/128 x limbs,
+// 128 threads):
+//   * fusedDotKSK_2_ (src/CKKS/ElemenwiseBatchKernels.cu:202-274), the KSK inner product, over
+//     the reference's digit pointer tables (LimbPartitionMGPU.cu:470-503): per digit the ModUp
+//     output and the two key halves in DIGIT order (special primes first, then the Q primes of
+//     the other digits, Context.cu:157-197), plus the own-digit (DECOMP) limbs;
+//   * hoistedRotateDotKSK_2_ (:277-377), the hoisted-rotation inner product with P c0 and the
+//     automorphism scatter, over the tables of LimbPartitionMGPU.cu:590-655;
+//   * automorph_ (src/Rotation.cu:10-12), SwitchModulus (src/CKKS/Rescale.cu:8-13),
+//     binomialMult_ (ElemenwiseBatchKernels.cu:1363-1398), add_ / sub_ / scalar_add_
+//     (src/AddSub.cu:31-111), mult_ / scalar_mult_ (src/ModMult.cu:8-21).
+// The digit metadata of the __constant__ block follows SetupConstants (src/ConstantsGPU.cu:
+// 638-681): primeid_digit (special primes: -1), pos_in_digit (DECOMP position for a digit's own
+// primes, DIGIT position otherwise), primeid_digit_to, P and its Shoup companion.
+// Outputs are bit-identical to this project's kernels and to the oracle for the same primes,
+// root and inputs (tests/test_ref_kernels.py), which is how the harness is validated before
+// timing.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -28,6 +43,11 @@
 
 #include "NTT.cu"
 #include "CKKS/Conv.cu"
+#include "CKKS/ElemenwiseBatchKernels.cu"
+#include "Rotation.cu"
+#include "CKKS/Rescale.cu"
+#include "AddSub.cu"
+#include "ModMult.cu"
 
 // The reference declares the block `extern __constant__` (src/ConstantsGPU.cuh:200) and
 // defines it in ConstantsGPU.cu, which cannot be built here; with relocatable device code
@@ -64,18 +84,27 @@ int bitw(uint64_t x) { return 64 - __builtin_clzll(x); }
 
 struct State {
   int logN = 0, N = 0, np = 0, nq = 0, K = 0, dnum = 1, alpha = 1;
-  std::vector<std::vector<int>> to;  // per digit: destination prime ids (primeid_digit_to order)
+  std::vector<std::vector<int>> to;  // per digit: destination prime ids (primeid_digit_to order:
+                                     // special primes first, then the other digits' Q primes)
   Global::Globals* d_globals = nullptr;
   std::vector<void*> d_tables;
   void** d_ptrs = nullptr;  // pointer tables (data, aux)
   size_t ptr_cap = 0;
+  void** d_ksk = nullptr;  // pointer tables of the key-switch kernels
+  size_t ksk_cap = 0;
+  uint64_t* d_scal = nullptr;  // scalar_add_'s per-prime scalars
+  std::vector<uint64_t> primes;
 } S;
+
+uint64_t S_primes(int id) { return S.primes[id]; }
 
 void release() {
   for (void* p : S.d_tables) cudaFree(p);
   S.d_tables.clear();
   if (S.d_globals) cudaFree(S.d_globals);
   if (S.d_ptrs) cudaFree(S.d_ptrs);
+  if (S.d_ksk) cudaFree(S.d_ksk);
+  if (S.d_scal) cudaFree(S.d_scal);
   S = State{};
 }
 
@@ -105,6 +134,7 @@ int ref_kernels_init(int logN, int n_q, int K, int dnum, const uint64_t* primes,
   S.K = K;
   S.dnum = dnum;
   S.alpha = (n_q + dnum - 1) / dnum;
+  S.primes.assign(primes, primes + np);
   Constants hc;
   std::memset(&hc, 0, sizeof(hc));
   hc.N = N;
@@ -129,13 +159,19 @@ int ref_kernels_init(int logN, int n_q, int K, int dnum, const uint64_t* primes,
       hc.primeid_digit[i] = d;
       hc.pos_in_digit[d][i] = i - lo;
     }
+    for (int k = 0; k < K; ++k) S.to[d].push_back(n_q + k);
     for (int i = 0; i < n_q; ++i)
       if (i < lo || i >= hi) S.to[d].push_back(i);
-    for (int k = 0; k < K; ++k) S.to[d].push_back(n_q + k);
-    for (int j = 0; j < (int)S.to[d].size(); ++j) hc.primeid_digit_to[d][j] = S.to[d][j];
+    for (int j = 0; j < (int)S.to[d].size(); ++j) {
+      hc.primeid_digit_to[d][j] = S.to[d][j];
+      hc.pos_in_digit[d][S.to[d][j]] = j;
+    }
     for (int n = 1; n <= n_q; ++n) {
       hc.num_primeid_digit_from[d][n - 1] = std::max(0, std::min(hi, n) - lo);
-      hc.num_primeid_digit_to[d][n - 1] = (int)S.to[d].size();
+      int cnt = K;  // special primes, then the other digits' primes active at level n
+      for (int i = 0; i < n; ++i)
+        if (i < lo || i >= hi) ++cnt;
+      hc.num_primeid_digit_to[d][n - 1] = cnt;
     }
     // pre-scale for every partial size c of the digit: (prod of the other c - 1 primes)^-1
     for (int c = 1; c <= hi - lo; ++c)
@@ -182,7 +218,10 @@ int ref_kernels_init(int logN, int n_q, int K, int dnum, const uint64_t* primes,
     uint64_t P = 1 % primes[j];
     for (int t = 0; t < K; ++t) P = mulm(P, primes[n_q + t], primes[j]);
     hc.P[j] = P;
+    hc.P_shoup[j] = shoup_h(P, primes[j]);
+    hc.primeid_digit[j] = j / alpha;
   }
+  for (int k = 0; k < K; ++k) hc.primeid_digit[n_q + k] = -1;  // special primes belong to no digit
   const int aw = (logN + 1) / 2;
   for (int i = 0; i < np; ++i) {
     const uint64_t q = primes[i], root = psi[i] % q, iroot = inv_h(root, q), ninv = inv_h((uint64_t)N % q, q);
@@ -344,6 +383,300 @@ int ref_moddown(const uint64_t* sp, int n, uint64_t* out, void* stream) {
     const dim3 block{64, 2};
     CKKS::ModDown2<ALGO_SHOUP><<<dim3(S.N / 64), block, sizeof(uint64_t) * S.K * 64, s>>>(S.d_ptrs, n, S.d_ptrs + n,
                                                                                     PARTITION(0, 0), S.d_globals);
+    return cudaSuccess;
+  });
+}
+
+
+}  // extern "C"
+
+namespace {
+
+// Uploads pointer tables into the key-switch table buffer (grown as needed), in order.
+void** upload_tables(const std::vector<void*>& h, cudaStream_t s) {
+  if (h.size() > S.ksk_cap) {
+    if (S.d_ksk) cudaFree(S.d_ksk);
+    S.d_ksk = nullptr;
+    if (cudaMalloc(&S.d_ksk, h.size() * sizeof(void*)) != cudaSuccess) return nullptr;
+    S.ksk_cap = h.size();
+  }
+  cudaMemcpyAsync(S.d_ksk, h.data(), h.size() * sizeof(void*), cudaMemcpyHostToDevice, s);
+  return S.d_ksk;
+}
+
+int digits_at(int level) { return (level + S.alpha - 1) / S.alpha; }
+
+// Times `reps` launches of f on s with events (after one untimed launch); *ms = the mean.
+template <typename F>
+int timed(F&& f, int reps, float* ms, cudaStream_t s) {
+  f();
+  if (reps <= 0) return run([] { return cudaSuccess; });
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, s);
+  for (int r = 0; r < reps; ++r) f();
+  cudaEventRecord(b, s);
+  cudaEventSynchronize(b);
+  float t = 0;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms) *ms = t / reps;
+  return run([] { return cudaSuccess; });
+}
+
+// Device pointer tables of one switching key in the reference's layout, for n_q + K primes:
+// per digit d the DIGIT-order limbs (at index pos_in_digit[d][id]) of each half, and the
+// DECOMP limbs (limb j of the prime's own digit).  Our key is [2][dnum][n_q + K][N].
+struct KeyTables {
+  std::vector<void*> a_digit[FIDESlib::MAXD], b_digit[FIDESlib::MAXD], a_dec, b_dec;
+};
+KeyTables key_tables(const uint64_t* key) {
+  KeyTables t;
+  const size_t N = S.N, np = S.np;
+  auto limb = [&](int half, int d, int id) { return (void*)(key + (((size_t)half * S.dnum + d) * np + id) * N); };
+  for (int d = 0; d < S.dnum; ++d)
+    for (int id : S.to[d]) {
+      t.a_digit[d].push_back(limb(0, d, id));
+      t.b_digit[d].push_back(limb(1, d, id));
+    }
+  for (int j = 0; j < S.nq; ++j) {
+    t.a_dec.push_back(limb(0, j / S.alpha, j));
+    t.b_dec.push_back(limb(1, j / S.alpha, j));
+  }
+  return t;
+}
+
+// DIGIT-order table of a ModUp output digit d at level l in our layout [beta][l + K][N]
+// (Q limbs, then special limbs); entries of inactive primes are null (never read).
+std::vector<void*> digit_table(const uint64_t* digits, int level, int d) {
+  const size_t N = S.N, ext = level + S.K;
+  std::vector<void*> v;
+  for (int id : S.to[d]) {
+    if (id >= S.nq)
+      v.push_back((void*)(digits + ((size_t)d * ext + level + (id - S.nq)) * N));
+    else if (id < level)
+      v.push_back((void*)(digits + ((size_t)d * ext + id) * N));
+    else
+      v.push_back(nullptr);
+  }
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+// KSK inner product through the reference's fusedDotKSK_2_: digits = the ModUp output of a
+// level-`level` polynomial in our layout [beta][level + K][N] (own-digit limbs included), key
+// = [2][dnum][n_q + K][N]; out_a / out_b [level + K][N] receive sum_d digit_d * key_(a/b, d).
+// reps > 0: *ms = mean time of `reps` further launches (tables uploaded once).
+int ref_ksk(const uint64_t* digits, int level, const uint64_t* key, uint64_t* out_a, uint64_t* out_b, int reps,
+            float* ms, void* stream) {
+  if (!S.d_globals || S.K < 1 || level < 1 || level > S.nq) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int dn = S.dnum, nd = digits_at(level), K = S.K;
+  const size_t N = S.N;
+  KeyTables kt = key_tables(key);
+  // flat host image: [6 dnum table pointers][tables...][4 output tables]
+  std::vector<std::vector<void*>> tabs(6 * dn);
+  std::vector<void*> src_dec, oa, ob, oas, obs;
+  for (int j = 0; j < level; ++j) {
+    src_dec.push_back((void*)(digits + ((size_t)(j / S.alpha) * (level + K) + j) * N));
+    oa.push_back(out_a + (size_t)j * N);
+    ob.push_back(out_b + (size_t)j * N);
+  }
+  for (int k = 0; k < K; ++k) {
+    oas.push_back(out_a + (size_t)(level + k) * N);
+    obs.push_back(out_b + (size_t)(level + k) * N);
+  }
+  for (int d = 0; d < nd; ++d) {
+    tabs[d] = digit_table(digits, level, d);
+    tabs[d + dn] = kt.a_digit[d];
+    tabs[d + 2 * dn] = kt.b_digit[d];
+    tabs[d + 3 * dn] = src_dec;
+    tabs[d + 4 * dn] = kt.a_dec;
+    tabs[d + 5 * dn] = kt.b_dec;
+  }
+  std::vector<void*> h(6 * dn, nullptr);
+  std::vector<size_t> at(6 * dn, 0);
+  for (int t = 0; t < 6 * dn; ++t) {
+    at[t] = h.size();
+    h.insert(h.end(), tabs[t].begin(), tabs[t].end());
+  }
+  const size_t o_oa = h.size();
+  h.insert(h.end(), oa.begin(), oa.end());
+  const size_t o_oas = h.size();
+  h.insert(h.end(), oas.begin(), oas.end());
+  const size_t o_ob = h.size();
+  h.insert(h.end(), ob.begin(), ob.end());
+  const size_t o_obs = h.size();
+  h.insert(h.end(), obs.begin(), obs.end());
+  // the table of tables holds device addresses: fix them up before the upload
+  void** base = nullptr;
+  if (h.size() > S.ksk_cap) {  // grow first so that the final address is known
+    if (!upload_tables(h, s)) return -2;
+  }
+  base = S.d_ksk;
+  for (int t = 0; t < 6 * dn; ++t) h[t] = tabs[t].empty() ? nullptr : (void*)(base + at[t]);
+  if (!upload_tables(h, s)) return -2;
+  using namespace FIDESlib;
+  auto launch = [&] {
+    CKKS::fusedDotKSK_2_<<<dim3(S.N / 128, K + level), 128, 0, s>>>(base + o_oa, base + o_oas, base + o_ob,
+                                                                      base + o_obs, (void***)base, nd, 0, K, 0);
+  };
+  return timed(launch, reps, ms, s);
+}
+
+// Hoisted-rotation inner product through the reference's hoistedRotateDotKSK_2_: one
+// ModUp output `digits` of c1 (our layout), c0 [level][N], n rotations with keys[r] and
+// automorphism indices ks[r]; out0[r] / out1[r] [level + K][N] receive the automorphism of
+// (sum_d digit_d key_(b, d) + P c0) and of sum_d digit_d key_(a, d).
+int ref_hoisted_ksk(const uint64_t* digits, const uint64_t* c0, int level, int n, const uint64_t* const* keys,
+                    const int* ks, uint64_t* const* out0, uint64_t* const* out1, int reps, float* ms, void* stream) {
+  if (!S.d_globals || S.K < 1 || level < 1 || level > S.nq || n < 1) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int dn = S.dnum, nd = digits_at(level), K = S.K;
+  const size_t N = S.N;
+  // table-of-tables layout (LimbPartitionMGPU.cu:590-655): rotation r's key tables at
+  // [r 6 dnum + (1, 2, 4, 5) dnum + d], the c1 digits at offset_c1 (+ 3 dnum for the DECOMP
+  // limbs), then per output kind n tables, then the indices.
+  const size_t off_c1 = (size_t)n * 6 * dn;
+  const size_t off_o1 = off_c1 + 6 * dn, off_o0 = off_o1 + n, off_o1s = off_o0 + n, off_o0s = off_o1s + n;
+  const size_t off_idx = off_o0s + n;
+  const size_t n_heads = off_idx + (n + 1) / 2 + 1;  // indices packed as ints
+  std::vector<std::vector<void*>> tabs(n_heads);
+  for (int r = 0; r < n; ++r) {
+    KeyTables kt = key_tables(keys[r]);
+    for (int d = 0; d < nd; ++d) {
+      tabs[r * 6 * dn + d + dn] = kt.a_digit[d];
+      tabs[r * 6 * dn + d + 2 * dn] = kt.b_digit[d];
+      tabs[r * 6 * dn + d + 4 * dn] = kt.a_dec;
+      tabs[r * 6 * dn + d + 5 * dn] = kt.b_dec;
+    }
+  }
+  std::vector<void*> c1_dec, c0_q;
+  for (int j = 0; j < level; ++j) {
+    c1_dec.push_back((void*)(digits + ((size_t)(j / S.alpha) * (level + K) + j) * N));
+    c0_q.push_back((void*)(c0 + (size_t)j * N));
+  }
+  for (int d = 0; d < nd; ++d) {
+    tabs[off_c1 + d] = digit_table(digits, level, d);
+    tabs[off_c1 + d + 3 * dn] = c1_dec;
+  }
+  for (int r = 0; r < n; ++r) {
+    std::vector<void*> q1, q0, s1, s0;
+    for (int j = 0; j < level; ++j) {
+      q1.push_back(out1[r] + (size_t)j * N);
+      q0.push_back(out0[r] + (size_t)j * N);
+    }
+    for (int k = 0; k < K; ++k) {
+      s1.push_back(out1[r] + (size_t)(level + k) * N);
+      s0.push_back(out0[r] + (size_t)(level + k) * N);
+    }
+    tabs[off_o1 + r] = q1;
+    tabs[off_o0 + r] = q0;
+    tabs[off_o1s + r] = s1;
+    tabs[off_o0s + r] = s0;
+  }
+  std::vector<void*> h(n_heads, nullptr);
+  std::vector<size_t> at(n_heads, 0);
+  for (size_t t = 0; t < n_heads; ++t) {
+    at[t] = h.size();
+    h.insert(h.end(), tabs[t].begin(), tabs[t].end());
+  }
+  const size_t o_c0 = h.size();
+  h.insert(h.end(), c0_q.begin(), c0_q.end());
+  if (h.size() > S.ksk_cap && !upload_tables(h, s)) return -2;
+  void** base = S.d_ksk;
+  for (size_t t = 0; t < n_heads; ++t) h[t] = tabs[t].empty() ? nullptr : (void*)(base + at[t]);
+  std::memset(&h[off_idx], 0, ((n + 1) / 2 + 1) * sizeof(void*));
+  std::memcpy(&h[off_idx], ks, n * sizeof(int));
+  if (!upload_tables(h, s)) return -2;
+  using namespace FIDESlib;
+  auto launch = [&] {
+    CKKS::hoistedRotateDotKSK_2_<<<dim3(S.N / 128, K + level), 128, sizeof(uint64_t) * 128 * nd, s>>>(
+        (void***)(base + off_c1), base + o_c0, (void***)(base + off_o1), (void***)(base + off_o1s),
+        (void***)(base + off_o0), (void***)(base + off_o0s), n, (const int*)(base + off_idx), (void***)base, nd, 0, K,
+        0, nullptr, false);
+  };
+  return timed(launch, reps, ms, s);
+}
+
+// automorph_ on one limb: out[automorph_slot(j)] = in[j] for automorphism index k.
+int ref_automorph(const uint64_t* in, uint64_t* out, int k, void* stream) {
+  if (!S.d_globals) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  using namespace FIDESlib;
+  return run([&] {
+    CKKS::automorph_<uint64_t><<<S.N / 128, 128, 0, s>>>(const_cast<uint64_t*>(in), out, k, 0);
+    return cudaSuccess;
+  });
+}
+
+// SwitchModulus of one coefficient vector (N words) from prime o_pid to prime n_pid.
+int ref_switch_modulus(const uint64_t* in, int o_pid, uint64_t* out, int n_pid, void* stream) {
+  if (!S.d_globals || o_pid < 0 || o_pid >= S.np || n_pid < 0 || n_pid >= S.np) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  using namespace FIDESlib;
+  return run([&] {
+    CKKS::SwitchModulus<uint64_t><<<S.N / 128, 128, 0, s>>>(in, o_pid, out, n_pid);
+    return cudaSuccess;
+  });
+}
+
+// Elementwise kernels over `level` Q limbs (limb j under prime j), in place on a:
+//   op 0: a += b (add_), 1: a -= b (sub_), 2: a *= b (mult_, Barrett), 3: a *= scalars[j]
+//   (scalar_mult_, Shoup), 4: a += scalars[j] (scalar_add_); scalars: host array of level words.
+int ref_elementwise(int op, uint64_t* a, const uint64_t* b, const uint64_t* scalars, int level, void* stream) {
+  if (!S.d_globals || level < 1 || level > S.nq || op < 0 || op > 4) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t N = S.N;
+  std::vector<void*> h;
+  for (int j = 0; j < level; ++j) h.push_back(a + (size_t)j * N);
+  for (int j = 0; j < level; ++j) h.push_back(b ? (void*)(b + (size_t)j * N) : nullptr);
+  if (!upload_tables(h, s)) return -2;
+  void** base = S.d_ksk;
+  if (op == 4) {
+    if (!S.d_scal && cudaMalloc(&S.d_scal, MAXP * sizeof(uint64_t)) != cudaSuccess) return -2;
+    cudaMemcpyAsync(S.d_scal, scalars, level * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
+  }
+  using namespace FIDESlib;
+  return run([&] {
+    const dim3 grid(S.N / 128, level);
+    if (op == 0) add_<<<grid, 128, 0, s>>>(base, base + level, PARTITION(0, 0));
+    if (op == 1) sub_<<<grid, 128, 0, s>>>(base, base + level, PARTITION(0, 0));
+    if (op == 4) scalar_add_<<<grid, 128, 0, s>>>(base, S.d_scal, PARTITION(0, 0));
+    for (int j = 0; op == 2 && j < level; ++j)
+      mult_<uint64_t, ALGO_BARRETT><<<S.N / 128, 128, 0, s>>>(a + j * N, b + j * N, j);
+    for (int j = 0; op == 3 && j < level; ++j) {
+      const uint64_t q = S_primes(j);
+      const uint64_t w = scalars[j] % q;
+      scalar_mult_<uint64_t, ALGO_SHOUP><<<S.N / 128, 128, 0, s>>>(a + j * N, w, j, shoup_h(w, q));
+    }
+    return cudaSuccess;
+  });
+}
+
+// binomialMult_ in place: (c0, c1, c2) <- (c0 d0, c0 d1 + c1 d0, c1 d1) over `level` Q limbs.
+int ref_tensor(uint64_t* c0, uint64_t* c1, uint64_t* c2, const uint64_t* d0, const uint64_t* d1, int level,
+               void* stream) {
+  if (!S.d_globals || level < 1 || level > S.nq) return -1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t N = S.N;
+  std::vector<void*> h;
+  for (uint64_t* p : {c0, c1, c2})
+    for (int j = 0; j < level; ++j) h.push_back(p + (size_t)j * N);
+  for (const uint64_t* p : {d0, d1})
+    for (int j = 0; j < level; ++j) h.push_back((void*)(p + (size_t)j * N));
+  if (!upload_tables(h, s)) return -2;
+  void** base = S.d_ksk;
+  using namespace FIDESlib;
+  return run([&] {
+    CKKS::binomialMult_<<<dim3(S.N / 128, level), 128, 0, s>>>(PARTITION(0, 0), base, base + level,
+                                                                base + 2 * level, base + 3 * level,
+                                                                base + 4 * level);
     return cudaSuccess;
   });
 }

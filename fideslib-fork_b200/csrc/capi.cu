@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fides_b200.h"
 #include "autotune.hpp"
 #include "capi_internal.hpp"
@@ -21,8 +23,25 @@
 namespace {
 thread_local std::string g_err;
 
+// Entry-point bracket: an NVTX range named after the entry point (the counterpart of the
+// reference's CudaNvtxRange on every operation, src/CudaUtils.cuh:662-690), exceptions turned
+// into status codes, and the caller's current device restored on return (entry points make the
+// context's device current while they run).
+struct EntryScope {
+  int prev_device = -1;
+  explicit EntryScope(const char* name) {
+    nvtxRangePushA(name);
+    if (cudaGetDevice(&prev_device) != cudaSuccess) prev_device = -1;
+  }
+  ~EntryScope() {
+    if (prev_device >= 0) cudaSetDevice(prev_device);
+    nvtxRangePop();
+  }
+};
+
 template <typename F>
-int guard(F&& f) {
+int guard_named(const char* name, F&& f) {
+  EntryScope scope(name);
   try {
     f();
     return FIDES_OK;
@@ -36,6 +55,18 @@ int guard(F&& f) {
     g_err = e.what();
     return FIDES_ERR_STATE;
   }
+}
+#define guard(...) guard_named(__func__, __VA_ARGS__)
+
+// After a synchronisation: a bounded device-side wait that gave up (status bit 0) makes the
+// call fail with FIDES_ERR_TIMEOUT.  The bit stays set (every later synchronising call fails
+// too) until fides_ctx_device_status clears it, since the affected outputs are incomplete.
+void check_device_status(fides::Context* c) {
+  uint32_t st = 0;
+  FIDES_CUDA(cudaMemcpy(&st, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (st & 1u)
+    throw fides::Error(FIDES_ERR_TIMEOUT,
+                       "a bounded device-side wait gave up: outputs since the last status clear are incomplete");
 }
 
 fides::Context* C(fides_ctx* x) {
@@ -127,6 +158,13 @@ int fides_f64_peak(int device, double* butterflies_per_s) {
   });
 }
 
+int fides_kernel_arch(int device, int* binary_version) {
+  return guard([&] {
+    need(binary_version, "binary_version");
+    *binary_version = fides::kernel_binary_version(device);
+  });
+}
+
 int fides_ctx_ntt_counts(fides_ctx* x, uint64_t* f64_limbs, uint64_t* int_limbs) {
   return guard([&] {
     auto* c = C(x);
@@ -178,6 +216,25 @@ int fides_ctx_device_status(fides_ctx* x, uint32_t* status, int clear) {
     FIDES_CUDA(cudaDeviceSynchronize());
     FIDES_CUDA(cudaMemcpy(status, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     if (clear) FIDES_CUDA(cudaMemset(c->d_status, 0, sizeof(uint32_t)));
+  });
+}
+
+int fides_ctx_synchronize(fides_ctx* x, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    FIDES_CUDA(cudaStreamSynchronize(S(stream)));
+    check_device_status(c);
+  });
+}
+
+int fides_ctx_inject_status(fides_ctx* x, uint32_t bits) {
+  return guard([&] {
+    auto* c = C(x);
+    FIDES_CUDA(cudaDeviceSynchronize());
+    uint32_t st = 0;
+    FIDES_CUDA(cudaMemcpy(&st, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    st |= bits;
+    FIDES_CUDA(cudaMemcpy(c->d_status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice));
   });
 }
 
@@ -448,6 +505,7 @@ int fides_ct_export(fides_ctx* x, int n_polys, const uint64_t* in, int level, in
     need(limbs, "limbs");
     if (format != 0 && format != 1) throw fides::Error(FIDES_ERR_ARG, "format must be 0 (EVAL) or 1 (COEFF)");
     fides::op_ct_export(c, n_polys, in, level, format, natural_order != 0, limbs, S(stream));
+    check_device_status(c);
   });
 }
 
@@ -707,6 +765,7 @@ void host_roundtrip(fides_ctx* x, const std::vector<const uint64_t*>& ins, int i
   for (int i = 0; i < n_out; ++i)
     FIDES_CUDA(cudaMemcpyAsync(outs[i], dout[i], sizeof(uint64_t) * N * out_limbs, cudaMemcpyDeviceToHost, s));
   FIDES_CUDA(cudaStreamSynchronize(s));
+  check_device_status(c);
 }
 // One item of a pipelined host batch: its host inputs and outputs (limb counts each).
 struct HostJob {
@@ -782,6 +841,7 @@ void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op) {
   FIDES_CUDA(e1);
   FIDES_CUDA(e2);
   FIDES_CUDA(e3);
+  check_device_status(c);
 }
 }  // namespace
 

@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(TC_M, 7)
   __syncthreads();
   tc_fence_after();
   bool ok = true;
+  int failed_chunk = -1;
   const uint32_t tbase = *slot;
   const uint32_t a0 = smem_addr(sA), b0 = smem_addr(sB);
   const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);
@@ -276,7 +277,10 @@ __global__ void __launch_bounds__(TC_M, 7)
       mma_commit(bar_a);
     }
     ok = __syncthreads_and(bar_wait_bounded(bar_a, c & 1));
-    if (!ok) break;
+    if (!ok) {
+      failed_chunk = c;
+      break;
+    }
     tc_fence_after();
     const int j0 = c * TC_DCHUNK;
     if (ndc == TC_DCHUNK && j0 + TC_DCHUNK <= nd)
@@ -293,7 +297,20 @@ __global__ void __launch_bounds__(TC_M, 7)
     __syncthreads();  // TMEM columns are free for the next chunk
     tc_fence_after();
   }
-  if (!ok && tid == 0) atomicOr(status, 1u);
+  if (!ok) {
+    // The commit of chunk failed_chunk has not arrived: its MMAs may still own the TMEM
+    // columns.  tcgen05.commit arrives on the mbarrier only after every MMA this thread issued
+    // before it has completed, so a second bounded wait on the same phase either sees them
+    // finish (the dealloc below is then safe) or gives up after about another second, when
+    // the tensor pipe is not progressing at all; the columns are freed in either case so the
+    // CTA can exit, and the status word marks every output of the launch as incomplete (the
+    // host's next synchronising call returns FIDES_ERR_TIMEOUT until it is cleared).
+    if (tid == 0) {
+      atomicOr(status, 1u);
+      bar_wait_bounded(bar_a, failed_chunk & 1);
+    }
+    __syncthreads();
+  }
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_COLS) : "memory");

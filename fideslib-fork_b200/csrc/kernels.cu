@@ -474,6 +474,13 @@ int fill(List& L, const Job* jobs, int n) {
 
 }  // namespace
 
+int kernel_binary_version(int device) {
+  FIDES_CUDA(cudaSetDevice(device));
+  cudaFuncAttributes a{};
+  FIDES_CUDA(cudaFuncGetAttributes(&a, addsub_kernel));
+  return a.binaryVersion;
+}
+
 void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
   static thread_local ConvJobList L;
   // Tables with a tensor-core form go to the tcgen05 kernel unless the SIMT engine is forced;

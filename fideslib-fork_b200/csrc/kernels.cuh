@@ -11,6 +11,10 @@ namespace fides {
 
 constexpr int EW_THREADS = 256;  // coefficients per CTA tile
 
+// Architecture of the library's device code as the runtime loaded it on `device`
+// (cudaFuncAttributes::binaryVersion of one of its kernels: 100 for sm_100a).
+int kernel_binary_version(int device);
+
 // ---- basis conversion (ModUp: DecompAndModUpConv, Conv.cu:274-423; ModDown: ModDown2, Conv.cu:27-133)
 struct ConvJob {
   ConvTable t;

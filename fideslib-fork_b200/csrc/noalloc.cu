@@ -17,11 +17,13 @@
 // In host code the array's name is only a stand-in; its device address comes from
 // cudaGetSymbolAddress, looked up on the first call on each device (with that device
 // current) and cached.  That first call should therefore come before any stream capture.
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/fides_b200.h"
 #include "capi_internal.hpp"
 #include "ntt.cuh"
+#include "ops.hpp"
 
 namespace {
 
@@ -50,6 +52,16 @@ uint64_t* scratch_on(int device) {
 }  // namespace
 
 extern "C" int fides_rescale_noalloc(fides_ctx* x, const uint64_t* in, int level, uint64_t* out, void* stream) {
+  // the caller's current device is restored on return, as by every other entry point
+  struct RestoreDevice {
+    int prev = -1;
+    RestoreDevice() {
+      if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~RestoreDevice() {
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  } restore;
   try {
     if (!x || !x->c) throw fides::Error(FIDES_ERR_ARG, "null context");
     fides::Context* c = x->c;
@@ -68,18 +80,18 @@ extern "C" int fides_rescale_noalloc(fides_ctx* x, const uint64_t* in, int level
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // INTT of the top limb into the static scratch, then one forward NTT per remaining limb
     // whose prologue applies SwitchModulus to that limb and whose epilogue forms
-    // q_l^-1 x_j + QlQlInvModqlDivqlModq_j t_j (the same kernels as fides_rescale).
-    fides::LimbRef r = fides::lref(top, level - 1);
-    r.src = in + (size_t)(level - 1) * N;
+    // q_l^-1 x_j + QlQlInvModqlDivqlModq_j t_j: the launches fides_rescale makes, built by the
+    // same helpers.  The limb descriptors go through a fixed array in chunks, so no level is
+    // too large for it and nothing is allocated on the host either.
+    fides::LimbRef r = fides::rescale_top_ref(c, in, level, top);
     fides::ntt_limbs(c, &r, 1, true, s);
-    fides::LimbRef refs[256];
-    for (int j = 0; j < level - 1; ++j) {
-      refs[j] = fides::lref(out + j * N, j);
-      refs[j].pro = top;
-      refs[j].ep0 = in + j * N;
-      refs[j].aux = level;
+    constexpr int kChunk = 128;
+    fides::LimbRef refs[kChunk];
+    for (int j0 = 0; j0 < level - 1; j0 += kChunk) {
+      const int m = std::min(kChunk, level - 1 - j0);
+      for (int k = 0; k < m; ++k) refs[k] = fides::rescale_limb_ref(c, in, level, top, out + (size_t)(j0 + k) * N, j0 + k);
+      fides::ntt_limbs(c, refs, m, false, s, fides::IN_SWITCH, fides::OUT_RESCALE);
     }
-    fides::ntt_limbs(c, refs, level - 1, false, s, fides::IN_SWITCH, fides::OUT_RESCALE);
     return FIDES_OK;
   } catch (const fides::Error& e) {
     fides::set_last_error(e.what());

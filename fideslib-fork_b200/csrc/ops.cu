@@ -259,6 +259,20 @@ void op_keyswitch_batch(Context* c, const KeySwitchItem* items, int n, cudaStrea
   keyswitch_stage(c, xs.data(), nullptr, ls.data(), keys.data(), f0.data(), f1.data(), a0.data(), a1.data(), n, s);
 }
 
+LimbRef rescale_top_ref(Context* c, const uint64_t* x, int l, uint64_t* top) {
+  LimbRef r = lref(top, l - 1);
+  r.src = x + (size_t)(l - 1) * c->N;
+  return r;
+}
+
+LimbRef rescale_limb_ref(Context* c, const uint64_t* x, int l, const uint64_t* top, uint64_t* dst, int j) {
+  LimbRef t = lref(dst, j);
+  t.pro = top;
+  t.ep0 = x + (size_t)j * c->N;
+  t.aux = l;
+  return t;
+}
+
 void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint64_t* const* outs, int n,
                       cudaStream_t s) {
   if (n <= 0) return;
@@ -286,16 +300,8 @@ void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint
       copies.push_back({dst, i});
     }
     uint64_t* top = bp.take(1);
-    LimbRef r = lref(top, l - 1);
-    r.src = xs[i] + (size_t)(l - 1) * N;
-    refs.push_back(r);
-    for (int j = 0; j < l - 1; ++j) {
-      LimbRef t = lref(dst + j * N, j);
-      t.pro = top;
-      t.ep0 = xs[i] + j * N;
-      t.aux = l;
-      refs2.push_back(t);
-    }
+    refs.push_back(rescale_top_ref(c, xs[i], l, top));
+    for (int j = 0; j < l - 1; ++j) refs2.push_back(rescale_limb_ref(c, xs[i], l, top, dst + j * N, j));
   }
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
   ntt_limbs(c, refs2.data(), (int)refs2.size(), false, s, IN_SWITCH, OUT_RESCALE);
@@ -401,13 +407,27 @@ void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStrea
     dig[i] = bp.take((size_t)c->beta(l) * ext);
   }
   modup_stage(c, xs.data(), nullptr, ls.data(), tmp.data(), dig.data(), n_items, s);
+  // Job order of the KSK pass.  One ciphertext: its rotations are consecutive, so groups share
+  // the digit tile.  Several: the jobs are ordered by (key, level), so the ciphertexts that use
+  // one rotation key at one level are consecutive and their groups read each key tile once --
+  // the key is the larger stream (2 beta (l + K) limbs against beta (l + K) of digits).
+  std::vector<std::pair<int, int>> order;  // (item, rotation)
+  for (int i = 0; i < n_items; ++i)
+    for (int j = 0; j < (int)items[i].keys.size(); ++j) order.push_back({i, j});
+  if (n_items > 1)
+    std::stable_sort(order.begin(), order.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+      const uint64_t *ka = items[a.first].keys[a.second], *kb = items[b.first].keys[b.second];
+      if (ka != kb) return std::less<const uint64_t*>()(ka, kb);
+      return items[a.first].l < items[b.first].l;
+    });
   std::vector<KskJob> kj;
   std::vector<uint64_t*> ex, conv, outs;
   std::vector<int> ls2;
-  for (int i = 0; i < n_items; ++i) {
-    const HoistItem& it = items[i];
-    const int l = it.l, ext = l + c->K;
-    for (size_t j = 0; j < it.keys.size(); ++j) {
+  for (const auto& ij : order) {
+    const HoistItem& it = items[ij.first];
+    const int i = ij.first, l = it.l, ext = l + c->K;
+    {
+      const int j = ij.second;
       uint64_t* A = bp.take(ext);
       uint64_t* B = bp.take(ext);
       kj.push_back(KskJob{it.c1, nullptr, dig[i], it.keys[j], it.c0, A, B, l, it.ks[j]});

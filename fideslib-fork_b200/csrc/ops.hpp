@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "ntt.cuh"
 
 namespace fides {
 
@@ -48,6 +49,17 @@ void op_ksk_ip(Context* c, const uint64_t* x, const uint64_t* digits, int l, con
 void op_moddown(Context* c, const uint64_t* x_ext, int l, uint64_t* out, cudaStream_t s);
 void op_tensor(Context* c, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0, const uint64_t* b1, int l,
                uint64_t* d0, uint64_t* d1, uint64_t* d2, cudaStream_t s);
+
+// The NTT limb descriptors of a rescale of one polynomial x at level l (FIXEDMANUAL
+// DropLastElementAndScale, Ciphertext::rescale, src/CKKS/Ciphertext.cpp:569-607):
+//   * rescale_top_ref: the inverse transform of the top limb x_(l-1) into `top` (one limb);
+//   * rescale_limb_ref: output limb j < l - 1 = the forward transform of SwitchModulus(top)
+//     (prologue IN_SWITCH) finished by q_(l-1)^-1 x_j + QlQlInvModqlDivqlModq_j t_j (epilogue
+//     OUT_RESCALE), written to dst.
+// Both rescale paths (op_rescale_batch and the allocation-free entry point) build their
+// launches from these, so they run the same transforms.
+LimbRef rescale_top_ref(Context* c, const uint64_t* x, int l, uint64_t* top);
+LimbRef rescale_limb_ref(Context* c, const uint64_t* x, int l, const uint64_t* top, uint64_t* dst, int j);
 
 void op_keyswitch_batch(Context* c, const KeySwitchItem* items, int n, cudaStream_t s);
 void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint64_t* const* outs, int n,

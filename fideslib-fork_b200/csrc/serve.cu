@@ -395,13 +395,23 @@ int fides_server_submit(fides_server* sv, const fides_request* r, uint64_t* tick
 }
 
 int fides_server_wait(fides_server* sv, uint64_t ticket, double* latency_ms, int* status) {
+  return fides_server_wait_timeout(sv, ticket, -1.0, latency_ms, status);
+}
+
+int fides_server_wait_timeout(fides_server* sv, uint64_t ticket, double timeout_ms, double* latency_ms,
+                              int* status) {
   return sguard([&] {
     if (!sv) throw fides::Error(FIDES_ERR_ARG, "null server");
     fides::Server* s = sv->s;
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->done.find(ticket);
     if (it == s->done.end()) throw fides::Error(FIDES_ERR_ARG, "unknown ticket");
-    s->done_cv.wait(lk, [&] { return s->done[ticket].ready; });
+    auto ready = [&] { return s->done[ticket].ready; };
+    if (timeout_ms < 0) {
+      s->done_cv.wait(lk, ready);
+    } else if (!s->done_cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ready)) {
+      throw fides::Error(FIDES_ERR_TIMEOUT, "request not complete within the timeout (the ticket stays valid)");
+    }
     fides::Done d = s->done[ticket];
     s->done.erase(ticket);
     if (latency_ms) *latency_ms = d.latency_ms;

@@ -115,6 +115,11 @@ def lib():
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
+        L.fides_ctx_synchronize.argtypes = [vp, vp]
+        L.fides_ctx_inject_status.argtypes = [vp, C.c_uint32]
+        L.fides_kernel_arch.argtypes = [C.c_int, C.POINTER(C.c_int)]
+        L.fides_server_wait_timeout.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(C.c_double),
+                                                C.POINTER(C.c_int)]
         L.fides_ctx_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                              C.POINTER(C.c_uint64)]
         L.fides_rotation_auto_index.argtypes = [C.c_int, C.c_int]
@@ -204,6 +209,14 @@ def f64_peak(device: int = 0) -> float:
     v = C.c_double()
     _check(lib().fides_f64_peak(device, C.byref(v)))
     return float(v.value)
+
+
+def kernel_arch(device: int = 0) -> int:
+    """cudaFuncAttributes::binaryVersion of the library's kernels as loaded on `device`
+    (100 = sm_100a code)."""
+    v = C.c_int()
+    _check(lib().fides_kernel_arch(device, C.byref(v)))
+    return int(v.value)
 
 
 def auto_index(logN: int, rotation: int) -> int:
@@ -309,6 +322,16 @@ class Context:
         st = C.c_uint32()
         _check(lib().fides_ctx_device_status(self._h, C.byref(st), 1 if clear else 0))
         return int(st.value)
+
+    def synchronize(self, stream=None):
+        """Synchronises `stream` (default: torch's current stream) and raises FidesError
+        TIMEOUT when a bounded device-side wait gave up since the status was last cleared."""
+        _check(lib().fides_ctx_synchronize(self._h, _stream() if stream is None else stream))
+
+    def inject_status(self, bits: int):
+        """Host-side fault injection: ORs `bits` into the device status word, as a kernel
+        whose bounded wait gave up would (tests of the failure path)."""
+        _check(lib().fides_ctx_inject_status(self._h, bits))
 
     KERNEL_FAMILIES = {"ntt": 0, "conv": 1, "ksk": 2, "elem": 3}
 
@@ -789,9 +812,14 @@ class Server:
         _check(lib().fides_server_submit(self._h, C.byref(r), C.byref(t)))
         return int(t.value)
 
-    def wait(self, ticket: int):
+    def wait(self, ticket: int, timeout_ms: float | None = None):
+        """(status, latency_ms) of a request; with timeout_ms, raises FidesError TIMEOUT
+        when it has not completed in time (the ticket stays valid)."""
         lat, st = C.c_double(), C.c_int()
-        _check(lib().fides_server_wait(self._h, ticket, C.byref(lat), C.byref(st)))
+        if timeout_ms is None:
+            _check(lib().fides_server_wait(self._h, ticket, C.byref(lat), C.byref(st)))
+        else:
+            _check(lib().fides_server_wait_timeout(self._h, ticket, float(timeout_ms), C.byref(lat), C.byref(st)))
         return int(st.value), float(lat.value)
 
     def stats(self) -> dict:

@@ -94,12 +94,26 @@ int fides_int_peak(int device, double* butterflies_per_s);
 /* The same for the FP64 butterfly the NTT uses for primes below 2^50 (its FP64-pipe
  * roofline).  No reference counterpart. */
 int fides_f64_peak(int device, double* butterflies_per_s);
+/* The architecture the runtime loaded the library's kernels for on `device`, as
+ * cudaFuncAttributes::binaryVersion (100 = sm_100a code).  No reference counterpart. */
+int fides_kernel_arch(int device, int* binary_version);
 /* Limb transforms submitted to the NTT since the context was created, by butterfly form:
  * FP64 (primes below 2^50) and 64-bit integer.  No reference counterpart. */
 int fides_ctx_ntt_counts(fides_ctx* ctx, uint64_t* f64_limbs, uint64_t* int_limbs);
 /* Synchronises the device and reads the context's device status word: bit 0 = a bounded
- * device-side wait gave up (the affected outputs are incomplete).  clear != 0 resets it. */
+ * device-side wait gave up (the affected outputs are incomplete), bit 1 = an encoded
+ * coefficient exceeded q_0 / 2.  clear != 0 resets it.  Every call that synchronises with
+ * the device on the caller's behalf (fides_ctx_synchronize, the host-buffer entry points,
+ * fides_ct_export) returns FIDES_ERR_TIMEOUT while bit 0 is set, until it is cleared here.
+ * Counterpart of the reference's CudaCheckErrorMod after a synchronisation
+ * (src/CudaUtils.cuh:706-757), for waits that give up instead of hanging. */
 int fides_ctx_device_status(fides_ctx* ctx, uint32_t* status, int clear);
+/* Synchronises `stream` and checks the device status word (FIDES_ERR_TIMEOUT as above). */
+int fides_ctx_synchronize(fides_ctx* ctx, void* stream);
+/* Host-side fault injection for tests of the failure path: synchronises the device and ORs
+ * `bits` into the device status word, as a kernel whose bounded wait gave up would.  No
+ * reference counterpart (the reference has no bounded device waits). */
+int fides_ctx_inject_status(fides_ctx* ctx, uint32_t bits);
 
 /* Profiling mode: when enabled, every kernel launch is bracketed by CUDA events on its
  * stream and attributed to a family (0 = NTT passes, 1 = basis conversion, 2 = KSK inner
@@ -314,6 +328,10 @@ int fides_server_submit(fides_server* s, const fides_request* req, uint64_t* tic
 /* Blocks until the request completed; *status is its result (FIDES_ERR_OOM when it can
  * never fit the budget), *latency_ms the time from submit to completion. */
 int fides_server_wait(fides_server* s, uint64_t ticket, double* latency_ms, int* status);
+/* fides_server_wait with a limit: FIDES_ERR_TIMEOUT when the request has not completed within
+ * timeout_ms (the ticket stays valid and can be waited for again); a negative timeout waits
+ * without limit.  The reference's callers block on stream synchronisation instead. */
+int fides_server_wait_timeout(fides_server* s, uint64_t ticket, double timeout_ms, double* latency_ms, int* status);
 int fides_server_get_stats(fides_server* s, fides_server_stats* out);
 /* Completes in-flight batches, fails requests never started (FIDES_ERR_STATE), frees. */
 int fides_server_destroy(fides_server* s);

@@ -548,6 +548,13 @@ static uint64_t switch_modulus(uint64_t a, uint64_t om, uint64_t nm) {
   return a;
 }
 
+/* SwitchModulus of n coefficients from prime src_id to prime dst_id (reference
+ * src/CKKS/Rescale.cuh:44-64, itself OpenFHE's NativeVector::SwitchModulus). */
+void or_switch_modulus(const or_ctx* c, const uint64_t* in, int n, int src_id, int dst_id, uint64_t* out) {
+  const uint64_t om = c->primes[src_id], nm = c->primes[dst_id];
+  for (int i = 0; i < n; ++i) out[i] = switch_modulus(in[i], om, nm);
+}
+
 /* Rescale (DropLastElementAndScale), reference src/NTTfusions.cuh:214-235 with
  * LimbPartition.cu:711-797: INTT of the top limb, SwitchModulus to each q_j, NTT, then
  * out_j = qlInv_j * x_j + QlQlInvModqlDivqlModq_j * t_j.  QlQlInvModqlDivqlModq_j

@@ -77,6 +77,9 @@ void or_moddown(const or_ctx* c, const uint64_t* in_ext, int l, uint64_t* out);
 /* Key switch of d (EVAL, level l): f0 = ModDown(sum d_j b_j), f1 = ModDown(sum d_j a_j). */
 void or_keyswitch(const or_ctx* c, const uint64_t* d, int l, const uint64_t* key, uint64_t* f0, uint64_t* f1);
 
+/* SwitchModulus of n coefficients from prime src_id to prime dst_id (Rescale.cuh:44-64). */
+void or_switch_modulus(const or_ctx* c, const uint64_t* in, int n, int src_id, int dst_id, uint64_t* out);
+
 /* ---- ciphertext ops (level l = number of active Q limbs) ---- */
 /* OpenFHE DropLastElementAndScale: out (l-1 limbs). */
 void or_rescale(const or_ctx* c, const uint64_t* x, int l, uint64_t* out);

@@ -69,6 +69,7 @@ def lib():
         L.or_moddown.argtypes = [C.c_void_p, u64p, C.c_int, u64p]
         L.or_keyswitch.argtypes = [C.c_void_p, u64p, C.c_int, u64p, u64p, u64p]
         L.or_rescale.argtypes = [C.c_void_p, u64p, C.c_int, u64p]
+        L.or_switch_modulus.argtypes = [C.c_void_p, u64p, C.c_int, C.c_int, C.c_int, u64p]
         L.or_hmult.argtypes = [C.c_void_p, u64p, u64p, u64p, u64p, C.c_int, u64p, C.c_int, u64p, u64p]
         L.or_rotate_auto.argtypes = [C.c_void_p, u64p, u64p, C.c_int, u64p, C.c_uint32, u64p, u64p]
         L.or_rotate_hoisted.argtypes = [C.c_void_p, u64p, u64p, C.c_int, C.POINTER(u64p), C.POINTER(C.c_uint32),
@@ -193,6 +194,13 @@ class Oracle:
         a = np.ascontiguousarray(a, dtype=np.uint64)
         out = np.zeros_like(a)
         lib().or_automorph(self._h, _p(a), _p(out), a.shape[0], k)
+        return out
+
+    def switch_modulus(self, a, src_id: int, dst_id: int) -> np.ndarray:
+        """SwitchModulus of a coefficient vector from prime src_id to prime dst_id."""
+        a = np.ascontiguousarray(a, dtype=np.uint64).reshape(-1)
+        out = np.empty_like(a)
+        lib().or_switch_modulus(self._h, _p(a), a.size, src_id, dst_id, _p(out))
         return out
 
     def auto_index(self, r: int) -> int:

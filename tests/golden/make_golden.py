@@ -1,7 +1,7 @@
 """Generate the golden fixtures that pin the CPU oracle to the reference.
 
-Run in a container that holds the reference tree (default /root/reference); the outputs
-are committed, so nothing at test time reads the reference.
+Run where the reference tree is checked out, with FIDES_REFERENCE=<its directory>; the
+outputs are committed, so nothing at test time reads the reference.
 
   * ref_params.json      -- the reference's own test moduli (test/ParametrizedTest.cuh:
                             p64 / sp64 lists) and the q=17, N=8 negacyclic known-answer
@@ -21,7 +21,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("FIDES_REFERENCE", "/root/reference")
+REF = os.environ.get("FIDES_REFERENCE", "")
+if not REF or not os.path.isdir(os.path.join(REF, "src")):
+    sys.exit("make_golden.py: set FIDES_REFERENCE to the reference source tree")
 
 
 def prime_list(text, name):

@@ -36,9 +36,18 @@ def test_exports_every_declared_symbol(libpath):
         getattr(L, n)
 
 
-def test_built_for_sm100a(libpath):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", libpath], capture_output=True, text=True)
-    assert "sm_100a" in out.stdout
+def test_build_targets_sm100a():
+    """The library's build recipe compiles for sm_100a only (the runtime check of the loaded
+    code is test_kernels_loaded_as_sm100 below)."""
+    mk = open(os.path.join(ROOT, "fideslib-fork_b200", "Makefile")).read()
+    arch = re.search(r"^ARCH\s*:=\s*(.*)$", mk, re.M).group(1)
+    assert arch.split() == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.gpu
+def test_kernels_loaded_as_sm100(fides):
+    """cudaFuncAttributes::binaryVersion of a library kernel on the GPU: sm_100 code."""
+    assert fides.kernel_arch(0) == 100
 
 
 def test_bad_parameters_are_rejected_without_a_gpu(libpath):

@@ -356,3 +356,30 @@ def test_decrypt_valid_config_c_k9(fides):
     rot = s.ctx.rotate(s.dev_ct(c), s.rot_d[1], 1)
     got = decode(s.kg.decrypt_limb0(fides.to_host(rot.c0), fides.to_host(rot.c1)), N, D)
     assert np.abs(got - np.roll(z1, -1)).max() < 1e-6
+
+
+@pytest.mark.parametrize("level", [30, 16, 6])
+def test_elementwise_kernels_config_c(Cfg, level):
+    """tensor_kernel (fides_tensor, the binomialMult_ counterpart), addsub_kernel's add / sub /
+    mul and scalar_kernel's mul / add against the oracle, residue for residue (config C)."""
+    F, o, ctx = Cfg.F, Cfg.o, Cfg.ctx
+    ids = list(range(level))
+    a, b = Cfg.rand_ct(level, 3100 + level), Cfg.rand_ct(level, 3200 + level)
+    d = ctx.tensor(Cfg.dev_ct(a), Cfg.dev_ct(b))
+    torch.cuda.synchronize()
+    for got, want in zip(d, o.tensor(a[0], a[1], b[0], b[1])):
+        assert eq(got, want)
+    A, B = F.to_device(a[0]), F.to_device(b[1])
+    assert eq(ctx.add_poly(A, B), o.add(a[0], b[1], ids))
+    assert eq(ctx.sub_poly(A, B), o.sub(a[0], b[1], ids))
+    assert eq(ctx.sub_poly(B, A), o.sub(b[1], a[0], ids))
+    assert eq(ctx.mul_poly(A, B), o.mul(a[0], b[1], ids))
+    # in place (out aliases an input)
+    C = F.to_device(a[0])
+    ctx.mul_poly(C, B, out=C)
+    assert eq(C, o.mul(a[0], b[1], ids))
+    sc = [int(v) % Cfg.prm.q[j] for j, v in enumerate(xrng(3300 + level).integers(0, 2**62, level))]
+    sc[0] = Cfg.prm.q[0] - 1
+    scal = np.array([[v] * Cfg.o.N for v in sc], dtype=np.uint64)
+    assert eq(ctx.mul_scalar_poly(A, sc), o.mul(a[0], scal, ids))
+    assert eq(ctx.add_scalar_poly(A, sc), o.add(a[0], scal, ids))

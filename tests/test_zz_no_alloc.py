@@ -17,13 +17,17 @@ pytestmark = pytest.mark.gpu
 
 
 def test_noalloc_rescale_matches_rescale_on_consecutive_calls(fides):
+    import oracle as O
     from fides_b200 import params as P
     prm = P.config_c(4)  # N = 2^16: the largest ring the static scratch holds
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
     ctx = fides.Context(prm.logN, prm.q, prm.p, prm.dnum)
-    cases = [(30, 4401), (17, 4402), (30, 4401)]  # consecutive calls; the last repeats the first input
+    # consecutive calls; the third repeats the first input, the last leaves one output limb
+    cases = [(30, 4401), (17, 4402), (30, 4401), (2, 4405)]
     free = []
     for level, seed in cases:
-        x = fides.to_device(uniform_limbs(xrng(seed), prm.q[:level], prm.N))
+        xh = uniform_limbs(xrng(seed), prm.q[:level], prm.N)
+        x = fides.to_device(xh)
         want = ctx.rescale_poly(x)
         got = ctx.empty(level - 1)
         torch.cuda.synchronize()
@@ -31,11 +35,14 @@ def test_noalloc_rescale_matches_rescale_on_consecutive_calls(fides):
         ctx.rescale_poly_noalloc(x, got)
         torch.cuda.synchronize()
         free.append((before, torch.cuda.mem_get_info()[0]))
-        assert torch.equal(got, want), f"level {level}"
+        assert torch.equal(got, want), f"level {level}: differs from fides_rescale"
+        if level in (17, 2):
+            assert np.array_equal(fides.to_host(got), o.rescale(xh)), f"level {level}: differs from the oracle"
     # after the first call (which may load the module), calls leave device memory untouched
     for before, after in free[1:]:
         assert before == after
     assert ctx.scratch_bytes == 0
+    assert torch.cuda.current_device() == 0
 
 
 def test_noalloc_rescale_refuses_unsupported_inputs(fides):

@@ -406,23 +406,29 @@ void** upload_tables(const std::vector<void*>& h, cudaStream_t s) {
 
 int digits_at(int level) { return (level + S.alpha - 1) / S.alpha; }
 
-// Times `reps` launches of f on s with events (after one untimed launch); *ms = the mean.
+// Times `reps` launches of f on s (after one untimed launch): each launch is bracketed by its
+// own pair of events, the way this project's profiling mode brackets its launches, and *ms is
+// the mean of the bracketed times (so host issue gaps between launches are not counted).
 template <typename F>
 int timed(F&& f, int reps, float* ms, cudaStream_t s) {
   f();
   if (reps <= 0) return run([] { return cudaSuccess; });
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  cudaEventRecord(a, s);
-  for (int r = 0; r < reps; ++r) f();
-  cudaEventRecord(b, s);
-  cudaEventSynchronize(b);
-  float t = 0;
-  cudaEventElapsedTime(&t, a, b);
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  if (ms) *ms = t / reps;
+  std::vector<cudaEvent_t> ev(2 * reps);
+  for (auto& e : ev) cudaEventCreate(&e);
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(ev[2 * r], s);
+    f();
+    cudaEventRecord(ev[2 * r + 1], s);
+  }
+  cudaEventSynchronize(ev.back());
+  float total = 0;
+  for (int r = 0; r < reps; ++r) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[2 * r], ev[2 * r + 1]);
+    total += t;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (ms) *ms = total / reps;
   return run([] { return cudaSuccess; });
 }
 

@@ -1,0 +1,1014 @@
+// CKKS bootstrapping in the library's C++ host layer: ModRaise -> CoeffsToSlots -> EvalMod ->
+// SlotsToCoeffs over the internal batched operations, for callers of the C ABI
+// (fides_boot_*, include/fides_b200.h).
+//
+// Follows the reference's CKKS::Bootstrap (src/CKKS/Bootstrap.cu:437-648): sparse-secret
+// encapsulation (keySwitchSparse, :257-290), ModRaise (:708+), EvalCoeffsToSlots /
+// EvalSlotsToCoeffs as baby-step / giant-step linear transforms over hoisted rotations
+// (src/CKKS/CoeffsToSlots.cu:75-151, src/CKKS/LinearTransform.cu), and approxModReduction: a
+// Chebyshev series of the scaled cosine then double-angle steps (src/CKKS/ApproxModEval.cu:45-167,
+// :527 evalChebyshevSeries, :873 applyDoubleAngleIterations).  OpenFHE's coefficient tables are
+// not available here, so every table is derived from the mathematics:
+//   * the special FFT z = U0 w (U0[j][k] = zeta^(5^j k), n = N/2 slots) is a radix-2
+//     decimation-in-time transform of the bit-reversed input, F = S_(n/2) ... S_1, where S_h
+//     pairs entries p and p + h of each block of 2h with the twiddle exp(i pi 5^(p mod h) / 4h);
+//     each S_h has the slot diagonals 0, +h, -h.  CoeffsToSlots applies n F^-1 (unnormalised
+//     inverse stages 2 S_h^-1), SlotsToCoeffs applies F, each grouped into `level budget`
+//     composed matrices evaluated by BSGS;
+//   * EvalMod: after CoeffsToSlots the real slots hold t = m'/(K q0) with m' = m + q0 I; the
+//     Chebyshev interpolant (degree 63 at the Chebyshev points of the first kind) of
+//     cos(2 pi K t / 2^r - pi / 2^(r+1)) followed by r double-angle steps c -> 2 c^2 - 1 gives
+//     sin(2 pi m' / q0) = sin(2 pi m / q0);
+//   * scales: level l has scale S_l with S_(l-1) = S_l^2 / q_(l-1) (FLEXIBLEAUTO's chain), so
+//     products of two level-l operands land on the next level's scale; an operand moved down
+//     several levels is multiplied by an integer constant that re-targets its scale first.
+// The operation sequence, the order of every batched launch and every integer constant are the
+// same as the Python driver's (fides_b200/bootstrap.py), so the two give the same residues on
+// the same tables.  Intermediates are stream-ordered allocations on the bootstrap's stream, so
+// a bootstrap can be captured in a CUDA graph like every other operation of the library.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <set>
+#include <vector>
+
+#include "../../include/fides_b200.h"
+#include "capi_internal.hpp"
+#include "encode.hpp"
+#include "kernels.cuh"
+#include "ntt.cuh"
+#include "ops.hpp"
+
+namespace fides {
+namespace boot {
+
+using cd = std::complex<double>;
+using Diags = std::map<int, std::vector<cd>>;  // slot offset -> diagonal (n values)
+
+// ---------------------------------------------------------------------- tables (host)
+// out = roll(v, k): out[(i + k) mod n] = v[i]
+std::vector<cd> roll(const std::vector<cd>& v, long k) {
+  const long n = (long)v.size();
+  std::vector<cd> out(n);
+  k = ((k % n) + n) % n;
+  for (long i = 0; i < n; ++i) out[(i + k) % n] = v[i];
+  return out;
+}
+
+// Slot diagonals of S_h (forward) or S_h^-1 (inverse); unnorm doubles the inverse stage.
+Diags stage(int n, int h, bool inverse, bool unnorm) {
+  std::vector<cd> tw(h);
+  const double M = 8.0 * h;
+  uint64_t e = 1;
+  for (int i = 0; i < h; ++i) {
+    const double ang = M_PI * (double)e / (4.0 * h);
+    tw[i] = cd(std::cos(ang), std::sin(ang));
+    e = (e * 5) % (uint64_t)M;
+  }
+  std::vector<cd> d0(n, 0.0), dp(n, 0.0), dm(n, 0.0);
+  for (int p = 0; p < n; ++p) {
+    const int r = p % (2 * h);
+    const bool lo = r < h;
+    const cd t = tw[lo ? r : r - h];
+    if (!inverse) {  // lo: a[p] + t a[p + h]; hi: a[p - h] - t a[p]
+      if (lo) {
+        d0[p] = 1.0;
+        dp[p] = t;
+      } else {
+        d0[p] = -t;
+        dm[p] = 1.0;
+      }
+    } else {  // lo: (a[p] + a[p + h]) / 2; hi: (a[p - h] - a[p]) / (2 t)
+      if (lo) {
+        d0[p] = 0.5;
+        dp[p] = 0.5;
+      } else {
+        d0[p] = -0.5 / t;
+        dm[p] = 0.5 / t;
+      }
+    }
+  }
+  Diags out;
+  out[0] = d0;
+  auto acc = [&](int k, const std::vector<cd>& v) {
+    auto it = out.find(k);
+    if (it == out.end())
+      out[k] = v;
+    else
+      for (int i = 0; i < n; ++i) it->second[i] += v[i];
+  };
+  if (h < n) {
+    acc(h % n, dp);
+    acc(((-h) % n + n) % n, dm);
+  }
+  if (inverse && unnorm)
+    for (auto& kv : out)
+      for (auto& x : kv.second) x *= 2.0;
+  return out;
+}
+
+// Diagonals of A B: (A B) v = sum_(r, s) (A_r * roll(B_s, -r)) * roll(v, -(r + s)).
+Diags compose(const Diags& A, const Diags& B, int n) {
+  Diags out;
+  for (const auto& [r, Ar] : A)
+    for (const auto& [s, Bs] : B) {
+      const int k = (r + s) % n;
+      const std::vector<cd> rb = roll(Bs, -r);
+      auto it = out.find(k);
+      if (it == out.end()) {
+        std::vector<cd> v(n);
+        for (int i = 0; i < n; ++i) v[i] = Ar[i] * rb[i];
+        out[k] = std::move(v);
+      } else {
+        for (int i = 0; i < n; ++i) it->second[i] += Ar[i] * rb[i];
+      }
+    }
+  for (auto it = out.begin(); it != out.end();) {
+    double mx = 0;
+    for (const auto& x : it->second) mx = std::max(mx, std::abs(x));
+    it = mx > 0 ? std::next(it) : out.erase(it);
+  }
+  return out;
+}
+
+// F (or F^-1, unnormalised: n F^-1) as `levels` composed matrices in application order; the
+// log2(n) stages are split into `levels` consecutive groups, the first (log2 n mod levels)
+// groups one stage longer.
+std::vector<Diags> fft_levels(int n, int levels, bool inverse, bool unnorm) {
+  std::vector<int> hs;
+  for (int h = 1; h < n; h <<= 1) hs.push_back(h);
+  if (inverse) std::reverse(hs.begin(), hs.end());
+  const int S = (int)hs.size(), base = S / levels, extra = S % levels;
+  std::vector<Diags> mats;
+  int at = 0;
+  for (int g = 0; g < levels; ++g) {
+    const int cnt = base + (g < extra ? 1 : 0);
+    Diags M;
+    bool first = true;
+    for (int i = at; i < at + cnt; ++i) {
+      Diags St = stage(n, hs[i], inverse, unnorm);
+      M = first ? St : compose(St, M, n);
+      first = false;
+    }
+    at += cnt;
+    mats.push_back(std::move(M));
+  }
+  return mats;
+}
+
+// Chebyshev interpolant of degree d of f on [-1, 1] (values at the d + 1 Chebyshev points of
+// the first kind): c_k = (2 / (d + 1)) sum_j f(x_j) T_k(x_j), c_0 halved.
+template <typename Fn>
+std::vector<double> cheb_interpolate(Fn f, int d) {
+  const int m = d + 1;
+  std::vector<double> fx(m), c(m, 0.0);
+  for (int j = 0; j < m; ++j) fx[j] = f(std::cos(M_PI * (j + 0.5) / m));
+  for (int k = 0; k < m; ++k) {
+    double s = 0;
+    for (int j = 0; j < m; ++j) s += fx[j] * std::cos(M_PI * k * (j + 0.5) / m);
+    c[k] = 2.0 * s / m;
+  }
+  c[0] *= 0.5;
+  return c;
+}
+
+long floordiv(long a, long b) {
+  long q = a / b;
+  if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+  return q;
+}
+long pymod(long a, long b) { return ((a % b) + b) % b; }
+
+// Round half to even, as Python's round() on a float.
+long long rint_even(double v) { return (long long)std::nearbyint(v); }
+
+// ---------------------------------------------------------------------- device values
+// A device polynomial buffer shared by the views (ciphertexts) that use it; freed on its stream
+// when the last view goes away.
+using Buf = std::shared_ptr<Scratch>;
+
+struct Ct {
+  Buf b0, b1;
+  const uint64_t* c0 = nullptr;
+  const uint64_t* c1 = nullptr;
+  int level = 0;
+  double scale = 0;
+};
+
+struct Plan {  // one BSGS matrix prepared at `level`
+  int step = 0, level = 0;
+  double pt_scale = 0;
+  std::map<int, std::vector<int>> giant;  // i -> baby indices j (ascending)
+  std::map<std::pair<int, int>, Buf> pts;  // (i, j) -> encoded diagonal (level limbs)
+};
+
+}  // namespace boot
+
+struct Bootstrapper {
+  Context* c;
+  fides_boot_params prm;
+  int n = 0;  // slots
+  std::vector<double> S;  // canonical scale of each level
+  std::vector<double> cheb;
+  std::vector<boot::Diags> cts, stc;
+  std::vector<int> rotations;
+  const uint64_t *relin = nullptr, *conj = nullptr, *to_sparse = nullptr, *to_dense = nullptr;
+  std::map<int, const uint64_t*> rot;
+  // prepared state
+  bool prepared = false;
+  std::vector<boot::Plan> cts_pl, stc_pl;
+  boot::Buf pt_i, pt_minus_i;
+  int top = 0, cts_out_level = 0, stc_in_level = 0, out_level = 0;
+  double in_scale = 0, msg_scale = 0;
+  std::vector<cudaStream_t> lanes;  // streams of fides_bootstrap_batch
+  std::vector<cudaEvent_t> lane_ev;
+  cudaStream_t own = nullptr;  // the prepared tables are allocated and freed on this stream
+
+  ~Bootstrapper() {
+    cts_pl.clear();
+    stc_pl.clear();
+    pt_i.reset();
+    pt_minus_i.reset();
+    if (own) {
+      cudaStreamSynchronize(own);
+      cudaStreamDestroy(own);
+    }
+    for (auto st : lanes) cudaStreamDestroy(st);
+    for (auto e : lane_ev) cudaEventDestroy(e);
+  }
+
+  // ---- BSGS plan of one composed matrix (the Python driver's _plan)
+  void plan(const boot::Diags& M, int& step, std::map<int, std::vector<int>>& giant) const {
+    const int g = prm.baby;
+    long st = n;
+    bool any = false;
+    for (const auto& kv : M)
+      if (kv.first) {
+        st = any ? std::gcd(st, (long)kv.first) : std::gcd((long)kv.first, (long)n);
+        any = true;
+      }
+    if (any) st = std::gcd(st, (long)n);
+    step = (int)st;
+    std::set<long> ts;
+    for (const auto& kv : M) ts.insert(boot::floordiv(boot::pymod(kv.first + n / 2, n) - n / 2, step));
+    giant.clear();
+    for (long t : ts) {
+      const long i = boot::floordiv(t, g), j = t - i * g;
+      giant[(int)i].push_back((int)j);
+    }
+  }
+
+  std::set<int> bsgs_rotations(const boot::Diags& M) const {
+    int step;
+    std::map<int, std::vector<int>> giant;
+    plan(M, step, giant);
+    std::set<int> rs;
+    for (const auto& [i, js] : giant) {
+      for (int j : js) rs.insert((int)boot::pymod((long)step * j, n));
+      rs.insert((int)boot::pymod((long)step * prm.baby * i, n));
+    }
+    return rs;
+  }
+
+  void build_tables() {
+    n = c->N / 2;
+    const double K = prm.K, r = prm.r;
+    cheb = boot::cheb_interpolate(
+        [&](double t) { return std::cos(2 * M_PI * K * t / std::pow(2.0, r) - M_PI / std::pow(2.0, r + 1)); },
+        prm.degree);
+    cts = boot::fft_levels(n, prm.level_budget_cts, true, true);
+    stc = boot::fft_levels(n, prm.level_budget_stc, false, false);
+    std::set<int> rs;
+    for (const auto* v : {&cts, &stc})
+      for (const auto& M : *v)
+        for (int x : bsgs_rotations(M)) rs.insert(x);
+    rs.erase(0);
+    rotations.assign(rs.begin(), rs.end());
+    const int L = c->n_q;
+    S.assign(L + 1, 0.0);
+    S[L] = prm.top_scale;
+    for (int l = L; l > 1; --l) S[l - 1] = S[l] * S[l] / (double)c->primes[l - 1];
+  }
+
+  // ---------------------------------------------------------------- device helpers
+  boot::Buf alloc(int limbs, cudaStream_t s) const {
+    return std::make_shared<Scratch>(c, sizeof(uint64_t) * (size_t)c->N * limbs, s);
+  }
+  boot::Ct fresh(int level, double scale, cudaStream_t s) const {
+    boot::Ct a;
+    a.b0 = alloc(level, s);
+    a.b1 = alloc(level, s);
+    a.c0 = a.b0->u64();
+    a.c1 = a.b1->u64();
+    a.level = level;
+    a.scale = scale;
+    return a;
+  }
+  static uint64_t* mut(const uint64_t* p) { return const_cast<uint64_t*>(p); }
+  uint64_t residue(long long v, int i) const {
+    const long long q = (long long)c->primes[i];
+    return (uint64_t)(((v % q) + q) % q);
+  }
+  uint64_t residue(__int128 v, int i) const {
+    const __int128 q = (__int128)c->primes[i];
+    return (uint64_t)(((v % q) + q) % q);
+  }
+
+  boot::Ct drop(const boot::Ct& a, int level) const {
+    boot::Ct b = a;
+    b.level = level;
+    return b;
+  }
+
+  // polynomial-wise add / sub / mul over `level` limbs (one launch per call, as the Python
+  // driver's add_poly / sub_poly / mul_poly)
+  void ew(int op, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, cudaStream_t s) const {
+    AddSubJob j{a, b, out, level, op};
+    launch_addsub(c, &j, 1, s);
+  }
+
+  boot::Ct add_raw(const boot::Ct& a, const boot::Ct& b, cudaStream_t s) const {
+    boot::Ct o = fresh(a.level, a.scale, s);
+    ew(EW_ADD, a.c0, b.c0, a.level, mut(o.c0), s);
+    ew(EW_ADD, a.c1, b.c1, a.level, mut(o.c1), s);
+    return o;
+  }
+  boot::Ct sub_raw(const boot::Ct& a, const boot::Ct& b, cudaStream_t s) const {
+    boot::Ct o = fresh(a.level, a.scale, s);
+    ew(EW_SUB, a.c0, b.c0, a.level, mut(o.c0), s);
+    ew(EW_SUB, a.c1, b.c1, a.level, mut(o.c1), s);
+    return o;
+  }
+  boot::Ct mul_plain_int(const boot::Ct& a, const boot::Buf& pt, cudaStream_t s) const {
+    boot::Ct o = fresh(a.level, a.scale, s);
+    ew(EW_MUL, a.c0, pt->u64(), a.level, mut(o.c0), s);
+    ew(EW_MUL, a.c1, pt->u64(), a.level, mut(o.c1), s);
+    return o;
+  }
+  boot::Ct mul_int(const boot::Ct& a, long long v, cudaStream_t s) const {
+    if (a.level > MAX_SCALAR_LIMBS) throw Error(-1, "bootstrap: scalar product over more than 64 limbs");
+    boot::Ct o = fresh(a.level, a.scale, s);
+    for (int k = 0; k < 2; ++k) {
+      ScalarJob j{};
+      j.a = k ? a.c1 : a.c0;
+      j.out = mut(k ? o.c1 : o.c0);
+      j.l = a.level;
+      j.op = EW_MUL_SCALAR;
+      for (int i = 0; i < a.level; ++i) j.s[i] = residue(v, i);
+      launch_scalar(c, &j, 1, s);
+    }
+    return o;
+  }
+
+  // the same integer combination of every lane (one launch): sum_t ints[t] lane[t] (+ add on c0)
+  std::vector<boot::Ct> lincomb_lanes(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<long long>& ints,
+                                      const long long* add, int level, double scale, cudaStream_t s) const {
+    if (lanes.empty() || lanes.size() > (size_t)MAX_LC_LANES || ints.empty() || ints.size() > (size_t)MAX_LC_TERMS)
+      throw Error(-1, "bootstrap: linear combination out of range");
+    static thread_local LinCombJob j;
+    std::vector<boot::Ct> outs;
+    for (size_t a = 0; a < lanes.size(); ++a) {
+      outs.push_back(fresh(level, scale, s));
+      j.out0[a] = mut(outs.back().c0);
+      j.out1[a] = mut(outs.back().c1);
+      for (size_t t = 0; t < ints.size(); ++t) {
+        j.x0[a][t] = lanes[a][t].c0;
+        j.x1[a][t] = lanes[a][t].c1;
+      }
+    }
+    for (size_t t = 0; t < ints.size(); ++t)
+      for (int i = 0; i < level; ++i) j.s[t][i] = residue(ints[t], i);
+    for (int i = 0; i < level; ++i) j.add0[i] = add ? residue(*add, i) : 0;
+    j.n = (int)ints.size();
+    j.l = level;
+    j.lanes = (int)lanes.size();
+    launch_lincomb(c, j, s);
+    return outs;
+  }
+
+  std::vector<boot::Ct> lincomb_many(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<long long>& ints,
+                                     double cst, cudaStream_t s) const {
+    const boot::Ct& a = lanes[0][0];
+    int l = a.level;
+    for (const auto& ln : lanes)
+      for (const auto& b : ln) l = std::min(l, b.level);
+    long long add = 0;
+    const bool has = cst != 0.0;
+    if (has) add = boot::rint_even(cst * a.scale);
+    return lincomb_lanes(lanes, ints, has ? &add : nullptr, l, a.scale, s);
+  }
+
+  std::vector<boot::Ct> add_many(const std::vector<boot::Ct>& xs, const std::vector<boot::Ct>& ys,
+                                 cudaStream_t s) const {
+    std::vector<std::vector<boot::Ct>> lanes;
+    for (size_t i = 0; i < xs.size(); ++i) lanes.push_back({xs[i], ys[i]});
+    return lincomb_many(lanes, {1, 1}, 0.0, s);
+  }
+
+  std::vector<boot::Ct> rescale_many_to(const std::vector<boot::Ct>& cts_, double new_scale, cudaStream_t s) const {
+    std::vector<const uint64_t*> xs;
+    std::vector<int> ls;
+    std::vector<uint64_t*> outs;
+    std::vector<boot::Ct> res;
+    for (const auto& a : cts_) {
+      res.push_back(fresh(a.level - 1, new_scale, s));
+      xs.push_back(a.c0);
+      xs.push_back(a.c1);
+      ls.push_back(a.level);
+      ls.push_back(a.level);
+      outs.push_back(mut(res.back().c0));
+      outs.push_back(mut(res.back().c1));
+    }
+    op_rescale_batch(c, xs.data(), ls.data(), outs.data(), (int)xs.size(), s);
+    return res;
+  }
+
+  std::vector<boot::Ct> to_level_many(const std::vector<boot::Ct>& cts_, int level, cudaStream_t s) const {
+    const boot::Ct& a = cts_[0];
+    if (a.level == level && std::abs(a.scale / S[level] - 1) < 1e-15) return cts_;
+    if (a.level <= level) throw Error(-4, "bootstrap: cannot raise a level");
+    const long long k = boot::rint_even(S[level] * (double)c->primes[level] / a.scale);
+    std::vector<std::vector<boot::Ct>> lanes;
+    for (const auto& b : cts_) lanes.push_back({drop(b, level + 1)});
+    return rescale_many_to(lincomb_many(lanes, {k}, 0.0, s), S[level], s);
+  }
+  boot::Ct to_level(const boot::Ct& a, int level, cudaStream_t s) const { return to_level_many({a}, level, s)[0]; }
+
+  std::vector<boot::Ct> lincomb_to_many(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& coefs,
+                                        double cst, int target, cudaStream_t s) const {
+    const double qt = (double)c->primes[target], St = S[target];
+    std::vector<int> keep;
+    std::vector<long long> ints;
+    for (size_t t = 0; t < coefs.size(); ++t) {
+      const boot::Ct& a = lanes[0][t];
+      if (a.level <= target) throw Error(-4, "bootstrap: operand below the combination's level");
+      const long long k = boot::rint_even(coefs[t] * St * qt / a.scale);
+      if (k) {
+        keep.push_back((int)t);
+        ints.push_back(k);
+      }
+    }
+    if (keep.empty()) {
+      keep = {0};
+      ints = {0};
+    }
+    const long long add = boot::rint_even(cst * St * qt);
+    std::vector<std::vector<boot::Ct>> sel;
+    for (const auto& ln : lanes) {
+      std::vector<boot::Ct> v;
+      for (int t : keep) v.push_back(ln[t]);
+      sel.push_back(v);
+    }
+    auto outs = lincomb_lanes(sel, ints, add ? &add : nullptr, target + 1, 0.0, s);
+    return rescale_many_to(outs, St, s);
+  }
+
+  std::vector<boot::Ct> mul_many(const std::vector<std::pair<boot::Ct, boot::Ct>>& pairs, cudaStream_t s) const {
+    std::vector<std::pair<boot::Ct, boot::Ct>> ab;
+    for (const auto& [a, b] : pairs) {
+      const int l = std::min(a.level, b.level);
+      ab.push_back({to_level(a, l, s), to_level(b, l, s)});
+    }
+    std::vector<HMultItem> items;
+    std::vector<boot::Ct> outs;
+    for (const auto& [a, b] : ab) {
+      outs.push_back(fresh(a.level - 1, S[a.level - 1], s));
+      items.push_back(HMultItem{a.c0, a.c1, b.c0, b.c1, mut(outs.back().c0), mut(outs.back().c1), a.level});
+    }
+    op_hmult_batch(c, items.data(), (int)items.size(), relin, true, s);
+    return outs;
+  }
+
+  boot::Ct conjugate(const boot::Ct& a, cudaStream_t s) const {
+    boot::Ct o = fresh(a.level, a.scale, s);
+    RotateItem it{a.c0, a.c1, mut(o.c0), mut(o.c1), conj, a.level, (uint32_t)(2 * c->N - 1)};
+    op_rotate_batch(c, &it, 1, s);
+    return o;
+  }
+
+  const uint64_t* rot_key(int r) const {
+    auto it = rot.find((int)boot::pymod(r, n));
+    if (it == rot.end()) throw Error(-5, "bootstrap: missing rotation key " + std::to_string(r));
+    return it->second;
+  }
+
+  std::vector<boot::Ct> rotate_many(const boot::Ct& a, const std::vector<int>& rs, cudaStream_t s) const {
+    HoistItem it;
+    it.c0 = a.c0;
+    it.c1 = a.c1;
+    it.l = a.level;
+    std::vector<int> idx;
+    std::vector<boot::Ct> res(rs.size());
+    for (size_t k = 0; k < rs.size(); ++k) {
+      if (boot::pymod(rs[k], n) == 0) {
+        res[k] = a;
+        continue;
+      }
+      res[k] = fresh(a.level, a.scale, s);
+      it.keys.push_back(rot_key(rs[k]));
+      it.ks.push_back(h_auto_index(c->logN, rs[k]));
+      it.out0.push_back(mut(res[k].c0));
+      it.out1.push_back(mut(res[k].c1));
+    }
+    if (!it.keys.empty()) op_hoisted_batch(c, &it, 1, s);
+    return res;
+  }
+
+  std::vector<boot::Ct> rotate_batch(const std::vector<std::pair<boot::Ct, int>>& jobs, cudaStream_t s) const {
+    std::vector<RotateItem> items;
+    std::vector<boot::Ct> outs;
+    for (const auto& [a, r] : jobs) {
+      outs.push_back(fresh(a.level, a.scale, s));
+      items.push_back(RotateItem{a.c0, a.c1, mut(outs.back().c0), mut(outs.back().c1), rot_key(r), a.level,
+                                 h_auto_index(c->logN, r)});
+    }
+    if (!items.empty()) op_rotate_batch(c, items.data(), (int)items.size(), s);
+    return outs;
+  }
+
+  boot::Ct keyswitch_add(const boot::Ct& a, const uint64_t* key, cudaStream_t s) const {
+    boot::Ct f = fresh(a.level, a.scale, s);
+    KeySwitchItem it{a.c1, a.level, key, mut(f.c0), mut(f.c1)};
+    op_keyswitch_batch(c, &it, 1, s);
+    boot::Ct o = fresh(a.level, a.scale, s);
+    ew(EW_ADD, a.c0, f.c0, a.level, mut(o.c0), s);
+    o.c1 = f.c1;
+    o.b1 = f.b1;
+    return o;
+  }
+
+  // ---------------------------------------------------------------- preparation
+  boot::Buf encode_pt(const std::vector<boot::cd>& z, int level, double scale, cudaStream_t s) const {
+    Scratch slots(c, sizeof(double) * 2 * z.size(), s);
+    FIDES_CUDA(cudaMemcpyAsync(slots.p, z.data(), sizeof(double) * 2 * z.size(), cudaMemcpyHostToDevice, s));
+    boot::Buf out = alloc(level, s);
+    op_encode(c, static_cast<const double*>(slots.p), (int)z.size(), 1, scale, level, out->u64(), s);
+    return out;
+  }
+
+  boot::Buf int_pt(const std::vector<long long>& coeff, int level, cudaStream_t s) const {
+    const size_t N = c->N;
+    std::vector<uint64_t> h((size_t)level * N);
+    for (int i = 0; i < level; ++i)
+      for (size_t k = 0; k < N; ++k) h[i * N + k] = residue(coeff[k], i);
+    boot::Buf out = alloc(level, s);
+    FIDES_CUDA(cudaMemcpyAsync(out->u64(), h.data(), sizeof(uint64_t) * h.size(), cudaMemcpyHostToDevice, s));
+    std::vector<int> ids(level);
+    std::iota(ids.begin(), ids.end(), 0);
+    ntt_polys(c, out->u64(), 1, level, ids.data(), false, s);
+    return out;
+  }
+
+  boot::Plan prepare_matrix(const boot::Diags& M, double fac, int level, double scale, cudaStream_t s) const {
+    boot::Plan P;
+    plan(M, P.step, P.giant);
+    P.level = level;
+    const double target = S[level - 1];
+    P.pt_scale = target * (double)c->primes[level - 1] / scale;
+    for (const auto& [i, js] : P.giant)
+      for (int j : js) {
+        const int off = (int)boot::pymod((long)P.step * (prm.baby * (long)i + j), n);
+        auto it = M.find(off);
+        if (it == M.end()) continue;
+        std::vector<boot::cd> d(it->second.size());
+        for (size_t k = 0; k < d.size(); ++k) d[k] = it->second[k] * fac;
+        P.pts[{i, j}] = encode_pt(boot::roll(d, (long)P.step * prm.baby * i), level, P.pt_scale, s);
+      }
+    return P;
+  }
+
+  // Prepares on the bootstrapper's own stream (after the work already on `user`), so that the
+  // tables outlive any stream of the caller; returns when they are ready.
+  void prepare(cudaStream_t user) {
+    if (!own) FIDES_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    cudaEvent_t ev;
+    FIDES_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, user);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(own, ev, 0);
+    cudaEventDestroy(ev);
+    FIDES_CUDA(e);
+    cts_pl.clear();
+    stc_pl.clear();
+    prepared = false;
+    cudaStream_t s = own;
+    const int top_level = prm.top_level;
+    top = top_level;
+    in_scale = S[top_level];
+    msg_scale = prm.msg_scale * (double)(1ll << prm.prescale_bits);
+    // 2 K q0 is formed exactly and rounded once to a double (as an integer product would be)
+    const double two_k_q0 = (double)((unsigned __int128)2 * (unsigned)prm.K * c->primes[0]);
+    const double gfac = std::pow(in_scale / two_k_q0 / n, 1.0 / (double)cts.size());
+    cts_pl.clear();
+    stc_pl.clear();
+    int level = top_level;
+    double scale = in_scale;
+    for (const auto& M : cts) {
+      cts_pl.push_back(prepare_matrix(M, gfac, level, scale, s));
+      level -= 1;
+      scale = S[level];
+    }
+    cts_out_level = level;
+    const int depth = (int)std::ceil(std::log2((double)prm.degree)) + 1 + prm.r;
+    stc_in_level = cts_out_level - depth;
+    if (stc_in_level - (int)stc.size() < 1) throw Error(-4, "bootstrap: not enough levels for the chosen budget");
+    const double sfac = std::pow((double)c->primes[0] / (2.0 * M_PI * msg_scale), 1.0 / (double)stc.size());
+    level = stc_in_level;
+    for (const auto& M : stc) {
+      stc_pl.push_back(prepare_matrix(M, sfac, level, S[level], s));
+      level -= 1;
+    }
+    out_level = level;
+    std::vector<long long> mono(c->N, 0);
+    mono[c->N / 2] = 1;  // X^(N/2): slots times i
+    pt_i = int_pt(mono, top_level, s);
+    mono[c->N / 2] = -1;
+    pt_minus_i = int_pt(mono, top_level, s);
+    FIDES_CUDA(cudaStreamSynchronize(s));
+    uint32_t st = 0;
+    FIDES_CUDA(cudaMemcpy(&st, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (st & 2u) throw Error(-1, "bootstrap: an encoded diagonal coefficient exceeded q_0 / 2");
+    prepared = true;
+  }
+
+  // ---------------------------------------------------------------- the linear transforms
+  boot::Ct apply(const boot::Ct& a, const boot::Plan& P, cudaStream_t s) const {
+    if (a.level != P.level) throw Error(-4, "bootstrap: linear transform at the wrong level");
+    const int g = prm.baby;
+    std::set<int> jset;
+    for (const auto& kv : P.giant)
+      for (int j : kv.second) jset.insert(j);
+    std::vector<int> js(jset.begin(), jset.end()), rs;
+    for (int j : js) rs.push_back((int)boot::pymod((long)P.step * j, n));
+    const std::vector<boot::Ct> bv = rotate_many(a, rs, s);
+    std::map<int, boot::Ct> baby;
+    for (size_t k = 0; k < js.size(); ++k) baby[js[k]] = bv[k];
+    std::vector<boot::Ct> parts;
+    std::vector<std::pair<boot::Ct, int>> turns;
+    for (const auto& [i, jl] : P.giant) {
+      std::vector<std::pair<boot::Ct, boot::Buf>> terms;
+      for (int j : jl) {
+        auto it = P.pts.find({i, j});
+        if (it != P.pts.end()) terms.push_back({baby[j], it->second});
+      }
+      if (terms.empty()) continue;
+      boot::Ct inner;
+      bool have = false;
+      for (size_t k = 0; k < terms.size(); k += MAX_DOT_TERMS) {
+        const size_t m = std::min<size_t>(MAX_DOT_TERMS, terms.size() - k);
+        boot::Ct d = fresh(a.level, a.scale, s);
+        DotJob j{};
+        for (size_t t = 0; t < m; ++t) {
+          j.c0[t] = terms[k + t].first.c0;
+          j.c1[t] = terms[k + t].first.c1;
+          j.pt[t] = terms[k + t].second->u64();
+        }
+        j.out0 = mut(d.c0);
+        j.out1 = mut(d.c1);
+        j.n = (int)m;
+        j.l = a.level;
+        launch_dot_plain(c, j, s);
+        inner = have ? add_many({inner}, {d}, s)[0] : d;
+        have = true;
+      }
+      const int r = (int)boot::pymod((long)P.step * g * i, n);
+      if (r)
+        turns.push_back({inner, r});
+      else
+        parts.push_back(inner);
+    }
+    for (auto& o : rotate_batch(turns, s)) parts.push_back(o);
+    while (parts.size() > 1) {
+      std::vector<boot::Ct> next;
+      for (size_t k = 0; k < parts.size(); k += 16) {
+        const size_t m = std::min<size_t>(16, parts.size() - k);
+        if (m > 1) {
+          std::vector<boot::Ct> grp(parts.begin() + k, parts.begin() + k + m);
+          next.push_back(lincomb_many({grp}, std::vector<long long>(m, 1), 0.0, s)[0]);
+        } else {
+          next.push_back(parts[k]);
+        }
+      }
+      parts = next;
+    }
+    return rescale_many_to({parts[0]}, S[a.level - 1], s)[0];
+  }
+
+  // ---------------------------------------------------------------- EvalMod
+  static constexpr int PS_BABY = 16;
+
+  struct Powers {
+    std::map<int, std::vector<boot::Ct>> T;
+    std::map<std::pair<int, int>, std::vector<boot::Ct>> at;
+  };
+
+  const std::vector<boot::Ct>& t_at(Powers& P, int k, int level, cudaStream_t s) const {
+    auto key = std::make_pair(k, level);
+    auto it = P.at.find(key);
+    if (it == P.at.end()) it = P.at.emplace(key, to_level_many(P.T.at(k), level, s)).first;
+    return it->second;
+  }
+
+  Powers cheb_powers(const std::vector<boot::Ct>& ts, cudaStream_t s) const {
+    Powers P;
+    P.T[1] = ts;
+    auto make = [&](int k) {
+      std::vector<std::pair<boot::Ct, boot::Ct>> pr;
+      if (k % 2 == 0) {
+        for (const auto& a : P.T.at(k / 2)) pr.push_back({a, a});
+        auto x = mul_many(pr, s);
+        std::vector<std::vector<boot::Ct>> lanes;
+        for (const auto& p : x) lanes.push_back({p});
+        P.T[k] = lincomb_many(lanes, {2}, -1.0, s);
+      } else {
+        const auto &A = P.T.at(k / 2), &B = P.T.at(k / 2 + 1);
+        for (size_t i = 0; i < A.size(); ++i) pr.push_back({A[i], B[i]});
+        auto x = mul_many(pr, s);
+        const auto& one = t_at(P, 1, x[0].level, s);
+        std::vector<std::vector<boot::Ct>> lanes;
+        for (size_t i = 0; i < x.size(); ++i) lanes.push_back({x[i], one[i]});
+        P.T[k] = lincomb_many(lanes, {2, -1}, 0.0, s);
+      }
+    };
+    for (int k = 2; k <= PS_BABY; ++k) make(k);
+    for (int m = 2 * PS_BABY; m <= prm.degree; m *= 2) make(m);
+    return P;
+  }
+
+  std::vector<boot::Ct> ps(const std::vector<double>& coeffs, int level_out, Powers& P, int nl, cudaStream_t s) const {
+    const int nc = (int)coeffs.size();
+    if (nc <= PS_BABY) {
+      std::vector<int> ks;
+      for (int k = 1; k < nc; ++k) ks.push_back(k);
+      if (ks.empty()) ks.push_back(1);
+      std::vector<double> cf;
+      for (int k : ks) cf.push_back(k < nc ? coeffs[k] : 0.0);
+      std::vector<std::vector<boot::Ct>> lanes(nl);
+      for (int i = 0; i < nl; ++i)
+        for (int k : ks) lanes[i].push_back(P.T.at(k)[i]);
+      return lincomb_to_many(lanes, cf, coeffs[0], level_out, s);
+    }
+    int m = 1;
+    while (m * 2 <= nc - 1) m *= 2;  // 1 << ((nc - 1).bit_length() - 1)
+    std::vector<double> q(nc - m, 0.0), r(coeffs.begin(), coeffs.begin() + m);
+    q[0] = coeffs[m];
+    for (int j = 1; j < nc - m; ++j) {
+      q[j] = 2 * coeffs[m + j];
+      r[m - j] -= coeffs[m + j];
+    }
+    auto qc = ps(q, level_out + 1, P, nl, s);
+    const auto& tm = t_at(P, m, level_out + 1, s);
+    std::vector<std::pair<boot::Ct, boot::Ct>> pr;
+    for (int i = 0; i < nl; ++i) pr.push_back({qc[i], tm[i]});
+    auto prod = mul_many(pr, s);
+    auto rc = ps(r, level_out, P, nl, s);
+    return add_many(prod, rc, s);
+  }
+
+  std::vector<boot::Ct> eval_mod_many(const std::vector<boot::Ct>& ts, cudaStream_t s) const {
+    Powers P = cheb_powers(ts, s);
+    const int depth = (int)std::ceil(std::log2((double)prm.degree)) + 1;
+    auto cs = ps(cheb, ts[0].level - depth, P, (int)ts.size(), s);
+    for (int k = 0; k < prm.r; ++k) {
+      std::vector<std::pair<boot::Ct, boot::Ct>> pr;
+      for (const auto& x : cs) pr.push_back({x, x});
+      auto sq = mul_many(pr, s);
+      std::vector<std::vector<boot::Ct>> lanes;
+      for (const auto& x : sq) lanes.push_back({x});
+      cs = lincomb_many(lanes, {2}, -1.0, s);
+    }
+    return cs;
+  }
+
+  // ---------------------------------------------------------------- the bootstrap
+  boot::Ct run(const uint64_t* c0, const uint64_t* c1, cudaStream_t s) const {
+    if (!prepared) throw Error(-7, "bootstrap: fides_boot_prepare has not run");
+    if (!relin || !conj) throw Error(-5, "bootstrap: relinearization / conjugation key not set");
+    boot::Ct x;
+    x.c0 = c0;
+    x.c1 = c1;
+    x.level = 1;
+    x.scale = prm.msg_scale;
+    if (prm.sparse_encapsulation) {
+      if (!to_sparse || !to_dense) throw Error(-5, "bootstrap: encapsulation keys not set");
+      x = keyswitch_add(x, to_sparse, s);  // dense -> sparse secret, at level 1
+    }
+    if (prm.prescale_bits) x = mul_int(x, 1ll << prm.prescale_bits, s);
+    boot::Ct a = fresh(top, in_scale, s);  // ModRaise: m -> m + q0 I on every limb of the top level
+    op_mod_raise(c, x.c0, top, mut(a.c0), s);
+    op_mod_raise(c, x.c1, top, mut(a.c1), s);
+    if (prm.sparse_encapsulation) a = keyswitch_add(a, to_dense, s);  // back to the dense secret
+    for (const auto& P : cts_pl) a = apply(a, P, s);
+    const boot::Ct cj = conjugate(a, s);
+    const boot::Ct t_re = add_raw(a, cj, s);
+    const boot::Ct t_im = mul_plain_int(sub_raw(a, cj, s), pt_minus_i, s);
+    auto sm = eval_mod_many({t_re, t_im}, s);
+    const boot::Ct s_re = to_level(sm[0], stc_in_level, s);
+    const boot::Ct s_im = to_level(sm[1], stc_in_level, s);
+    boot::Ct u = add_raw(s_re, mul_plain_int(s_im, pt_i, s), s);
+    for (const auto& P : stc_pl) u = apply(u, P, s);
+    return u;
+  }
+
+  void run_into(const uint64_t* c0, const uint64_t* c1, uint64_t* o0, uint64_t* o1, cudaStream_t s) const {
+    const boot::Ct u = run(c0, c1, s);
+    const size_t bytes = sizeof(uint64_t) * (size_t)c->N * u.level;
+    FIDES_CUDA(cudaMemcpyAsync(o0, u.c0, bytes, cudaMemcpyDeviceToDevice, s));
+    FIDES_CUDA(cudaMemcpyAsync(o1, u.c1, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+};
+
+}  // namespace fides
+
+struct fides_boot {
+  fides_ctx* ctx;
+  std::unique_ptr<fides::Bootstrapper> b;
+};
+
+namespace {
+template <typename F>
+int bguard(const char* name, F&& f) {
+  (void)name;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  int rc = FIDES_OK;
+  try {
+    f();
+  } catch (const fides::Error& e) {
+    fides::set_last_error(e.what());
+    rc = e.code;
+  } catch (const std::bad_alloc&) {
+    fides::set_last_error("host allocation failed");
+    rc = FIDES_ERR_OOM;
+  } catch (const std::exception& e) {
+    fides::set_last_error(e.what());
+    rc = FIDES_ERR_STATE;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
+}
+
+fides::Bootstrapper* B(fides_boot* b) {
+  if (!b || !b->b) throw fides::Error(FIDES_ERR_ARG, "null bootstrapper");
+  FIDES_CUDA(cudaSetDevice(b->b->c->device));
+  return b->b.get();
+}
+}  // namespace
+
+extern "C" {
+
+int fides_boot_create(fides_ctx* ctx, const fides_boot_params* p, fides_boot** out) {
+  return bguard(__func__, [&] {
+    if (!ctx || !ctx->c || !p || !out) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    fides::Context* c = ctx->c;
+    FIDES_CUDA(cudaSetDevice(c->device));
+    if (p->level_budget_cts < 1 || p->level_budget_stc < 1 || p->level_budget_cts > c->logN - 1 ||
+        p->level_budget_stc > c->logN - 1)
+      throw fides::Error(FIDES_ERR_ARG, "level budget out of range");
+    if (p->top_level < 2 || p->top_level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "top level out of range");
+    if (!(p->top_scale > 0) || !(p->msg_scale > 0)) throw fides::Error(FIDES_ERR_ARG, "scales must be positive");
+    if (p->degree < 2 || p->K < 1 || p->r < 0 || p->baby < 1 || p->prescale_bits < 0 || p->prescale_bits > 30)
+      throw fides::Error(FIDES_ERR_ARG, "EvalMod / BSGS parameters out of range");
+    if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "bootstrapping needs special primes");
+    auto* bs = new fides::Bootstrapper{};
+    bs->c = c;
+    bs->prm = *p;
+    try {
+      bs->build_tables();
+    } catch (...) {
+      delete bs;
+      throw;
+    }
+    *out = new fides_boot{ctx, std::unique_ptr<fides::Bootstrapper>(bs)};
+  });
+}
+
+int fides_boot_destroy(fides_boot* b) {
+  return bguard(__func__, [&] {
+    if (!b) return;
+    if (b->b) {
+      cudaSetDevice(b->b->c->device);
+      cudaDeviceSynchronize();
+    }
+    delete b;
+  });
+}
+
+int fides_boot_rotations(const fides_boot* b, int* out, int cap) {
+  if (!b || !b->b) return FIDES_ERR_ARG;
+  const auto& r = b->b->rotations;
+  for (int i = 0; out && i < cap && i < (int)r.size(); ++i) out[i] = r[i];
+  return (int)r.size();
+}
+
+int fides_boot_set_keys(fides_boot* b, const uint64_t* relin_key, const uint64_t* conj_key, const uint64_t* to_sparse,
+                        const uint64_t* to_dense) {
+  return bguard(__func__, [&] {
+    auto* bs = B(b);
+    if (!relin_key || !conj_key) throw fides::Error(FIDES_ERR_KEY, "relinearization and conjugation keys needed");
+    if (bs->prm.sparse_encapsulation && (!to_sparse || !to_dense))
+      throw fides::Error(FIDES_ERR_KEY, "sparse encapsulation needs both switching keys");
+    bs->relin = relin_key;
+    bs->conj = conj_key;
+    bs->to_sparse = to_sparse;
+    bs->to_dense = to_dense;
+  });
+}
+
+int fides_boot_set_rotation_key(fides_boot* b, int rotation, const uint64_t* key) {
+  return bguard(__func__, [&] {
+    auto* bs = B(b);
+    if (!key) throw fides::Error(FIDES_ERR_KEY, "null rotation key");
+    bs->rot[(int)fides::boot::pymod(rotation, bs->n)] = key;
+  });
+}
+
+int fides_boot_prepare(fides_boot* b, void* stream) {
+  return bguard(__func__, [&] {
+    auto* bs = B(b);
+    for (int r : bs->rotations)
+      if (!bs->rot.count(r)) throw fides::Error(FIDES_ERR_KEY, "missing rotation key " + std::to_string(r));
+    bs->prepare(static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fides_boot_levels(const fides_boot* b, int* out_level, double* out_scale) {
+  if (!b || !b->b || !b->b->prepared) return FIDES_ERR_STATE;
+  if (out_level) *out_level = b->b->out_level;
+  if (out_scale) *out_scale = b->b->S[b->b->out_level];
+  return FIDES_OK;
+}
+
+int fides_bootstrap(fides_boot* b, const uint64_t* c0, const uint64_t* c1, uint64_t* out0, uint64_t* out1,
+                    void* stream) {
+  return bguard(__func__, [&] {
+    auto* bs = B(b);
+    if (!c0 || !c1 || !out0 || !out1) throw fides::Error(FIDES_ERR_ARG, "null polynomial pointer");
+    bs->run_into(c0, c1, out0, out1, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fides_bootstrap_batch(fides_boot* b, int n, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                          uint64_t* const* out0s, uint64_t* const* out1s, void* stream) {
+  return bguard(__func__, [&] {
+    auto* bs = B(b);
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    if (n == 0) return;
+    if (!c0s || !c1s || !out0s || !out1s) throw fides::Error(FIDES_ERR_ARG, "null pointer array");
+    cudaStream_t main = static_cast<cudaStream_t>(stream);
+    while ((int)bs->lanes.size() < n) {
+      cudaStream_t s;
+      cudaEvent_t e;
+      FIDES_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      FIDES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      bs->lanes.push_back(s);
+      bs->lane_ev.push_back(e);
+    }
+    // fork: every lane waits for the caller's stream; join: the caller's stream waits for every
+    // lane (one graph with a parallel branch per ciphertext when captured)
+    cudaEvent_t fork = bs->lane_ev[0];
+    FIDES_CUDA(cudaEventRecord(fork, main));
+    for (int i = 0; i < n; ++i) FIDES_CUDA(cudaStreamWaitEvent(bs->lanes[i], fork, 0));
+    for (int i = 0; i < n; ++i) {
+      if (!c0s[i] || !c1s[i] || !out0s[i] || !out1s[i]) throw fides::Error(FIDES_ERR_ARG, "null polynomial pointer");
+      bs->run_into(c0s[i], c1s[i], out0s[i], out1s[i], bs->lanes[i]);
+    }
+    for (int i = 0; i < n; ++i) {
+      FIDES_CUDA(cudaEventRecord(bs->lane_ev[i], bs->lanes[i]));
+      FIDES_CUDA(cudaStreamWaitEvent(main, bs->lane_ev[i], 0));
+    }
+  });
+}
+
+int fides_boot_chebyshev(const fides_boot* b, double* coeffs, int cap) {
+  if (!b || !b->b) return FIDES_ERR_ARG;
+  const auto& v = b->b->cheb;
+  for (int i = 0; coeffs && i < cap && i < (int)v.size(); ++i) coeffs[i] = v[i];
+  return (int)v.size();
+}
+
+int fides_boot_table(const fides_boot* b, int which, int m, int* offsets, int cap, double* diags) {
+  if (!b || !b->b || (which != 0 && which != 1)) return FIDES_ERR_ARG;
+  const auto& mats = which == 0 ? b->b->cts : b->b->stc;
+  if (m < 0 || m >= (int)mats.size()) return FIDES_ERR_ARG;
+  const auto& M = mats[m];
+  int k = 0;
+  for (const auto& [off, d] : M) {
+    if (k < cap) {
+      if (offsets) offsets[k] = off;
+      if (diags) std::memcpy(diags + (size_t)k * 2 * d.size(), d.data(), sizeof(double) * 2 * d.size());
+    }
+    ++k;
+  }
+  return k;
+}
+
+int fides_boot_matrices(const fides_boot* b, int which) {
+  if (!b || !b->b || (which != 0 && which != 1)) return FIDES_ERR_ARG;
+  return (int)(which == 0 ? b->b->cts : b->b->stc).size();
+}
+
+}  // extern "C"

@@ -124,8 +124,16 @@ __device__ __forceinline__ uint64_t ksk_canon_f64(double s, double q, double qin
   return (uint64_t)__double_as_longlong(__dadd_rn(r, 4503599627370496.0)) & ((1ull << 52) - 1);
 }
 
+// Three CTAs (24 warps) per SM: 80 registers.  The grouped forms spill a few registers there
+// (measured faster than two CTAs per SM); the single-job forms with up to three digits fit
+// without spills (they took 96-120 registers, two CTAs per SM, when unbounded).
+template <int MAXB, int JG>
+struct KskMinBlocks {
+  static constexpr int value = (JG > 1 || (MAXB >= 1 && MAXB <= 3)) ? 3 : 1;
+};
+
 template <int MAXB, int JG, int CPT, bool SHARE_DIGITS = false>
-__global__ void __launch_bounds__(EW_THREADS, JG > 1 ? 3 : 1) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
+__global__ void __launch_bounds__(EW_THREADS, KskMinBlocks<MAXB, JG>::value) ksk_kernel(const __grid_constant__ KskJobList L, const DevPrime* primes,
                                                             const ShoupConst* pmod, const F64Prime* f64, int logN,
                                                             int n_q, int K, int dnum, int alpha) {
   using V = KVec<CPT>;

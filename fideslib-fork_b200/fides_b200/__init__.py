@@ -80,6 +80,12 @@ class _RotateItem(C.Structure):
                 ("auto_index", C.c_uint32)]
 
 
+class _BootParams(C.Structure):
+    _fields_ = [("level_budget_cts", C.c_int), ("level_budget_stc", C.c_int), ("top_level", C.c_int),
+                ("top_scale", C.c_double), ("msg_scale", C.c_double), ("K", C.c_int), ("r", C.c_int),
+                ("degree", C.c_int), ("baby", C.c_int), ("prescale_bits", C.c_int), ("sparse_encapsulation", C.c_int)]
+
+
 def build(force: bool = False) -> str:
     """Compile libfides_b200.so for sm_100a with nvcc (make, in-tree)."""
     if force or not os.path.exists(LIB_PATH):
@@ -116,6 +122,18 @@ def lib():
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_synchronize.argtypes = [vp, vp]
+        L.fides_boot_create.argtypes = [vp, C.POINTER(_BootParams), C.POINTER(vp)]
+        L.fides_boot_destroy.argtypes = [vp]
+        L.fides_boot_rotations.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
+        L.fides_boot_set_keys.argtypes = [vp, vp, vp, vp, vp]
+        L.fides_boot_set_rotation_key.argtypes = [vp, C.c_int, vp]
+        L.fides_boot_prepare.argtypes = [vp, vp]
+        L.fides_boot_levels.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.fides_bootstrap.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.fides_bootstrap_batch.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
+        L.fides_boot_chebyshev.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
+        L.fides_boot_matrices.argtypes = [vp, C.c_int]
+        L.fides_boot_table.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, vp]
         L.fides_ctx_inject_status.argtypes = [vp, C.c_uint32]
         L.fides_kernel_arch.argtypes = [C.c_int, C.POINTER(C.c_int)]
         L.fides_server_wait_timeout.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(C.c_double),
@@ -776,6 +794,100 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+class NativeBootstrapper:
+    """The library's C++ bootstrapper (fides_boot_*): tables derived at creation, device keys set
+    by the caller (kept referenced here), full packing (N/2 slots).  bootstrap() reads limb q_0
+    of (c0, c1) and returns the output Ciphertext at out_level limbs, scale out_scale."""
+
+    def __init__(self, ctx: "Context", top_level: int, top_scale: float, msg_scale: float, budget=(3, 3),
+                 K: int = 12, r: int = 3, degree: int = 63, baby: int = 8, prescale_bits: int = 0,
+                 encapsulation: bool = False):
+        self.ctx = ctx
+        p = _BootParams(budget[0], budget[1], top_level, float(top_scale), float(msg_scale), K, r, degree, baby,
+                        prescale_bits, 1 if encapsulation else 0)
+        h = vp()
+        _check(lib().fides_boot_create(ctx._h, C.byref(p), C.byref(h)))
+        self._h = h
+        self._keys = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fides_boot_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rotations(self) -> list[int]:
+        n = lib().fides_boot_rotations(self._h, None, 0)
+        buf = (C.c_int * max(1, n))()
+        lib().fides_boot_rotations(self._h, buf, n)
+        return list(buf[:n])
+
+    def set_keys(self, relin, conj, to_sparse=None, to_dense=None):
+        self._keys += [relin, conj, to_sparse, to_dense]
+        _check(lib().fides_boot_set_keys(self._h, _ptr(relin), _ptr(conj), _ptr(to_sparse), _ptr(to_dense)))
+
+    def set_rotation_key(self, rotation: int, key):
+        self._keys.append(key)
+        _check(lib().fides_boot_set_rotation_key(self._h, rotation, _ptr(key)))
+
+    def prepare(self):
+        _check(lib().fides_boot_prepare(self._h, _stream()))
+
+    @property
+    def out_level(self) -> int:
+        lv, sc = C.c_int(), C.c_double()
+        _check(lib().fides_boot_levels(self._h, C.byref(lv), C.byref(sc)))
+        return int(lv.value)
+
+    @property
+    def out_scale(self) -> float:
+        lv, sc = C.c_int(), C.c_double()
+        _check(lib().fides_boot_levels(self._h, C.byref(lv), C.byref(sc)))
+        return float(sc.value)
+
+    def bootstrap(self, ct: "Ciphertext") -> "Ciphertext":
+        lo = self.out_level
+        out = Ciphertext(self.ctx.empty(lo), self.ctx.empty(lo))
+        _check(lib().fides_bootstrap(self._h, _ptr(ct.c0), _ptr(ct.c1), _ptr(out.c0), _ptr(out.c1), _stream()))
+        return out
+
+    def bootstrap_batch(self, cts) -> list:
+        n, lo = len(cts), self.out_level
+        outs = [Ciphertext(self.ctx.empty(lo), self.ctx.empty(lo)) for _ in cts]
+        arr = lambda xs: (vp * n)(*xs)
+        _check(lib().fides_bootstrap_batch(self._h, n, arr([_ptr(c.c0) for c in cts]), arr([_ptr(c.c1) for c in cts]),
+                                           arr([_ptr(o.c0) for o in outs]), arr([_ptr(o.c1) for o in outs]),
+                                           _stream()))
+        return outs
+
+    def chebyshev(self):
+        import numpy as np
+        n = lib().fides_boot_chebyshev(self._h, None, 0)
+        buf = np.empty(n, dtype=np.float64)
+        lib().fides_boot_chebyshev(self._h, buf.ctypes.data_as(C.POINTER(C.c_double)), n)
+        return buf
+
+    def matrices(self, which: str) -> list:
+        """The composed special-FFT matrices of 'cts' (CoeffsToSlots) or 'stc' (SlotsToCoeffs)
+        as dicts slot offset -> complex diagonal (numpy)."""
+        import numpy as np
+        w = {"cts": 0, "stc": 1}[which]
+        mats = []
+        n = self.ctx.N // 2
+        for m in range(lib().fides_boot_matrices(self._h, w)):
+            cnt = lib().fides_boot_table(self._h, w, m, None, 0, None)
+            offs = (C.c_int * cnt)()
+            d = np.empty((cnt, n), dtype=np.complex128)
+            lib().fides_boot_table(self._h, w, m, offs, cnt, d.ctypes.data)
+            mats.append({int(o): d[k] for k, o in enumerate(offs)})
+        return mats
 
 
 class Server:

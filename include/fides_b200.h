@@ -395,6 +395,64 @@ int fides_rotate_host_batch(fides_ctx* ctx, const fides_rotate_host_item* items,
 int fides_mixed_host_batch(fides_ctx* ctx, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
                            int rescale, const fides_rotate_host_item* rot, int n_rot);
 
+/* ---- bootstrapping ---------------------------------------------------------------------
+ * CKKS bootstrapping driven from the library's C++ host layer: replaces CKKS::Bootstrap
+ * (src/CKKS/Bootstrap.cu:437-648) behind CudaEngine::evalBootstrap and
+ * CryptoContext::EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap
+ * (api/CryptoContext.hpp:306-458).  Sequence: optional sparse-secret encapsulation
+ * (keySwitchSparse, Bootstrap.cu:257-290: the level-1 input is switched to a sparse secret
+ * before ModRaise and back right after it), an optional power-of-two prescale, ModRaise,
+ * CoeffsToSlots (level_budget_cts BSGS linear transforms of the special FFT, CoeffsToSlots.cu:
+ * 75-151), EvalMod on the real and imaginary parts (Chebyshev series of the scaled cosine by
+ * Paterson-Stockmeyer, then r double-angle steps; ApproxModEval.cu:45-167, 527, 873) and
+ * SlotsToCoeffs (level_budget_stc transforms).  Full packing: N/2 slots.  Scales follow the
+ * FLEXIBLEAUTO chain S_(l-1) = S_l^2 / q_(l-1) from S_(n_q) = top_scale.  The tables (special-FFT
+ * diagonals, Chebyshev coefficients) are derived from the mathematics at creation. */
+typedef struct fides_boot_params {
+  int level_budget_cts, level_budget_stc; /* levels of CoeffsToSlots / SlotsToCoeffs ({3, 3}) */
+  int top_level;         /* limbs after ModRaise (<= n_q) */
+  double top_scale;      /* S_(n_q): the scale chain's top */
+  double msg_scale;      /* scale of the input ciphertexts' slots */
+  int K;                 /* EvalMod range: |m + q_0 I| < K q_0 */
+  int r;                 /* double-angle steps */
+  int degree;            /* Chebyshev degree */
+  int baby;              /* BSGS baby steps */
+  int prescale_bits;     /* input multiplied by 2^prescale_bits before ModRaise (divided out after) */
+  int sparse_encapsulation; /* 1: switch to a sparse secret around ModRaise (keys below) */
+} fides_boot_params;
+typedef struct fides_boot fides_boot;
+int fides_boot_create(fides_ctx* ctx, const fides_boot_params* params, fides_boot** out);
+int fides_boot_destroy(fides_boot* b);
+/* Rotation amounts (slots, in [1, N/2)) whose keys the linear transforms use: writes up to cap
+ * of them and returns the count (EvalBootstrapKeyGen's rotation list). */
+int fides_boot_rotations(const fides_boot* b, int* out, int cap);
+/* Device keys (owned by the caller, kept for the bootstrapper's lifetime): relinearisation,
+ * conjugation (automorphism 2N - 1) and, with sparse_encapsulation, the switching keys dense ->
+ * sparse and sparse -> dense secret. */
+int fides_boot_set_keys(fides_boot* b, const uint64_t* relin_key, const uint64_t* conj_key, const uint64_t* to_sparse,
+                        const uint64_t* to_dense);
+int fides_boot_set_rotation_key(fides_boot* b, int rotation, const uint64_t* key);
+/* Encodes the linear transforms' diagonals on the device (synchronises `stream`). */
+int fides_boot_prepare(fides_boot* b, void* stream);
+/* Level (limbs) and scale of the bootstrapped output. */
+int fides_boot_levels(const fides_boot* b, int* out_level, double* out_scale);
+/* Bootstraps (c0, c1) (limb q_0 is read) into out0 / out1 (out_level limbs each) on `stream`. */
+int fides_bootstrap(fides_boot* b, const uint64_t* c0, const uint64_t* c1, uint64_t* out0, uint64_t* out1,
+                    void* stream);
+/* n bootstraps at once, each on its own internal stream forked from and joined back to
+ * `stream` (one CUDA graph with a parallel branch per ciphertext when captured).  Results equal
+ * fides_bootstrap's, ciphertext by ciphertext.  No reference counterpart (the reference
+ * bootstraps one ciphertext per call). */
+int fides_bootstrap_batch(fides_boot* b, int n, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                          uint64_t* const* out0s, uint64_t* const* out1s, void* stream);
+/* The derived tables, for inspection and comparison: the Chebyshev coefficients (returns the
+ * count); the number of composed matrices of CoeffsToSlots (which = 0) or SlotsToCoeffs (1);
+ * matrix m's slot-diagonal offsets and, when diags is not NULL, its diagonals as
+ * [count][N/2][re, im] doubles (returns the count; cap bounds what is written). */
+int fides_boot_chebyshev(const fides_boot* b, double* coeffs, int cap);
+int fides_boot_matrices(const fides_boot* b, int which);
+int fides_boot_table(const fides_boot* b, int which, int m, int* offsets, int cap, double* diags);
+
 /* ---- allocation-free entry point ----------------------------------------------------
  * No counterpart in the reference.  fides_rescale_noalloc computes exactly what
  * fides_rescale computes for one polynomial, but takes its scratch (one limb) from a

@@ -271,3 +271,176 @@ def test_bootstrap_sparse_secret_encapsulation(fides):
     bits = -math.log2(np.abs(got - z).max())
     print(f"bootstrap with encapsulation N=2^12: {bits:.1f} bits, out level {out.level}")
     assert bits > 12
+
+
+def make_config_d(F, seed=21):
+    """Config D: N = 2^16, L+1 = 24 (60-bit q_0, 50-bit scaling primes), dnum 3, dense uniform
+    ternary secret with HW-32 sparse-secret encapsulation, CtS / StC level budget {3, 3},
+    input scale 2^50 pre-scaled by 2^5 (the bench's bootstrap)."""
+    from fides_b200 import params as P
+    from fides_b200 import bootstrap as B
+    prm = P.chain(16, 60, 50, 24, 3, name="D")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=seed)
+    sparse = KeyGen(o, seed_stream=seed + 1000, hamming_weight=32)
+    ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    encaps = (F.to_device(kg.switching_key(sparse.s_eval, kg.s_eval)),
+              F.to_device(kg.switching_key(kg.s_eval, sparse.s_eval)))
+    ev = B.Evaluator(F, ctx, F.to_device(kg.relin_key()), {}, F.to_device(kg.auto_key(2 * prm.N - 1)),
+                     top_scale=2.0 ** 50)
+    bs = B.Bootstrapper(ev, K=12, prescale_bits=5, encapsulation=encaps)
+    assert bs.cts_levels == 3
+    ev.rot_keys = {r: F.to_device(kg.rotation_key(r)) for r in bs.needed_rotations()}
+    bs.prepare(top_level=prm.n_q, msg_scale=2.0 ** 50)
+    return prm, o, kg, ctx, ev, bs
+
+
+@pytest.fixture(scope="module")
+def config_d(fides):
+    return make_config_d(fides)
+
+
+@pytest.mark.gpu
+def test_bootstrap_config_d_n65536_batch8(fides, config_d):
+    """Config D at full size: 2^15 slots uniform in [-1, 1]; every ciphertext of a batch of 8
+    decrypts within 2^-15 of the FP64 plaintext (reference measure:
+    test/BootstrapPrecisionTests.cu:141-259), and the batch bootstrapped on 8 parallel streams
+    equals the one-at-a-time bootstraps bit for bit."""
+    import torch
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm, o, kg, ctx, ev, bs = config_d
+    delta = 2.0 ** 50
+    n = prm.N // 2
+    assert n == 1 << 15
+    rng = xrng(22)
+    zs, cts = [], []
+    for _ in range(8):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        zs.append(z)
+        cts.append(B.Ct(F.to_device(c0), F.to_device(c1), delta))
+    seq = [bs.bootstrap(c) for c in cts]
+    par = B.bootstrap_concurrent(bs, cts, [torch.cuda.Stream() for _ in cts])
+    torch.cuda.synchronize()
+    bits = []
+    for i, (a, b, z) in enumerate(zip(seq, par, zs)):
+        assert torch.equal(a.c0, b.c0) and torch.equal(a.c1, b.c1), f"ciphertext {i}: batch != single"
+        got = decode(kg.decrypt_limb0(F.to_host(a.c0), F.to_host(a.c1)), prm.N, a.scale)
+        bits.append(-math.log2(np.abs(got - z).max()))
+    print(f"config D bootstrap: out level {seq[0].level}, precision {min(bits):.2f}..{max(bits):.2f} bits")
+    assert seq[0].level >= 8
+    assert min(bits) >= 15.0
+
+
+# ---------------------------------------------------------------- the library's C++ bootstrapper
+def native_for(F, prm, ev, bs, encaps=None):
+    """A NativeBootstrapper with the Python driver's parameters and keys."""
+    nb = F.NativeBootstrapper(ev.ctx, top_level=prm.n_q, top_scale=ev.S[prm.n_q], msg_scale=2.0 ** 50,
+                              budget=(bs.cts_levels, bs.stc_levels), K=bs.K, r=bs.r, degree=bs.degree, baby=bs.baby,
+                              prescale_bits=bs.prescale.bit_length() - 1, encapsulation=encaps is not None)
+    nb.set_keys(ev.rk, ev.conj_key, *(encaps or (None, None)))
+    for r in nb.rotations():
+        nb.set_rotation_key(r, ev.rot_keys[r])
+    return nb
+
+
+def python_with_native_tables(bs, nb):
+    """The Python driver re-prepared on the C++ driver's tables (special-FFT diagonals and
+    Chebyshev coefficients), so that the two drivers can be compared residue for residue."""
+    bs.cts, bs.stc, bs.cheb = nb.matrices("cts"), nb.matrices("stc"), nb.chebyshev()
+    bs.prepare(top_level=bs.top, msg_scale=2.0 ** 50)
+    return bs
+
+
+@pytest.mark.gpu
+def test_native_tables_match_numpy(fides):
+    """The C++ driver's derived tables equal the Python driver's numpy ones to rounding: the
+    composed special-FFT diagonals (same offsets), the Chebyshev coefficients and the rotation
+    list."""
+    from fides_b200 import bootstrap as B
+    prm, o, kg, ctx, ev, bs = make_boot(fides, 12)
+    nb = native_for(fides, prm, ev, bs)
+    assert nb.rotations() == bs.needed_rotations()
+    assert np.abs(nb.chebyshev() - np.asarray(bs.cheb)).max() < 1e-13
+    for which, ref in (("cts", bs.cts), ("stc", bs.stc)):
+        mats = nb.matrices(which)
+        assert len(mats) == len(ref)
+        for M, R in zip(mats, ref):
+            assert sorted(M) == sorted(R)
+            for k in M:
+                assert np.abs(M[k] - R[k]).max() <= 1e-12 * max(1.0, np.abs(R[k]).max())
+
+
+@pytest.mark.gpu
+def test_native_bootstrap_equals_python_driver_n4096(fides):
+    """N = 2^12: the C++ bootstrapper's output equals the Python driver's on the same tables
+    bit for bit, decrypts to the FP64 plaintext (> 12 bits), and a batch through
+    fides_bootstrap_batch equals the single bootstraps."""
+    import torch
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    nb = native_for(F, prm, ev, bs)
+    nb.prepare()
+    bs.top = prm.n_q
+    python_with_native_tables(bs, nb)
+    assert nb.out_level == bs.out_level
+    delta = 2.0 ** 50
+    rng = xrng(67)
+    n = prm.N // 2
+    zs, cts = [], []
+    for _ in range(3):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        zs.append(z)
+        cts.append(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    py = bs.bootstrap(B.Ct(cts[0].c0, cts[0].c1, delta))
+    nat = nb.bootstrap(cts[0])
+    batch = nb.bootstrap_batch(cts)
+    torch.cuda.synchronize()
+    assert torch.equal(py.c0, nat.c0) and torch.equal(py.c1, nat.c1)
+    for i, (ct, out) in enumerate(zip(cts, batch)):
+        single = nat if i == 0 else nb.bootstrap(ct)
+        torch.cuda.synchronize()
+        assert torch.equal(single.c0, out.c0) and torch.equal(single.c1, out.c1), f"batch item {i}"
+        got = decode(kg.decrypt_limb0(F.to_host(out.c0), F.to_host(out.c1)), prm.N, nb.out_scale)
+        assert -math.log2(np.abs(got - zs[i]).max()) > 12
+    nb.close()
+
+
+@pytest.mark.gpu
+def test_native_bootstrap_config_d_n65536(fides, config_d):
+    """Config D through the C++ bootstrapper: encapsulation, prescale 2^5, budget {3, 3};
+    >= 15 bits for a batch of 8 (fides_bootstrap_batch), batch = single bit for bit, and the
+    single equals the Python driver's on the same tables."""
+    import torch
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm, o, kg, ctx, ev, bs = config_d
+    nb = native_for(F, prm, ev, bs, encaps=bs.encapsulation)
+    nb.prepare()
+    delta = 2.0 ** 50
+    rng = xrng(23)
+    n = prm.N // 2
+    zs, cts = [], []
+    for _ in range(8):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        zs.append(z)
+        cts.append(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    batch = nb.bootstrap_batch(cts)
+    single = nb.bootstrap(cts[0])
+    torch.cuda.synchronize()
+    assert torch.equal(single.c0, batch[0].c0) and torch.equal(single.c1, batch[0].c1)
+    bits = []
+    for out, z in zip(batch, zs):
+        got = decode(kg.decrypt_limb0(F.to_host(out.c0), F.to_host(out.c1)), prm.N, nb.out_scale)
+        bits.append(-math.log2(np.abs(got - z).max()))
+    print(f"config D, C++ bootstrapper: out level {nb.out_level}, precision {min(bits):.2f}..{max(bits):.2f} bits")
+    assert min(bits) >= 15.0
+    python_with_native_tables(bs, nb)
+    py = bs.bootstrap(B.Ct(cts[0].c0, cts[0].c1, delta))
+    torch.cuda.synchronize()
+    assert torch.equal(py.c0, single.c0) and torch.equal(py.c1, single.c1)
+    nb.close()

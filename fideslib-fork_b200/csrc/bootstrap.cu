@@ -183,8 +183,26 @@ long floordiv(long a, long b) {
 }
 long pymod(long a, long b) { return ((a % b) + b) % b; }
 
-// Round half to even, as Python's round() on a float.
-long long rint_even(double v) { return (long long)std::nearbyint(v); }
+// Round half to even, as Python's round() on a float.  The result is an integer held exactly
+// in a double: constants such as round(c_0 S_t q_t) reach ~2^100, so they are reduced modulo
+// each prime from the double itself (residue_of), never through a 64-bit integer.
+double rint_even(double v) { return std::nearbyint(v); }
+
+// w mod q for an integer-valued double w (any magnitude), as a residue in [0, q).
+uint64_t residue_of(double w, uint64_t q) {
+  const bool neg = w < 0;
+  const double a = std::fabs(w);
+  uint64_t r;
+  if (a < 9223372036854775808.0) {  // 2^63: exact in an unsigned 64-bit integer
+    r = (uint64_t)a % q;
+  } else {  // a = m 2^k with m < 2^53 an integer and k >= 11
+    int e = 0;
+    const double fr = std::frexp(a, &e);  // a = fr 2^e, 0.5 <= fr < 1
+    const uint64_t m = (uint64_t)std::ldexp(fr, 53);
+    r = h_mulmod(m % q, h_powmod(2, (uint64_t)(e - 53), q), q);
+  }
+  return neg && r ? q - r : r;
+}
 
 // ---------------------------------------------------------------------- device values
 // A device polynomial buffer shared by the views (ciphertexts) that use it; freed on its stream
@@ -309,14 +327,7 @@ struct Bootstrapper {
     return a;
   }
   static uint64_t* mut(const uint64_t* p) { return const_cast<uint64_t*>(p); }
-  uint64_t residue(long long v, int i) const {
-    const long long q = (long long)c->primes[i];
-    return (uint64_t)(((v % q) + q) % q);
-  }
-  uint64_t residue(__int128 v, int i) const {
-    const __int128 q = (__int128)c->primes[i];
-    return (uint64_t)(((v % q) + q) % q);
-  }
+  uint64_t residue(double v, int i) const { return boot::residue_of(v, c->primes[i]); }
 
   boot::Ct drop(const boot::Ct& a, int level) const {
     boot::Ct b = a;
@@ -349,7 +360,7 @@ struct Bootstrapper {
     ew(EW_MUL, a.c1, pt->u64(), a.level, mut(o.c1), s);
     return o;
   }
-  boot::Ct mul_int(const boot::Ct& a, long long v, cudaStream_t s) const {
+  boot::Ct mul_int(const boot::Ct& a, double v, cudaStream_t s) const {
     if (a.level > MAX_SCALAR_LIMBS) throw Error(-1, "bootstrap: scalar product over more than 64 limbs");
     boot::Ct o = fresh(a.level, a.scale, s);
     for (int k = 0; k < 2; ++k) {
@@ -365,8 +376,9 @@ struct Bootstrapper {
   }
 
   // the same integer combination of every lane (one launch): sum_t ints[t] lane[t] (+ add on c0)
-  std::vector<boot::Ct> lincomb_lanes(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<long long>& ints,
-                                      const long long* add, int level, double scale, cudaStream_t s) const {
+  // ints / add: integers held exactly in doubles (see rint_even)
+  std::vector<boot::Ct> lincomb_lanes(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& ints,
+                                      const double* add, int level, double scale, cudaStream_t s) const {
     if (lanes.empty() || lanes.size() > (size_t)MAX_LC_LANES || ints.empty() || ints.size() > (size_t)MAX_LC_TERMS)
       throw Error(-1, "bootstrap: linear combination out of range");
     static thread_local LinCombJob j;
@@ -390,13 +402,13 @@ struct Bootstrapper {
     return outs;
   }
 
-  std::vector<boot::Ct> lincomb_many(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<long long>& ints,
+  std::vector<boot::Ct> lincomb_many(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& ints,
                                      double cst, cudaStream_t s) const {
     const boot::Ct& a = lanes[0][0];
     int l = a.level;
     for (const auto& ln : lanes)
       for (const auto& b : ln) l = std::min(l, b.level);
-    long long add = 0;
+    double add = 0;
     const bool has = cst != 0.0;
     if (has) add = boot::rint_even(cst * a.scale);
     return lincomb_lanes(lanes, ints, has ? &add : nullptr, l, a.scale, s);
@@ -431,7 +443,7 @@ struct Bootstrapper {
     const boot::Ct& a = cts_[0];
     if (a.level == level && std::abs(a.scale / S[level] - 1) < 1e-15) return cts_;
     if (a.level <= level) throw Error(-4, "bootstrap: cannot raise a level");
-    const long long k = boot::rint_even(S[level] * (double)c->primes[level] / a.scale);
+    const double k = boot::rint_even(S[level] * (double)c->primes[level] / a.scale);
     std::vector<std::vector<boot::Ct>> lanes;
     for (const auto& b : cts_) lanes.push_back({drop(b, level + 1)});
     return rescale_many_to(lincomb_many(lanes, {k}, 0.0, s), S[level], s);
@@ -442,12 +454,12 @@ struct Bootstrapper {
                                         double cst, int target, cudaStream_t s) const {
     const double qt = (double)c->primes[target], St = S[target];
     std::vector<int> keep;
-    std::vector<long long> ints;
+    std::vector<double> ints;
     for (size_t t = 0; t < coefs.size(); ++t) {
       const boot::Ct& a = lanes[0][t];
       if (a.level <= target) throw Error(-4, "bootstrap: operand below the combination's level");
-      const long long k = boot::rint_even(coefs[t] * St * qt / a.scale);
-      if (k) {
+      const double k = boot::rint_even(coefs[t] * St * qt / a.scale);
+      if (k != 0) {
         keep.push_back((int)t);
         ints.push_back(k);
       }
@@ -456,14 +468,14 @@ struct Bootstrapper {
       keep = {0};
       ints = {0};
     }
-    const long long add = boot::rint_even(cst * St * qt);
+    const double add = boot::rint_even(cst * St * qt);
     std::vector<std::vector<boot::Ct>> sel;
     for (const auto& ln : lanes) {
       std::vector<boot::Ct> v;
       for (int t : keep) v.push_back(ln[t]);
       sel.push_back(v);
     }
-    auto outs = lincomb_lanes(sel, ints, add ? &add : nullptr, target + 1, 0.0, s);
+    auto outs = lincomb_lanes(sel, ints, add != 0 ? &add : nullptr, target + 1, 0.0, s);
     return rescale_many_to(outs, St, s);
   }
 
@@ -550,7 +562,7 @@ struct Bootstrapper {
     return out;
   }
 
-  boot::Buf int_pt(const std::vector<long long>& coeff, int level, cudaStream_t s) const {
+  boot::Buf int_pt(const std::vector<double>& coeff, int level, cudaStream_t s) const {
     const size_t N = c->N;
     std::vector<uint64_t> h((size_t)level * N);
     for (int i = 0; i < level; ++i)
@@ -622,7 +634,7 @@ struct Bootstrapper {
       level -= 1;
     }
     out_level = level;
-    std::vector<long long> mono(c->N, 0);
+    std::vector<double> mono(c->N, 0.0);
     mono[c->N / 2] = 1;  // X^(N/2): slots times i
     pt_i = int_pt(mono, top_level, s);
     mono[c->N / 2] = -1;
@@ -687,7 +699,7 @@ struct Bootstrapper {
         const size_t m = std::min<size_t>(16, parts.size() - k);
         if (m > 1) {
           std::vector<boot::Ct> grp(parts.begin() + k, parts.begin() + k + m);
-          next.push_back(lincomb_many({grp}, std::vector<long long>(m, 1), 0.0, s)[0]);
+          next.push_back(lincomb_many({grp}, std::vector<double>(m, 1.0), 0.0, s)[0]);
         } else {
           next.push_back(parts[k]);
         }
@@ -796,7 +808,7 @@ struct Bootstrapper {
       if (!to_sparse || !to_dense) throw Error(-5, "bootstrap: encapsulation keys not set");
       x = keyswitch_add(x, to_sparse, s);  // dense -> sparse secret, at level 1
     }
-    if (prm.prescale_bits) x = mul_int(x, 1ll << prm.prescale_bits, s);
+    if (prm.prescale_bits) x = mul_int(x, (double)(1ll << prm.prescale_bits), s);
     boot::Ct a = fresh(top, in_scale, s);  // ModRaise: m -> m + q0 I on every limb of the top level
     op_mod_raise(c, x.c0, top, mut(a.c0), s);
     op_mod_raise(c, x.c1, top, mut(a.c1), s);
@@ -1004,6 +1016,19 @@ int fides_boot_table(const fides_boot* b, int which, int m, int* offsets, int ca
     ++k;
   }
   return k;
+}
+
+int fides_boot_plaintext(const fides_boot* b, int which, int m, int i, int j, uint64_t* out, void* stream) {
+  return bguard(__func__, [&] {
+    if (!b || !b->b || !b->b->prepared || !out) throw fides::Error(FIDES_ERR_STATE, "bootstrapper not prepared");
+    const auto& pl = which == 0 ? b->b->cts_pl : b->b->stc_pl;
+    if (m < 0 || m >= (int)pl.size()) throw fides::Error(FIDES_ERR_ARG, "matrix index out of range");
+    auto it = pl[m].pts.find({i, j});
+    if (it == pl[m].pts.end()) throw fides::Error(FIDES_ERR_ARG, "no diagonal at (i, j)");
+    FIDES_CUDA(cudaSetDevice(b->b->c->device));
+    FIDES_CUDA(cudaMemcpyAsync(out, it->second->u64(), sizeof(uint64_t) * (size_t)b->b->c->N * pl[m].level,
+                               cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  });
 }
 
 int fides_boot_matrices(const fides_boot* b, int which) {

@@ -639,6 +639,28 @@ int fides_rotate_hoisted(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, i
   });
 }
 
+int fides_rotate_hoisted_digits(fides_ctx* x, const uint64_t* c0, const uint64_t* digits, int level,
+                                const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                                uint64_t* const* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(c0, "c0");
+    need(digits, "digits");
+    need(keys, "keys");
+    need(rotations, "rotations");
+    need(out0, "out0");
+    need(out1, "out1");
+    if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
+    std::vector<uint32_t> ks(n);
+    for (int j = 0; j < n; ++j) {
+      need(out0[j], "out0[j]");
+      need(out1[j], "out1[j]");
+      ks[j] = fides::h_auto_index(c->logN, rotations[j]);
+    }
+    fides::op_hoisted_digits(c, c0, digits, level, keys, ks.data(), n, out0, out1, S(stream));
+  });
+}
+
 int fides_rotate_hoisted_batch(fides_ctx* x, const fides_hoist_item* items, int n_items, void* stream) {
   return guard([&] {
     auto* c = C(x);
@@ -720,7 +742,7 @@ int fides_key_upload(fides_ctx* x, const uint64_t* host_key, uint64_t** dev_key)
       cudaGetLastError();
       throw fides::Error(FIDES_ERR_OOM, std::string("key allocation failed: ") + cudaGetErrorString(e));
     }
-    e = cudaMemcpy(p, host_key, bytes, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(p, host_key, bytes, cudaMemcpyDefault);  // host or device source (unified addressing)
     if (e != cudaSuccess) {
       cudaFree(p);
       throw fides::Error(FIDES_ERR_CUDA, std::string("key upload failed: ") + cudaGetErrorString(e));

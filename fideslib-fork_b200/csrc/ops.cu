@@ -447,6 +447,39 @@ void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStrea
 
 void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) { op_hoisted_batch(c, &it, 1, s); }
 
+void op_hoisted_digits(Context* c, const uint64_t* c0, const uint64_t* digits, int l, const uint64_t* const* keys,
+                       const uint32_t* ks, int n, uint64_t* const* out0, uint64_t* const* out1, cudaStream_t s) {
+  // The second half of op_hoisted_batch for digits raised earlier (EvalFastRotationPrecompute):
+  // one KSK pass over the n rotations (they share the digit tile), adding P c0 and scattering by
+  // each automorphism, then one ModDown over the 2n outputs.  The own-digit limbs are read from
+  // the digits (op_modup writes them).
+  check_level(c, l);
+  if (n <= 0) return;
+  const size_t N = c->N;
+  const int ext = l + c->K;
+  Scratch sc(c, sizeof(uint64_t) * N * (size_t)n * (2 * ext + 2 * l), s);
+  Bump bp{sc.u64(), N};
+  std::vector<KskJob> kj;
+  std::vector<uint64_t*> ex, conv, outs;
+  std::vector<int> ls2;
+  for (int j = 0; j < n; ++j) {
+    if (!keys[j]) throw Error(-5, "null rotation key");
+    uint64_t* A = bp.take(ext);
+    uint64_t* B = bp.take(ext);
+    kj.push_back(KskJob{nullptr, nullptr, digits, keys[j], c0, A, B, l, ks[j]});
+    ex.push_back(B);
+    ex.push_back(A);
+    conv.push_back(bp.take(l));
+    conv.push_back(bp.take(l));
+    outs.push_back(out0[j]);
+    outs.push_back(out1[j]);
+    ls2.push_back(l);
+    ls2.push_back(l);
+  }
+  launch_ksk(c, kj.data(), (int)kj.size(), s);
+  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, (int)outs.size(), s);
+}
+
 void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s) {
   check_level(c, out_level);
   const size_t N = c->N;

@@ -71,6 +71,10 @@ void op_hoisted(Context* c, const HoistItem& item, cudaStream_t s);
 // Hoisted rotations of several ciphertexts (any levels, own rotation lists) in one launch
 // sequence per stage.
 void op_hoisted_batch(Context* c, const HoistItem* items, int n, cudaStream_t s);
+// Hoisted rotations from ModUp digits computed earlier (op_modup of c1, own-digit limbs included):
+// rotation j = automorphism ks[j] with key keys[j]; outputs [l][N] each.
+void op_hoisted_digits(Context* c, const uint64_t* c0, const uint64_t* digits, int l, const uint64_t* const* keys,
+                       const uint32_t* ks, int n, uint64_t* const* out0, uint64_t* const* out1, cudaStream_t s);
 // ModRaise (reference Bootstrap.cu ModRaise): a level-1 polynomial (limb q_0, EVAL) raised to
 // `out_level` limbs: INTT, SwitchModulus(q_0 -> q_j) of the centred residues, NTT.
 void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s);

@@ -133,6 +133,7 @@ def lib():
         L.fides_bootstrap_batch.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
         L.fides_boot_chebyshev.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
         L.fides_boot_matrices.argtypes = [vp, C.c_int]
+        L.fides_boot_plaintext.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
         L.fides_boot_table.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, vp]
         L.fides_ctx_inject_status.argtypes = [vp, C.c_uint32]
         L.fides_kernel_arch.argtypes = [C.c_int, C.POINTER(C.c_int)]
@@ -873,6 +874,12 @@ class NativeBootstrapper:
         buf = np.empty(n, dtype=np.float64)
         lib().fides_boot_chebyshev(self._h, buf.ctypes.data_as(C.POINTER(C.c_double)), n)
         return buf
+
+    def plaintext(self, which: str, m: int, i: int, j: int, level: int):
+        """The encoded diagonal (giant step i, baby step j) of matrix m, `level` limbs."""
+        out = self.ctx.empty(level)
+        _check(lib().fides_boot_plaintext(self._h, {"cts": 0, "stc": 1}[which], m, i, j, _ptr(out), _stream()))
+        return out
 
     def matrices(self, which: str) -> list:
         """The composed special-FFT matrices of 'cts' (CoeffsToSlots) or 'stc' (SlotsToCoeffs)

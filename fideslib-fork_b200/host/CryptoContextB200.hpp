@@ -1,0 +1,331 @@
+// The evaluation facade of the B200 CKKS core, shaped like the reference's
+// fideslib::CryptoContextImpl<DCRTPoly> (api/CryptoContext.hpp:306-458, bodies in
+// api/CryptoContext.cpp:1120-1299 over CudaEngine, api/engine/cuda/CudaEngine.cpp:429-1150):
+// EvalAdd / EvalSub (ciphertexts and real constants), EvalMult / EvalSquare, Rescale,
+// EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
+// EvalBootstrap, with the reference's level and scale management:
+//   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
+//     Rescale divides by the top prime and drops it; operands of an addition or a product are
+//     brought to the lower level by dropping limbs (Ciphertext::adjustBeforeMult,
+//     src/CKKS/Ciphertext.cpp:643-657);
+//   * FLEXIBLEAUTO: every level l has the canonical scale S_l of OpenFHE's FLEXIBLE chain,
+//     S_(l-1) = S_l^2 / q_(l-1) from the top scale, and operands are adjusted to a common level
+//     at its canonical scale before they meet (adjustScaleAndLevel, Ciphertext.cpp:1917-2068:
+//     a constant multiple that re-targets the scale, then a rescale).  EvalMult returns the
+//     product already rescaled (degree 1, level l - 1, scale S_(l-1)): the library fuses the
+//     rescale into the key switch's ModDown, so the product is never held at degree 2; OpenFHE
+//     holds it at degree 2 and rescales before the next product, which gives the same value one
+//     call later.  Rescale is therefore a copy under FLEXIBLEAUTO, as OpenFHE's is a no-op in its
+//     automatic modes.
+// OpenFHE types stay out of this header: keys and ciphertexts arrive as the raw formats of
+// FIDESlibB200.hpp (RawKeySwitchKey / RawCipherText) or as device arrays, and key generation and
+// encryption remain with the caller (OpenFHE in the reference's setting).
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "FIDESlibB200.hpp"
+
+namespace FIDESlib {
+namespace B200 {
+
+enum ScalingTechnique { FIXEDMANUAL = 0, FLEXIBLEAUTO = 1 };
+
+// The ModUp of a ciphertext's c1, kept for any number of EvalFastRotation calls (the
+// reference's EvalFastRotationPrecompute result).
+struct FastRotationPrecompute {
+  DeviceLimbs digits;  // [beta][level + K][N]
+  int level = 0;
+};
+
+class CryptoContextImpl {
+  Context* cc_;
+  ScalingTechnique tech_;
+  std::vector<double> S_;  // canonical scale of each level (FLEXIBLEAUTO)
+  fides_boot* boot_ = nullptr;
+  double boot_msg_scale_ = 0;
+  std::unique_ptr<KeySwitchingKey> to_sparse_, to_dense_;
+
+  int N() const { return cc_->N; }
+  uint64_t q(int i) const { return cc_->primes[i]; }
+
+  static double round_even(double v) { return std::nearbyint(v); }
+  // w mod q_i for an integer held exactly in a double (any magnitude)
+  uint64_t residue(double w, int i) const {
+    const uint64_t qi = q(i);
+    const bool neg = w < 0;
+    const double a = std::fabs(w);
+    uint64_t r;
+    if (a < 9223372036854775808.0) {
+      r = (uint64_t)a % qi;
+    } else {
+      int e = 0;
+      const double fr = std::frexp(a, &e);
+      const uint64_t m = (uint64_t)std::ldexp(fr, 53);
+      unsigned __int128 p = 1, b = 2 % qi;
+      for (uint64_t k = (uint64_t)(e - 53); k; k >>= 1, b = b * b % qi)
+        if (k & 1) p = p * b % qi;
+      r = (uint64_t)((unsigned __int128)(m % qi) * p % qi);
+    }
+    return neg && r ? qi - r : r;
+  }
+  std::vector<uint64_t> residues(double w, int level) const {
+    std::vector<uint64_t> v(level);
+    for (int i = 0; i < level; ++i) v[i] = residue(w, i);
+    return v;
+  }
+
+  Ciphertext fresh(int level, double scale, int degree, int slots) const {
+    Ciphertext c(*cc_);
+    c.alloc(level);
+    c.NoiseFactor = scale;
+    c.NoiseLevel = degree;
+    c.slots = slots;
+    return c;
+  }
+  static bool same_scale(double a, double b) { return std::abs(a / b - 1) < 1e-12; }
+
+  // a * k (an integer constant) on its first `level` limbs, then rescaled: level - 1 limbs at
+  // scale new_scale
+  Ciphertext mul_int_rescale(const Ciphertext& a, int level, double k, double new_scale) const {
+    const auto s = residues(k, level);
+    Ciphertext t = fresh(level, 0, 1, a.slots);
+    check(fides_mul_scalar(cc_->handle(), a.c0(), level, s.data(), t.c0(), cc_->stream()));
+    check(fides_mul_scalar(cc_->handle(), a.c1(), level, s.data(), t.c1(), cc_->stream()));
+    Ciphertext o = fresh(level - 1, new_scale, 1, a.slots);
+    check(fides_rescale(cc_->handle(), t.c0(), level, o.c0(), cc_->stream()));
+    check(fides_rescale(cc_->handle(), t.c1(), level, o.c1(), cc_->stream()));
+    cc_->synchronize();  // t is released at scope exit
+    return o;
+  }
+
+  Ciphertext copy_of(const Ciphertext& a, int level) const {
+    Ciphertext o = fresh(level, a.NoiseFactor, a.NoiseLevel, a.slots);
+    const size_t bytes = sizeof(uint64_t) * (size_t)N() * level;
+    check_cuda(cudaMemcpyAsync(o.c0(), a.c0(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+    check_cuda(cudaMemcpyAsync(o.c1(), a.c1(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+    return o;
+  }
+
+ public:
+  // top_scale: the scale of the top level (FLEXIBLEAUTO's S_(L+1); under FIXEDMANUAL only the
+  // default scale of EvalBootstrap's inputs).
+  CryptoContextImpl(Context& cc, ScalingTechnique tech, double top_scale) : cc_(&cc), tech_(tech) {
+    const int L = cc.L;
+    S_.assign(L + 1, 0.0);
+    S_[L] = top_scale;
+    for (int l = L; l > 1; --l) S_[l - 1] = S_[l] * S_[l] / (double)cc.primes[l - 1];
+  }
+  ~CryptoContextImpl() {
+    if (boot_) fides_boot_destroy(boot_);
+  }
+  CryptoContextImpl(const CryptoContextImpl&) = delete;
+  CryptoContextImpl& operator=(const CryptoContextImpl&) = delete;
+
+  ScalingTechnique GetScalingTechnique() const { return tech_; }
+  // the canonical scale of `level` limbs (OpenFHE's GetScalingFactorReal)
+  double GetScalingFactorReal(int level) const { return S_.at(level); }
+
+  // A ciphertext at `level` limbs with the canonical scale of that level (FLEXIBLEAUTO), or the
+  // same value on fewer limbs (FIXEDMANUAL, scale unchanged).
+  Ciphertext AdjustToLevel(const Ciphertext& a, int level) const {
+    if (level < 1 || level > a.getLevel()) throw Error(FIDES_ERR_LEVEL, "cannot raise a ciphertext's level");
+    if (a.NoiseLevel != 1) throw Error(FIDES_ERR_STATE, "adjust a degree-2 ciphertext after Rescale");
+    if (tech_ == FIXEDMANUAL || (a.getLevel() == level && same_scale(a.NoiseFactor, S_[level])))
+      return copy_of(a, level);
+    if (a.getLevel() == level)
+      throw Error(FIDES_ERR_LEVEL, "scale differs from the level's canonical scale and no level is left to adjust it");
+    const double k = round_even(S_[level] * (double)q(level) / a.NoiseFactor);
+    return mul_int_rescale(a, level + 1, k, S_[level]);
+  }
+
+  // ---- additive operations (CryptoContextImpl::EvalAdd / EvalSub)
+  Ciphertext EvalAdd(const Ciphertext& a, const Ciphertext& b) const { return add_sub(a, b, false); }
+  Ciphertext EvalSub(const Ciphertext& a, const Ciphertext& b) const { return add_sub(a, b, true); }
+  Ciphertext EvalAdd(const Ciphertext& a, double c) const { return add_const(a, c); }
+  Ciphertext EvalSub(const Ciphertext& a, double c) const { return add_const(a, -c); }
+
+  // ---- multiplicative operations (EvalMult, EvalSquare, Rescale)
+  Ciphertext EvalMult(const Ciphertext& a, const Ciphertext& b) const {
+    if (tech_ == FIXEDMANUAL) {
+      const int l = std::min(a.getLevel(), b.getLevel());
+      Ciphertext A = copy_of(a, l), B = copy_of(b, l);
+      Ciphertext o = fresh(l, a.NoiseFactor * b.NoiseFactor, a.NoiseLevel + b.NoiseLevel, a.slots);
+      check(fides_hmult(cc_->handle(), A.c0(), A.c1(), B.c0(), B.c1(), l, cc_->GetEvalKey().device(), 0, o.c0(),
+                        o.c1(), cc_->stream()));
+      cc_->synchronize();
+      return o;
+    }
+    const int l = std::min(a.getLevel(), b.getLevel());
+    if (l < 2) throw Error(FIDES_ERR_LEVEL, "no level left for the product's rescale");
+    Ciphertext A = AdjustToLevel(a, l), B = AdjustToLevel(b, l);
+    Ciphertext o = fresh(l - 1, S_[l - 1], 1, a.slots);
+    check(fides_hmult(cc_->handle(), A.c0(), A.c1(), B.c0(), B.c1(), l, cc_->GetEvalKey().device(), 1, o.c0(),
+                      o.c1(), cc_->stream()));
+    cc_->synchronize();
+    return o;
+  }
+  Ciphertext EvalSquare(const Ciphertext& a) const { return EvalMult(a, a); }
+  // Multiplication by a real constant: FLEXIBLEAUTO lands on level l - 1 at S_(l-1); FIXEDMANUAL
+  // multiplies by round(c q_(l-1)) and raises the degree (the next Rescale divides q_(l-1) out).
+  Ciphertext EvalMult(const Ciphertext& a, double c) const {
+    const int l = a.getLevel();
+    if (tech_ == FIXEDMANUAL) {
+      const double k = round_even(c * (double)q(l - 1));
+      const auto s = residues(k, l);
+      Ciphertext o = fresh(l, a.NoiseFactor * (double)q(l - 1), a.NoiseLevel + 1, a.slots);
+      check(fides_mul_scalar(cc_->handle(), a.c0(), l, s.data(), o.c0(), cc_->stream()));
+      check(fides_mul_scalar(cc_->handle(), a.c1(), l, s.data(), o.c1(), cc_->stream()));
+      return o;
+    }
+    if (l < 2) throw Error(FIDES_ERR_LEVEL, "no level left for the product's rescale");
+    const double k = round_even(c * S_[l - 1] * (double)q(l - 1) / a.NoiseFactor);
+    return mul_int_rescale(a, l, k, S_[l - 1]);
+  }
+  Ciphertext Rescale(const Ciphertext& a) const {
+    if (tech_ == FLEXIBLEAUTO) return copy_of(a, a.getLevel());
+    Ciphertext o = copy_of(a, a.getLevel());
+    o.rescale();
+    return o;
+  }
+
+  // ---- rotations (EvalRotate, EvalFastRotationPrecompute, EvalFastRotation)
+  Ciphertext EvalRotate(const Ciphertext& a, int index) const {
+    Ciphertext o = fresh(a.getLevel(), a.NoiseFactor, a.NoiseLevel, a.slots);
+    check(fides_rotate(cc_->handle(), a.c0(), a.c1(), a.getLevel(), cc_->GetRotationKey(index).device(), index,
+                       o.c0(), o.c1(), cc_->stream()));
+    return o;
+  }
+  std::shared_ptr<FastRotationPrecompute> EvalFastRotationPrecompute(const Ciphertext& a) const {
+    auto p = std::make_shared<FastRotationPrecompute>();
+    const int l = a.getLevel(), beta = (l + fides_ctx_alpha(cc_->handle()) - 1) / fides_ctx_alpha(cc_->handle());
+    p->level = l;
+    p->digits = DeviceLimbs((size_t)beta * (l + cc_->K) * N());
+    check(fides_modup(cc_->handle(), a.c1(), l, p->digits.get(), cc_->stream()));
+    return p;
+  }
+  // `m` (the cyclotomic order 2N) is accepted for signature parity with the reference.
+  Ciphertext EvalFastRotation(const Ciphertext& a, int index, uint32_t m,
+                              const std::shared_ptr<FastRotationPrecompute>& pre) const {
+    (void)m;
+    auto v = EvalFastRotation(a, std::vector<int>{index}, pre);
+    return std::move(v.at(0));
+  }
+  // Several indexes from one precomputation, in one launch sequence.
+  std::vector<Ciphertext> EvalFastRotation(const Ciphertext& a, const std::vector<int>& indexes,
+                                           const std::shared_ptr<FastRotationPrecompute>& pre) const {
+    if (!pre || pre->level != a.getLevel()) throw Error(FIDES_ERR_STATE, "precomputation of another level");
+    std::vector<Ciphertext> outs;
+    std::vector<const uint64_t*> keys;
+    std::vector<uint64_t*> o0, o1;
+    for (int r : indexes) {
+      outs.push_back(fresh(a.getLevel(), a.NoiseFactor, a.NoiseLevel, a.slots));
+      keys.push_back(cc_->GetRotationKey(r).device());
+    }
+    for (auto& o : outs) {
+      o0.push_back(o.c0());
+      o1.push_back(o.c1());
+    }
+    check(fides_rotate_hoisted_digits(cc_->handle(), a.c0(), pre->digits.get(), a.getLevel(), keys.data(),
+                                      indexes.data(), (int)indexes.size(), o0.data(), o1.data(), cc_->stream()));
+    return outs;
+  }
+
+  // ---- bootstrapping (EvalBootstrapSetup, EvalBootstrapKeyGen's key list, EvalBootstrap)
+  // levelBudget = {CoeffsToSlots levels, SlotsToCoeffs levels}; dim1 (BSGS baby steps; 0 = 8);
+  // numSlots must be N/2 (full packing) or 0; correctionFactor = the input prescale in bits (0 =
+  // none).  msgScale = the scale of the inputs' slots (0 = the canonical level-1 scale S_1).
+  void EvalBootstrapSetup(std::vector<uint32_t> levelBudget = {3, 3}, std::vector<uint32_t> dim1 = {0, 0},
+                          uint32_t numSlots = 0, uint32_t correctionFactor = 0, double msgScale = 0) {
+    if (numSlots != 0 && (int)numSlots != N() / 2)
+      throw Error(FIDES_ERR_ARG, "bootstrapping supports full packing (N/2 slots) only");
+    if (levelBudget.size() != 2) throw Error(FIDES_ERR_ARG, "levelBudget = {CoeffsToSlots, SlotsToCoeffs}");
+    if (boot_) fides_boot_destroy(boot_), boot_ = nullptr;
+    boot_msg_scale_ = msgScale > 0 ? msgScale : S_[1];
+    fides_boot_params p{(int)levelBudget[0], (int)levelBudget[1], cc_->L, S_[cc_->L], boot_msg_scale_, 12, 3, 63,
+                        dim1.empty() || dim1[0] == 0 ? 8 : (int)dim1[0], (int)correctionFactor,
+                        to_sparse_ && to_dense_ ? 1 : 0};
+    check(fides_boot_create(cc_->handle(), &p, &boot_));
+  }
+  // Rotation indexes whose keys EvalBootstrap needs (register them with Context::AddRotationKey,
+  // with the conjugation key 2N - 1 and the relinearisation key).
+  std::vector<int> GetBootstrapRotations() const {
+    if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
+    std::vector<int> r(fides_boot_rotations(boot_, nullptr, 0));
+    fides_boot_rotations(boot_, r.data(), (int)r.size());
+    return r;
+  }
+  // Sparse-secret encapsulation keys (dense -> sparse, sparse -> dense), set before
+  // EvalBootstrapSetup (the reference's keySwitchSparse, src/CKKS/Bootstrap.cu:257-290).
+  void SetSparseEncapsulationKeys(KeySwitchingKey&& to_sparse, KeySwitchingKey&& to_dense) {
+    to_sparse_ = std::make_unique<KeySwitchingKey>(std::move(to_sparse));
+    to_dense_ = std::make_unique<KeySwitchingKey>(std::move(to_dense));
+  }
+  // Binds the context's keys and encodes the linear transforms (once, after the keys are in).
+  void EvalBootstrapPrepare() {
+    if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
+    check(fides_boot_set_keys(boot_, cc_->GetEvalKey().device(), cc_->GetRotationKey(2 * N() - 1).device(),
+                              to_sparse_ ? to_sparse_->device() : nullptr, to_dense_ ? to_dense_->device() : nullptr));
+    for (int r : GetBootstrapRotations()) check(fides_boot_set_rotation_key(boot_, r, cc_->GetRotationKey(r).device()));
+    check(fides_boot_prepare(boot_, cc_->stream()));
+  }
+  // The input's limb q_0 is bootstrapped; its slots must be at the setup's msgScale.
+  Ciphertext EvalBootstrap(const Ciphertext& a) const {
+    if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
+    int lo = 0;
+    double sc = 0;
+    check(fides_boot_levels(boot_, &lo, &sc));
+    Ciphertext o = fresh(lo, sc, 1, a.slots);
+    check(fides_bootstrap(boot_, a.c0(), a.c1(), o.c0(), o.c1(), cc_->stream()));
+    cc_->synchronize();
+    return o;
+  }
+  // Several inputs bootstrapped concurrently (one stream each); results equal EvalBootstrap's.
+  std::vector<Ciphertext> EvalBootstrap(const std::vector<const Ciphertext*>& in) const {
+    if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
+    int lo = 0;
+    double sc = 0;
+    check(fides_boot_levels(boot_, &lo, &sc));
+    std::vector<Ciphertext> outs;
+    std::vector<const uint64_t *> c0, c1;
+    std::vector<uint64_t *> o0, o1;
+    for (const Ciphertext* a : in) {
+      outs.push_back(fresh(lo, sc, 1, a->slots));
+      c0.push_back(a->c0());
+      c1.push_back(a->c1());
+    }
+    for (auto& o : outs) {
+      o0.push_back(o.c0());
+      o1.push_back(o.c1());
+    }
+    check(fides_bootstrap_batch(boot_, (int)in.size(), c0.data(), c1.data(), o0.data(), o1.data(), cc_->stream()));
+    cc_->synchronize();
+    return outs;
+  }
+
+ private:
+  Ciphertext add_sub(const Ciphertext& a, const Ciphertext& b, bool sub) const {
+    const int l = std::min(a.getLevel(), b.getLevel());
+    Ciphertext A = AdjustToLevel(a, l), B = AdjustToLevel(b, l);
+    if (tech_ == FIXEDMANUAL && (A.NoiseLevel != B.NoiseLevel || !same_scale(A.NoiseFactor, B.NoiseFactor)))
+      throw Error(FIDES_ERR_STATE, "operands at different scales (rescale first)");
+    Ciphertext o = fresh(l, A.NoiseFactor, A.NoiseLevel, a.slots);
+    auto f = sub ? fides_sub : fides_add;
+    check(f(cc_->handle(), A.c0(), B.c0(), l, o.c0(), cc_->stream()));
+    check(f(cc_->handle(), A.c1(), B.c1(), l, o.c1(), cc_->stream()));
+    cc_->synchronize();
+    return o;
+  }
+  Ciphertext add_const(const Ciphertext& a, double c) const {
+    const int l = a.getLevel();
+    const auto s = residues(round_even(c * a.NoiseFactor), l);
+    Ciphertext o = copy_of(a, l);
+    check(fides_add_scalar(cc_->handle(), a.c0(), l, s.data(), o.c0(), cc_->stream()));
+    return o;
+  }
+};
+
+}  // namespace B200
+}  // namespace FIDESlib

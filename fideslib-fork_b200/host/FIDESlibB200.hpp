@@ -90,6 +90,7 @@ class DeviceLimbs {
 };
 
 class Context;
+class CryptoContextImpl;
 
 class KeySwitchingKey {
   Context* cc_;
@@ -107,7 +108,8 @@ class KeySwitchingKey {
   ~KeySwitchingKey();
   // reference KeySwitchingKey::Initialize (KeySwitchingKey.cu:19-35)
   void Initialize(const RawKeySwitchKey& rkk);
-  // Flat host array [2][dnum][n_q + K][N].
+  // Flat array [2][dnum][n_q + K][N] in host memory or in device memory on the context's GPU
+  // (copied either way).
   void InitializeFlat(const uint64_t* host);
   const uint64_t* device() const { return dev_; }
 };
@@ -150,9 +152,12 @@ class Context {
     if (!eval_) throw Error(FIDES_ERR_KEY, "no relinearization key");
     return *eval_;
   }
+  // index 2N - 1 is the conjugation key (automorphism 2N - 1); other indexes are slot rotations
   void AddRotationKey(int index, KeySwitchingKey&& k) {
-    index %= N / 2;
-    if (index < 0) index += N / 2;
+    if (index != 2 * N - 1) {
+      index %= N / 2;
+      if (index < 0) index += N / 2;
+    }
     rot_.erase(index);
     rot_.emplace(index, std::move(k));
   }
@@ -196,6 +201,7 @@ inline void KeySwitchingKey::Initialize(const RawKeySwitchKey& rkk) {
 }
 
 class Ciphertext {
+  friend class CryptoContextImpl;
   Context* cc_;
   DeviceLimbs c0_, c1_;
   int level_ = 0;

@@ -1,0 +1,154 @@
+// Test driver of the C++ evaluation facade (CryptoContextB200.hpp), loaded by the GPU test suite
+// (tests/test_bootstrap.py) as a shared library: it builds its own Context from the primes,
+// imports the evaluation keys from device arrays (KeySwitchingKey::InitializeFlat), loads host
+// ciphertexts through RawCipherText, runs the facade's calls and stores every result back to
+// host arrays for the suite to compare with the oracle, the Python driver and the C ABI.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "CryptoContextB200.hpp"
+
+using namespace FIDESlib::B200;
+
+namespace {
+RawCipherText raw_of(const uint64_t* c0, const uint64_t* c1, int l, int N, double scale) {
+  RawCipherText r;
+  r.N = N;
+  r.numRes = l;
+  r.Noise = scale;
+  r.NoiseLevel = 1;
+  for (int i = 0; i < l; ++i) {
+    r.sub_0.emplace_back(c0 + (size_t)i * N, c0 + (size_t)(i + 1) * N);
+    r.sub_1.emplace_back(c1 + (size_t)i * N, c1 + (size_t)(i + 1) * N);
+  }
+  return r;
+}
+void put(const Ciphertext& ct, uint64_t*& out) {
+  RawCipherText r;
+  ct.store(r);
+  for (auto& v : r.sub_0) out = std::copy(v.begin(), v.end(), out);
+  for (auto& v : r.sub_1) out = std::copy(v.begin(), v.end(), out);
+}
+KeySwitchingKey key_from(Context& cc, const uint64_t* dev) {
+  KeySwitchingKey k(cc);
+  k.InitializeFlat(dev);
+  return k;
+}
+}  // namespace
+
+extern "C" {
+
+// The facade's bootstrap of n_boot level-1 ciphertexts (host arrays, one limb each): singly
+// (EvalBootstrap) into boot_out0/1 and as one batch (the vector form) into batch_out0/1, each
+// output of *out_level limbs.  Keys are device arrays of the caller's context; rots lists the
+// rotation keys given (every rotation GetBootstrapRotations names must be among them).
+int facade_bootstrap(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale,
+                     const uint64_t* relin, const uint64_t* conj, int n_rot, const int* rots,
+                     const uint64_t* const* rot_keys, const uint64_t* to_sparse, const uint64_t* to_dense,
+                     double msg_scale, int prescale_bits, int n_boot, const uint64_t* const* c0s,
+                     const uint64_t* const* c1s, uint64_t* const* out0, uint64_t* const* out1, uint64_t* const* bo0,
+                     uint64_t* const* bo1, int* out_level, double* out_scale, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    cc.AddEvalKey(key_from(cc, relin));
+    cc.AddRotationKey(2 * N - 1, key_from(cc, conj));
+    for (int i = 0; i < n_rot; ++i) cc.AddRotationKey(rots[i], key_from(cc, rot_keys[i]));
+    {
+      CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+      if (to_sparse && to_dense) ev.SetSparseEncapsulationKeys(key_from(cc, to_sparse), key_from(cc, to_dense));
+      ev.EvalBootstrapSetup({3, 3}, {0, 0}, (uint32_t)(N / 2), (uint32_t)prescale_bits, msg_scale);
+      ev.EvalBootstrapPrepare();
+      std::vector<Ciphertext> in;
+      for (int i = 0; i < n_boot; ++i) in.emplace_back(cc, raw_of(c0s[i], c1s[i], 1, N, msg_scale));
+      std::vector<const Ciphertext*> ptrs;
+      for (auto& c : in) ptrs.push_back(&c);
+      auto batch = ev.EvalBootstrap(ptrs);
+      for (int i = 0; i < n_boot; ++i) {
+        Ciphertext o = ev.EvalBootstrap(in[i]);
+        *out_level = o.getLevel();
+        *out_scale = o.NoiseFactor;
+        uint64_t* w = out0[i];
+        RawCipherText r;
+        o.store(r);
+        for (auto& v : r.sub_0) w = std::copy(v.begin(), v.end(), w);
+        w = out1[i];
+        for (auto& v : r.sub_1) w = std::copy(v.begin(), v.end(), w);
+        RawCipherText rb;
+        batch[i].store(rb);
+        w = bo0[i];
+        for (auto& v : rb.sub_0) w = std::copy(v.begin(), v.end(), w);
+        w = bo1[i];
+        for (auto& v : rb.sub_1) w = std::copy(v.begin(), v.end(), w);
+      }
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
+// The facade's arithmetic on a and b (host, level l, scale S_l of a FLEXIBLEAUTO chain from
+// top_scale), results packed into out in this order:
+//   EvalMult(a, b) [l-1] | EvalRotate(a, rot) [l] | EvalFastRotation(a, rot) from
+//   EvalFastRotationPrecompute(a) [l] | EvalAdd(a, b) [l] | EvalSub(a, b) [l] |
+//   EvalAdd(a, 0.25) [l] | EvalMult(a, 0.5) [l-1] | EvalSquare(a) [l-1] |
+//   EvalMult(EvalMult(a, b), a) [l-2] (operands at different levels, adjusted)
+// each as c0 limbs then c1 limbs.  And under FIXEDMANUAL (out_manual):
+//   EvalMult(a, b) [l] (degree 2, not rescaled) | Rescale of it [l-1]
+int facade_arith(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, const uint64_t* relin,
+                 int rot, const uint64_t* rot_key, int l, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
+                 const uint64_t* b1, uint64_t* out, uint64_t* out_manual, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    cc.AddEvalKey(key_from(cc, relin));
+    cc.AddRotationKey(rot, key_from(cc, rot_key));
+    {
+      CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+      const double S = ev.GetScalingFactorReal(l);
+      Ciphertext A(cc, raw_of(a0, a1, l, N, S)), B(cc, raw_of(b0, b1, l, N, S));
+      uint64_t* w = out;
+      Ciphertext M = ev.EvalMult(A, B);
+      put(M, w);
+      put(ev.EvalRotate(A, rot), w);
+      auto pre = ev.EvalFastRotationPrecompute(A);
+      put(ev.EvalFastRotation(A, rot, 2 * N, pre), w);
+      put(ev.EvalAdd(A, B), w);
+      put(ev.EvalSub(A, B), w);
+      put(ev.EvalAdd(A, 0.25), w);
+      put(ev.EvalMult(A, 0.5), w);
+      put(ev.EvalSquare(A), w);
+      put(ev.EvalMult(M, A), w);
+    }
+    {
+      CryptoContextImpl man(cc, FIXEDMANUAL, top_scale);
+      Ciphertext A(cc, raw_of(a0, a1, l, N, 1.0)), B(cc, raw_of(b0, b1, l, N, 1.0));
+      uint64_t* w = out_manual;
+      Ciphertext M = man.EvalMult(A, B);
+      if (M.NoiseLevel != 2 || M.getLevel() != l) throw Error(FIDES_ERR_STATE, "FIXEDMANUAL product metadata");
+      put(M, w);
+      Ciphertext R = man.Rescale(M);
+      if (R.NoiseLevel != 1 || R.getLevel() != l - 1) throw Error(FIDES_ERR_STATE, "FIXEDMANUAL rescale metadata");
+      put(R, w);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
+}  // extern "C"

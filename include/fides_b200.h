@@ -229,6 +229,13 @@ int fides_rotate_auto(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, in
 int fides_rotate_hoisted(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                          const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
                          uint64_t* const* out1, void* stream);
+/* Hoisted rotations from a ModUp computed earlier: digits = fides_modup(c1) ([beta][level+K][N]),
+ * reused for any number of calls.  The reference's EvalFastRotationPrecompute (the ModUp) and
+ * EvalFastRotation (KSK with P c0, automorphism, ModDown), CudaEngine.cpp:536-585 over
+ * hoistedRotateDotKSK_2_ (ElemenwiseBatchKernels.cu:277-377).  Results equal fides_rotate. */
+int fides_rotate_hoisted_digits(fides_ctx* ctx, const uint64_t* c0, const uint64_t* digits, int level,
+                                const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                                uint64_t* const* out1, void* stream);
 /* Hoisted rotations of a batch of ciphertexts at any levels, each with its own rotation
  * list: one ModUp launch sequence over all c1, one KSK pass over every (ciphertext,
  * rotation) pair, one ModDown over every output.  Replaces fusedHoistedRotateBatch /
@@ -337,7 +344,8 @@ int fides_server_get_stats(fides_server* s, fides_server_stats* out);
 int fides_server_destroy(fides_server* s);
 
 /* ---- host-buffer entry points (end-to-end path) ------------------------------------- */
-/* Upload a key from host memory into a new device buffer owned by the context. */
+/* Upload a key ([2][dnum][n_q + K][N]) into a new device buffer owned by the context; host_key
+ * may be host memory or another device buffer on the same GPU (copied either way). */
 int fides_key_upload(fides_ctx* ctx, const uint64_t* host_key, uint64_t** dev_key);
 /* Interop with the reference's raw host formats (src/CKKS/openfhe-interface/RawCiphertext.cuh:
  * RawCipherText :20-37, RawKeySwitchKey :90-95), replacing Ciphertext::load / store
@@ -452,6 +460,9 @@ int fides_bootstrap_batch(fides_boot* b, int n, const uint64_t* const* c0s, cons
 int fides_boot_chebyshev(const fides_boot* b, double* coeffs, int cap);
 int fides_boot_matrices(const fides_boot* b, int which);
 int fides_boot_table(const fides_boot* b, int which, int m, int* offsets, int cap, double* diags);
+/* After fides_boot_prepare: copies the encoded diagonal (i, j) (giant step i, baby step j) of
+ * matrix m into out (the matrix's level limbs, EVALUATION form). */
+int fides_boot_plaintext(const fides_boot* b, int which, int m, int i, int j, uint64_t* out, void* stream);
 
 /* ---- allocation-free entry point ----------------------------------------------------
  * No counterpart in the reference.  fides_rescale_noalloc computes exactly what

@@ -395,10 +395,20 @@ def test_native_bootstrap_equals_python_driver_n4096(fides):
         c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
         zs.append(z)
         cts.append(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    # same encoded diagonals
+    for which, plans in (("cts", bs.cts_pts), ("stc", bs.stc_pts)):
+        for m, P in enumerate(plans):
+            for (i, j), pt in P["pts"].items():
+                assert torch.equal(nb.plaintext(which, m, i, j, P["level"]), pt), f"{which} {m} ({i}, {j})"
     py = bs.bootstrap(B.Ct(cts[0].c0, cts[0].c1, delta))
     nat = nb.bootstrap(cts[0])
     batch = nb.bootstrap_batch(cts)
     torch.cuda.synchronize()
+    bits_py = -math.log2(np.abs(decode(kg.decrypt_limb0(F.to_host(py.c0), F.to_host(py.c1)), prm.N, py.scale)
+                                - zs[0]).max())
+    bits_nat = -math.log2(np.abs(decode(kg.decrypt_limb0(F.to_host(nat.c0), F.to_host(nat.c1)), prm.N, nb.out_scale)
+                                 - zs[0]).max())
+    print(f"N=2^12 bootstrap: Python driver {bits_py:.2f} bits, C++ driver {bits_nat:.2f} bits")
     assert torch.equal(py.c0, nat.c0) and torch.equal(py.c1, nat.c1)
     for i, (ct, out) in enumerate(zip(cts, batch)):
         single = nat if i == 0 else nb.bootstrap(ct)
@@ -443,4 +453,161 @@ def test_native_bootstrap_config_d_n65536(fides, config_d):
     py = bs.bootstrap(B.Ct(cts[0].c0, cts[0].c1, delta))
     torch.cuda.synchronize()
     assert torch.equal(py.c0, single.c0) and torch.equal(py.c1, single.c1)
+    # the C++ facade (EvalBootstrap, single and vector forms) on two of the inputs
+    host = [(F.to_host(c.c0), F.to_host(c.c1)) for c in cts[:2]]
+    fs, fb, L, _ = facade_bootstrap(F, prm, ev, bs, host, encaps=bs.encapsulation)
+    assert L == nb.out_level
+    for i in range(2):
+        for got in (fs[i], fb[i]):
+            assert np.array_equal(got[0], F.to_host(batch[i].c0)) and np.array_equal(got[1], F.to_host(batch[i].c1))
     nb.close()
+
+
+# ---------------------------------------------------------------- the C++ evaluation facade
+def _facade_lib():
+    import ctypes as C
+    import os
+    from conftest import ROOT
+    lib = C.CDLL(os.path.join(ROOT, "fideslib-fork_b200", "libfacade_test.so"))
+    vp, u64p, dp, ip = C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_int)
+    vpp = C.POINTER(vp)
+    lib.facade_bootstrap.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, vp, C.c_int, ip, vpp,
+                                     vp, vp, C.c_double, C.c_int, C.c_int, vpp, vpp, vpp, vpp, vpp, vpp, ip, dp,
+                                     C.c_char_p, C.c_int]
+    lib.facade_arith.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, C.c_int, vp, C.c_int,
+                                 u64p, u64p, u64p, u64p, u64p, u64p, C.c_char_p, C.c_int]
+    return lib
+
+
+def facade_bootstrap(F, prm, ev, bs, cts_host, encaps=None):
+    """Runs the facade's EvalBootstrap (single and batch) on host level-1 ciphertexts; returns
+    (singles, batch, out_level, out_scale) as host arrays."""
+    import ctypes as C
+    lib = _facade_lib()
+    vp = C.c_void_p
+    rots = sorted(ev.rot_keys)
+    N, nb_ = prm.N, len(cts_host)
+    # the facade reports its output level after the first bootstrap; the output arrays are sized
+    # for the top level and trimmed afterwards
+    outs = [[np.zeros((prm.n_q, N), dtype=np.uint64) for _ in range(2)] for _ in range(2 * nb_)]
+    ins = [np.ascontiguousarray(c, dtype=np.uint64) for ct in cts_host for c in ct]
+    arr = lambda xs: (vp * len(xs))(*[x.ctypes.data for x in xs])
+    lvl, sc = C.c_int(), C.c_double()
+    err = C.create_string_buffer(512)
+    primes = np.array(prm.q + prm.p, dtype=np.uint64)
+    rc = lib.facade_bootstrap(prm.logN, prm.n_q, prm.K, prm.dnum, primes.ctypes.data_as(C.POINTER(C.c_uint64)),
+                              ev.S[prm.n_q], ev.rk.data_ptr(), ev.conj_key.data_ptr(), len(rots),
+                              (C.c_int * len(rots))(*rots), (vp * len(rots))(*[ev.rot_keys[r].data_ptr() for r in rots]),
+                              encaps[0].data_ptr() if encaps else None, encaps[1].data_ptr() if encaps else None,
+                              2.0 ** 50, bs.prescale.bit_length() - 1, nb_, arr(ins[0::2]), arr(ins[1::2]),
+                              arr([o[0] for o in outs[:nb_]]), arr([o[1] for o in outs[:nb_]]),
+                              arr([o[0] for o in outs[nb_:]]), arr([o[1] for o in outs[nb_:]]), C.byref(lvl),
+                              C.byref(sc), err, 512)
+    assert rc == 0, err.value.decode()
+    L = lvl.value
+    singles = [(o[0][:L], o[1][:L]) for o in outs[:nb_]]
+    batch = [(o[0][:L], o[1][:L]) for o in outs[nb_:]]
+    return singles, batch, L, sc.value
+
+
+@pytest.mark.gpu
+def test_cpp_facade_bootstrap_n4096(fides):
+    """The C++ facade (CryptoContextImpl::EvalBootstrapSetup / EvalBootstrap, single and vector
+    forms) at N = 2^12, through a compiled driver: bit-identical to the ABI bootstrapper and to
+    the Python driver on the same tables, > 12 bits against the FP64 plaintext."""
+    import torch
+    from fides_b200 import bootstrap as B
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    delta = 2.0 ** 50
+    rng = xrng(68)
+    n = prm.N // 2
+    zs, cts = [], []
+    for _ in range(2):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        zs.append(z)
+        cts.append(kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1))
+    singles, batch, L, scale = facade_bootstrap(F, prm, ev, bs, cts)
+    nb = native_for(F, prm, ev, bs)
+    nb.prepare()
+    bs.top = prm.n_q
+    python_with_native_tables(bs, nb)
+    assert L == nb.out_level
+    for i, (c, z) in enumerate(zip(cts, zs)):
+        ct = F.Ciphertext(F.to_device(c[0]), F.to_device(c[1]))
+        nat = nb.bootstrap(ct)
+        py = bs.bootstrap(B.Ct(ct.c0, ct.c1, delta))
+        torch.cuda.synchronize()
+        for got in (singles[i], batch[i]):
+            assert np.array_equal(got[0], F.to_host(nat.c0)) and np.array_equal(got[1], F.to_host(nat.c1))
+            assert np.array_equal(got[0], F.to_host(py.c0)) and np.array_equal(got[1], F.to_host(py.c1))
+        bits = -math.log2(np.abs(decode(kg.decrypt_limb0(*singles[i]), prm.N, scale) - z).max())
+        assert bits > 12
+    nb.close()
+
+
+@pytest.mark.gpu
+def test_cpp_facade_arithmetic(fides):
+    """The C++ facade's EvalMult / EvalSquare / EvalRotate / EvalFastRotation(Precompute) /
+    EvalAdd / EvalSub and constant forms under FLEXIBLEAUTO (operands adjusted to a common level
+    at its canonical scale S_l, S_(l-1) = S_l^2 / q_(l-1)), and EvalMult + Rescale under
+    FIXEDMANUAL, residue for residue against the oracle."""
+    import ctypes as C
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 50, 8, 2, name="facade")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=69)
+    rk, rot = kg.relin_key(), 5
+    kr = kg.rotation_key(rot)
+    rk_d, kr_d = F.to_device(rk), F.to_device(kr)
+    N, l, q = prm.N, prm.n_q, prm.q
+    S = [0.0] * (l + 1)
+    S[l] = 2.0 ** 45
+    for k in range(l, 1, -1):
+        S[k - 1] = S[k] * S[k] / q[k - 1]
+    rng = xrng(70)
+    a = [uniform_limbs(rng, q, N) for _ in range(2)]
+    b = [uniform_limbs(rng, q, N) for _ in range(2)]
+    sizes = [l - 1, l, l, l, l, l, l - 1, l - 1, l - 2]
+    out = np.zeros(2 * sum(sizes) * N, dtype=np.uint64)
+    out_m = np.zeros(2 * (2 * l - 1) * N, dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    u64 = lambda x: np.ascontiguousarray(x, dtype=np.uint64).ctypes.data_as(C.POINTER(C.c_uint64))
+    primes = np.array(q + prm.p, dtype=np.uint64)
+    rc = _facade_lib().facade_arith(prm.logN, l, prm.K, prm.dnum, u64(primes), S[l], rk_d.data_ptr(), rot,
+                                    kr_d.data_ptr(), l, u64(a[0]), u64(a[1]), u64(b[0]), u64(b[1]), u64(out),
+                                    u64(out_m), err, 512)
+    assert rc == 0, err.value.decode()
+    got, pos = [], 0
+    for s_ in sizes:
+        c0 = out[pos:pos + s_ * N].reshape(s_, N)
+        c1 = out[pos + s_ * N:pos + 2 * s_ * N].reshape(s_, N)
+        got.append((c0, c1))
+        pos += 2 * s_ * N
+    ids = lambda k: list(range(k))
+    const = lambda v, k: np.array([[int(v) % q[i]] * N for i in range(k)], dtype=np.uint64)
+    mult = o.hmult(a[0], a[1], b[0], b[1], rk, rescale=True)
+    kh = round(0.5 * S[l - 1] * q[l - 1] / S[l])
+    kadj = round(S[l - 1] * q[l - 1] / S[l])
+    adj = [o.rescale(o.mul(a[i], const(kadj, l), ids(l))) for i in range(2)]
+    want = [mult,
+            o.rotate(a[0], a[1], kr, rot),
+            o.rotate(a[0], a[1], kr, rot),
+            (o.add(a[0], b[0], ids(l)), o.add(a[1], b[1], ids(l))),
+            (o.sub(a[0], b[0], ids(l)), o.sub(a[1], b[1], ids(l))),
+            (o.add(a[0], const(round(0.25 * S[l]), l), ids(l)), a[1]),
+            tuple(o.rescale(o.mul(a[i], const(kh, l), ids(l))) for i in range(2)),
+            o.hmult(a[0], a[1], a[0], a[1], rk, rescale=True),
+            o.hmult(mult[0], mult[1], adj[0], adj[1], rk, rescale=True)]
+    names = ["EvalMult", "EvalRotate", "EvalFastRotation", "EvalAdd", "EvalSub", "EvalAdd(const)",
+             "EvalMult(const)", "EvalSquare", "EvalMult(level-adjusted)"]
+    for name, (g0, g1), (w0, w1) in zip(names, got, want):
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name
+    m0 = out_m[:l * N].reshape(l, N)
+    m1 = out_m[l * N:2 * l * N].reshape(l, N)
+    r0 = out_m[2 * l * N:(3 * l - 1) * N].reshape(l - 1, N)
+    r1 = out_m[(3 * l - 1) * N:].reshape(l - 1, N)
+    w0, w1 = o.hmult(a[0], a[1], b[0], b[1], rk, rescale=False)
+    assert np.array_equal(m0, w0) and np.array_equal(m1, w1), "FIXEDMANUAL EvalMult"
+    assert np.array_equal(r0, o.rescale(w0)) and np.array_equal(r1, o.rescale(w1)), "FIXEDMANUAL Rescale"

@@ -581,12 +581,14 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     auto same_digits = [](const KskJob& a, const KskJob& b) {
       return a.digits == b.digits && a.x == b.x && a.x2 == b.x2 && a.l == b.l && !a.a0 == !b.a0 && !a.c0 == !b.c0;
     };
-    auto group = [&](auto same) {
+    // groups sharing a key take up to 8 jobs; groups sharing a digit tile at most 4 (the
+    // shared-digit form with 8 jobs spills heavily at three digits)
+    auto group = [&](auto same, int cap) {
       L.ngroups = 0;
       int gm = 1;
       for (int i = 0; i < m;) {
         int k = 1;
-        while (i + k < m && k < MAX_KSK_GROUP && same(L.j[i], L.j[i + k])) ++k;
+        while (i + k < m && k < cap && same(L.j[i], L.j[i + k])) ++k;
         L.gstart[L.ngroups] = (uint8_t)i;
         L.gcount[L.ngroups] = (uint8_t)k;
         ++L.ngroups;
@@ -595,16 +597,16 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
       }
       return gm;
     };
-    int gmax = group(same_key);
+    int gmax = group(same_key, MAX_KSK_GROUP);
     bool share_digits = false;
     if (gmax == 1) {
-      gmax = group(same_digits);
+      gmax = group(same_digits, 4);
       share_digits = gmax > 1;
-      if (!share_digits) group(same_key);
+      if (!share_digits) group(same_key, MAX_KSK_GROUP);
     }
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
-    const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : 4;
+    const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : gmax <= 4 ? 4 : 8;
     dim3 grid(c->N / (2 * EW_THREADS), mx, L.ngroups);
     // algorithmic bytes: each job's digits, outputs and extra operands, and each group's key once
     double bytes = 0;
@@ -623,18 +625,23 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     LaunchScope ls(c, s, KK_KSK, bytes);
     auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->d_f64, c->logN, c->n_q,
                                                               c->K, c->dnum, c->alpha); };
-    switch (maxb * 8 + jg + (share_digits ? 64 : 0)) {
+    switch (maxb * 16 + jg + (share_digits ? 128 : 0)) {
 #define FIDES_KSK_CASE(B, G)                    \
-  case B * 8 + G:                               \
+  case B * 16 + G:                              \
     go(ksk_kernel<B, G, 2>);                    \
     break;                                      \
-  case 64 + B * 8 + G:                          \
+  case 128 + B * 16 + G:                        \
     go(ksk_kernel<B, G, 2, true>);              \
     break;
-      FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4)
-      FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4)
-      FIDES_KSK_CASE(3, 1) FIDES_KSK_CASE(3, 2) FIDES_KSK_CASE(3, 4)
-      FIDES_KSK_CASE(4, 1) FIDES_KSK_CASE(4, 2) FIDES_KSK_CASE(4, 4)
+#define FIDES_KSK_CASE8(B)                      \
+  case B * 16 + 8:                              \
+    go(ksk_kernel<B, 8, 2>);                    \
+    break;
+      FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4) FIDES_KSK_CASE8(1)
+      FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4) FIDES_KSK_CASE8(2)
+      FIDES_KSK_CASE(3, 1) FIDES_KSK_CASE(3, 2) FIDES_KSK_CASE(3, 4) FIDES_KSK_CASE8(3)
+      FIDES_KSK_CASE(4, 1) FIDES_KSK_CASE(4, 2) FIDES_KSK_CASE(4, 4) FIDES_KSK_CASE8(4)
+#undef FIDES_KSK_CASE8
 #undef FIDES_KSK_CASE
       default:
         go(ksk_kernel<0, 1, 2>);

@@ -48,9 +48,9 @@ struct KskJob {
 };
 constexpr int MAX_KSK_JOBS = 64;
 // Jobs that share a switching key (one relinearisation or rotation key for a batch) and the
-// same level and extras form a group of up to 4; one CTA runs a whole group, reading each key
-// tile once for all of its jobs.
-constexpr int MAX_KSK_GROUP = 4;
+// same level and extras form a group of up to 8; one CTA runs a whole group, reading each key
+// tile once for all of its jobs (a batch of 8 reads the key once).
+constexpr int MAX_KSK_GROUP = 8;
 struct KskJobList {
   int n, max_ext, ngroups, pad1;
   uint8_t gstart[MAX_KSK_JOBS], gcount[MAX_KSK_JOBS];

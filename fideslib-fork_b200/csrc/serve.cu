@@ -61,10 +61,11 @@ struct Server {
   std::vector<cudaStream_t> streams;
   struct BootEngine {
     cudaGraphExec_t exec;
-    const uint64_t *in0, *in1, *out0, *out1;
+    std::vector<const uint64_t*> in0, in1, out0, out1;  // one static slot per ciphertext it holds
     int in_level, out_level;
     cudaStream_t stream;
     bool busy;
+    int capacity() const { return (int)in0.size(); }
   };
   std::deque<BootEngine> boot;  // a deque: registering an engine keeps references to the others valid
   std::vector<bool> busy;
@@ -77,6 +78,11 @@ struct Server {
   uint64_t next_ticket = 1;
   size_t in_use = 0;
   bool stop = false;
+  // batches of one operation type allowed on the device at once (0 = up to n_streams): with 1,
+  // requests that arrive while their type's batch runs wait for it and form the next, larger
+  // batch (continuous batching under load), while a type with nothing in flight still starts at once
+  int max_inflight_per_op = 0;
+  std::map<int, int> inflight;  // op -> batches on the device
   fides_server_stats st{};
   std::thread worker;
 
@@ -102,6 +108,7 @@ struct Server {
     std::vector<Clock::time_point> arrivals;
     size_t bytes;
     int status;
+    int op = -1;
   };
 
   static void CUDART_CB on_done(void* p) {
@@ -118,10 +125,12 @@ struct Server {
         s->st.completed++;
       }
       s->in_use -= b->bytes;
-      if (b->stream >= 0)
+      if (b->stream >= 0) {
         s->busy[b->stream] = false;
-      else
+        if (b->op >= 0) s->inflight[b->op]--;
+      } else {
         s->boot[-1 - b->stream].busy = false;
+      }
     }
     s->cv.notify_all();
     s->done_cv.notify_all();
@@ -136,20 +145,30 @@ struct Server {
     st.rejected++;
   }
 
-  // Copy in, graph launch, copy out on the engine's stream, then the completion callback.
-  void launch_bootstrap(BootEngine& e, int index, const Pending& p) {
-    auto* b = new Batch{this, -1 - index, {p.ticket}, {p.arrival}, 0, FIDES_OK};
+  // Copy in, graph launch, copy out on the engine's stream, then the completion callback.  An
+  // engine that holds several ciphertexts takes up to that many requests at once; slots left
+  // empty keep their previous (ignored) contents.
+  void launch_bootstrap(BootEngine& e, int index, const std::vector<Pending>& ps) {
+    auto* b = new Batch{this, -1 - index, {}, {}, 0, FIDES_OK};
+    for (const auto& p : ps) {
+      b->tickets.push_back(p.ticket);
+      b->arrivals.push_back(p.arrival);
+    }
     const size_t lb = c->limb_bytes();
     cudaError_t err = cudaSetDevice(c->device);
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in0), p.r.c0, lb * e.in_level, cudaMemcpyDeviceToDevice, e.stream);
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in1), p.r.c1, lb * e.in_level, cudaMemcpyDeviceToDevice, e.stream);
+    for (size_t k = 0; k < ps.size() && err == cudaSuccess; ++k) {
+      err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in0[k]), ps[k].r.c0, lb * e.in_level, cudaMemcpyDeviceToDevice,
+                            e.stream);
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(const_cast<uint64_t*>(e.in1[k]), ps[k].r.c1, lb * e.in_level,
+                              cudaMemcpyDeviceToDevice, e.stream);
+    }
     if (err == cudaSuccess) err = cudaGraphLaunch(e.exec, e.stream);
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(p.r.out0, e.out0, lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(p.r.out1, e.out1, lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
+    for (size_t k = 0; k < ps.size() && err == cudaSuccess; ++k) {
+      err = cudaMemcpyAsync(ps[k].r.out0, e.out0[k], lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(ps[k].r.out1, e.out1[k], lb * e.out_level, cudaMemcpyDeviceToDevice, e.stream);
+    }
     if (err != cudaSuccess) b->status = FIDES_ERR_CUDA;
     if (cudaLaunchHostFunc(e.stream, on_done, b) != cudaSuccess) {
       b->status = FIDES_ERR_CUDA;
@@ -176,28 +195,48 @@ struct Server {
         done_cv.notify_all();
         break;
       }
-      // bootstrap requests: one per idle engine, oldest first
+      // bootstrap requests, oldest first: the idle engine that best fits the queue (the largest
+      // whose capacity the queued bootstraps fill, else the smallest), filled from the queue
       bool launched_boot = false;
-      for (auto it = pending.begin(); it != pending.end();) {
-        if (it->r.op != FIDES_OP_BOOTSTRAP) {
-          ++it;
-          continue;
+      for (;;) {
+        int queued = 0;
+        for (const auto& p : pending) queued += p.r.op == FIDES_OP_BOOTSTRAP;
+        if (!queued) break;
+        int best = -1;
+        for (size_t e = 0; e < boot.size(); ++e) {
+          if (boot[e].busy) continue;
+          const int cap = boot[e].capacity();
+          if (best < 0) {
+            best = (int)e;
+            continue;
+          }
+          const int bc = boot[best].capacity();
+          const bool fits = cap <= queued, best_fits = bc <= queued;
+          if ((fits && (!best_fits || cap > bc)) || (!fits && !best_fits && cap < bc)) best = (int)e;
         }
-        auto eng = std::find_if(boot.begin(), boot.end(), [](const BootEngine& e) { return !e.busy; });
-        if (eng == boot.end()) break;
-        Pending p = *it;
-        it = pending.erase(it);
-        eng->busy = true;
+        if (best < 0) break;
+        BootEngine& eng = boot[best];
+        std::vector<Pending> take;
+        for (auto it = pending.begin(); it != pending.end() && (int)take.size() < eng.capacity();) {
+          if (it->r.op == FIDES_OP_BOOTSTRAP) {
+            take.push_back(*it);
+            it = pending.erase(it);
+          } else {
+            ++it;
+          }
+        }
+        eng.busy = true;
         st.batches++;
-        st.batched_requests++;
+        st.batched_requests += take.size();
         launched_boot = true;
         lk.unlock();
-        launch_bootstrap(*eng, (int)(eng - boot.begin()), p);
+        launch_bootstrap(eng, best, take);
         lk.lock();
-        it = pending.begin();  // the deque may have changed while unlocked
       }
-      const auto first = std::find_if(pending.begin(), pending.end(),
-                                      [](const Pending& p) { return p.r.op != FIDES_OP_BOOTSTRAP; });
+      // the oldest request of a type whose batches may still start (in-flight limit)
+      const auto first = std::find_if(pending.begin(), pending.end(), [&](const Pending& p) {
+        return p.r.op != FIDES_OP_BOOTSTRAP && (max_inflight_per_op <= 0 || inflight[p.r.op] < max_inflight_per_op);
+      });
       const auto free_slot = std::find(busy.begin(), busy.end(), false);
       if (first == pending.end() || free_slot == busy.end()) {
         if (!launched_boot) cv.wait_for(lk, std::chrono::microseconds(200));
@@ -230,12 +269,13 @@ struct Server {
         continue;
       }
       busy[slot] = true;
+      inflight[op]++;
       in_use += bytes;
       st.batches++;
       st.batched_requests += take.size();
       st.peak_bytes = std::max<uint64_t>(st.peak_bytes, in_use);
       lk.unlock();
-      auto* b = new Batch{this, slot, {}, {}, bytes, FIDES_OK};
+      auto* b = new Batch{this, slot, {}, {}, bytes, FIDES_OK, op};
       for (auto& p : take) {
         b->tickets.push_back(p.ticket);
         b->arrivals.push_back(p.arrival);
@@ -344,19 +384,42 @@ int fides_server_add_rotation_key(fides_server* sv, int rotation, const uint64_t
 
 int fides_server_add_bootstrap(fides_server* sv, void* graph_exec, const uint64_t* in0, const uint64_t* in1,
                                int in_level, const uint64_t* out0, const uint64_t* out1, int out_level) {
+  return fides_server_add_bootstrap_batch(sv, graph_exec, 1, &in0, &in1, in_level, &out0, &out1, out_level);
+}
+
+int fides_server_add_bootstrap_batch(fides_server* sv, void* graph_exec, int capacity, const uint64_t* const* in0,
+                                     const uint64_t* const* in1, int in_level, const uint64_t* const* out0,
+                                     const uint64_t* const* out1, int out_level) {
   return sguard([&] {
     if (!sv || !graph_exec || !in0 || !in1 || !out0 || !out1) throw fides::Error(FIDES_ERR_ARG, "null argument");
+    if (capacity < 1 || capacity > 64) throw fides::Error(FIDES_ERR_ARG, "engine capacity must be 1..64");
     fides::Server* s = sv->s;
     if (in_level < 1 || in_level > s->c->n_q || out_level < 1 || out_level > s->c->n_q)
       throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    fides::Server::BootEngine e{static_cast<cudaGraphExec_t>(graph_exec), {}, {}, {}, {}, in_level, out_level,
+                                nullptr, false};
+    for (int k = 0; k < capacity; ++k) {
+      if (!in0[k] || !in1[k] || !out0[k] || !out1[k]) throw fides::Error(FIDES_ERR_ARG, "null engine buffer");
+      e.in0.push_back(in0[k]);
+      e.in1.push_back(in1[k]);
+      e.out0.push_back(out0[k]);
+      e.out1.push_back(out1[k]);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (!s->boot.empty() && (s->boot[0].in_level != in_level || s->boot[0].out_level != out_level))
       throw fides::Error(FIDES_ERR_ARG, "bootstrap engines must share their levels");
-    fides::Server::BootEngine e{static_cast<cudaGraphExec_t>(graph_exec), in0, in1, out0, out1, in_level,
-                                out_level, nullptr, false};
     FIDES_CUDA(cudaSetDevice(s->c->device));
     FIDES_CUDA(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
     s->boot.push_back(e);
+  });
+}
+
+int fides_server_set_max_inflight(fides_server* sv, int max_inflight_per_op) {
+  return sguard([&] {
+    if (!sv) throw fides::Error(FIDES_ERR_ARG, "null server");
+    if (max_inflight_per_op < 0) throw fides::Error(FIDES_ERR_ARG, "negative limit");
+    std::lock_guard<std::mutex> lk(sv->s->mu);
+    sv->s->max_inflight_per_op = max_inflight_per_op;
   });
 }
 

@@ -117,6 +117,9 @@ def lib():
         L.fides_ctx_autotune.argtypes = [vp, C.POINTER(C.c_float)]
         L.fides_ctx_reserve_scratch.argtypes = [vp, C.c_size_t]
         L.fides_server_add_bootstrap.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_int]
+        L.fides_server_add_bootstrap_batch.argtypes = [vp, vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.c_int,
+                                                       C.POINTER(vp), C.POINTER(vp), C.c_int]
+        L.fides_server_set_max_inflight.argtypes = [vp, C.c_int]
         L.fides_rotate_hoisted_batch.argtypes = [vp, C.POINTER(_HoistItem), C.c_int, vp]
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
@@ -923,6 +926,21 @@ class Server:
         _check(lib().fides_server_add_bootstrap(self._h, graph.raw_cuda_graph_exec(), _ptr(static_in.c0),
                                                 _ptr(static_in.c1), static_in.level, _ptr(static_out.c0),
                                                 _ptr(static_out.c1), static_out.level))
+
+    def add_bootstrap_batch(self, graph, static_ins: list, static_outs: list):
+        """Register an engine that bootstraps len(static_ins) ciphertexts per graph launch (see
+        fides_b200.bootstrap.make_batch_engine); the scheduler fills it from the queue."""
+        n = len(static_ins)
+        self._keep += [graph, static_ins, static_outs]
+        arr = lambda xs: (vp * n)(*xs)
+        _check(lib().fides_server_add_bootstrap_batch(
+            self._h, graph.raw_cuda_graph_exec(), n, arr([_ptr(c.c0) for c in static_ins]),
+            arr([_ptr(c.c1) for c in static_ins]), static_ins[0].level, arr([_ptr(c.c0) for c in static_outs]),
+            arr([_ptr(c.c1) for c in static_outs]), static_outs[0].level))
+
+    def set_max_inflight(self, k: int):
+        """At most k batches of one operation type on the device at once (0 = n_streams)."""
+        _check(lib().fides_server_set_max_inflight(self._h, k))
 
     def submit(self, op: int, a: Ciphertext, out: Ciphertext, b: Ciphertext | None = None, rotation: int = 0) -> int:
         r = _Request(op, a.level, _ptr(a.c0), _ptr(a.c1), _ptr(b.c0) if b else None, _ptr(b.c1) if b else None,

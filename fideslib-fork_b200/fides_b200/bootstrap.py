@@ -633,3 +633,25 @@ def make_engine(bs: Bootstrapper, scale: float):
         out = bs.bootstrap(static)
     torch.cuda.synchronize()
     return g, F.Ciphertext(c0, c1), F.Ciphertext(out.c0, out.c1)
+
+
+def make_batch_engine(bs: Bootstrapper, scale: float, capacity: int):
+    """A bootstrap engine holding `capacity` ciphertexts (fides_server_add_bootstrap_batch): one
+    CUDA graph, captured once, that bootstraps `capacity` static one-limb inputs on parallel
+    branches (bootstrap_concurrent) into static outputs.  Returns (graph, inputs, outputs)."""
+    import torch
+    F, ctx = bs.ev.F, bs.ev.ctx
+    ins = []
+    for _ in range(capacity):
+        c0, c1 = ctx.empty(1), ctx.empty(1)
+        c0.view(torch.int64).zero_()
+        c1.view(torch.int64).zero_()
+        ins.append(Ct(c0, c1, scale))
+    streams = [torch.cuda.Stream() for _ in range(capacity)]
+    bootstrap_concurrent(bs, ins, streams)  # warm-up outside the capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        outs = bootstrap_concurrent(bs, ins, streams)
+    torch.cuda.synchronize()
+    return (g, [F.Ciphertext(c.c0, c.c1) for c in ins], [F.Ciphertext(o.c0, o.c1) for o in outs])

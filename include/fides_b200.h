@@ -330,6 +330,19 @@ int fides_server_add_rotation_key(fides_server* s, int rotation, const uint64_t*
  * reference counterpart (the reference has no request loop). */
 int fides_server_add_bootstrap(fides_server* s, void* graph_exec, const uint64_t* in0, const uint64_t* in1,
                                int in_level, const uint64_t* out0, const uint64_t* out1, int out_level);
+/* A bootstrap engine that holds `capacity` ciphertexts: the graph bootstraps in0[k], in1[k] into
+ * out0[k], out1[k] for every k (e.g. one graph with a parallel branch per ciphertext).  The
+ * scheduler fills it with up to `capacity` queued bootstrap requests in one launch, preferring
+ * the largest idle engine the queue fills.  fides_server_add_bootstrap is capacity 1.  No
+ * reference counterpart. */
+int fides_server_add_bootstrap_batch(fides_server* s, void* graph_exec, int capacity, const uint64_t* const* in0,
+                                     const uint64_t* const* in1, int in_level, const uint64_t* const* out0,
+                                     const uint64_t* const* out1, int out_level);
+/* At most this many batches of one operation type on the device at once (0 = no limit beyond
+ * n_streams, the default).  With 1, requests that arrive while their type's batch runs form the
+ * next batch together (batches grow under load), and a type with nothing in flight starts at
+ * once.  No reference counterpart. */
+int fides_server_set_max_inflight(fides_server* s, int max_inflight_per_op);
 /* Thread-safe, non-blocking; rejects malformed requests and missing keys immediately. */
 int fides_server_submit(fides_server* s, const fides_request* req, uint64_t* ticket);
 /* Blocks until the request completed; *status is its result (FIDES_ERR_OOM when it can

@@ -175,10 +175,11 @@ def test_served_bootstraps_in_a_mix(fides):
     delta = 2.0 ** 50
     bs.prepare(top_level=prm.n_q, msg_scale=delta)
     engines = [B.make_engine(bs, delta) for _ in range(2)]
+    batch_engine = B.make_batch_engine(bs, delta, 3)  # one graph, three ciphertexts per launch
     rng = xrng(65)
     n = prm.N // 2
     boot_in, boot_ref = [], []
-    for _ in range(4):
+    for _ in range(6):
         z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
         c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
         ct = F.Ciphertext(F.to_device(c0[:1]), F.to_device(c1[:1]))
@@ -204,8 +205,10 @@ def test_served_bootstraps_in_a_mix(fides):
     try:
         srv.set_relin_key(ev.rk)
         srv.add_rotation_key(1, rot_key)
+        srv.set_max_inflight(1)
         for g, sin, sout in engines:
             srv.add_bootstrap(g, sin, sout)
+        srv.add_bootstrap_batch(*batch_engine)
         out_lvl = engines[0][2].level
         jobs = [("b", i) for i in range(len(boot_in))] + [("o", i) for i in range(len(reqs))]
         random.Random(8).shuffle(jobs)

@@ -95,11 +95,15 @@ def run_mixed(env, srv, reqs, threads=3, max_gap_us=300):
     return outs, lat
 
 
-def test_alone_equals_mixed_config_a(fides):
+@pytest.mark.parametrize("max_inflight", [0, 1])
+def test_alone_equals_mixed_config_a(fides, max_inflight):
+    """max_inflight = 1: at most one batch per operation type on the device, so requests that
+    arrive meanwhile form the next batch (batches grow under load); results are unchanged."""
     from fides_b200 import params as P
     env = Env(fides, P.config_a(), rots=(1, -1, 2))
     reqs = env.requests(40, seed=3, levels=[2, 3, 4, 5, 6])
     srv = env.server(n_streams=3, max_batch=6)
+    srv.set_max_inflight(max_inflight)
     try:
         alone = run_alone(env, srv, reqs)
         mixed, lat = run_mixed(env, srv, reqs)

@@ -65,3 +65,27 @@ def test_per_ciphertext_rotation_lists(env):
         for j in range(len(rs)):
             assert np.array_equal(F.to_host(res[j].c0), h0[j])
             assert np.array_equal(F.to_host(res[j].c1), h1[j])
+
+
+def test_batch_of_32_ciphertexts_level_29(env):
+    """Config C's largest batch: 32 ciphertexts at level 29, the 16 rotations each, in one
+    launch sequence (the KSK pass groups the ciphertexts that share a key, so each key tile is
+    read once per group of 8).  Every output equals the single-ciphertext hoisted path; two
+    ciphertexts are also checked against the oracle on three rotations."""
+    F, prm, o, ctx, keys, keys_d = env
+    host = [ct(F, prm, 29, 1700 + i) for i in range(32)]
+    dev = [F.Ciphertext(F.to_device(c[0]), F.to_device(c[1])) for c in host]
+    outs = ctx.rotate_hoisted_batch(dev, [keys_d[r] for r in ROTS], ROTS)
+    assert len(outs) == 32 and all(len(x) == 16 for x in outs)
+    for i in (0, 13, 31):
+        single = ctx.rotate_hoisted(dev[i], [keys_d[r] for r in ROTS], ROTS)
+        for a, b in zip(outs[i], single):
+            assert np.array_equal(F.to_host(a.c0), F.to_host(b.c0))
+            assert np.array_equal(F.to_host(a.c1), F.to_host(b.c1))
+    sub = [2, -32, 128]
+    for i in (7, 30):
+        h0, h1 = o.rotate_hoisted(*host[i], [keys[r] for r in sub], sub)
+        for j, r in enumerate(sub):
+            k = ROTS.index(r)
+            assert np.array_equal(F.to_host(outs[i][k].c0), h0[j])
+            assert np.array_equal(F.to_host(outs[i][k].c1), h1[j])

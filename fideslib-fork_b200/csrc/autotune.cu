@@ -24,11 +24,13 @@ __global__ void fill_residues(uint64_t* x, const DevPrime* primes, const int* pr
 
 constexpr int SIZES[4] = {4, 16, 64, 256};  // one representative launch per size class
 constexpr int SHAPES[3] = {4, 8, 16};
+// chunk sizes tried on a list of MAX_NTT_LIMBS limbs (a launch of 224 MB at N = 2^16)
+constexpr int CHUNKS[6] = {0, 224, 160, 112, 80, 56};
 
 }  // namespace
 
 void autotune_ntt(Context* c, float* best_ms) {
-  const int max_limbs = SIZES[3];
+  const int max_limbs = MAX_NTT_LIMBS;
   const int np = c->n_q + c->K;
   cudaStream_t s = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -37,6 +39,8 @@ void autotune_ntt(Context* c, float* best_ms) {
   FIDES_CUDA(cudaEventCreate(&e1));
   uint8_t saved[2][2][4];
   std::copy(&c->ntt_g[0][0][0], &c->ntt_g[0][0][0] + 16, &saved[0][0][0]);
+  const int saved_chunk = c->ntt_chunk;
+  c->ntt_chunk = 0;  // the shapes are timed on unsplit launches
   try {
     Scratch data(c, c->limb_bytes() * max_limbs, s);
     Scratch ids(c, sizeof(int) * max_limbs, s);
@@ -83,8 +87,31 @@ void autotune_ntt(Context* c, float* best_ms) {
         // the other direction of the timing pair uses its current table entries
         if (best_ms) best_ms[inv * 4 + cls] = best;
       }
+    // chunk size of long limb lists: a forward + inverse round trip of MAX_NTT_LIMBS limbs
+    {
+      const int n = max_limbs;
+      float best = 1e30f;
+      int pick = 0;
+      for (int ch : CHUNKS) {
+        c->ntt_chunk = ch;
+        float t = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {  // the first repetition warms up
+          FIDES_CUDA(cudaEventRecord(e0, s));
+          ntt_limbs(c, refs.data(), n, false, s);
+          ntt_limbs(c, refs.data(), n, true, s);
+          FIDES_CUDA(cudaEventRecord(e1, s));
+          FIDES_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          FIDES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep) t = std::min(t, ms);
+        }
+        if (t < best) best = t, pick = ch;
+      }
+      c->ntt_chunk = pick;
+    }
     FIDES_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
+    c->ntt_chunk = saved_chunk;
     std::copy(&saved[0][0][0], &saved[0][0][0] + 16, &c->ntt_g[0][0][0]);
     cudaStreamSynchronize(s);
     cudaEventDestroy(e0);

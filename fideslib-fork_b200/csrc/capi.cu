@@ -201,6 +201,17 @@ int fides_ctx_set_ntt_shape(fides_ctx* x, int inverse, int pass, int size_class,
   });
 }
 
+int fides_ctx_ntt_chunk(fides_ctx* x, int set_limbs) {
+  int out = 0;
+  const int rc = guard([&] {
+    auto* c = C(x);
+    if (set_limbs > 0) c->ntt_chunk = std::min(set_limbs, fides::MAX_NTT_LIMBS);
+    if (set_limbs == 0) c->ntt_chunk = 0;
+    out = c->ntt_chunk > 0 ? c->ntt_chunk : fides::MAX_NTT_LIMBS;
+  });
+  return rc == FIDES_OK ? out : rc;
+}
+
 int fides_ctx_set_conv_engine(fides_ctx* x, int engine) {
   return guard([&] {
     if (engine < fides::CONV_AUTO || engine > fides::CONV_TENSOR) throw fides::Error(FIDES_ERR_ARG, "bad engine");

@@ -115,6 +115,11 @@ struct Context {
   // fides_ctx_autotune replaces them with timed choices.
   uint8_t ntt_g[2][2][4] = {{{4, 8, 16, 16}, {4, 8, 16, 16}}, {{4, 8, 16, 16}, {4, 8, 16, 16}}};
   static int ntt_size_class(int limbs) { return limbs <= 8 ? 0 : limbs <= 32 ? 1 : limbs <= 128 ? 2 : 3; }
+  // Limbs per transform launch pair: a list longer than this runs as balanced chunks, each chunk's
+  // column and row passes back to back, so that a chunk that fits in L2 has its intermediate read
+  // by the second pass from L2 (and overwritten there in place, never written to DRAM).  0 = the
+  // largest launch (MAX_NTT_LIMBS); fides_ctx_autotune picks it by timing.
+  int ntt_chunk = 0;
   int ntt_shape(bool inverse, int pass, int limbs) const { return ntt_g[inverse][pass][ntt_size_class(limbs)]; }
   uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up,
                                  // bit 1 = an encoded coefficient exceeded q_0 / 2

@@ -581,8 +581,7 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     auto same_digits = [](const KskJob& a, const KskJob& b) {
       return a.digits == b.digits && a.x == b.x && a.x2 == b.x2 && a.l == b.l && !a.a0 == !b.a0 && !a.c0 == !b.c0;
     };
-    // groups sharing a key take up to 8 jobs; groups sharing a digit tile at most 4 (the
-    // shared-digit form with 8 jobs spills heavily at three digits)
+    // groups of up to MAX_KSK_GROUP jobs sharing a key, or else sharing a digit tile
     auto group = [&](auto same, int cap) {
       L.ngroups = 0;
       int gm = 1;
@@ -606,7 +605,7 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     }
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
-    const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : gmax <= 4 ? 4 : 8;
+    const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : 4;
     dim3 grid(c->N / (2 * EW_THREADS), mx, L.ngroups);
     // algorithmic bytes: each job's digits, outputs and extra operands, and each group's key once
     double bytes = 0;
@@ -633,15 +632,10 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
   case 128 + B * 16 + G:                        \
     go(ksk_kernel<B, G, 2, true>);              \
     break;
-#define FIDES_KSK_CASE8(B)                      \
-  case B * 16 + 8:                              \
-    go(ksk_kernel<B, 8, 2>);                    \
-    break;
-      FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4) FIDES_KSK_CASE8(1)
-      FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4) FIDES_KSK_CASE8(2)
-      FIDES_KSK_CASE(3, 1) FIDES_KSK_CASE(3, 2) FIDES_KSK_CASE(3, 4) FIDES_KSK_CASE8(3)
-      FIDES_KSK_CASE(4, 1) FIDES_KSK_CASE(4, 2) FIDES_KSK_CASE(4, 4) FIDES_KSK_CASE8(4)
-#undef FIDES_KSK_CASE8
+      FIDES_KSK_CASE(1, 1) FIDES_KSK_CASE(1, 2) FIDES_KSK_CASE(1, 4)
+      FIDES_KSK_CASE(2, 1) FIDES_KSK_CASE(2, 2) FIDES_KSK_CASE(2, 4)
+      FIDES_KSK_CASE(3, 1) FIDES_KSK_CASE(3, 2) FIDES_KSK_CASE(3, 4)
+      FIDES_KSK_CASE(4, 1) FIDES_KSK_CASE(4, 2) FIDES_KSK_CASE(4, 4)
 #undef FIDES_KSK_CASE
       default:
         go(ksk_kernel<0, 1, 2>);

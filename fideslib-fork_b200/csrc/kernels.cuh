@@ -48,9 +48,10 @@ struct KskJob {
 };
 constexpr int MAX_KSK_JOBS = 64;
 // Jobs that share a switching key (one relinearisation or rotation key for a batch) and the
-// same level and extras form a group of up to 8; one CTA runs a whole group, reading each key
-// tile once for all of its jobs (a batch of 8 reads the key once).
-constexpr int MAX_KSK_GROUP = 8;
+// same level and extras form a group of up to 4; one CTA runs a whole group, reading each key
+// tile once for all of its jobs.  (Groups of 8 read the key half as often but measured 20 %
+// slower on the bench step: half as many CTAs, each running twice as long, and more spills.)
+constexpr int MAX_KSK_GROUP = 4;
 struct KskJobList {
   int n, max_ext, ngroups, pad1;
   uint8_t gstart[MAX_KSK_JOBS], gcount[MAX_KSK_JOBS];

@@ -36,8 +36,11 @@ void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream
     c->ntt_limbs_by_form[1] += (uint64_t)n - nf;
   }
   static thread_local NttLimbList L;  // ~25 KB: keep off the stack
-  for (int off = 0; off < n; off += MAX_NTT_LIMBS) {
-    L.n = std::min(MAX_NTT_LIMBS, n - off);
+  // balanced chunks of at most the context's chunk size, both passes of a chunk back to back
+  const int cap = c->ntt_chunk > 0 ? std::min(c->ntt_chunk, MAX_NTT_LIMBS) : MAX_NTT_LIMBS;
+  const int nchunks = (n + cap - 1) / cap, per = (n + nchunks - 1) / nchunks;
+  for (int off = 0; off < n; off += per) {
+    L.n = std::min(per, n - off);
     std::copy(limbs + off, limbs + off + L.n, L.limbs);
     switch (c->logN) {
       case 10: ntt_transform_10(c, a, L, inverse, in, out, s); break;

@@ -125,6 +125,7 @@ def lib():
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_synchronize.argtypes = [vp, vp]
+        L.fides_ctx_ntt_chunk.argtypes = [vp, C.c_int]
         L.fides_boot_create.argtypes = [vp, C.POINTER(_BootParams), C.POINTER(vp)]
         L.fides_boot_destroy.argtypes = [vp]
         L.fides_boot_rotations.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
@@ -321,7 +322,16 @@ class Context:
         Returns the shape table and each class's representative transform time."""
         ms = (C.c_float * 8)()
         _check(lib().fides_ctx_autotune(self._h, ms))
-        return {"shapes": self.ntt_shapes(), "transform_ms": {"forward": list(ms[0:4]), "inverse": list(ms[4:8])}}
+        return {"shapes": self.ntt_shapes(), "transform_ms": {"forward": list(ms[0:4]), "inverse": list(ms[4:8])},
+                "chunk_limbs": self.ntt_chunk()}
+
+    def ntt_chunk(self, set_limbs: int = -1) -> int:
+        """Limbs per NTT launch pair (fides_ctx_ntt_chunk): set_limbs > 0 sets it, 0 restores
+        the largest launch, -1 only reads.  Returns the current value."""
+        rc = lib().fides_ctx_ntt_chunk(self._h, set_limbs)
+        if rc < 0:
+            _check(rc)
+        return int(rc)
 
     def ntt_shapes(self) -> dict:
         """Sub-transforms per CTA by direction / pass / launch-size class."""

@@ -84,6 +84,12 @@ int fides_ctx_set_conv_engine(fides_ctx* ctx, int engine);
  * not run it concurrently with other work on the context.  No reference counterpart: the
  * reference fixes its NTT launch geometry (src/CKKS/LimbPartition.cu:444-472). */
 int fides_ctx_autotune(fides_ctx* ctx, float* best_ms);
+/* Limbs per NTT launch pair: longer limb lists run as balanced chunks of at most this many
+ * limbs, each chunk's two passes back to back, so that a chunk small enough for L2 has its
+ * between-pass intermediate served from L2.  set_limbs > 0 sets it, 0 restores the largest
+ * launch, < 0 only reads; returns the current value (or a negative status).  fides_ctx_autotune
+ * picks it by timing. */
+int fides_ctx_ntt_chunk(fides_ctx* ctx, int set_limbs);
 /* The 16 shape entries, index [inverse][pass][size class]. */
 int fides_ctx_ntt_shapes(fides_ctx* ctx, uint8_t* shapes);
 int fides_ctx_set_ntt_shape(fides_ctx* ctx, int inverse, int pass, int size_class, int subs_per_cta);

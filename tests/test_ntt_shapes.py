@@ -88,3 +88,29 @@ def test_bad_shape_rejected(env):
         with pytest.raises(F.FidesError) as e:
             ctx.set_ntt_shape(*args)
         assert e.value.code == -1
+
+
+@pytest.mark.parametrize("chunk", [7, 56, 0])
+def test_chunked_launches_equal_oracle(env, chunk):
+    """A limb list longer than the chunk size runs as balanced chunks (both passes of a chunk
+    back to back); the transforms and a batched HMult built on them stay bit-exact."""
+    F, prm, o, ctx, rk, rk_d = env
+    old = ctx.ntt_chunk()
+    try:
+        assert ctx.ntt_chunk(chunk) == (chunk or 448)
+        polys = 4
+        x = np.stack([uniform_limbs(xrng(4100 + i), prm.q, prm.N) for i in range(polys)])  # 120 limbs
+        d = F.to_device(x)
+        ctx.ntt(d)
+        got = F.to_host(d)
+        for i in range(polys):
+            assert np.array_equal(got[i], o.ntt(x[i], list(range(prm.n_q)))), f"poly {i}"
+        ctx.intt(d)
+        assert eq(d, x)
+        a = [uniform_limbs(xrng(4200 + i), prm.q, prm.N) for i in range(4)]
+        out = ctx.mult_batch([(F.Ciphertext(F.to_device(a[0]), F.to_device(a[1])),
+                               F.Ciphertext(F.to_device(a[2]), F.to_device(a[3])))], rk_d, rescale=True)[0]
+        w0, w1 = o.hmult(a[0], a[1], a[2], a[3], rk, rescale=True)
+        assert eq(out.c0, w0) and eq(out.c1, w1)
+    finally:
+        ctx.ntt_chunk(old)

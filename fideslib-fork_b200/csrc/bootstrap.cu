@@ -242,6 +242,7 @@ struct Bootstrapper {
   boot::Buf pt_i, pt_minus_i;
   int top = 0, cts_out_level = 0, stc_in_level = 0, out_level = 0;
   double in_scale = 0, msg_scale = 0;
+  double corr = 0;  // correction_bits > 0: round(q_1 / 2^correction_bits)
   std::vector<cudaStream_t> lanes;  // streams of fides_bootstrap_batch
   std::vector<cudaEvent_t> lane_ev;
   cudaStream_t own = nullptr;  // the prepared tables are allocated and freed on this stream
@@ -611,6 +612,10 @@ struct Bootstrapper {
     top = top_level;
     in_scale = S[top_level];
     msg_scale = prm.msg_scale * (double)(1ll << prm.prescale_bits);
+    if (prm.correction_bits > 0) {  // the input is scaled by round(q_1 / 2^k) / q_1 first
+      corr = boot::rint_even((double)c->primes[1] / std::ldexp(1.0, prm.correction_bits));
+      msg_scale = msg_scale * corr / (double)c->primes[1];
+    }
     // 2 K q0 is formed exactly and rounded once to a double (as an integer product would be)
     const double two_k_q0 = (double)((unsigned __int128)2 * (unsigned)prm.K * c->primes[0]);
     const double gfac = std::pow(in_scale / two_k_q0 / n, 1.0 / (double)cts.size());
@@ -804,6 +809,10 @@ struct Bootstrapper {
     x.c1 = c1;
     x.level = 1;
     x.scale = prm.msg_scale;
+    if (prm.correction_bits > 0) {  // scale down by ~2^k: times round(q_1 / 2^k) at level 2, rescale by q_1
+      x.level = 2;
+      x = rescale_many_to({mul_int(x, corr, s)}, x.scale * corr / (double)c->primes[1], s)[0];
+    }
     if (prm.sparse_encapsulation) {
       if (!to_sparse || !to_dense) throw Error(-5, "bootstrap: encapsulation keys not set");
       x = keyswitch_add(x, to_sparse, s);  // dense -> sparse secret, at level 1
@@ -884,6 +893,8 @@ int fides_boot_create(fides_ctx* ctx, const fides_boot_params* p, fides_boot** o
     if (!(p->top_scale > 0) || !(p->msg_scale > 0)) throw fides::Error(FIDES_ERR_ARG, "scales must be positive");
     if (p->degree < 2 || p->K < 1 || p->r < 0 || p->baby < 1 || p->prescale_bits < 0 || p->prescale_bits > 30)
       throw fides::Error(FIDES_ERR_ARG, "EvalMod / BSGS parameters out of range");
+    if (p->correction_bits < 0 || p->correction_bits > 40 || (p->correction_bits > 0 && c->n_q < 3))
+      throw fides::Error(FIDES_ERR_ARG, "correction_bits out of range (and needs q_1)");
     if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "bootstrapping needs special primes");
     auto* bs = new fides::Bootstrapper{};
     bs->c = c;

@@ -446,6 +446,10 @@ typedef struct fides_boot_params {
   int baby;              /* BSGS baby steps */
   int prescale_bits;     /* input multiplied by 2^prescale_bits before ModRaise (divided out after) */
   int sparse_encapsulation; /* 1: switch to a sparse secret around ModRaise (keys below) */
+  int correction_bits;   /* > 0: the input (at least 2 limbs) is first scaled down by about
+                          * 2^correction_bits -- multiplied by round(q_1 / 2^k) and rescaled by q_1 --
+                          * so that a message at a scale close to q_0 (scaling primes nearly as
+                          * large as q_0) leaves EvalMod room; OpenFHE's correction factor */
 } fides_boot_params;
 typedef struct fides_boot fides_boot;
 int fides_boot_create(fides_ctx* ctx, const fides_boot_params* params, fides_boot** out);
@@ -463,7 +467,8 @@ int fides_boot_set_rotation_key(fides_boot* b, int rotation, const uint64_t* key
 int fides_boot_prepare(fides_boot* b, void* stream);
 /* Level (limbs) and scale of the bootstrapped output. */
 int fides_boot_levels(const fides_boot* b, int* out_level, double* out_scale);
-/* Bootstraps (c0, c1) (limb q_0 is read) into out0 / out1 (out_level limbs each) on `stream`. */
+/* Bootstraps (c0, c1) (limb q_0 is read; limbs q_0, q_1 with correction_bits) into out0 / out1
+ * (out_level limbs each) on `stream`. */
 int fides_bootstrap(fides_boot* b, const uint64_t* c0, const uint64_t* c1, uint64_t* out0, uint64_t* out1,
                     void* stream);
 /* n bootstraps at once, each on its own internal stream forked from and joined back to

@@ -614,3 +614,37 @@ def test_cpp_facade_arithmetic(fides):
     w0, w1 = o.hmult(a[0], a[1], b[0], b[1], rk, rescale=False)
     assert np.array_equal(m0, w0) and np.array_equal(m1, w1), "FIXEDMANUAL EvalMult"
     assert np.array_equal(r0, o.rescale(w0)) and np.array_equal(r1, o.rescale(w1)), "FIXEDMANUAL Rescale"
+
+
+@pytest.mark.gpu
+def test_native_bootstrap_59bit_chain_correction(fides):
+    """The reference example's modulus sizes (60-bit q_0, 59-bit scaling primes) at N = 2^12:
+    the level-2 input, at a scale close to q_0, is scaled down by 2^9 before ModRaise
+    (correction_bits, OpenFHE's correction factor) and decrypts within 2^-12 after bootstrapping."""
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 59, 20, 4, name="boot59 N=2^12")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=61, hamming_weight=32)
+    S = [0.0] * (prm.n_q + 1)
+    S[prm.n_q] = 2.0 ** 59
+    for l in range(prm.n_q, 1, -1):
+        S[l - 1] = S[l] * S[l] / prm.q[l - 1]
+    nb = F.NativeBootstrapper(ctx, top_level=prm.n_q, top_scale=S[prm.n_q], msg_scale=S[2], correction_bits=9)
+    keys = [F.to_device(kg.relin_key()), F.to_device(kg.auto_key(2 * prm.N - 1))]
+    nb.set_keys(*keys)
+    rk = {r: F.to_device(kg.rotation_key(r)) for r in nb.rotations()}
+    for r, k in rk.items():
+        nb.set_rotation_key(r, k)
+    nb.prepare()
+    rng = xrng(69)
+    n = prm.N // 2
+    z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    c0, c1 = kg.encrypt(encode(z, prm.N, S[2]).astype(np.int64), 2)
+    out = nb.bootstrap(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    got = decode(kg.decrypt_limb0(F.to_host(out.c0), F.to_host(out.c1)), prm.N, nb.out_scale)
+    bits = -math.log2(np.abs(got - z).max())
+    print(f"59-bit chain bootstrap N=2^12: {bits:.1f} bits, out level {nb.out_level}")
+    assert bits > 12
+    nb.close()

@@ -647,7 +647,7 @@ struct Bootstrapper {
     FIDES_CUDA(cudaStreamSynchronize(s));
     uint32_t st = 0;
     FIDES_CUDA(cudaMemcpy(&st, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (st & 2u) throw Error(-1, "bootstrap: an encoded diagonal coefficient exceeded q_0 / 2");
+    if (st & 2u) throw Error(-1, "bootstrap: an encoded diagonal coefficient exceeded 2^62");
     prepared = true;
   }
 

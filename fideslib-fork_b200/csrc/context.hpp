@@ -122,7 +122,7 @@ struct Context {
   int ntt_chunk = 0;
   int ntt_shape(bool inverse, int pass, int limbs) const { return ntt_g[inverse][pass][ntt_size_class(limbs)]; }
   uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up,
-                                 // bit 1 = an encoded coefficient exceeded q_0 / 2
+                                 // bit 1 = an encoded coefficient exceeded 2^62
   // special-FFT twiddles of the slot encoder, [N/2] (double, double) pairs: entry h + j
   // (h = len / 2, j < h) = exp(-2 pi i (5^j mod 4 len) / (4 len))
   void* d_sfft = nullptr;

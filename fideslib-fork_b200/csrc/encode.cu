@@ -13,13 +13,14 @@
 //     stride S (a CTA holds several sub-problems with consecutive offsets, so every global
 //     access is a run of consecutive elements);
 //   * a contiguous pass: the stages len = S .. 2 on blocks of S consecutive elements, then the
-//     bit reversal, scaling and rounding, writing the coefficients as residues mod q_0.  A CTA
-//     takes the blocks whose bit-reversed indices are consecutive, so the scattered output of
-//     the bit reversal becomes runs of consecutive coefficients.
-// The residues mod q_0 feed the library's forward NTT with the SwitchModulus prologue
-// (centred lift from q_0 to each q_j, the identity for q_0 itself), so all limbs of a batch
-// of plaintexts are one NTT launch pair.  |m| must stay below q_0 / 2; a larger coefficient
-// sets bit 1 of the context's device status word and is written as 0.
+//     bit reversal, scaling and rounding, writing the coefficients as signed 64-bit integers.
+//     A CTA takes the blocks whose bit-reversed indices are consecutive, so the scattered output
+//     of the bit reversal becomes runs of consecutive coefficients.
+// The signed coefficients feed the library's forward NTT with the signed-integer prologue (each
+// limb reduces them modulo its own prime), so all limbs of a batch of plaintexts are one NTT
+// launch pair and a coefficient may exceed any single prime (plaintext diagonals at scales
+// close to q_0, e.g. with 59-bit scaling primes and a 60-bit q_0).  |m| must stay below 2^62;
+// a larger coefficient sets bit 1 of the context's device status word and is written as 0.
 //
 // Decode is the transpose: INTT of limb 0, centred lift and 1/scale while loading in
 // bit-reversed order, the Cooley-Tukey stages len = 2 .. S, then len = 2S .. n, giving the
@@ -104,7 +105,8 @@ __global__ void __launch_bounds__(SF_THREADS) sfft_strided(const double2* __rest
 
 // Contiguous encode pass: blocks b = brev_la(c0 + u), u < G (la = logn - ls), each of S = 2^ls
 // elements; DIF stages len = S .. 2, then coefficient k = brev_logn(b S + r) = brev_ls(r) 2^la
-// + c0 + u takes Re / Im of the element times scale / n, rounded to nearest, as a residue mod q0.
+// + c0 + u takes Re / Im of the element times scale / n, rounded to nearest, as a signed 64-bit
+// integer (each limb's NTT prologue reduces it modulo its own prime).
 __global__ void __launch_bounds__(SF_THREADS) sfft_encode_finish(const double2* __restrict__ in, uint64_t* __restrict__ coef,
                                                                  const double2* __restrict__ tw, int logn, int ls,
                                                                  int logN, double mult, uint64_t q0,
@@ -131,7 +133,8 @@ __global__ void __launch_bounds__(SF_THREADS) sfft_encode_finish(const double2* 
   }
   const int gap = 1 << (logN - 1 - logn);
   uint64_t* out = coef + ((size_t)blockIdx.y << logN);
-  const double lim = (double)(q0 >> 1);
+  (void)q0;
+  const double lim = 4611686018427387904.0;  // 2^62
   bool bad = false;
   for (int e = threadIdx.x; e < G * S; e += blockDim.x) {
     const int u = e % G, rr = e / G;
@@ -140,9 +143,8 @@ __global__ void __launch_bounds__(SF_THREADS) sfft_encode_finish(const double2* 
     const double re = w.x * mult, im = w.y * mult;
     uint64_t mr = 0, mi = 0;
     if (fabs(re) < lim && fabs(im) < lim) {
-      const long long a = __double2ll_rn(re), b = __double2ll_rn(im);
-      mr = a < 0 ? q0 - (uint64_t)(-a) : (uint64_t)a;
-      mi = b < 0 ? q0 - (uint64_t)(-b) : (uint64_t)b;
+      mr = (uint64_t)__double2ll_rn(re);
+      mi = (uint64_t)__double2ll_rn(im);
     } else {
       bad = true;
     }
@@ -237,11 +239,10 @@ void op_encode(Context* c, const double* slots, int n_slots, int n_pts, double s
   for (int p = 0; p < n_pts; ++p)
     for (int j = 0; j < level; ++j) {
       LimbRef r = lref(out + ((size_t)p * level + j) * N, j);
-      r.pro = coef + p * N;
-      r.aux = 1;  // SwitchModulus from q_0
+      r.pro = coef + p * N;  // signed coefficients, reduced by each limb's prologue
       refs.push_back(r);
     }
-  ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_SWITCH, OUT_PLAIN);
+  ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_SIGNED, OUT_PLAIN);
 }
 
 void op_decode(Context* c, const uint64_t* pts, int level, int n_pts, int n_slots, double scale, double* slots,

@@ -67,6 +67,14 @@ __device__ __forceinline__ uint64_t mulmod(uint64_t a, uint64_t b, const DevPrim
   return reduce128(t, p);
 }
 
+// A signed integer (two's complement, |v| < 2^63) as its residue modulo q.
+__device__ __forceinline__ uint64_t signed_mod(uint64_t v, const DevPrime& p) {
+  const bool neg = (int64_t)v < 0;
+  const uint64_t a = neg ? 0 - v : v;
+  const uint64_t r = shoup(a, 1, p.one_s, p.q);
+  return neg && r ? p.q - r : r;
+}
+
 // OpenFHE SwitchModulus as restated in the reference (src/CKKS/Rescale.cuh:44-64): a
 // residue of the old prime `om` re-expressed modulo `nm` with the centred lift.
 __device__ __forceinline__ uint64_t switch_modulus(uint64_t a, const DevPrime& om, const DevPrime& nm) {

@@ -12,7 +12,7 @@ void ntt_limbs(Context* c, const LimbRef* limbs, int n, bool inverse, cudaStream
   if (c->logN < 10) throw Error(-1, "GPU NTT needs logN >= 10");
   const bool ok = inverse ? ((in == IN_PLAIN || in == IN_MUL || in == IN_ADD_PMUL) &&
                              (out == OUT_PLAIN || out == OUT_SUB_PINV))
-                          : ((in == IN_PLAIN || in == IN_SWITCH || in == IN_CONV_SW) &&
+                          : ((in == IN_PLAIN || in == IN_SWITCH || in == IN_CONV_SW || in == IN_SIGNED) &&
                              (out == OUT_PLAIN || out == OUT_MODDOWN || out == OUT_RESCALE || out == OUT_MDRS));
   if (!ok) throw Error(-1, "NTT prologue/epilogue not available in this direction");
   nttk::PassArgs a;

@@ -34,6 +34,7 @@ enum NttIn {
   IN_SWITCH = 2,   // forward only: x = SwitchModulus(pro[i]) from prime aux - 1 (rescale)
   IN_CONV_SW = 3,  // forward only: x = src[i] + P SwitchModulus(pro[i]) from prime aux - 1
   IN_ADD_PMUL = 4, // inverse only: x = src[i] + P pro[i]
+  IN_SIGNED = 5,   // forward only: x = pro[i] read as a signed 64-bit integer, reduced mod q (encode)
 };
 // What the last pass stores to ptr.
 enum NttOut {

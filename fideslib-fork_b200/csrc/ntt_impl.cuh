@@ -399,6 +399,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   if (IN == IN_CONV_SW || IN == IN_ADD_PMUL) pm = a.pmod[lr.prime];
   auto load = [&](size_t i) -> uint64_t {
     if (first_pass && IN == IN_SWITCH) return switch_modulus(lr.pro[i], opr, pr);
+    if (first_pass && IN == IN_SIGNED) return signed_mod(lr.pro[i], pr);
     if (first_pass && IN == IN_MUL) return mulmod(in[i], lr.pro[i], pr);
     if (first_pass && IN == IN_CONV_SW) return in[i];  // + P SwitchModulus(top) below
     if (first_pass && IN == IN_ADD_PMUL) return addmod(in[i], shoup(lr.pro[i], pm.w, pm.ws, pr.q), pr.q);
@@ -582,6 +583,8 @@ void run_transform(Context* c, const PassArgs& a, const NttLimbList& L, bool inv
   if (!inverse) {
     if (in == IN_SWITCH)
       launch_pass<LOGN, COL, true, IN_SWITCH, OUT_PLAIN>(c, a, L, s);
+    else if (in == IN_SIGNED)
+      launch_pass<LOGN, COL, true, IN_SIGNED, OUT_PLAIN>(c, a, L, s);
     else if (in == IN_CONV_SW)
       launch_pass<LOGN, COL, true, IN_CONV_SW, OUT_PLAIN>(c, a, L, s);
     else

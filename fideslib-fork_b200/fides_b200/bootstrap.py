@@ -425,7 +425,7 @@ class Bootstrapper:
         self.pt_i = self._int_pt(mono, top_level)
         self.pt_minus_i = self._int_pt(-mono, top_level)
         if ev.ctx.device_status(clear=False) & 2:
-            raise ValueError("an encoded diagonal coefficient exceeded q_0 / 2")
+            raise ValueError("an encoded diagonal coefficient exceeded 2^62 in magnitude")
 
     def _prepare_matrix(self, M: dict, fac: float, level: int, scale: float):
         """Pre-rotated, encoded diagonals for BSGS at `level` (input scale `scale`)."""

@@ -108,7 +108,7 @@ int fides_kernel_arch(int device, int* binary_version);
 int fides_ctx_ntt_counts(fides_ctx* ctx, uint64_t* f64_limbs, uint64_t* int_limbs);
 /* Synchronises the device and reads the context's device status word: bit 0 = a bounded
  * device-side wait gave up (the affected outputs are incomplete), bit 1 = an encoded
- * coefficient exceeded q_0 / 2.  clear != 0 resets it.  Every call that synchronises with
+ * coefficient exceeded 2^62 in magnitude.  clear != 0 resets it.  Every call that synchronises with
  * the device on the caller's behalf (fides_ctx_synchronize, the host-buffer entry points,
  * fides_ct_export) returns FIDES_ERR_TIMEOUT while bit 0 is set, until it is cleared here.
  * Counterpart of the reference's CudaCheckErrorMod after a synchronisation
@@ -202,8 +202,9 @@ int fides_rescale_batch(fides_ctx* ctx, const uint64_t* const* xs, const int* le
  * device memory; n_slots a power of two <= N/2) are multiplied by `scale`, mapped to
  * coefficients by the inverse special FFT (coefficient gap N / (2 n_slots)), rounded to the
  * nearest integer and written as `level` limbs in EVALUATION form, out = [n_pts][level][N].
- * Every coefficient must stay below q_0 / 2 in magnitude; a larger one is written as 0 and
- * sets bit 1 of the device status word (fides_ctx_device_status). */
+ * Each limb reduces the signed integer coefficient modulo its own prime, so a coefficient may
+ * exceed q_0; every coefficient must stay below 2^62 in magnitude, a larger one is written as 0
+ * and sets bit 1 of the device status word (fides_ctx_device_status). */
 int fides_encode(fides_ctx* ctx, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
                  void* stream);
 /* CKKS slot decode on the device: n_pts plaintexts [n_pts][level][N] in EVALUATION form ->

@@ -105,7 +105,7 @@ def test_encode_overflow_sets_status_and_bad_sizes_raise(fides, C):
     N = prm.N
     ctx.device_status(clear=True)
     z = np.full(N // 2, 1.0 + 0j)
-    ctx.encode(torch.from_numpy(z), 2.0 ** 62, 2)  # coefficients ~2^62 > q_0 / 2
+    ctx.encode(torch.from_numpy(z), 2.0 ** 66, 2)  # coefficients ~2^66 beyond the 2^62 limit
     assert ctx.device_status(clear=True) & 2
     ctx.encode(torch.from_numpy(z), 2.0 ** 40, 2)
     assert ctx.device_status(clear=True) == 0

@@ -70,7 +70,7 @@ def test_per_ciphertext_rotation_lists(env):
 def test_batch_of_32_ciphertexts_level_29(env):
     """Config C's largest batch: 32 ciphertexts at level 29, the 16 rotations each, in one
     launch sequence (the KSK pass groups the ciphertexts that share a key, so each key tile is
-    read once per group of 8).  Every output equals the single-ciphertext hoisted path; two
+    read once per group of 4).  Every output equals the single-ciphertext hoisted path; two
     ciphertexts are also checked against the oracle on three rotations."""
     F, prm, o, ctx, keys, keys_d = env
     host = [ct(F, prm, 29, 1700 + i) for i in range(32)]

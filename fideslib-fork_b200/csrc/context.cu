@@ -247,8 +247,8 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       for (size_t j = 0; j < (size_t)N; ++j) {
         tff[i * N + j] = make_double2((double)tf[i * N + j].w, (double)tf[i * N + j].w / qd);
         tfi[i * N + j] = make_double2((double)ti[i * N + j].w, (double)ti[i * N + j].w / qd);
-        twf_w[i * N + j] = (double)tf[i * N + j].w;
-        twi_w[i * N + j] = (double)ti[i * N + j].w;
+        twf_w[i * N + j] = (double)tf[i * N + j].w / qd;  // correctly rounded w / q
+        twi_w[i * N + j] = (double)ti[i * N + j].w / qd;
       }
       f64[i] = F64Prime{qd, 1.0 / qd, (double)d.ninv, (double)d.ninv / qd, (double)il[i].w, (double)il[i].w / qd};
     };

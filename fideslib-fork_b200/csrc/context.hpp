@@ -98,7 +98,7 @@ struct Context {
   ShoupConst* d_inv_last = nullptr;  // [n_q + K]: psi_rev^-1[1] * N^-1 (last GS stage)
   double2* d_twf_fwd = nullptr;      // [n_q + K][N]: (w, w / q) of d_tw_fwd as doubles (q < 2^50)
   double2* d_twf_inv = nullptr;      // [n_q + K][N]: the same for d_tw_inv
-  double* d_tww_fwd = nullptr;       // [n_q + K][N]: w alone (row passes derive w / q)
+  double* d_tww_fwd = nullptr;       // [n_q + K][N]: w / q alone, correctly rounded (row passes derive w)
   double* d_tww_inv = nullptr;
   F64Prime* d_f64 = nullptr;         // [n_q + K]
   ShoupConst* d_pinv = nullptr;      // [n_q]: P^-1 mod q_j

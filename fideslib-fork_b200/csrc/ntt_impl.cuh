@@ -128,8 +128,8 @@ struct PassArgs {
   const DevPrime* primes;
   const ShoupConst* tw;        // forward or inverse twiddles, [prime][N]
   const double2* twf;          // the same twiddles as (w, w / q) doubles (q < 2^50)
-  const double* tww;           // w alone: the row passes (one twiddle per row and stage each) read
-                               // half the bytes and derive w / q
+  const double* tww;           // w / q alone: the row passes (one twiddle per row and stage each)
+                               // read half the bytes and derive w
   const F64Prime* f64;         // [prime]
   const ShoupConst* inv_last;  // [prime]: psi_rev^-1[1] * N^-1
   const ShoupConst* pinv;      // [Q prime]: P^-1 mod q (OUT_MODDOWN)
@@ -224,10 +224,10 @@ __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int
       } else {
         double2 w;
         if constexpr (PASS == ROW) {
-          // w / q correctly rounded from w: a Newton step on fl(w / q) (exact residual by fma)
-          w.x = ld_tww(tww + base + hi, pol);
-          const double q0 = __dmul_rn(w.x, fp.qinv);
-          w.y = __fma_rn(__fma_rn(-q0, fp.q, w.x), fp.qinv, q0);
+          // w from the stored, correctly rounded w / q: (w / q) q lies within q 2^-54 < 1/2
+          // of the integer w, so one fma with the rounding constant recovers w exactly
+          w.y = ld_tww(tww + base + hi, pol);
+          w.x = __dadd_rn(__fma_rn(w.y, fp.q, F64_RND), -F64_RND);
         } else {
           w = ld_twf(tw + base + hi, pol);
         }
@@ -463,8 +463,10 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
     const F64Prime fp = a.f64[lr.prime];
     double xf[E];
     if (first_pass) {
+      // canonical inputs in [0, q): the first stage reduces (forward: the x operand, as on every
+      // even stage; inverse: every sum) and takes operands below q into its products
 #pragma unroll
-      for (int r = 0; r < E; ++r) xf[r] = f_reduce(f_from_u64(x[r]), fp.q, fp.qinv);  // inputs < 2^52
+      for (int r = 0; r < E; ++r) xf[r] = f_from_u64(x[r]);
     } else {
 #pragma unroll
       for (int r = 0; r < E; ++r) xf[r] = __longlong_as_double((long long)x[r]);  // the first pass's doubles

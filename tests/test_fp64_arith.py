@@ -6,7 +6,8 @@ fused multiply-add through rational arithmetic) on random and extreme operands, 
 with exact integer arithmetic:
 
 * the NTT butterfly product for primes below 2^50 (`f_mulmod`, `f_reduce`,
-  fideslib-fork_b200/csrc/ntt_impl.cuh) and the row passes' w / q from one Newton step;
+  fideslib-fork_b200/csrc/ntt_impl.cuh), the row passes' twiddle w recovered from its stored
+  w / q, and the first stage of a transform on uncentred inputs in [0, q);
 * the key-switch inner product's data x data product and final reduction (`ksk_mul_f64`,
   `ksk_canon_f64`, csrc/kernels.cu);
 * the tensor-core conversion's fold of eight s32 byte planes with a one-sided quotient
@@ -70,15 +71,42 @@ def test_ntt_fp64_butterfly_product_is_exact():
             assert (int(xr) - x) % q == 0 and abs(xr) <= q / 2 + 1
 
 
-def test_row_twiddle_quotient_is_correctly_rounded():
+def test_row_twiddle_recovered_from_quotient():
+    """Row passes store the correctly rounded w / q and recover w = fma(w / q, q, RND) - RND."""
     rng = random.Random(12)
-    for q in primes50():
+    for q in primes50() + [(1 << 50) - 27, 12289]:
+        qd = float(q)
+        ws = [rng.randrange(1, q) for _ in range(300)] + [1, 2, q - 1, q - 2, q // 2]
+        for w in ws:
+            wq = w / q  # correctly rounded, as the host builds the table
+            assert wq == float(Fraction(w, q))
+            assert fma(wq, qd, RND) - RND == float(w)
+
+
+def test_first_stage_on_uncentred_inputs():
+    """The first pass converts canonical residues in [0, q) without centring them: the
+    forward first stage reduces its x operand and multiplies y < q; the inverse first stage
+    reduces the sum (< 2q) and multiplies the difference (|d| < q).  Both stay exact and leave
+    the bounds the later stages assume (forward: |x +- r| <= 1.125 q + 1; inverse: q / 2 + 1)."""
+    rng = random.Random(13)
+    for q in primes50()[:4] + [(1 << 50) - 27]:
         qd, qinv = float(q), 1.0 / q
-        for _ in range(300):
-            w = float(rng.randrange(1, q))
-            q0 = w * qinv
-            wq = fma(fma(-q0, qd, w), qinv, q0)
-            assert wq == float(Fraction(int(w), q))
+        for it in range(300):
+            w = rng.randrange(1, q)
+            wq = w / q
+            x, y = rng.randrange(0, q), rng.randrange(0, q)
+            if it % 50 == 0:
+                x, y = q - 1, q - 1
+            # forward butterfly
+            a = f_reduce(float(x), qd, qinv)
+            r = f_mulmod(float(y), float(w), wq, qd)
+            for v, ref in ((a + r, x + y * w), (a - r, x - y * w)):
+                assert v == int(v) and (int(v) - ref) % q == 0 and abs(v) <= 1.125 * q + 1
+            # inverse butterfly
+            s0 = f_reduce(float(x) + float(y), qd, qinv)
+            s1 = f_mulmod(float(x) - float(y), float(w), wq, qd)
+            assert (int(s0) - (x + y)) % q == 0 and abs(s0) <= q / 2 + 1
+            assert (int(s1) - (x - y) * w) % q == 0 and abs(s1) <= q * (0.5 + q * 2.0 ** -53) + 1
 
 
 def ksk_mul_f64(a, b, q, qinv):

@@ -243,8 +243,6 @@ struct Bootstrapper {
   int top = 0, cts_out_level = 0, stc_in_level = 0, out_level = 0;
   double in_scale = 0, msg_scale = 0;
   double corr = 0;  // correction_bits > 0: round(q_1 / 2^correction_bits)
-  std::vector<cudaStream_t> lanes;  // streams of fides_bootstrap_batch
-  std::vector<cudaEvent_t> lane_ev;
   cudaStream_t own = nullptr;  // the prepared tables are allocated and freed on this stream
 
   ~Bootstrapper() {
@@ -256,8 +254,6 @@ struct Bootstrapper {
       cudaStreamSynchronize(own);
       cudaStreamDestroy(own);
     }
-    for (auto st : lanes) cudaStreamDestroy(st);
-    for (auto e : lane_ev) cudaEventDestroy(e);
   }
 
   // ---- BSGS plan of one composed matrix (the Python driver's _plan)
@@ -343,63 +339,82 @@ struct Bootstrapper {
     launch_addsub(c, &j, 1, s);
   }
 
-  boot::Ct add_raw(const boot::Ct& a, const boot::Ct& b, cudaStream_t s) const {
-    boot::Ct o = fresh(a.level, a.scale, s);
-    ew(EW_ADD, a.c0, b.c0, a.level, mut(o.c0), s);
-    ew(EW_ADD, a.c1, b.c1, a.level, mut(o.c1), s);
-    return o;
-  }
-  boot::Ct sub_raw(const boot::Ct& a, const boot::Ct& b, cudaStream_t s) const {
-    boot::Ct o = fresh(a.level, a.scale, s);
-    ew(EW_SUB, a.c0, b.c0, a.level, mut(o.c0), s);
-    ew(EW_SUB, a.c1, b.c1, a.level, mut(o.c1), s);
-    return o;
-  }
-  boot::Ct mul_plain_int(const boot::Ct& a, const boot::Buf& pt, cudaStream_t s) const {
-    boot::Ct o = fresh(a.level, a.scale, s);
-    ew(EW_MUL, a.c0, pt->u64(), a.level, mut(o.c0), s);
-    ew(EW_MUL, a.c1, pt->u64(), a.level, mut(o.c1), s);
-    return o;
-  }
-  boot::Ct mul_int(const boot::Ct& a, double v, cudaStream_t s) const {
-    if (a.level > MAX_SCALAR_LIMBS) throw Error(-1, "bootstrap: scalar product over more than 64 limbs");
-    boot::Ct o = fresh(a.level, a.scale, s);
-    for (int k = 0; k < 2; ++k) {
-      ScalarJob j{};
-      j.a = k ? a.c1 : a.c0;
-      j.out = mut(k ? o.c1 : o.c0);
-      j.l = a.level;
-      j.op = EW_MUL_SCALAR;
-      for (int i = 0; i < a.level; ++i) j.s[i] = residue(v, i);
-      launch_scalar(c, &j, 1, s);
+  // polynomial-wise op of every ciphertext of a batch with its partner (bs) or with one
+  // plaintext (pt), both polynomials of all of them in one launch
+  std::vector<boot::Ct> ew_many(int op, const std::vector<boot::Ct>& as, const std::vector<boot::Ct>* bs,
+                                const uint64_t* pt, cudaStream_t s) const {
+    std::vector<boot::Ct> outs;
+    std::vector<AddSubJob> jobs;
+    for (size_t i = 0; i < as.size(); ++i) {
+      const boot::Ct& a = as[i];
+      outs.push_back(fresh(a.level, a.scale, s));
+      const uint64_t* b0 = bs ? (*bs)[i].c0 : pt;
+      const uint64_t* b1 = bs ? (*bs)[i].c1 : pt;
+      jobs.push_back(AddSubJob{a.c0, b0, mut(outs.back().c0), a.level, op});
+      jobs.push_back(AddSubJob{a.c1, b1, mut(outs.back().c1), a.level, op});
     }
-    return o;
+    launch_addsub(c, jobs.data(), (int)jobs.size(), s);
+    return outs;
+  }
+  std::vector<boot::Ct> add_raw_many(const std::vector<boot::Ct>& as, const std::vector<boot::Ct>& bs,
+                                     cudaStream_t s) const {
+    return ew_many(EW_ADD, as, &bs, nullptr, s);
+  }
+  std::vector<boot::Ct> sub_raw_many(const std::vector<boot::Ct>& as, const std::vector<boot::Ct>& bs,
+                                     cudaStream_t s) const {
+    return ew_many(EW_SUB, as, &bs, nullptr, s);
+  }
+  std::vector<boot::Ct> mul_plain_int_many(const std::vector<boot::Ct>& as, const boot::Buf& pt,
+                                           cudaStream_t s) const {
+    return ew_many(EW_MUL, as, nullptr, pt->u64(), s);
+  }
+  std::vector<boot::Ct> mul_int_many(const std::vector<boot::Ct>& as, double v, cudaStream_t s) const {
+    std::vector<boot::Ct> outs;
+    std::vector<ScalarJob> jobs;
+    for (const auto& a : as) {
+      if (a.level > MAX_SCALAR_LIMBS) throw Error(-1, "bootstrap: scalar product over more than 64 limbs");
+      outs.push_back(fresh(a.level, a.scale, s));
+      for (int k = 0; k < 2; ++k) {
+        ScalarJob j{};
+        j.a = k ? a.c1 : a.c0;
+        j.out = mut(k ? outs.back().c1 : outs.back().c0);
+        j.l = a.level;
+        j.op = EW_MUL_SCALAR;
+        for (int i = 0; i < a.level; ++i) j.s[i] = residue(v, i);
+        jobs.push_back(j);
+      }
+    }
+    launch_scalar(c, jobs.data(), (int)jobs.size(), s);
+    return outs;
   }
 
   // the same integer combination of every lane (one launch): sum_t ints[t] lane[t] (+ add on c0)
   // ints / add: integers held exactly in doubles (see rint_even)
   std::vector<boot::Ct> lincomb_lanes(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& ints,
                                       const double* add, int level, double scale, cudaStream_t s) const {
-    if (lanes.empty() || lanes.size() > (size_t)MAX_LC_LANES || ints.empty() || ints.size() > (size_t)MAX_LC_TERMS)
+    if (lanes.empty() || ints.empty() || ints.size() > (size_t)MAX_LC_TERMS)
       throw Error(-1, "bootstrap: linear combination out of range");
     static thread_local LinCombJob j;
-    std::vector<boot::Ct> outs;
-    for (size_t a = 0; a < lanes.size(); ++a) {
-      outs.push_back(fresh(level, scale, s));
-      j.out0[a] = mut(outs.back().c0);
-      j.out1[a] = mut(outs.back().c1);
-      for (size_t t = 0; t < ints.size(); ++t) {
-        j.x0[a][t] = lanes[a][t].c0;
-        j.x1[a][t] = lanes[a][t].c1;
-      }
-    }
     for (size_t t = 0; t < ints.size(); ++t)
       for (int i = 0; i < level; ++i) j.s[t][i] = residue(ints[t], i);
     for (int i = 0; i < level; ++i) j.add0[i] = add ? residue(*add, i) : 0;
     j.n = (int)ints.size();
     j.l = level;
-    j.lanes = (int)lanes.size();
-    launch_lincomb(c, j, s);
+    std::vector<boot::Ct> outs;
+    for (size_t a0 = 0; a0 < lanes.size(); a0 += MAX_LC_LANES) {  // lanes in launches of up to 8
+      const size_t m = std::min<size_t>(MAX_LC_LANES, lanes.size() - a0);
+      for (size_t a = 0; a < m; ++a) {
+        outs.push_back(fresh(level, scale, s));
+        j.out0[a] = mut(outs.back().c0);
+        j.out1[a] = mut(outs.back().c1);
+        for (size_t t = 0; t < ints.size(); ++t) {
+          j.x0[a][t] = lanes[a0 + a][t].c0;
+          j.x1[a][t] = lanes[a0 + a][t].c1;
+        }
+      }
+      j.lanes = (int)m;
+      launch_lincomb(c, j, s);
+    }
     return outs;
   }
 
@@ -449,7 +464,6 @@ struct Bootstrapper {
     for (const auto& b : cts_) lanes.push_back({drop(b, level + 1)});
     return rescale_many_to(lincomb_many(lanes, {k}, 0.0, s), S[level], s);
   }
-  boot::Ct to_level(const boot::Ct& a, int level, cudaStream_t s) const { return to_level_many({a}, level, s)[0]; }
 
   std::vector<boot::Ct> lincomb_to_many(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& coefs,
                                         double cst, int target, cudaStream_t s) const {
@@ -480,12 +494,41 @@ struct Bootstrapper {
     return rescale_many_to(outs, St, s);
   }
 
-  std::vector<boot::Ct> mul_many(const std::vector<std::pair<boot::Ct, boot::Ct>>& pairs, cudaStream_t s) const {
-    std::vector<std::pair<boot::Ct, boot::Ct>> ab;
-    for (const auto& [a, b] : pairs) {
-      const int l = std::min(a.level, b.level);
-      ab.push_back({to_level(a, l, s), to_level(b, l, s)});
+  // to_level of every operand, batched: operands sharing (level, scale, target) are brought
+  // down together (lanes of a batch run the same computation, so they share all three)
+  std::vector<boot::Ct> to_levels(const std::vector<boot::Ct>& xs, const std::vector<int>& targets,
+                                  cudaStream_t s) const {
+    std::vector<boot::Ct> out(xs.size());
+    std::vector<bool> done(xs.size(), false);
+    for (size_t i = 0; i < xs.size(); ++i) {
+      if (done[i]) continue;
+      std::vector<size_t> grp;
+      for (size_t k = i; k < xs.size(); ++k)
+        if (!done[k] && xs[k].level == xs[i].level && xs[k].scale == xs[i].scale && targets[k] == targets[i])
+          grp.push_back(k);
+      std::vector<boot::Ct> in;
+      for (size_t k : grp) in.push_back(xs[k]);
+      const std::vector<boot::Ct> r = to_level_many(in, targets[i], s);
+      for (size_t m = 0; m < grp.size(); ++m) {
+        out[grp[m]] = r[m];
+        done[grp[m]] = true;
+      }
     }
+    return out;
+  }
+
+  std::vector<boot::Ct> mul_many(const std::vector<std::pair<boot::Ct, boot::Ct>>& pairs, cudaStream_t s) const {
+    std::vector<boot::Ct> as, bs;
+    std::vector<int> ls;
+    for (const auto& [a, b] : pairs) {
+      as.push_back(a);
+      bs.push_back(b);
+      ls.push_back(std::min(a.level, b.level));
+    }
+    as = to_levels(as, ls, s);
+    bs = to_levels(bs, ls, s);
+    std::vector<std::pair<boot::Ct, boot::Ct>> ab;
+    for (size_t i = 0; i < pairs.size(); ++i) ab.push_back({as[i], bs[i]});
     std::vector<HMultItem> items;
     std::vector<boot::Ct> outs;
     for (const auto& [a, b] : ab) {
@@ -496,11 +539,16 @@ struct Bootstrapper {
     return outs;
   }
 
-  boot::Ct conjugate(const boot::Ct& a, cudaStream_t s) const {
-    boot::Ct o = fresh(a.level, a.scale, s);
-    RotateItem it{a.c0, a.c1, mut(o.c0), mut(o.c1), conj, a.level, (uint32_t)(2 * c->N - 1)};
-    op_rotate_batch(c, &it, 1, s);
-    return o;
+  std::vector<boot::Ct> conjugate_many(const std::vector<boot::Ct>& as, cudaStream_t s) const {
+    std::vector<RotateItem> items;
+    std::vector<boot::Ct> outs;
+    for (const auto& a : as) {
+      outs.push_back(fresh(a.level, a.scale, s));
+      items.push_back(RotateItem{a.c0, a.c1, mut(outs.back().c0), mut(outs.back().c1), conj, a.level,
+                                 (uint32_t)(2 * c->N - 1)});
+    }
+    op_rotate_batch(c, items.data(), (int)items.size(), s);
+    return outs;
   }
 
   const uint64_t* rot_key(int r) const {
@@ -509,25 +557,31 @@ struct Bootstrapper {
     return it->second;
   }
 
-  std::vector<boot::Ct> rotate_many(const boot::Ct& a, const std::vector<int>& rs, cudaStream_t s) const {
-    HoistItem it;
-    it.c0 = a.c0;
-    it.c1 = a.c1;
-    it.l = a.level;
-    std::vector<int> idx;
-    std::vector<boot::Ct> res(rs.size());
-    for (size_t k = 0; k < rs.size(); ++k) {
-      if (boot::pymod(rs[k], n) == 0) {
-        res[k] = a;
-        continue;
+  // hoisted rotations of every ciphertext of a batch by the same list rs (one ModUp each, the
+  // key-switch inner products of all of them grouped by key): res[b][k] = rotate(as[b], rs[k])
+  std::vector<std::vector<boot::Ct>> rotate_many(const std::vector<boot::Ct>& as, const std::vector<int>& rs,
+                                                 cudaStream_t s) const {
+    std::vector<HoistItem> items(as.size());
+    std::vector<std::vector<boot::Ct>> res(as.size(), std::vector<boot::Ct>(rs.size()));
+    for (size_t b = 0; b < as.size(); ++b) {
+      const boot::Ct& a = as[b];
+      HoistItem& it = items[b];
+      it.c0 = a.c0;
+      it.c1 = a.c1;
+      it.l = a.level;
+      for (size_t k = 0; k < rs.size(); ++k) {
+        if (boot::pymod(rs[k], n) == 0) {
+          res[b][k] = a;
+          continue;
+        }
+        res[b][k] = fresh(a.level, a.scale, s);
+        it.keys.push_back(rot_key(rs[k]));
+        it.ks.push_back(h_auto_index(c->logN, rs[k]));
+        it.out0.push_back(mut(res[b][k].c0));
+        it.out1.push_back(mut(res[b][k].c1));
       }
-      res[k] = fresh(a.level, a.scale, s);
-      it.keys.push_back(rot_key(rs[k]));
-      it.ks.push_back(h_auto_index(c->logN, rs[k]));
-      it.out0.push_back(mut(res[k].c0));
-      it.out1.push_back(mut(res[k].c1));
     }
-    if (!it.keys.empty()) op_hoisted_batch(c, &it, 1, s);
+    if (!items.empty() && !items[0].keys.empty()) op_hoisted_batch(c, items.data(), (int)items.size(), s);
     return res;
   }
 
@@ -543,15 +597,18 @@ struct Bootstrapper {
     return outs;
   }
 
-  boot::Ct keyswitch_add(const boot::Ct& a, const uint64_t* key, cudaStream_t s) const {
-    boot::Ct f = fresh(a.level, a.scale, s);
-    KeySwitchItem it{a.c1, a.level, key, mut(f.c0), mut(f.c1)};
-    op_keyswitch_batch(c, &it, 1, s);
-    boot::Ct o = fresh(a.level, a.scale, s);
-    ew(EW_ADD, a.c0, f.c0, a.level, mut(o.c0), s);
-    o.c1 = f.c1;
-    o.b1 = f.b1;
-    return o;
+  // (c0, c1) -> (c0 + ks(c1)_0, ks(c1)_1) for every ciphertext of a batch, one key (the c0
+  // addition is the ModDown epilogue's addend)
+  std::vector<boot::Ct> keyswitch_add_many(const std::vector<boot::Ct>& as, const uint64_t* key,
+                                           cudaStream_t s) const {
+    std::vector<boot::Ct> outs;
+    std::vector<KeySwitchItem> items;
+    for (const auto& a : as) {
+      outs.push_back(fresh(a.level, a.scale, s));
+      items.push_back(KeySwitchItem{a.c1, a.level, key, mut(outs.back().c0), mut(outs.back().c1), a.c0, nullptr});
+    }
+    op_keyswitch_batch(c, items.data(), (int)items.size(), s);
+    return outs;
   }
 
   // ---------------------------------------------------------------- preparation
@@ -652,66 +709,92 @@ struct Bootstrapper {
   }
 
   // ---------------------------------------------------------------- the linear transforms
-  boot::Ct apply(const boot::Ct& a, const boot::Plan& P, cudaStream_t s) const {
-    if (a.level != P.level) throw Error(-4, "bootstrap: linear transform at the wrong level");
-    const int g = prm.baby;
+  // One BSGS linear transform applied to every ciphertext of a batch: the baby-step rotations
+  // of all of them in one hoisted batch, each giant step's plaintext inner products in one
+  // launch (the diagonals shared by the lanes), all giant-step rotations in one batched key
+  // switch, the sums and the rescale batched.
+  std::vector<boot::Ct> apply_many(const std::vector<boot::Ct>& as, const boot::Plan& P, cudaStream_t s) const {
+    const size_t B = as.size();
+    for (const auto& a : as)
+      if (a.level != P.level) throw Error(-4, "bootstrap: linear transform at the wrong level");
+    const int g = prm.baby, level = as[0].level;
+    const double scale = as[0].scale;
     std::set<int> jset;
     for (const auto& kv : P.giant)
       for (int j : kv.second) jset.insert(j);
     std::vector<int> js(jset.begin(), jset.end()), rs;
     for (int j : js) rs.push_back((int)boot::pymod((long)P.step * j, n));
-    const std::vector<boot::Ct> bv = rotate_many(a, rs, s);
-    std::map<int, boot::Ct> baby;
-    for (size_t k = 0; k < js.size(); ++k) baby[js[k]] = bv[k];
-    std::vector<boot::Ct> parts;
+    const std::vector<std::vector<boot::Ct>> bv = rotate_many(as, rs, s);  // [b][index in js]
+    std::map<int, size_t> jpos;
+    for (size_t k = 0; k < js.size(); ++k) jpos[js[k]] = k;
+    std::vector<std::vector<boot::Ct>> parts(B);
     std::vector<std::pair<boot::Ct, int>> turns;
+    std::vector<size_t> owner;
     for (const auto& [i, jl] : P.giant) {
-      std::vector<std::pair<boot::Ct, boot::Buf>> terms;
+      std::vector<std::pair<int, boot::Buf>> terms;  // (baby index, diagonal)
       for (int j : jl) {
         auto it = P.pts.find({i, j});
-        if (it != P.pts.end()) terms.push_back({baby[j], it->second});
+        if (it != P.pts.end()) terms.push_back({j, it->second});
       }
       if (terms.empty()) continue;
-      boot::Ct inner;
+      std::vector<boot::Ct> inner(B);
       bool have = false;
       for (size_t k = 0; k < terms.size(); k += MAX_DOT_TERMS) {
         const size_t m = std::min<size_t>(MAX_DOT_TERMS, terms.size() - k);
-        boot::Ct d = fresh(a.level, a.scale, s);
-        DotJob j{};
-        for (size_t t = 0; t < m; ++t) {
-          j.c0[t] = terms[k + t].first.c0;
-          j.c1[t] = terms[k + t].first.c1;
-          j.pt[t] = terms[k + t].second->u64();
+        std::vector<boot::Ct> d(B);
+        for (size_t b0 = 0; b0 < B; b0 += MAX_DOT_LANES) {
+          const size_t nl = std::min<size_t>(MAX_DOT_LANES, B - b0);
+          DotJob dj{};
+          for (size_t t = 0; t < m; ++t) dj.pt[t] = terms[k + t].second->u64();
+          for (size_t ln = 0; ln < nl; ++ln) {
+            const size_t b = b0 + ln;
+            d[b] = fresh(level, scale, s);
+            for (size_t t = 0; t < m; ++t) {
+              const boot::Ct& x = bv[b][jpos.at(terms[k + t].first)];
+              dj.c0[ln][t] = x.c0;
+              dj.c1[ln][t] = x.c1;
+            }
+            dj.out0[ln] = mut(d[b].c0);
+            dj.out1[ln] = mut(d[b].c1);
+          }
+          dj.n = (int)m;
+          dj.l = level;
+          dj.lanes = (int)nl;
+          launch_dot_plain(c, dj, s);
         }
-        j.out0 = mut(d.c0);
-        j.out1 = mut(d.c1);
-        j.n = (int)m;
-        j.l = a.level;
-        launch_dot_plain(c, j, s);
-        inner = have ? add_many({inner}, {d}, s)[0] : d;
+        inner = have ? add_many(inner, d, s) : d;
         have = true;
       }
       const int r = (int)boot::pymod((long)P.step * g * i, n);
-      if (r)
-        turns.push_back({inner, r});
-      else
-        parts.push_back(inner);
-    }
-    for (auto& o : rotate_batch(turns, s)) parts.push_back(o);
-    while (parts.size() > 1) {
-      std::vector<boot::Ct> next;
-      for (size_t k = 0; k < parts.size(); k += 16) {
-        const size_t m = std::min<size_t>(16, parts.size() - k);
-        if (m > 1) {
-          std::vector<boot::Ct> grp(parts.begin() + k, parts.begin() + k + m);
-          next.push_back(lincomb_many({grp}, std::vector<double>(m, 1.0), 0.0, s)[0]);
+      for (size_t b = 0; b < B; ++b) {
+        if (r) {
+          turns.push_back({inner[b], r});
+          owner.push_back(b);
         } else {
-          next.push_back(parts[k]);
+          parts[b].push_back(inner[b]);
+        }
+      }
+    }
+    const std::vector<boot::Ct> turned = rotate_batch(turns, s);
+    for (size_t k = 0; k < turned.size(); ++k) parts[owner[k]].push_back(turned[k]);
+    while (parts[0].size() > 1) {  // every ciphertext has the same number of parts
+      std::vector<std::vector<boot::Ct>> next(B);
+      for (size_t k = 0; k < parts[0].size(); k += 16) {
+        const size_t m = std::min<size_t>(16, parts[0].size() - k);
+        if (m > 1) {
+          std::vector<std::vector<boot::Ct>> lanes(B);
+          for (size_t b = 0; b < B; ++b) lanes[b].assign(parts[b].begin() + k, parts[b].begin() + k + m);
+          const auto sums = lincomb_many(lanes, std::vector<double>(m, 1.0), 0.0, s);
+          for (size_t b = 0; b < B; ++b) next[b].push_back(sums[b]);
+        } else {
+          for (size_t b = 0; b < B; ++b) next[b].push_back(parts[b][k]);
         }
       }
       parts = next;
     }
-    return rescale_many_to({parts[0]}, S[a.level - 1], s)[0];
+    std::vector<boot::Ct> sums;
+    for (size_t b = 0; b < B; ++b) sums.push_back(parts[b][0]);
+    return rescale_many_to(sums, S[level - 1], s);
   }
 
   // ---------------------------------------------------------------- EvalMod
@@ -801,44 +884,67 @@ struct Bootstrapper {
   }
 
   // ---------------------------------------------------------------- the bootstrap
-  boot::Ct run(const uint64_t* c0, const uint64_t* c1, cudaStream_t s) const {
+  // Bootstraps a batch of level-1 ciphertexts (c0s[b], c1s[b]) together: every step is one
+  // launch sequence over the whole batch (EvalMod runs 2 x batch lanes: the real and imaginary
+  // halves of each ciphertext).  Each ciphertext's arithmetic is the same as alone.
+  std::vector<boot::Ct> run_many(const std::vector<const uint64_t*>& c0s, const std::vector<const uint64_t*>& c1s,
+                                 cudaStream_t s) const {
     if (!prepared) throw Error(-7, "bootstrap: fides_boot_prepare has not run");
     if (!relin || !conj) throw Error(-5, "bootstrap: relinearization / conjugation key not set");
-    boot::Ct x;
-    x.c0 = c0;
-    x.c1 = c1;
-    x.level = 1;
-    x.scale = prm.msg_scale;
+    const size_t B = c0s.size();
+    std::vector<boot::Ct> x(B);
+    for (size_t b = 0; b < B; ++b) {
+      x[b].c0 = c0s[b];
+      x[b].c1 = c1s[b];
+      x[b].level = 1;
+      x[b].scale = prm.msg_scale;
+    }
     if (prm.correction_bits > 0) {  // scale down by ~2^k: times round(q_1 / 2^k) at level 2, rescale by q_1
-      x.level = 2;
-      x = rescale_many_to({mul_int(x, corr, s)}, x.scale * corr / (double)c->primes[1], s)[0];
+      for (auto& v : x) v.level = 2;
+      x = rescale_many_to(mul_int_many(x, corr, s), x[0].scale * corr / (double)c->primes[1], s);
     }
     if (prm.sparse_encapsulation) {
       if (!to_sparse || !to_dense) throw Error(-5, "bootstrap: encapsulation keys not set");
-      x = keyswitch_add(x, to_sparse, s);  // dense -> sparse secret, at level 1
+      x = keyswitch_add_many(x, to_sparse, s);  // dense -> sparse secret, at level 1
     }
-    if (prm.prescale_bits) x = mul_int(x, (double)(1ll << prm.prescale_bits), s);
-    boot::Ct a = fresh(top, in_scale, s);  // ModRaise: m -> m + q0 I on every limb of the top level
-    op_mod_raise(c, x.c0, top, mut(a.c0), s);
-    op_mod_raise(c, x.c1, top, mut(a.c1), s);
-    if (prm.sparse_encapsulation) a = keyswitch_add(a, to_dense, s);  // back to the dense secret
-    for (const auto& P : cts_pl) a = apply(a, P, s);
-    const boot::Ct cj = conjugate(a, s);
-    const boot::Ct t_re = add_raw(a, cj, s);
-    const boot::Ct t_im = mul_plain_int(sub_raw(a, cj, s), pt_minus_i, s);
-    auto sm = eval_mod_many({t_re, t_im}, s);
-    const boot::Ct s_re = to_level(sm[0], stc_in_level, s);
-    const boot::Ct s_im = to_level(sm[1], stc_in_level, s);
-    boot::Ct u = add_raw(s_re, mul_plain_int(s_im, pt_i, s), s);
-    for (const auto& P : stc_pl) u = apply(u, P, s);
+    if (prm.prescale_bits) x = mul_int_many(x, (double)(1ll << prm.prescale_bits), s);
+    std::vector<boot::Ct> a;
+    for (size_t b = 0; b < B; ++b) {  // ModRaise: m -> m + q0 I on every limb of the top level
+      a.push_back(fresh(top, in_scale, s));
+      op_mod_raise(c, x[b].c0, top, mut(a.back().c0), s);
+      op_mod_raise(c, x[b].c1, top, mut(a.back().c1), s);
+    }
+    if (prm.sparse_encapsulation) a = keyswitch_add_many(a, to_dense, s);  // back to the dense secret
+    for (const auto& P : cts_pl) a = apply_many(a, P, s);
+    const std::vector<boot::Ct> cj = conjugate_many(a, s);
+    const std::vector<boot::Ct> t_re = add_raw_many(a, cj, s);
+    const std::vector<boot::Ct> t_im = mul_plain_int_many(sub_raw_many(a, cj, s), pt_minus_i, s);
+    std::vector<boot::Ct> ts;
+    for (size_t b = 0; b < B; ++b) {
+      ts.push_back(t_re[b]);
+      ts.push_back(t_im[b]);
+    }
+    const std::vector<boot::Ct> sm = eval_mod_many(ts, s);
+    std::vector<boot::Ct> sre, sim;
+    for (size_t b = 0; b < B; ++b) {
+      sre.push_back(sm[2 * b]);
+      sim.push_back(sm[2 * b + 1]);
+    }
+    sre = to_level_many(sre, stc_in_level, s);
+    sim = to_level_many(sim, stc_in_level, s);
+    std::vector<boot::Ct> u = add_raw_many(sre, mul_plain_int_many(sim, pt_i, s), s);
+    for (const auto& P : stc_pl) u = apply_many(u, P, s);
     return u;
   }
 
-  void run_into(const uint64_t* c0, const uint64_t* c1, uint64_t* o0, uint64_t* o1, cudaStream_t s) const {
-    const boot::Ct u = run(c0, c1, s);
-    const size_t bytes = sizeof(uint64_t) * (size_t)c->N * u.level;
-    FIDES_CUDA(cudaMemcpyAsync(o0, u.c0, bytes, cudaMemcpyDeviceToDevice, s));
-    FIDES_CUDA(cudaMemcpyAsync(o1, u.c1, bytes, cudaMemcpyDeviceToDevice, s));
+  void run_into(const std::vector<const uint64_t*>& c0s, const std::vector<const uint64_t*>& c1s,
+                const std::vector<uint64_t*>& o0s, const std::vector<uint64_t*>& o1s, cudaStream_t s) const {
+    const std::vector<boot::Ct> us = run_many(c0s, c1s, s);
+    for (size_t b = 0; b < us.size(); ++b) {
+      const size_t bytes = sizeof(uint64_t) * (size_t)c->N * us[b].level;
+      FIDES_CUDA(cudaMemcpyAsync(o0s[b], us[b].c0, bytes, cudaMemcpyDeviceToDevice, s));
+      FIDES_CUDA(cudaMemcpyAsync(o1s[b], us[b].c1, bytes, cudaMemcpyDeviceToDevice, s));
+    }
   }
 };
 
@@ -970,7 +1076,7 @@ int fides_bootstrap(fides_boot* b, const uint64_t* c0, const uint64_t* c1, uint6
   return bguard(__func__, [&] {
     auto* bs = B(b);
     if (!c0 || !c1 || !out0 || !out1) throw fides::Error(FIDES_ERR_ARG, "null polynomial pointer");
-    bs->run_into(c0, c1, out0, out1, static_cast<cudaStream_t>(stream));
+    bs->run_into({c0}, {c1}, {out0}, {out1}, static_cast<cudaStream_t>(stream));
   });
 }
 
@@ -981,27 +1087,21 @@ int fides_bootstrap_batch(fides_boot* b, int n, const uint64_t* const* c0s, cons
     if (n < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
     if (n == 0) return;
     if (!c0s || !c1s || !out0s || !out1s) throw fides::Error(FIDES_ERR_ARG, "null pointer array");
-    cudaStream_t main = static_cast<cudaStream_t>(stream);
-    while ((int)bs->lanes.size() < n) {
-      cudaStream_t s;
-      cudaEvent_t e;
-      FIDES_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-      FIDES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      bs->lanes.push_back(s);
-      bs->lane_ev.push_back(e);
-    }
-    // fork: every lane waits for the caller's stream; join: the caller's stream waits for every
-    // lane (one graph with a parallel branch per ciphertext when captured)
-    cudaEvent_t fork = bs->lane_ev[0];
-    FIDES_CUDA(cudaEventRecord(fork, main));
-    for (int i = 0; i < n; ++i) FIDES_CUDA(cudaStreamWaitEvent(bs->lanes[i], fork, 0));
-    for (int i = 0; i < n; ++i) {
-      if (!c0s[i] || !c1s[i] || !out0s[i] || !out1s[i]) throw fides::Error(FIDES_ERR_ARG, "null polynomial pointer");
-      bs->run_into(c0s[i], c1s[i], out0s[i], out1s[i], bs->lanes[i]);
-    }
-    for (int i = 0; i < n; ++i) {
-      FIDES_CUDA(cudaEventRecord(bs->lane_ev[i], bs->lanes[i]));
-      FIDES_CUDA(cudaStreamWaitEvent(main, bs->lane_ev[i], 0));
+    // batches of up to 16 ciphertexts through one launch sequence each (bounds the memory of
+    // the hoisted rotations' extended-basis intermediates)
+    constexpr int kChunk = 16;
+    for (int i0 = 0; i0 < n; i0 += kChunk) {
+      const int m = std::min(kChunk, n - i0);
+      std::vector<const uint64_t*> a0, a1;
+      std::vector<uint64_t*> o0, o1;
+      for (int i = i0; i < i0 + m; ++i) {
+        if (!c0s[i] || !c1s[i] || !out0s[i] || !out1s[i]) throw fides::Error(FIDES_ERR_ARG, "null polynomial pointer");
+        a0.push_back(c0s[i]);
+        a1.push_back(c1s[i]);
+        o0.push_back(out0s[i]);
+        o1.push_back(out1s[i]);
+      }
+      bs->run_into(a0, a1, o0, o1, static_cast<cudaStream_t>(stream));
     }
   });
 }

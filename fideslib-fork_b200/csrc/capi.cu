@@ -401,14 +401,15 @@ int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* co
       need(c0s[t], "c0s[t]");
       need(c1s[t], "c1s[t]");
       need(pts[t], "pts[t]");
-      j.c0[t] = c0s[t];
-      j.c1[t] = c1s[t];
+      j.c0[0][t] = c0s[t];
+      j.c1[0][t] = c1s[t];
       j.pt[t] = pts[t];
     }
-    j.out0 = out0;
-    j.out1 = out1;
+    j.out0[0] = out0;
+    j.out1[0] = out1;
     j.n = n_terms;
     j.l = level;
+    j.lanes = 1;
     fides::launch_dot_plain(c, j, S(stream));
   });
 }

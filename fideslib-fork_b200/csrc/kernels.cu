@@ -424,9 +424,9 @@ __global__ void __launch_bounds__(EW_THREADS) scalar_kernel(const __grid_constan
 // 2^128 before a reduction.
 __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_constant__ DotJob J,
                                                                const DevPrime* primes, int logN) {
-  const int j = blockIdx.y;
+  const int lane = blockIdx.x, j = blockIdx.z;
   const DevPrime p = primes[j];
-  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const size_t off = ((size_t)j << logN) + 2 * (blockIdx.y * blockDim.x + threadIdx.x);
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
   for (int t = 0; t < J.n; ++t) {
@@ -436,14 +436,14 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
       b0 = U128{reduce128(b0, p), 0};
       b1 = U128{reduce128(b1, p), 0};
     }
-    const ulonglong2 w = ld2(J.pt[t] + off), x = ld2(J.c0[t] + off), y = ld2(J.c1[t] + off);
+    const ulonglong2 w = ld2(J.pt[t] + off), x = ld2(J.c0[lane][t] + off), y = ld2(J.c1[lane][t] + off);
     mac128(a0, w.x, x.x);
     mac128(a1, w.y, x.y);
     mac128(b0, w.x, y.x);
     mac128(b1, w.y, y.y);
   }
-  *reinterpret_cast<ulonglong2*>(J.out0 + off) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
-  *reinterpret_cast<ulonglong2*>(J.out1 + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
+  *reinterpret_cast<ulonglong2*>(J.out0[lane] + off) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
+  *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
 }
 
 __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
@@ -551,8 +551,9 @@ void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
 
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s) {
   if (job.n < 1 || job.n > MAX_DOT_TERMS) throw Error(-1, "dot product needs 1..32 terms");
-  dim3 grid(c->N / (2 * EW_THREADS), job.l);
-  LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (3.0 * job.n + 2));
+  if (job.lanes < 1 || job.lanes > MAX_DOT_LANES) throw Error(-1, "dot product needs 1..8 lanes");
+  dim3 grid(job.lanes, c->N / (2 * EW_THREADS), job.l);
+  LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (job.n + job.lanes * (2.0 * job.n + 2)));
   dot_plain_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
   FIDES_CUDA(cudaGetLastError());
 }

@@ -151,14 +151,18 @@ void launch_scalar(Context* c, const ScalarJob* jobs, int n, cudaStream_t s);
 // (LTdotProductPtBatch / dotProductLtBatchedPt___, LimbPartitionBatch.cu:266,
 // ElemenwiseBatchKernels.cu:682-1106): out_k = sum_t pt_t * c_k,t mod q, k = 0, 1, with
 // 128-bit accumulation, one launch per giant step instead of two products and two sums per
-// diagonal.
+// diagonal.  Up to MAX_DOT_LANES ciphertexts (lanes) share the plaintext diagonals: the
+// lanes of one (limb, coefficient tile) are adjacent CTAs, so each diagonal tile is read from
+// DRAM once per launch and from L2 by the other lanes.
 constexpr int MAX_DOT_TERMS = 32;
+constexpr int MAX_DOT_LANES = 8;
 struct DotJob {
-  const uint64_t* c0[MAX_DOT_TERMS];
-  const uint64_t* c1[MAX_DOT_TERMS];
+  const uint64_t* c0[MAX_DOT_LANES][MAX_DOT_TERMS];
+  const uint64_t* c1[MAX_DOT_LANES][MAX_DOT_TERMS];
   const uint64_t* pt[MAX_DOT_TERMS];
-  uint64_t *out0, *out1;
-  int n, l;
+  uint64_t* out0[MAX_DOT_LANES];
+  uint64_t* out1[MAX_DOT_LANES];
+  int n, l, lanes;
 };
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 

@@ -472,10 +472,11 @@ int fides_boot_levels(const fides_boot* b, int* out_level, double* out_scale);
  * (out_level limbs each) on `stream`. */
 int fides_bootstrap(fides_boot* b, const uint64_t* c0, const uint64_t* c1, uint64_t* out0, uint64_t* out1,
                     void* stream);
-/* n bootstraps at once, each on its own internal stream forked from and joined back to
- * `stream` (one CUDA graph with a parallel branch per ciphertext when captured).  Results equal
- * fides_bootstrap's, ciphertext by ciphertext.  No reference counterpart (the reference
- * bootstraps one ciphertext per call). */
+/* n bootstraps at once on `stream`: up to 16 ciphertexts go through one launch sequence
+ * together (every hoisted rotation, key switch, HMult, plaintext inner product, linear
+ * combination and rescale of the batch in the same launches, EvalMod on 2 x 16 lanes).
+ * Results equal fides_bootstrap's, ciphertext by ciphertext.  No reference counterpart (the
+ * reference bootstraps one ciphertext per call). */
 int fides_bootstrap_batch(fides_boot* b, int n, const uint64_t* const* c0s, const uint64_t* const* c1s,
                           uint64_t* const* out0s, uint64_t* const* out1s, void* stream);
 /* The derived tables, for inspection and comparison: the Chebyshev coefficients (returns the

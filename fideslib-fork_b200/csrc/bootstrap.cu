@@ -727,51 +727,85 @@ struct Bootstrapper {
     const std::vector<std::vector<boot::Ct>> bv = rotate_many(as, rs, s);  // [b][index in js]
     std::map<int, size_t> jpos;
     for (size_t k = 0; k < js.size(); ++k) jpos[js[k]] = k;
-    std::vector<std::vector<boot::Ct>> parts(B);
-    std::vector<std::pair<boot::Ct, int>> turns;
-    std::vector<size_t> owner;
+    // the giant steps that have terms, with their (baby index, diagonal) pairs
+    std::vector<std::pair<int, std::vector<std::pair<int, boot::Buf>>>> gs;
     for (const auto& [i, jl] : P.giant) {
-      std::vector<std::pair<int, boot::Buf>> terms;  // (baby index, diagonal)
+      std::vector<std::pair<int, boot::Buf>> terms;
       for (int j : jl) {
         auto it = P.pts.find({i, j});
         if (it != P.pts.end()) terms.push_back({j, it->second});
       }
-      if (terms.empty()) continue;
-      std::vector<boot::Ct> inner(B);
-      bool have = false;
-      for (size_t k = 0; k < terms.size(); k += MAX_DOT_TERMS) {
-        const size_t m = std::min<size_t>(MAX_DOT_TERMS, terms.size() - k);
-        std::vector<boot::Ct> d(B);
-        for (size_t b0 = 0; b0 < B; b0 += MAX_DOT_LANES) {
-          const size_t nl = std::min<size_t>(MAX_DOT_LANES, B - b0);
-          DotJob dj{};
-          for (size_t t = 0; t < m; ++t) dj.pt[t] = terms[k + t].second->u64();
-          for (size_t ln = 0; ln < nl; ++ln) {
-            const size_t b = b0 + ln;
-            d[b] = fresh(level, scale, s);
-            for (size_t t = 0; t < m; ++t) {
-              const boot::Ct& x = bv[b][jpos.at(terms[k + t].first)];
-              dj.c0[ln][t] = x.c0;
-              dj.c1[ln][t] = x.c1;
-            }
-            dj.out0[ln] = mut(d[b].c0);
-            dj.out1[ln] = mut(d[b].c1);
+      if (!terms.empty()) gs.push_back({i, terms});
+    }
+    std::vector<std::vector<boot::Ct>> inner(gs.size(), std::vector<boot::Ct>(B));  // [giant step][b]
+    if (js.size() <= (size_t)MAX_BSGS_BABY && gs.size() <= (size_t)MAX_BSGS_GIANT) {
+      // every giant step's inner product in one launch per 8 ciphertexts
+      for (size_t b0 = 0; b0 < B; b0 += MAX_BSGS_LANES) {
+        const size_t nl = std::min<size_t>(MAX_BSGS_LANES, B - b0);
+        BsgsJob bj{};
+        bj.nb = (int)js.size();
+        bj.ng = (int)gs.size();
+        bj.l = level;
+        bj.lanes = (int)nl;
+        for (size_t gi = 0; gi < gs.size(); ++gi)
+          for (const auto& [j, pt] : gs[gi].second) bj.pt[gi][jpos.at(j)] = pt->u64();
+        for (size_t ln = 0; ln < nl; ++ln) {
+          const size_t b = b0 + ln;
+          for (size_t k = 0; k < js.size(); ++k) {
+            bj.x0[ln][k] = bv[b][k].c0;
+            bj.x1[ln][k] = bv[b][k].c1;
           }
-          dj.n = (int)m;
-          dj.l = level;
-          dj.lanes = (int)nl;
-          launch_dot_plain(c, dj, s);
+          for (size_t gi = 0; gi < gs.size(); ++gi) {
+            inner[gi][b] = fresh(level, scale, s);
+            bj.out0[ln][gi] = mut(inner[gi][b].c0);
+            bj.out1[ln][gi] = mut(inner[gi][b].c1);
+          }
         }
-        inner = have ? add_many(inner, d, s) : d;
-        have = true;
+        launch_bsgs_dot(c, bj, s);
       }
-      const int r = (int)boot::pymod((long)P.step * g * i, n);
+    } else {
+      for (size_t gi = 0; gi < gs.size(); ++gi) {
+        const auto& terms = gs[gi].second;
+        bool have = false;
+        for (size_t k = 0; k < terms.size(); k += MAX_DOT_TERMS) {
+          const size_t m = std::min<size_t>(MAX_DOT_TERMS, terms.size() - k);
+          std::vector<boot::Ct> d(B);
+          for (size_t b0 = 0; b0 < B; b0 += MAX_DOT_LANES) {
+            const size_t nl = std::min<size_t>(MAX_DOT_LANES, B - b0);
+            DotJob dj{};
+            for (size_t t = 0; t < m; ++t) dj.pt[t] = terms[k + t].second->u64();
+            for (size_t ln = 0; ln < nl; ++ln) {
+              const size_t b = b0 + ln;
+              d[b] = fresh(level, scale, s);
+              for (size_t t = 0; t < m; ++t) {
+                const boot::Ct& x = bv[b][jpos.at(terms[k + t].first)];
+                dj.c0[ln][t] = x.c0;
+                dj.c1[ln][t] = x.c1;
+              }
+              dj.out0[ln] = mut(d[b].c0);
+              dj.out1[ln] = mut(d[b].c1);
+            }
+            dj.n = (int)m;
+            dj.l = level;
+            dj.lanes = (int)nl;
+            launch_dot_plain(c, dj, s);
+          }
+          inner[gi] = have ? add_many(inner[gi], d, s) : d;
+          have = true;
+        }
+      }
+    }
+    std::vector<std::vector<boot::Ct>> parts(B);
+    std::vector<std::pair<boot::Ct, int>> turns;
+    std::vector<size_t> owner;
+    for (size_t gi = 0; gi < gs.size(); ++gi) {
+      const int r = (int)boot::pymod((long)P.step * g * gs[gi].first, n);
       for (size_t b = 0; b < B; ++b) {
         if (r) {
-          turns.push_back({inner[b], r});
+          turns.push_back({inner[gi][b], r});
           owner.push_back(b);
         } else {
-          parts[b].push_back(inner[b]);
+          parts[b].push_back(inner[gi][b]);
         }
       }
     }
@@ -909,11 +943,16 @@ struct Bootstrapper {
     }
     if (prm.prescale_bits) x = mul_int_many(x, (double)(1ll << prm.prescale_bits), s);
     std::vector<boot::Ct> a;
+    std::vector<const uint64_t*> rin;
+    std::vector<uint64_t*> rout;
     for (size_t b = 0; b < B; ++b) {  // ModRaise: m -> m + q0 I on every limb of the top level
       a.push_back(fresh(top, in_scale, s));
-      op_mod_raise(c, x[b].c0, top, mut(a.back().c0), s);
-      op_mod_raise(c, x[b].c1, top, mut(a.back().c1), s);
+      rin.push_back(x[b].c0);
+      rin.push_back(x[b].c1);
+      rout.push_back(mut(a.back().c0));
+      rout.push_back(mut(a.back().c1));
     }
+    op_mod_raise_batch(c, rin.data(), (int)rin.size(), top, rout.data(), s);
     if (prm.sparse_encapsulation) a = keyswitch_add_many(a, to_dense, s);  // back to the dense secret
     for (const auto& P : cts_pl) a = apply_many(a, P, s);
     const std::vector<boot::Ct> cj = conjugate_many(a, s);

@@ -446,6 +446,32 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
   *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
 }
 
+__global__ void __launch_bounds__(EW_THREADS) bsgs_dot_kernel(const __grid_constant__ BsgsJob J,
+                                                              const DevPrime* primes, int logN) {
+  const int lane = blockIdx.x, j = blockIdx.z;
+  const DevPrime p = primes[j];
+  const size_t off = ((size_t)j << logN) + blockIdx.y * blockDim.x + threadIdx.x;
+  uint64_t a[MAX_BSGS_BABY], b[MAX_BSGS_BABY];
+#pragma unroll
+  for (int k = 0; k < MAX_BSGS_BABY; ++k)
+    if (k < J.nb) {
+      a[k] = J.x0[lane][k][off];
+      b[k] = J.x1[lane][k][off];
+    }
+  for (int i = 0; i < J.ng; ++i) {
+    U128 s0{0, 0}, s1{0, 0};  // at most 8 products of values below 2^62
+#pragma unroll
+    for (int k = 0; k < MAX_BSGS_BABY; ++k)
+      if (k < J.nb && J.pt[i][k]) {
+        const uint64_t w = J.pt[i][k][off];
+        mac128(s0, w, a[k]);
+        mac128(s1, w, b[k]);
+      }
+    J.out0[lane][i][off] = reduce128(s0, p);
+    J.out1[lane][i][off] = reduce128(s1, p);
+  }
+}
+
 __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
                                                              const DevPrime* primes, int logN) {
   const int j = blockIdx.y, lane = blockIdx.z;
@@ -555,6 +581,19 @@ void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s) {
   dim3 grid(job.lanes, c->N / (2 * EW_THREADS), job.l);
   LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (job.n + job.lanes * (2.0 * job.n + 2)));
   dot_plain_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+  FIDES_CUDA(cudaGetLastError());
+}
+
+void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s) {
+  if (job.nb < 1 || job.nb > MAX_BSGS_BABY || job.ng < 1 || job.ng > MAX_BSGS_GIANT || job.lanes < 1 ||
+      job.lanes > MAX_BSGS_LANES || job.l < 1)
+    throw Error(-1, "BSGS inner products need 1..8 baby steps, 1..16 giant steps, 1..8 lanes");
+  int terms = 0;
+  for (int i = 0; i < job.ng; ++i)
+    for (int k = 0; k < job.nb; ++k) terms += job.pt[i][k] != nullptr;
+  dim3 grid(job.lanes, c->N / EW_THREADS, job.l);
+  LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (terms + job.lanes * 2.0 * (job.nb + job.ng)));
+  bsgs_dot_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
   FIDES_CUDA(cudaGetLastError());
 }
 

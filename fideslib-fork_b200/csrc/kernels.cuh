@@ -166,6 +166,24 @@ struct DotJob {
 };
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 
+// ---- every giant step's inner product of a BSGS linear transform in one launch:
+// out_i = sum_j pt[i][j] * x_j for all giant steps i, reading each baby-step ciphertext x_j
+// once (one launch per giant step reads each of them once per giant step).  A thread keeps its
+// coefficient of all baby steps in registers and runs the giant steps over them; lanes (the
+// ciphertexts of a batch) share the diagonals as in DotJob.
+constexpr int MAX_BSGS_BABY = 8;
+constexpr int MAX_BSGS_GIANT = 16;
+constexpr int MAX_BSGS_LANES = 8;
+struct BsgsJob {
+  const uint64_t* x0[MAX_BSGS_LANES][MAX_BSGS_BABY];
+  const uint64_t* x1[MAX_BSGS_LANES][MAX_BSGS_BABY];
+  const uint64_t* pt[MAX_BSGS_GIANT][MAX_BSGS_BABY];  // diagonal (i, j), or null (no term)
+  uint64_t* out0[MAX_BSGS_LANES][MAX_BSGS_GIANT];
+  uint64_t* out1[MAX_BSGS_LANES][MAX_BSGS_GIANT];
+  int nb, ng, l, lanes;
+};
+void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s);
+
 // ---- ciphertext linear combination with per-limb integer constants:
 // out0 = sum_t s_t * x0_t + add0, out1 = sum_t s_t * x1_t (mod q_j per limb j).  The scalar
 // steps of a Chebyshev series in one launch: the weighted sums of the Paterson-Stockmeyer

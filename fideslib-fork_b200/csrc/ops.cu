@@ -480,21 +480,31 @@ void op_hoisted_digits(Context* c, const uint64_t* c0, const uint64_t* digits, i
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, (int)outs.size(), s);
 }
 
-void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s) {
+void op_mod_raise_batch(Context* c, const uint64_t* const* xs, int n, int out_level, uint64_t* const* outs,
+                        cudaStream_t s) {
   check_level(c, out_level);
+  if (n <= 0) return;
   const size_t N = c->N;
-  Scratch sc(c, sizeof(uint64_t) * N, s);
-  LimbRef r = lref(sc.u64(), 0);
-  r.src = x;
-  ntt_limbs(c, &r, 1, true, s);
-  std::vector<LimbRef> refs;
-  for (int j = 0; j < out_level; ++j) {
-    LimbRef t = lref(out + j * N, j);
-    t.pro = sc.u64();
-    t.aux = 1;  // source prime = aux - 1 = q_0
-    refs.push_back(t);
+  Scratch sc(c, sizeof(uint64_t) * N * n, s);
+  std::vector<LimbRef> in(n);
+  for (int i = 0; i < n; ++i) {
+    in[i] = lref(sc.u64() + i * N, 0);
+    in[i].src = xs[i];
   }
+  ntt_limbs(c, in.data(), n, true, s);
+  std::vector<LimbRef> refs;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < out_level; ++j) {
+      LimbRef t = lref(outs[i] + j * N, j);
+      t.pro = sc.u64() + i * N;
+      t.aux = 1;  // source prime = aux - 1 = q_0
+      refs.push_back(t);
+    }
   ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_SWITCH, OUT_PLAIN);
+}
+
+void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s) {
+  op_mod_raise_batch(c, &x, 1, out_level, &out, s);
 }
 
 }  // namespace fides

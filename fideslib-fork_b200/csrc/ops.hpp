@@ -78,5 +78,8 @@ void op_hoisted_digits(Context* c, const uint64_t* c0, const uint64_t* digits, i
 // ModRaise (reference Bootstrap.cu ModRaise): a level-1 polynomial (limb q_0, EVAL) raised to
 // `out_level` limbs: INTT, SwitchModulus(q_0 -> q_j) of the centred residues, NTT.
 void op_mod_raise(Context* c, const uint64_t* x, int out_level, uint64_t* out, cudaStream_t s);
+// op_mod_raise of n polynomials in one launch pair each for the INTT and the NTT.
+void op_mod_raise_batch(Context* c, const uint64_t* const* xs, int n, int out_level, uint64_t* const* outs,
+                        cudaStream_t s);
 
 }  // namespace fides

@@ -655,3 +655,29 @@ def make_batch_engine(bs: Bootstrapper, scale: float, capacity: int):
         outs = bootstrap_concurrent(bs, ins, streams)
     torch.cuda.synchronize()
     return (g, [F.Ciphertext(c.c0, c.c1) for c in ins], [F.Ciphertext(o.c0, o.c1) for o in outs])
+
+
+def make_native_engine(nb, capacity: int = 1):
+    """A bootstrap engine for the request loop backed by the library's C++ bootstrapper
+    (NativeBootstrapper): `capacity` static one-limb inputs and one CUDA graph, captured once,
+    that bootstraps them into static outputs -- fides_bootstrap for capacity 1,
+    fides_bootstrap_batch (the whole batch in one launch sequence) otherwise.  Returns
+    (graph, input, output) for capacity 1 (Server.add_bootstrap) and (graph, inputs, outputs)
+    otherwise (Server.add_bootstrap_batch)."""
+    import torch
+    from . import Ciphertext
+    ctx = nb.ctx
+    ins = []
+    for _ in range(capacity):
+        c0, c1 = ctx.empty(1), ctx.empty(1)
+        c0.view(torch.int64).zero_()
+        c1.view(torch.int64).zero_()
+        ins.append(Ciphertext(c0, c1))
+    run = (lambda: [nb.bootstrap(ins[0])]) if capacity == 1 else (lambda: nb.bootstrap_batch(ins))
+    run()  # warm-up outside the capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        outs = run()
+    torch.cuda.synchronize()
+    return (g, ins[0], outs[0]) if capacity == 1 else (g, ins, outs)

@@ -162,10 +162,12 @@ def test_concurrent_batch_equals_sequential(fides):
 
 
 @pytest.mark.gpu
-def test_served_bootstraps_in_a_mix(fides):
-    """Bootstrap requests through the request loop (two engines) mixed with HMult / HRotate
-    requests submitted from several threads: every bootstrap equals the direct bootstrap of
-    its input and every HMult / HRotate equals the same request run alone."""
+@pytest.mark.parametrize("driver", ["python", "native"])
+def test_served_bootstraps_in_a_mix(fides, driver):
+    """Bootstrap requests through the request loop (two engines and a batch engine; graphs of
+    the Python driver or of the C++ bootstrapper) mixed with HMult / HRotate requests submitted
+    from several threads: every bootstrap equals the direct bootstrap of its input and every
+    HMult / HRotate equals the same request run alone."""
     import random
     import threading
     import torch
@@ -174,8 +176,17 @@ def test_served_bootstraps_in_a_mix(fides):
     prm, o, kg, ctx, ev, bs = make_boot(F, 12)
     delta = 2.0 ** 50
     bs.prepare(top_level=prm.n_q, msg_scale=delta)
-    engines = [B.make_engine(bs, delta) for _ in range(2)]
-    batch_engine = B.make_batch_engine(bs, delta, 3)  # one graph, three ciphertexts per launch
+    nb = None
+    if driver == "native":
+        nb = native_for(F, prm, ev, bs)
+        nb.prepare()
+        engines = [B.make_native_engine(nb, 1) for _ in range(2)]
+        batch_engine = B.make_native_engine(nb, 3)  # one graph: three ciphertexts in one launch sequence
+        direct = lambda ct: nb.bootstrap(ct)
+    else:
+        engines = [B.make_engine(bs, delta) for _ in range(2)]
+        batch_engine = B.make_batch_engine(bs, delta, 3)  # one graph, three ciphertexts per launch
+        direct = lambda ct: bs.bootstrap(B.Ct(ct.c0, ct.c1, delta))
     rng = xrng(65)
     n = prm.N // 2
     boot_in, boot_ref = [], []
@@ -184,7 +195,7 @@ def test_served_bootstraps_in_a_mix(fides):
         c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
         ct = F.Ciphertext(F.to_device(c0[:1]), F.to_device(c1[:1]))
         boot_in.append(ct)
-        r = bs.bootstrap(B.Ct(ct.c0, ct.c1, delta))
+        r = direct(ct)
         boot_ref.append((r.c0.clone(), r.c1.clone()))
     torch.cuda.synchronize()
     rot_key = F.to_device(kg.rotation_key(1))
@@ -239,6 +250,9 @@ def test_served_bootstraps_in_a_mix(fides):
         srv.close()
     for i, (r0, r1) in enumerate(boot_ref):
         assert torch.equal(outs[("b", i)].c0, r0) and torch.equal(outs[("b", i)].c1, r1), f"bootstrap {i}"
+    if nb is not None:
+        del engines, batch_engine
+        nb.close()
     for i, x in enumerate(alone):
         assert torch.equal(outs[("o", i)].c0, x.c0) and torch.equal(outs[("o", i)].c1, x.c1), f"request {i}"
 

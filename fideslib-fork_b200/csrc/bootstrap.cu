@@ -323,6 +323,18 @@ struct Bootstrapper {
     a.scale = scale;
     return a;
   }
+  // an extended-basis ciphertext: `level` Q limbs followed by the K special limbs (level stays
+  // the Q level)
+  boot::Ct fresh_ext(int level, double scale, cudaStream_t s) const {
+    boot::Ct a;
+    a.b0 = alloc(level + c->K, s);
+    a.b1 = alloc(level + c->K, s);
+    a.c0 = a.b0->u64();
+    a.c1 = a.b1->u64();
+    a.level = level;
+    a.scale = scale;
+    return a;
+  }
   static uint64_t* mut(const uint64_t* p) { return const_cast<uint64_t*>(p); }
   uint64_t residue(double v, int i) const { return boot::residue_of(v, c->primes[i]); }
 
@@ -390,21 +402,25 @@ struct Bootstrapper {
 
   // the same integer combination of every lane (one launch): sum_t ints[t] lane[t] (+ add on c0)
   // ints / add: integers held exactly in doubles (see rint_even)
+  // ext > 0: the operands are extended-basis polynomials (level Q limbs + ext special limbs)
   std::vector<boot::Ct> lincomb_lanes(const std::vector<std::vector<boot::Ct>>& lanes, const std::vector<double>& ints,
-                                      const double* add, int level, double scale, cudaStream_t s) const {
+                                      const double* add, int level, double scale, cudaStream_t s, int ext = 0) const {
     if (lanes.empty() || ints.empty() || ints.size() > (size_t)MAX_LC_TERMS)
       throw Error(-1, "bootstrap: linear combination out of range");
     static thread_local LinCombJob j;
+    const int limbs = level + ext;
+    j.lq = ext ? level : 0;
+    j.nq = c->n_q;
     for (size_t t = 0; t < ints.size(); ++t)
-      for (int i = 0; i < level; ++i) j.s[t][i] = residue(ints[t], i);
-    for (int i = 0; i < level; ++i) j.add0[i] = add ? residue(*add, i) : 0;
+      for (int i = 0; i < limbs; ++i) j.s[t][i] = residue(ints[t], ext_prime(i, j.lq, j.nq));
+    for (int i = 0; i < limbs; ++i) j.add0[i] = add ? residue(*add, ext_prime(i, j.lq, j.nq)) : 0;
     j.n = (int)ints.size();
-    j.l = level;
+    j.l = limbs;
     std::vector<boot::Ct> outs;
     for (size_t a0 = 0; a0 < lanes.size(); a0 += MAX_LC_LANES) {  // lanes in launches of up to 8
       const size_t m = std::min<size_t>(MAX_LC_LANES, lanes.size() - a0);
       for (size_t a = 0; a < m; ++a) {
-        outs.push_back(fresh(level, scale, s));
+        outs.push_back(ext ? fresh_ext(level, scale, s) : fresh(level, scale, s));
         j.out0[a] = mut(outs.back().c0);
         j.out1[a] = mut(outs.back().c1);
         for (size_t t = 0; t < ints.size(); ++t) {
@@ -612,11 +628,11 @@ struct Bootstrapper {
   }
 
   // ---------------------------------------------------------------- preparation
-  boot::Buf encode_pt(const std::vector<boot::cd>& z, int level, double scale, cudaStream_t s) const {
+  boot::Buf encode_pt(const std::vector<boot::cd>& z, int level, double scale, cudaStream_t s, int special = 0) const {
     Scratch slots(c, sizeof(double) * 2 * z.size(), s);
     FIDES_CUDA(cudaMemcpyAsync(slots.p, z.data(), sizeof(double) * 2 * z.size(), cudaMemcpyHostToDevice, s));
-    boot::Buf out = alloc(level, s);
-    op_encode(c, static_cast<const double*>(slots.p), (int)z.size(), 1, scale, level, out->u64(), s);
+    boot::Buf out = alloc(level + special, s);
+    op_encode_ext(c, static_cast<const double*>(slots.p), (int)z.size(), 1, scale, level, special, out->u64(), s);
     return out;
   }
 
@@ -646,7 +662,8 @@ struct Bootstrapper {
         if (it == M.end()) continue;
         std::vector<boot::cd> d(it->second.size());
         for (size_t k = 0; k < d.size(); ++k) d[k] = it->second[k] * fac;
-        P.pts[{i, j}] = encode_pt(boot::roll(d, (long)P.step * prm.baby * i), level, P.pt_scale, s);
+        P.pts[{i, j}] = encode_pt(boot::roll(d, (long)P.step * prm.baby * i), level, P.pt_scale, s,
+                                  prm.double_hoist ? c->K : 0);
       }
     return P;
   }
@@ -831,6 +848,175 @@ struct Bootstrapper {
     return rescale_many_to(sums, S[level - 1], s);
   }
 
+  // P mod q_i for the Q limbs (the extended-basis form of an unrotated baby step is P a)
+  std::vector<uint64_t> p_mod_q() const {
+    std::vector<uint64_t> v(c->n_q);
+    for (int i = 0; i < c->n_q; ++i) {
+      const uint64_t q = c->primes[i];
+      uint64_t x = 1 % q;
+      for (int k = 0; k < c->K; ++k) x = h_mulmod(x, c->primes[c->n_q + k] % q, q);
+      v[i] = x;
+    }
+    return v;
+  }
+
+  // The linear transform double-hoisted: the baby-step rotations of every ciphertext are left
+  // in the extended basis (the KSK outputs with P c0 added and the automorphism applied, no
+  // ModDown), each giant step's inner product is taken there against diagonals encoded with
+  // the special limbs too, a rotated giant step's c1 alone is brought down (one ModDown) and
+  // key-switched with its extended-basis c0 added to the output as it is, and the giant steps
+  // are summed in the extended basis and brought down once, fused with the rescale.  Every
+  // term carries the factor P, so the final ModDown divides it out; the rounding differs from
+  // the single-hoisted form's by one ModDown rounding per giant step and transform (each term
+  // below K / 2 per coefficient before the secret's multiplication).
+  std::vector<boot::Ct> apply_many_dh(const std::vector<boot::Ct>& as, const boot::Plan& P, cudaStream_t s) const {
+    const size_t B = as.size();
+    for (const auto& a : as)
+      if (a.level != P.level) throw Error(-4, "bootstrap: linear transform at the wrong level");
+    const int g = prm.baby, l = as[0].level, K = c->K;
+    const size_t N = c->N;
+    const double scale = as[0].scale;
+    std::set<int> jset;
+    for (const auto& kv : P.giant)
+      for (int j : kv.second) jset.insert(j);
+    std::vector<int> js(jset.begin(), jset.end()), rs;
+    for (int j : js) rs.push_back((int)boot::pymod((long)P.step * j, n));
+    std::map<int, size_t> jpos;
+    for (size_t k = 0; k < js.size(); ++k) jpos[js[k]] = k;
+    // baby steps: X[b][k] = P rotate(a_b, rs[k]) in the extended basis
+    std::vector<std::vector<boot::Ct>> X(B, std::vector<boot::Ct>(js.size()));
+    std::vector<HoistItem> items(B);
+    std::vector<ScalarJob> pj;
+    const std::vector<uint64_t> pq = p_mod_q();
+    for (size_t b = 0; b < B; ++b) {
+      const boot::Ct& a = as[b];
+      HoistItem& it = items[b];
+      it.c0 = a.c0;
+      it.c1 = a.c1;
+      it.l = l;
+      for (size_t k = 0; k < js.size(); ++k) {
+        X[b][k] = fresh_ext(l, scale, s);
+        if (boot::pymod(rs[k], n) == 0) {
+          for (int poly = 0; poly < 2; ++poly) {
+            ScalarJob j{};
+            j.a = poly ? a.c1 : a.c0;
+            j.out = mut(poly ? X[b][k].c1 : X[b][k].c0);
+            j.l = l;
+            j.op = EW_MUL_SCALAR;
+            for (int i = 0; i < l; ++i) j.s[i] = pq[i];
+            pj.push_back(j);
+            FIDES_CUDA(cudaMemsetAsync(j.out + (size_t)l * N, 0, sizeof(uint64_t) * N * K, s));
+          }
+        } else {
+          it.keys.push_back(rot_key(rs[k]));
+          it.ks.push_back(h_auto_index(c->logN, rs[k]));
+          it.out0.push_back(mut(X[b][k].c0));
+          it.out1.push_back(mut(X[b][k].c1));
+        }
+      }
+    }
+    if (!pj.empty()) launch_scalar(c, pj.data(), (int)pj.size(), s);
+    if (!items.empty() && !items[0].keys.empty()) op_hoisted_ext_batch(c, items.data(), (int)items.size(), s);
+    // the giant steps that have terms
+    std::vector<std::pair<int, std::vector<std::pair<int, boot::Buf>>>> gs;
+    for (const auto& [i, jl] : P.giant) {
+      std::vector<std::pair<int, boot::Buf>> terms;
+      for (int j : jl) {
+        auto it = P.pts.find({i, j});
+        if (it != P.pts.end()) terms.push_back({j, it->second});
+      }
+      if (!terms.empty()) gs.push_back({i, terms});
+    }
+    if (js.size() > (size_t)MAX_BSGS_BABY || gs.size() > (size_t)MAX_BSGS_GIANT || gs.size() > (size_t)MAX_LC_TERMS)
+      throw Error(-1, "bootstrap: double hoisting needs at most 16 baby and 16 giant steps");
+    std::vector<std::vector<boot::Ct>> Y(gs.size(), std::vector<boot::Ct>(B));  // [giant step][b], extended
+    for (size_t b0 = 0; b0 < B; b0 += MAX_BSGS_LANES) {
+      const size_t nl = std::min<size_t>(MAX_BSGS_LANES, B - b0);
+      BsgsJob bj{};
+      bj.nb = (int)js.size();
+      bj.ng = (int)gs.size();
+      bj.l = l + K;
+      bj.lq = l;
+      bj.nq = c->n_q;
+      bj.lanes = (int)nl;
+      for (size_t gi = 0; gi < gs.size(); ++gi)
+        for (const auto& [j, pt] : gs[gi].second) bj.pt[gi][jpos.at(j)] = pt->u64();
+      for (size_t ln = 0; ln < nl; ++ln) {
+        const size_t b = b0 + ln;
+        for (size_t k = 0; k < js.size(); ++k) {
+          bj.x0[ln][k] = X[b][k].c0;
+          bj.x1[ln][k] = X[b][k].c1;
+        }
+        for (size_t gi = 0; gi < gs.size(); ++gi) {
+          Y[gi][b] = fresh_ext(l, scale, s);
+          bj.out0[ln][gi] = mut(Y[gi][b].c0);
+          bj.out1[ln][gi] = mut(Y[gi][b].c1);
+        }
+      }
+      launch_bsgs_dot(c, bj, s);
+    }
+    X.clear();
+    // rotated giant steps: c1 down to the Q basis, then key-switched in the extended basis
+    std::vector<uint64_t*> md_in, md_out;
+    std::vector<int> md_l;
+    std::vector<boot::Buf> c1q;
+    std::vector<HoistItem> gitems;
+    std::vector<std::vector<boot::Ct>> Z(gs.size(), std::vector<boot::Ct>(B));
+    for (size_t gi = 0; gi < gs.size(); ++gi) {
+      const int r = (int)boot::pymod((long)P.step * g * gs[gi].first, n);
+      if (!r) continue;
+      for (size_t b = 0; b < B; ++b) {
+        c1q.push_back(alloc(l, s));
+        md_in.push_back(mut(Y[gi][b].c1));
+        md_out.push_back(c1q.back()->u64());
+        md_l.push_back(l);
+        Z[gi][b] = fresh_ext(l, scale, s);
+        HoistItem it;
+        it.c0 = nullptr;
+        it.c1 = c1q.back()->u64();
+        it.l = l;
+        it.keys.push_back(rot_key(r));
+        it.ks.push_back(h_auto_index(c->logN, r));
+        it.out0.push_back(mut(Z[gi][b].c0));
+        it.out1.push_back(mut(Z[gi][b].c1));
+        it.c0x = Y[gi][b].c0;
+        gitems.push_back(it);
+      }
+    }
+    op_moddown_batch(c, md_in.data(), md_l.data(), md_out.data(), (int)md_in.size(), s);
+    if (!gitems.empty()) op_hoisted_ext_batch(c, gitems.data(), (int)gitems.size(), s);
+    // the sum of every ciphertext's giant steps, in the extended basis
+    std::vector<std::vector<boot::Ct>> lanes(B);
+    for (size_t gi = 0; gi < gs.size(); ++gi) {
+      const bool rot = boot::pymod((long)P.step * g * gs[gi].first, n) != 0;
+      for (size_t b = 0; b < B; ++b) lanes[b].push_back(rot ? Z[gi][b] : Y[gi][b]);
+    }
+    std::vector<boot::Ct> acc;
+    if (lanes[0].size() == 1) {
+      for (size_t b = 0; b < B; ++b) acc.push_back(lanes[b][0]);
+    } else {
+      acc = lincomb_lanes(lanes, std::vector<double>(lanes[0].size(), 1.0), nullptr, l, scale, s, K);
+    }
+    lanes.clear();
+    Y.clear();
+    Z.clear();
+    // one ModDown per polynomial, fused with the rescale by q_(l-1)
+    std::vector<boot::Ct> outs;
+    std::vector<uint64_t*> ex, o;
+    std::vector<int> ls2;
+    for (size_t b = 0; b < B; ++b) {
+      outs.push_back(fresh(l - 1, S[l - 1], s));
+      ex.push_back(mut(acc[b].c0));
+      ex.push_back(mut(acc[b].c1));
+      o.push_back(mut(outs.back().c0));
+      o.push_back(mut(outs.back().c1));
+      ls2.push_back(l);
+      ls2.push_back(l);
+    }
+    op_moddown_rescale_batch(c, ex.data(), ls2.data(), o.data(), (int)ex.size(), s);
+    return outs;
+  }
+
   // ---------------------------------------------------------------- EvalMod
   static constexpr int PS_BABY = 16;
 
@@ -954,7 +1140,7 @@ struct Bootstrapper {
     }
     op_mod_raise_batch(c, rin.data(), (int)rin.size(), top, rout.data(), s);
     if (prm.sparse_encapsulation) a = keyswitch_add_many(a, to_dense, s);  // back to the dense secret
-    for (const auto& P : cts_pl) a = apply_many(a, P, s);
+    for (const auto& P : cts_pl) a = prm.double_hoist ? apply_many_dh(a, P, s) : apply_many(a, P, s);
     const std::vector<boot::Ct> cj = conjugate_many(a, s);
     const std::vector<boot::Ct> t_re = add_raw_many(a, cj, s);
     const std::vector<boot::Ct> t_im = mul_plain_int_many(sub_raw_many(a, cj, s), pt_minus_i, s);
@@ -972,7 +1158,7 @@ struct Bootstrapper {
     sre = to_level_many(sre, stc_in_level, s);
     sim = to_level_many(sim, stc_in_level, s);
     std::vector<boot::Ct> u = add_raw_many(sre, mul_plain_int_many(sim, pt_i, s), s);
-    for (const auto& P : stc_pl) u = apply_many(u, P, s);
+    for (const auto& P : stc_pl) u = prm.double_hoist ? apply_many_dh(u, P, s) : apply_many(u, P, s);
     return u;
   }
 

@@ -429,6 +429,7 @@ int fides_lincomb(fides_ctx* x, int n_lanes, const uint64_t* const* c0s, const u
     need(out0s, "out0s");
     need(out1s, "out1s");
     static thread_local fides::LinCombJob j;
+    j.lq = j.nq = 0;  // Q limbs only
     for (int a = 0; a < n_lanes; ++a) {
       need(out0s[a], "out0s[lane]");
       need(out1s[a], "out1s[lane]");

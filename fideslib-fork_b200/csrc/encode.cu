@@ -207,6 +207,12 @@ void check_slots(Context* c, int n_slots) {
 
 void op_encode(Context* c, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
                cudaStream_t s) {
+  op_encode_ext(c, slots, n_slots, n_pts, scale, level, 0, out, s);
+}
+
+void op_encode_ext(Context* c, const double* slots, int n_slots, int n_pts, double scale, int level, int special,
+                   uint64_t* out, cudaStream_t s) {
+  if (special < 0 || special > c->K) throw Error(-1, "special limbs out of range");
   check_slots(c, n_slots);
   if (n_pts < 1) throw Error(-1, "n_pts < 1");
   if (level < 1 || level > c->n_q) throw Error(-4, "level out of range");
@@ -235,10 +241,11 @@ void op_encode(Context* c, const double* slots, int n_slots, int n_pts, double s
     FIDES_CUDA(cudaGetLastError());
   }
   std::vector<LimbRef> refs;
-  refs.reserve((size_t)n_pts * level);
+  const int limbs = level + special;
+  refs.reserve((size_t)n_pts * limbs);
   for (int p = 0; p < n_pts; ++p)
-    for (int j = 0; j < level; ++j) {
-      LimbRef r = lref(out + ((size_t)p * level + j) * N, j);
+    for (int j = 0; j < limbs; ++j) {
+      LimbRef r = lref(out + ((size_t)p * limbs + j) * N, j < level ? j : c->n_q + (j - level));
       r.pro = coef + p * N;  // signed coefficients, reduced by each limb's prologue
       refs.push_back(r);
     }

@@ -260,6 +260,11 @@ __global__ void __launch_bounds__(EW_THREADS, KskMinBlocks<MAXB, JG>::value) ksk
 #pragma unroll
       for (int c = 0; c < CPT; ++c) rb[c] = addmod(rb[c], shoup(cv.c[c], pm.w, pm.ws, p.q), p.q);
     }
+    if (J.c0x) {
+      const V cv = kld<CPT>(J.c0x + off);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) rb[c] = addmod(rb[c], cv.c[c], p.q);
+    }
     uint64_t* oa = J.out_a + (size_t)i * N;
     uint64_t* ob = J.out_b + (size_t)i * N;
     if (J.auto_k) {
@@ -425,7 +430,7 @@ __global__ void __launch_bounds__(EW_THREADS) scalar_kernel(const __grid_constan
 __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_constant__ DotJob J,
                                                                const DevPrime* primes, int logN) {
   const int lane = blockIdx.x, j = blockIdx.z;
-  const DevPrime p = primes[j];
+  const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.y * blockDim.x + threadIdx.x);
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
@@ -446,27 +451,34 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
   *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
 }
 
+// NB: register capacity for the baby steps (8: 56 registers; 16: about 126)
+template <int NB>
 __global__ void __launch_bounds__(EW_THREADS) bsgs_dot_kernel(const __grid_constant__ BsgsJob J,
                                                               const DevPrime* primes, int logN) {
   const int lane = blockIdx.x, j = blockIdx.z;
-  const DevPrime p = primes[j];
+  const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
   const size_t off = ((size_t)j << logN) + blockIdx.y * blockDim.x + threadIdx.x;
-  uint64_t a[MAX_BSGS_BABY], b[MAX_BSGS_BABY];
+  uint64_t a[NB], b[NB];
 #pragma unroll
-  for (int k = 0; k < MAX_BSGS_BABY; ++k)
+  for (int k = 0; k < NB; ++k)
     if (k < J.nb) {
       a[k] = J.x0[lane][k][off];
       b[k] = J.x1[lane][k][off];
     }
   for (int i = 0; i < J.ng; ++i) {
-    U128 s0{0, 0}, s1{0, 0};  // at most 8 products of values below 2^62
+    U128 s0{0, 0}, s1{0, 0};
 #pragma unroll
-    for (int k = 0; k < MAX_BSGS_BABY; ++k)
+    for (int k = 0; k < NB; ++k) {
+      if (k == 15) {  // keep the sums below 2^128: at most 15 products of values below 2^62
+        s0 = U128{reduce128(s0, p), 0};
+        s1 = U128{reduce128(s1, p), 0};
+      }
       if (k < J.nb && J.pt[i][k]) {
         const uint64_t w = J.pt[i][k][off];
         mac128(s0, w, a[k]);
         mac128(s1, w, b[k]);
       }
+    }
     J.out0[lane][i][off] = reduce128(s0, p);
     J.out1[lane][i][off] = reduce128(s1, p);
   }
@@ -475,7 +487,7 @@ __global__ void __launch_bounds__(EW_THREADS) bsgs_dot_kernel(const __grid_const
 __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
                                                              const DevPrime* primes, int logN) {
   const int j = blockIdx.y, lane = blockIdx.z;
-  const DevPrime p = primes[j];
+  const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
@@ -587,13 +599,16 @@ void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s) {
 void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s) {
   if (job.nb < 1 || job.nb > MAX_BSGS_BABY || job.ng < 1 || job.ng > MAX_BSGS_GIANT || job.lanes < 1 ||
       job.lanes > MAX_BSGS_LANES || job.l < 1)
-    throw Error(-1, "BSGS inner products need 1..8 baby steps, 1..16 giant steps, 1..8 lanes");
+    throw Error(-1, "BSGS inner products need 1..16 baby steps, 1..16 giant steps, 1..8 lanes");
   int terms = 0;
   for (int i = 0; i < job.ng; ++i)
     for (int k = 0; k < job.nb; ++k) terms += job.pt[i][k] != nullptr;
   dim3 grid(job.lanes, c->N / EW_THREADS, job.l);
   LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (terms + job.lanes * 2.0 * (job.nb + job.ng)));
-  bsgs_dot_kernel<<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+  if (job.nb <= 8)
+    bsgs_dot_kernel<8><<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+  else
+    bsgs_dot_kernel<MAX_BSGS_BABY><<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
   FIDES_CUDA(cudaGetLastError());
 }
 
@@ -616,10 +631,11 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     // switching key), or else with one digit set (hoisted rotations of one ciphertext)
     auto same_key = [](const KskJob& a, const KskJob& b) {
       return a.key == b.key && a.l == b.l && a.auto_k == b.auto_k && !a.x2 == !b.x2 && !a.a0 == !b.a0 &&
-             !a.c0 == !b.c0 && !a.x == !b.x;
+             !a.c0 == !b.c0 && !a.x == !b.x && !a.c0x == !b.c0x;
     };
     auto same_digits = [](const KskJob& a, const KskJob& b) {
-      return a.digits == b.digits && a.x == b.x && a.x2 == b.x2 && a.l == b.l && !a.a0 == !b.a0 && !a.c0 == !b.c0;
+      return a.digits == b.digits && a.x == b.x && a.x2 == b.x2 && a.l == b.l && !a.a0 == !b.a0 && !a.c0 == !b.c0 &&
+             !a.c0x == !b.c0x;
     };
     // groups of up to MAX_KSK_GROUP jobs sharing a key, or else sharing a digit tile
     auto group = [&](auto same, int cap) {
@@ -651,7 +667,8 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     double bytes = 0;
     for (int i = 0; i < m; ++i) {
       const int l = L.j[i].l, ext = l + c->K, b = c->beta(l);
-      bytes += 8.0 * c->N * ((double)ext * (b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0));
+      bytes += 8.0 * c->N * ((double)ext * (b + 2) + (L.j[i].c0 ? l : 0) + (L.j[i].a0 ? 2 * l : 0) +
+                             (L.j[i].c0x ? ext : 0));
     }
     for (int g = 0; g < L.ngroups; ++g) {
       const int l = L.j[L.gstart[g]].l, b = c->beta(l), ext = l + c->K;

@@ -45,6 +45,10 @@ struct KskJob {
   // P (a0 b1 + a1 b0) to out_a's Q limbs, so that ModDown yields ModDown(.) + d0 / + d1
   const uint64_t* a0 = nullptr;
   const uint64_t* b0 = nullptr;
+  // optional extended-basis addend of out_b, every limb, not multiplied by P (the c0 of a
+  // ciphertext kept in the extended basis, double-hoisted linear transforms); before the
+  // automorphism scatter
+  const uint64_t* c0x = nullptr;
 };
 constexpr int MAX_KSK_JOBS = 64;
 // Jobs that share a switching key (one relinearisation or rotation key for a batch) and the
@@ -163,7 +167,11 @@ struct DotJob {
   uint64_t* out0[MAX_DOT_LANES];
   uint64_t* out1[MAX_DOT_LANES];
   int n, l, lanes;
+  int lq = 0, nq = 0;  // extended-basis operands: limbs >= lq are special limb (limb - lq) (lq = 0: none)
 };
+// Prime id of limb j of an operand whose first lq limbs are Q limbs 0..lq-1 and whose others
+// are the special limbs (lq = 0: every limb is a Q limb).
+__host__ __device__ inline int ext_prime(int j, int lq, int nq) { return (lq == 0 || j < lq) ? j : nq + (j - lq); }
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 
 // ---- every giant step's inner product of a BSGS linear transform in one launch:
@@ -171,7 +179,7 @@ void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 // once (one launch per giant step reads each of them once per giant step).  A thread keeps its
 // coefficient of all baby steps in registers and runs the giant steps over them; lanes (the
 // ciphertexts of a batch) share the diagonals as in DotJob.
-constexpr int MAX_BSGS_BABY = 8;
+constexpr int MAX_BSGS_BABY = 16;
 constexpr int MAX_BSGS_GIANT = 16;
 constexpr int MAX_BSGS_LANES = 8;
 struct BsgsJob {
@@ -181,6 +189,7 @@ struct BsgsJob {
   uint64_t* out0[MAX_BSGS_LANES][MAX_BSGS_GIANT];
   uint64_t* out1[MAX_BSGS_LANES][MAX_BSGS_GIANT];
   int nb, ng, l, lanes;
+  int lq = 0, nq = 0;  // as DotJob
 };
 void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s);
 
@@ -203,6 +212,7 @@ struct LinCombJob {
   uint64_t s[MAX_LC_TERMS][MAX_LC_LIMBS];
   uint64_t add0[MAX_LC_LIMBS];
   int n, l, lanes;
+  int lq = 0, nq = 0;  // as DotJob (s and add0 hold residues modulo each limb's own prime)
 };
 void launch_lincomb(Context* c, const LinCombJob& job, cudaStream_t s);
 

@@ -375,11 +375,16 @@ void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s)
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
 }
 
-void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStream_t s) {
+namespace {
+// Hoisted rotations of several ciphertexts: with `ext_out` the key-switch outputs are left in
+// the extended basis in the items' out buffers (l + K limbs each), otherwise one ModDown
+// covers every output.
+void hoisted_batch(Context* c, const HoistItem* items, int n_items, bool ext_out, cudaStream_t s) {
   // Every ciphertext's c1 is raised once (one ModUp launch sequence over all of them), the KSK
-  // pass covers every (ciphertext, rotation) pair -- adding P c0 and scattering by the
-  // automorphism -- and one ModDown covers every output (hoistedRotateDotKSK_2_ and
-  // fusedHoistedRotateBatch, ElemenwiseBatchKernels.cu:277-377, LimbPartitionBatch.cu:526+).
+  // pass covers every (ciphertext, rotation) pair -- adding P c0 (or an extended-basis c0)
+  // and scattering by the automorphism -- and one ModDown covers every output
+  // (hoistedRotateDotKSK_2_ and fusedHoistedRotateBatch, ElemenwiseBatchKernels.cu:277-377,
+  // LimbPartitionBatch.cu:526+).
   if (n_items <= 0) return;
   const size_t N = c->N;
   size_t total = 0;
@@ -389,8 +394,9 @@ void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStrea
     check_level(c, it.l);
     for (auto* k : it.keys)
       if (!k) throw Error(-5, "null rotation key");
+    if (it.c0 && it.c0x) throw Error(-1, "hoisted rotation: c0 and an extended-basis c0 both given");
     const int l = it.l, ext = l + c->K, r = (int)it.keys.size();
-    total += (size_t)l + (size_t)c->beta(l) * ext + (size_t)r * (2 * ext + 2 * l);
+    total += (size_t)l + (size_t)c->beta(l) * ext + (ext_out ? 0 : (size_t)r * (2 * ext + 2 * l));
     n_out += r;
   }
   if (n_out == 0) return;
@@ -425,12 +431,13 @@ void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStrea
   std::vector<int> ls2;
   for (const auto& ij : order) {
     const HoistItem& it = items[ij.first];
-    const int i = ij.first, l = it.l, ext = l + c->K;
-    {
-      const int j = ij.second;
-      uint64_t* A = bp.take(ext);
-      uint64_t* B = bp.take(ext);
-      kj.push_back(KskJob{it.c1, nullptr, dig[i], it.keys[j], it.c0, A, B, l, it.ks[j]});
+    const int i = ij.first, l = it.l, ext = l + c->K, j = ij.second;
+    uint64_t* A = ext_out ? it.out1[j] : bp.take(ext);
+    uint64_t* B = ext_out ? it.out0[j] : bp.take(ext);
+    KskJob job{it.c1, nullptr, dig[i], it.keys[j], it.c0, A, B, l, it.ks[j]};
+    job.c0x = it.c0x;
+    kj.push_back(job);
+    if (!ext_out) {
       ex.push_back(B);
       ex.push_back(A);
       conv.push_back(bp.take(l));
@@ -442,7 +449,48 @@ void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStrea
     }
   }
   launch_ksk(c, kj.data(), (int)kj.size(), s);
-  moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, (int)outs.size(), s);
+  if (!ext_out) moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, (int)outs.size(), s);
+}
+}  // namespace
+
+void op_hoisted_batch(Context* c, const HoistItem* items, int n_items, cudaStream_t s) {
+  hoisted_batch(c, items, n_items, false, s);
+}
+
+void op_hoisted_ext_batch(Context* c, const HoistItem* items, int n_items, cudaStream_t s) {
+  hoisted_batch(c, items, n_items, true, s);
+}
+
+void op_moddown_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    check_level(c, ls[i]);
+    total += ls[i];
+  }
+  Scratch sc(c, sizeof(uint64_t) * c->N * total, s);
+  Bump bp{sc.u64(), (size_t)c->N};
+  std::vector<uint64_t*> conv(n);
+  for (int i = 0; i < n; ++i) conv[i] = bp.take(ls[i]);
+  moddown_stage(c, exts, ls, conv.data(), outs, nullptr, n, s);
+}
+
+void op_moddown_rescale_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n,
+                              cudaStream_t s) {
+  if (n <= 0) return;
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    check_level(c, ls[i], 2);
+    total += ls[i] + 1;
+  }
+  Scratch sc(c, sizeof(uint64_t) * c->N * total, s);
+  Bump bp{sc.u64(), (size_t)c->N};
+  std::vector<uint64_t*> conv(n), tops(n);
+  for (int i = 0; i < n; ++i) {
+    conv[i] = bp.take(ls[i]);
+    tops[i] = bp.take(1);
+  }
+  moddown_rescale_stage(c, exts, ls, conv.data(), tops.data(), outs, nullptr, n, s);
 }
 
 void op_hoisted(Context* c, const HoistItem& it, cudaStream_t s) { op_hoisted_batch(c, &it, 1, s); }

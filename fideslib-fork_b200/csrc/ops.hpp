@@ -41,6 +41,8 @@ struct HoistItem {
   std::vector<const uint64_t*> keys;
   std::vector<uint32_t> ks;
   std::vector<uint64_t*> out0, out1;
+  // instead of P c0 (c0 in the Q basis): an extended-basis c0 (l + K limbs) added as it is
+  const uint64_t* c0x = nullptr;
 };
 
 void op_modup(Context* c, const uint64_t* x, int l, uint64_t* digits, cudaStream_t s);
@@ -71,6 +73,16 @@ void op_hoisted(Context* c, const HoistItem& item, cudaStream_t s);
 // Hoisted rotations of several ciphertexts (any levels, own rotation lists) in one launch
 // sequence per stage.
 void op_hoisted_batch(Context* c, const HoistItem* items, int n, cudaStream_t s);
+// op_hoisted_batch without the ModDown: out0 / out1 of every rotation are extended-basis
+// buffers (l + K limbs) that receive the automorphism-scattered key-switch outputs (+ P c0, or
+// + c0x), i.e. P times the rotated ciphertext up to the ModDown rounding.
+void op_hoisted_ext_batch(Context* c, const HoistItem* items, int n_items, cudaStream_t s);
+// ModDown of n extended-basis polynomials exts[i] (l_i + K limbs; their special limbs are
+// transformed in place) into outs[i] (l_i limbs), EVAL in and out.
+void op_moddown_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n, cudaStream_t s);
+// ModDown followed by the rescale by q_(l_i - 1), fused (outs[i]: l_i - 1 limbs).
+void op_moddown_rescale_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n,
+                              cudaStream_t s);
 // Hoisted rotations from ModUp digits computed earlier (op_modup of c1, own-digit limbs included):
 // rotation j = automorphism ks[j] with key keys[j]; outputs [l][N] each.
 void op_hoisted_digits(Context* c, const uint64_t* c0, const uint64_t* digits, int l, const uint64_t* const* keys,

@@ -84,7 +84,7 @@ class _BootParams(C.Structure):
     _fields_ = [("level_budget_cts", C.c_int), ("level_budget_stc", C.c_int), ("top_level", C.c_int),
                 ("top_scale", C.c_double), ("msg_scale", C.c_double), ("K", C.c_int), ("r", C.c_int),
                 ("degree", C.c_int), ("baby", C.c_int), ("prescale_bits", C.c_int), ("sparse_encapsulation", C.c_int),
-                ("correction_bits", C.c_int)]
+                ("correction_bits", C.c_int), ("double_hoist", C.c_int)]
 
 
 def build(force: bool = False) -> str:
@@ -818,10 +818,10 @@ class NativeBootstrapper:
 
     def __init__(self, ctx: "Context", top_level: int, top_scale: float, msg_scale: float, budget=(3, 3),
                  K: int = 12, r: int = 3, degree: int = 63, baby: int = 8, prescale_bits: int = 0,
-                 encapsulation: bool = False, correction_bits: int = 0):
+                 encapsulation: bool = False, correction_bits: int = 0, double_hoist: bool = True):
         self.ctx = ctx
         p = _BootParams(budget[0], budget[1], top_level, float(top_scale), float(msg_scale), K, r, degree, baby,
-                        prescale_bits, 1 if encapsulation else 0, correction_bits)
+                        prescale_bits, 1 if encapsulation else 0, correction_bits, 1 if double_hoist else 0)
         h = vp()
         _check(lib().fides_boot_create(ctx._h, C.byref(p), C.byref(h)))
         self._h = h

@@ -46,6 +46,7 @@ class CryptoContextImpl {
   std::vector<double> S_;  // canonical scale of each level (FLEXIBLEAUTO)
   fides_boot* boot_ = nullptr;
   double boot_msg_scale_ = 0;
+  bool boot_double_hoist_ = true;
   std::unique_ptr<KeySwitchingKey> to_sparse_, to_dense_;
 
   int N() const { return cc_->N; }
@@ -246,9 +247,13 @@ class CryptoContextImpl {
     boot_msg_scale_ = msgScale > 0 ? msgScale : S_[1];
     fides_boot_params p{(int)levelBudget[0], (int)levelBudget[1], cc_->L, S_[cc_->L], boot_msg_scale_, 12, 3, 63,
                         dim1.empty() || dim1[0] == 0 ? 8 : (int)dim1[0], (int)correctionFactor,
-                        to_sparse_ && to_dense_ ? 1 : 0, 0};
+                        to_sparse_ && to_dense_ ? 1 : 0, 0, boot_double_hoist_ ? 1 : 0};
     check(fides_boot_create(cc_->handle(), &p, &boot_));
   }
+  // Double-hoisted linear transforms in the bootstrap (fides_boot_params::double_hoist; on by
+  // default, about 8-10 % faster).  Set before EvalBootstrapSetup; off gives the single-hoisted
+  // form's results bit for bit.
+  void SetBootstrapDoubleHoisting(bool on) { boot_double_hoist_ = on; }
   // Rotation indexes whose keys EvalBootstrap needs (register them with Context::AddRotationKey,
   // with the conjugation key 2N - 1 and the relinearisation key).
   std::vector<int> GetBootstrapRotations() const {

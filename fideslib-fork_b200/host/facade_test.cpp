@@ -46,7 +46,7 @@ extern "C" {
 int facade_bootstrap(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale,
                      const uint64_t* relin, const uint64_t* conj, int n_rot, const int* rots,
                      const uint64_t* const* rot_keys, const uint64_t* to_sparse, const uint64_t* to_dense,
-                     double msg_scale, int prescale_bits, int n_boot, const uint64_t* const* c0s,
+                     double msg_scale, int prescale_bits, int double_hoist, int n_boot, const uint64_t* const* c0s,
                      const uint64_t* const* c1s, uint64_t* const* out0, uint64_t* const* out1, uint64_t* const* bo0,
                      uint64_t* const* bo1, int* out_level, double* out_scale, char* err, int err_len) {
   try {
@@ -63,6 +63,7 @@ int facade_bootstrap(int logN, int n_q, int K, int dnum, const uint64_t* primes,
     {
       CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
       if (to_sparse && to_dense) ev.SetSparseEncapsulationKeys(key_from(cc, to_sparse), key_from(cc, to_dense));
+      ev.SetBootstrapDoubleHoisting(double_hoist != 0);
       ev.EvalBootstrapSetup({3, 3}, {0, 0}, (uint32_t)(N / 2), (uint32_t)prescale_bits, msg_scale);
       ev.EvalBootstrapPrepare();
       std::vector<Ciphertext> in;

@@ -451,6 +451,11 @@ typedef struct fides_boot_params {
                           * 2^correction_bits -- multiplied by round(q_1 / 2^k) and rescaled by q_1 --
                           * so that a message at a scale close to q_0 (scaling primes nearly as
                           * large as q_0) leaves EvalMod room; OpenFHE's correction factor */
+  int double_hoist;      /* 1: the linear transforms keep their baby-step rotations and giant-step
+                          * outputs in the extended basis Q P (diagonals encoded with the special
+                          * limbs too): no ModDown per baby step, one ModDown of c1 per giant step
+                          * and one ModDown + rescale per transform.  Results then differ from
+                          * the single-hoisted form in the ModDown rounding only. */
 } fides_boot_params;
 typedef struct fides_boot fides_boot;
 int fides_boot_create(fides_ctx* ctx, const fides_boot_params* params, fides_boot** out);

@@ -355,7 +355,8 @@ def native_for(F, prm, ev, bs, encaps=None):
     """A NativeBootstrapper with the Python driver's parameters and keys."""
     nb = F.NativeBootstrapper(ev.ctx, top_level=prm.n_q, top_scale=ev.S[prm.n_q], msg_scale=2.0 ** 50,
                               budget=(bs.cts_levels, bs.stc_levels), K=bs.K, r=bs.r, degree=bs.degree, baby=bs.baby,
-                              prescale_bits=bs.prescale.bit_length() - 1, encapsulation=encaps is not None)
+                              prescale_bits=bs.prescale.bit_length() - 1, encapsulation=encaps is not None,
+                              double_hoist=False)  # the Python driver's single-hoisted form
     nb.set_keys(ev.rk, ev.conj_key, *(encaps or (None, None)))
     for r in nb.rotations():
         nb.set_rotation_key(r, ev.rot_keys[r])
@@ -489,14 +490,14 @@ def _facade_lib():
     vp, u64p, dp, ip = C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_int)
     vpp = C.POINTER(vp)
     lib.facade_bootstrap.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, vp, C.c_int, ip, vpp,
-                                     vp, vp, C.c_double, C.c_int, C.c_int, vpp, vpp, vpp, vpp, vpp, vpp, ip, dp,
-                                     C.c_char_p, C.c_int]
+                                     vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, vpp, vpp, vpp, vpp, vpp, vpp, ip,
+                                     dp, C.c_char_p, C.c_int]
     lib.facade_arith.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, C.c_int, vp, C.c_int,
                                  u64p, u64p, u64p, u64p, u64p, u64p, C.c_char_p, C.c_int]
     return lib
 
 
-def facade_bootstrap(F, prm, ev, bs, cts_host, encaps=None):
+def facade_bootstrap(F, prm, ev, bs, cts_host, encaps=None, double_hoist=False):
     """Runs the facade's EvalBootstrap (single and batch) on host level-1 ciphertexts; returns
     (singles, batch, out_level, out_scale) as host arrays."""
     import ctypes as C
@@ -516,7 +517,8 @@ def facade_bootstrap(F, prm, ev, bs, cts_host, encaps=None):
                               ev.S[prm.n_q], ev.rk.data_ptr(), ev.conj_key.data_ptr(), len(rots),
                               (C.c_int * len(rots))(*rots), (vp * len(rots))(*[ev.rot_keys[r].data_ptr() for r in rots]),
                               encaps[0].data_ptr() if encaps else None, encaps[1].data_ptr() if encaps else None,
-                              2.0 ** 50, bs.prescale.bit_length() - 1, nb_, arr(ins[0::2]), arr(ins[1::2]),
+                              2.0 ** 50, bs.prescale.bit_length() - 1, 1 if double_hoist else 0, nb_,
+                              arr(ins[0::2]), arr(ins[1::2]),
                               arr([o[0] for o in outs[:nb_]]), arr([o[1] for o in outs[:nb_]]),
                               arr([o[0] for o in outs[nb_:]]), arr([o[1] for o in outs[nb_:]]), C.byref(lvl),
                               C.byref(sc), err, 512)
@@ -662,3 +664,52 @@ def test_native_bootstrap_59bit_chain_correction(fides):
     print(f"59-bit chain bootstrap N=2^12: {bits:.1f} bits, out level {nb.out_level}")
     assert bits > 12
     nb.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("baby", [8, 16])
+def test_native_double_hoisted_n4096(fides, baby):
+    """N = 2^12, the C++ bootstrapper with double-hoisted linear transforms (baby steps and
+    giant-step outputs in the extended basis, one ModDown + rescale per transform): the
+    precision stays within half a bit of the single-hoisted form's on the same inputs, and a
+    batch through fides_bootstrap_batch equals the single bootstraps bit for bit."""
+    import torch
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    delta = 2.0 ** 50
+    rng = xrng(71)
+    n = prm.N // 2
+    zs, cts = [], []
+    for _ in range(3):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        zs.append(z)
+        cts.append(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    bits = {}
+    for dh in (False, True):
+        nb = F.NativeBootstrapper(ctx, top_level=prm.n_q, top_scale=ev.S[prm.n_q], msg_scale=delta, K=bs.K, r=bs.r,
+                                  degree=bs.degree, baby=baby, prescale_bits=bs.prescale.bit_length() - 1,
+                                  double_hoist=dh)
+        nb.set_keys(ev.rk, ev.conj_key)
+        for r in nb.rotations():
+            if r not in ev.rot_keys:
+                ev.rot_keys[r] = F.to_device(kg.rotation_key(r))
+            nb.set_rotation_key(r, ev.rot_keys[r])
+        nb.prepare()
+        batch = nb.bootstrap_batch(cts)
+        single = nb.bootstrap(cts[1])
+        torch.cuda.synchronize()
+        assert torch.equal(single.c0, batch[1].c0) and torch.equal(single.c1, batch[1].c1)
+        errs = [np.abs(decode(kg.decrypt_limb0(F.to_host(x.c0), F.to_host(x.c1)), prm.N, nb.out_scale) - z).max()
+                for x, z in zip(batch, zs)]
+        bits[dh] = -math.log2(max(errs))
+        if dh and baby == 8:  # the C++ facade's EvalBootstrap in the same form
+            host = [(F.to_host(c.c0), F.to_host(c.c1)) for c in cts[:2]]
+            fs, fb, L, _ = facade_bootstrap(F, prm, ev, bs, host, double_hoist=True)
+            assert L == nb.out_level
+            for i in range(2):
+                for got in (fs[i], fb[i]):
+                    assert np.array_equal(got[0], F.to_host(batch[i].c0)) and np.array_equal(got[1], F.to_host(batch[i].c1))
+        nb.close()
+    print(f"N=2^12 baby {baby}: single-hoisted {bits[False]:.2f} bits, double-hoisted {bits[True]:.2f} bits")
+    assert bits[True] > 12 and bits[True] >= bits[False] - 0.5

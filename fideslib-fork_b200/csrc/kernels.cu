@@ -451,37 +451,41 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
   *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
 }
 
-// NB: register capacity for the baby steps (8: 56 registers; 16: about 126)
+// One CTA per (giant step, lane, coefficient tile, limb): a thread loads its coefficient of the
+// lane's baby steps and of the giant step's diagonals in one round of independent loads and
+// forms one output pair.  The CTAs of one (tile, limb) are adjacent (giant step fastest, then
+// lane), so the other giant steps' reads of a baby-step tile and the other lanes' reads of a
+// diagonal tile come from L2: DRAM reads each tile once.  (Looping over the giant steps inside a
+// thread exposed one memory latency per giant step: 15 long-scoreboard stalls per issue.)
+// NB: register capacity for the baby steps.
 template <int NB>
 __global__ void __launch_bounds__(EW_THREADS) bsgs_dot_kernel(const __grid_constant__ BsgsJob J,
                                                               const DevPrime* primes, int logN) {
-  const int lane = blockIdx.x, j = blockIdx.z;
+  const int i = blockIdx.x % J.ng, lane = blockIdx.x / J.ng, j = blockIdx.z;
   const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
   const size_t off = ((size_t)j << logN) + blockIdx.y * blockDim.x + threadIdx.x;
-  uint64_t a[NB], b[NB];
+  uint64_t a[NB], b[NB], w[NB];
 #pragma unroll
   for (int k = 0; k < NB; ++k)
-    if (k < J.nb) {
+    if (k < J.nb && J.pt[i][k]) {
+      w[k] = J.pt[i][k][off];
       a[k] = J.x0[lane][k][off];
       b[k] = J.x1[lane][k][off];
     }
-  for (int i = 0; i < J.ng; ++i) {
-    U128 s0{0, 0}, s1{0, 0};
+  U128 s0{0, 0}, s1{0, 0};
 #pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      if (k == 15) {  // keep the sums below 2^128: at most 15 products of values below 2^62
-        s0 = U128{reduce128(s0, p), 0};
-        s1 = U128{reduce128(s1, p), 0};
-      }
-      if (k < J.nb && J.pt[i][k]) {
-        const uint64_t w = J.pt[i][k][off];
-        mac128(s0, w, a[k]);
-        mac128(s1, w, b[k]);
-      }
+  for (int k = 0; k < NB; ++k) {
+    if (k == 15) {  // keep the sums below 2^128: at most 15 products of values below 2^62
+      s0 = U128{reduce128(s0, p), 0};
+      s1 = U128{reduce128(s1, p), 0};
     }
-    J.out0[lane][i][off] = reduce128(s0, p);
-    J.out1[lane][i][off] = reduce128(s1, p);
+    if (k < J.nb && J.pt[i][k]) {
+      mac128(s0, w[k], a[k]);
+      mac128(s1, w[k], b[k]);
+    }
   }
+  J.out0[lane][i][off] = reduce128(s0, p);
+  J.out1[lane][i][off] = reduce128(s1, p);
 }
 
 __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
@@ -603,7 +607,7 @@ void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s) {
   int terms = 0;
   for (int i = 0; i < job.ng; ++i)
     for (int k = 0; k < job.nb; ++k) terms += job.pt[i][k] != nullptr;
-  dim3 grid(job.lanes, c->N / EW_THREADS, job.l);
+  dim3 grid(job.lanes * job.ng, c->N / EW_THREADS, job.l);
   LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (terms + job.lanes * 2.0 * (job.nb + job.ng)));
   if (job.nb <= 8)
     bsgs_dot_kernel<8><<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
@@ -662,6 +666,8 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
     int mx = 0;
     for (int i = 0; i < m; ++i) mx = std::max(mx, L.j[i].l + c->K);
     const int jg = gmax == 1 ? 1 : gmax == 2 ? 2 : 4;
+    int maxb = 0;
+    for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     dim3 grid(c->N / (2 * EW_THREADS), mx, L.ngroups);
     // algorithmic bytes: each job's digits, outputs and extra operands, and each group's key once
     double bytes = 0;
@@ -676,8 +682,6 @@ void launch_ksk(Context* c, const KskJob* jobs, int n, cudaStream_t s) {
       bytes += 8.0 * c->N * (share_digits ? (double)b * ext + 2.0 * b * ext * L.gcount[g] - (double)b * ext * L.gcount[g]
                                           : 2.0 * b * ext);
     }
-    int maxb = 0;
-    for (int i = 0; i < m; ++i) maxb = std::max(maxb, c->beta(L.j[i].l));
     LaunchScope ls(c, s, KK_KSK, bytes);
     auto go = [&](auto kern) { kern<<<grid, EW_THREADS, 0, s>>>(L, c->d_prime, c->d_pmod, c->d_f64, c->logN, c->n_q,
                                                               c->K, c->dnum, c->alpha); };

@@ -175,10 +175,9 @@ __host__ __device__ inline int ext_prime(int j, int lq, int nq) { return (lq == 
 void launch_dot_plain(Context* c, const DotJob& job, cudaStream_t s);
 
 // ---- every giant step's inner product of a BSGS linear transform in one launch:
-// out_i = sum_j pt[i][j] * x_j for all giant steps i, reading each baby-step ciphertext x_j
-// once (one launch per giant step reads each of them once per giant step).  A thread keeps its
-// coefficient of all baby steps in registers and runs the giant steps over them; lanes (the
-// ciphertexts of a batch) share the diagonals as in DotJob.
+// out_i = sum_j pt[i][j] * x_j for all giant steps i, each baby-step ciphertext x_j and each
+// diagonal read from DRAM once (one launch per giant step reads each x_j once per giant step);
+// lanes (the ciphertexts of a batch) share the diagonals as in DotJob.
 constexpr int MAX_BSGS_BABY = 16;
 constexpr int MAX_BSGS_GIANT = 16;
 constexpr int MAX_BSGS_LANES = 8;

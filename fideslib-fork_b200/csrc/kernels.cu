@@ -427,6 +427,8 @@ __global__ void __launch_bounds__(EW_THREADS) scalar_kernel(const __grid_constan
 
 // Two adjacent coefficients per thread; sums of up to 15 products (< 2^124 each) stay below
 // 2^128 before a reduction.
+constexpr int LC_BLOCK = 4;  // terms per block of loads (lincomb_kernel, dot_plain_kernel)
+
 __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_constant__ DotJob J,
                                                                const DevPrime* primes, int logN) {
   const int lane = blockIdx.x, j = blockIdx.z;
@@ -434,18 +436,29 @@ __global__ void __launch_bounds__(EW_THREADS) dot_plain_kernel(const __grid_cons
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.y * blockDim.x + threadIdx.x);
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
-  for (int t = 0; t < J.n; ++t) {
-    if (t && t % 15 == 0) {
+  for (int t0 = 0; t0 < J.n; t0 += LC_BLOCK) {  // as lincomb_kernel
+    if (t0 && t0 % 12 == 0) {
       a0 = U128{reduce128(a0, p), 0};
       a1 = U128{reduce128(a1, p), 0};
       b0 = U128{reduce128(b0, p), 0};
       b1 = U128{reduce128(b1, p), 0};
     }
-    const ulonglong2 w = ld2(J.pt[t] + off), x = ld2(J.c0[lane][t] + off), y = ld2(J.c1[lane][t] + off);
-    mac128(a0, w.x, x.x);
-    mac128(a1, w.y, x.y);
-    mac128(b0, w.x, y.x);
-    mac128(b1, w.y, y.y);
+    ulonglong2 w[LC_BLOCK], x[LC_BLOCK], y[LC_BLOCK];
+#pragma unroll
+    for (int u = 0; u < LC_BLOCK; ++u)
+      if (t0 + u < J.n) {
+        w[u] = ld2(J.pt[t0 + u] + off);
+        x[u] = ld2(J.c0[lane][t0 + u] + off);
+        y[u] = ld2(J.c1[lane][t0 + u] + off);
+      }
+#pragma unroll
+    for (int u = 0; u < LC_BLOCK; ++u)
+      if (t0 + u < J.n) {
+        mac128(a0, w[u].x, x[u].x);
+        mac128(a1, w[u].y, x[u].y);
+        mac128(b0, w[u].x, y[u].x);
+        mac128(b1, w[u].y, y[u].y);
+      }
   }
   *reinterpret_cast<ulonglong2*>(J.out0[lane] + off) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
   *reinterpret_cast<ulonglong2*>(J.out1[lane] + off) = make_ulonglong2(reduce128(b0, p), reduce128(b1, p));
@@ -495,19 +508,32 @@ __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_consta
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
   U128 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
-  for (int t = 0; t < J.n; ++t) {
-    if (t && t % 15 == 0) {
+  // terms in blocks of LC_BLOCK whose loads are all issued before their products, so that a
+  // thread waits for memory once per block rather than once per term; the sums are reduced
+  // every 12 terms (below 2^128: a residue plus 12 products of values below 2^62)
+  for (int t0 = 0; t0 < J.n; t0 += LC_BLOCK) {
+    if (t0 && t0 % 12 == 0) {
       a0 = U128{reduce128(a0, p), 0};
       a1 = U128{reduce128(a1, p), 0};
       b0 = U128{reduce128(b0, p), 0};
       b1 = U128{reduce128(b1, p), 0};
     }
-    const uint64_t w = J.s[t][j];
-    const ulonglong2 x = ld2(J.x0[lane][t] + off), y = ld2(J.x1[lane][t] + off);
-    mac128(a0, w, x.x);
-    mac128(a1, w, x.y);
-    mac128(b0, w, y.x);
-    mac128(b1, w, y.y);
+    ulonglong2 x[LC_BLOCK], y[LC_BLOCK];
+#pragma unroll
+    for (int u = 0; u < LC_BLOCK; ++u)
+      if (t0 + u < J.n) {
+        x[u] = ld2(J.x0[lane][t0 + u] + off);
+        y[u] = ld2(J.x1[lane][t0 + u] + off);
+      }
+#pragma unroll
+    for (int u = 0; u < LC_BLOCK; ++u)
+      if (t0 + u < J.n) {
+        const uint64_t w = J.s[t0 + u][j];
+        mac128(a0, w, x[u].x);
+        mac128(a1, w, x[u].y);
+        mac128(b0, w, y[u].x);
+        mac128(b1, w, y[u].y);
+      }
   }
   const uint64_t ad = J.add0[j];
   *reinterpret_cast<ulonglong2*>(J.out0[lane] + off) =

@@ -441,7 +441,8 @@ def test_native_bootstrap_equals_python_driver_n4096(fides):
 def test_native_bootstrap_config_d_n65536(fides, config_d):
     """Config D through the C++ bootstrapper: encapsulation, prescale 2^5, budget {3, 3};
     >= 15 bits for a batch of 8 (fides_bootstrap_batch), batch = single bit for bit, and the
-    single equals the Python driver's on the same tables."""
+    single equals the Python driver's on the same tables; the double-hoisted form likewise
+    >= 15 bits with batch = single."""
     import torch
     from fides_b200 import bootstrap as B
     F = fides
@@ -479,6 +480,23 @@ def test_native_bootstrap_config_d_n65536(fides, config_d):
         for got in (fs[i], fb[i]):
             assert np.array_equal(got[0], F.to_host(batch[i].c0)) and np.array_equal(got[1], F.to_host(batch[i].c1))
     nb.close()
+    # the double-hoisted form (the library's default) on the same inputs and keys
+    nd = F.NativeBootstrapper(ctx, top_level=prm.n_q, top_scale=ev.S[prm.n_q], msg_scale=delta,
+                              budget=(bs.cts_levels, bs.stc_levels), K=bs.K, r=bs.r, degree=bs.degree, baby=bs.baby,
+                              prescale_bits=bs.prescale.bit_length() - 1, encapsulation=True, double_hoist=True)
+    nd.set_keys(ev.rk, ev.conj_key, *bs.encapsulation)
+    for r in nd.rotations():
+        nd.set_rotation_key(r, ev.rot_keys[r])
+    nd.prepare()
+    dbatch = nd.bootstrap_batch(cts)
+    dsingle = nd.bootstrap(cts[3])
+    torch.cuda.synchronize()
+    assert torch.equal(dsingle.c0, dbatch[3].c0) and torch.equal(dsingle.c1, dbatch[3].c1)
+    dbits = [-math.log2(np.abs(decode(kg.decrypt_limb0(F.to_host(x.c0), F.to_host(x.c1)), prm.N, nd.out_scale)
+                                - z).max()) for x, z in zip(dbatch, zs)]
+    print(f"config D, double-hoisted: precision {min(dbits):.2f}..{max(dbits):.2f} bits")
+    assert min(dbits) >= 15.0
+    nd.close()
 
 
 # ---------------------------------------------------------------- the C++ evaluation facade

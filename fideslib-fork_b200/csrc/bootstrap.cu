@@ -703,6 +703,10 @@ struct Bootstrapper {
       scale = S[level];
     }
     cts_out_level = level;
+    if (prm.double_hoist)  // the double-hoisted transform sums its giant steps in one combination
+      for (const auto& P : cts_pl)
+        if (P.giant.size() > (size_t)MAX_BSGS_GIANT || P.giant.size() > (size_t)MAX_LC_TERMS)
+          throw Error(FIDES_ERR_ARG, "double hoisting supports at most 16 giant steps per transform");
     const int depth = (int)std::ceil(std::log2((double)prm.degree)) + 1 + prm.r;
     stc_in_level = cts_out_level - depth;
     if (stc_in_level - (int)stc.size() < 1) throw Error(-4, "bootstrap: not enough levels for the chosen budget");
@@ -713,6 +717,10 @@ struct Bootstrapper {
       level -= 1;
     }
     out_level = level;
+    if (prm.double_hoist)
+      for (const auto& P : stc_pl)
+        if (P.giant.size() > (size_t)MAX_BSGS_GIANT || P.giant.size() > (size_t)MAX_LC_TERMS)
+          throw Error(FIDES_ERR_ARG, "double hoisting supports at most 16 giant steps per transform");
     std::vector<double> mono(c->N, 0.0);
     mono[c->N / 2] = 1;  // X^(N/2): slots times i
     pt_i = int_pt(mono, top_level, s);
@@ -1226,6 +1234,8 @@ int fides_boot_create(fides_ctx* ctx, const fides_boot_params* p, fides_boot** o
       throw fides::Error(FIDES_ERR_ARG, "EvalMod / BSGS parameters out of range");
     if (p->correction_bits < 0 || p->correction_bits > 40 || (p->correction_bits > 0 && c->n_q < 3))
       throw fides::Error(FIDES_ERR_ARG, "correction_bits out of range (and needs q_1)");
+    if (p->double_hoist && p->baby > fides::MAX_BSGS_BABY)
+      throw fides::Error(FIDES_ERR_ARG, "double hoisting supports at most 16 baby steps");
     if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "bootstrapping needs special primes");
     auto* bs = new fides::Bootstrapper{};
     bs->c = c;

@@ -725,6 +725,33 @@ int fides_hmult_batch(fides_ctx* x, const fides_hmult_item* items, int n, const 
   });
 }
 
+int fides_mixed_batch(fides_ctx* x, const fides_hmult_item* hm, int n_hm, const uint64_t* relin_key, int rescale,
+                      const fides_rotate_item* rot, int n_rot, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (n_hm < 0 || n_rot < 0) throw fides::Error(FIDES_ERR_ARG, "negative batch");
+    if ((n_hm && !hm) || (n_rot && !rot)) throw fides::Error(FIDES_ERR_ARG, "null items");
+    std::vector<fides::HMultItem> vh(n_hm);
+    for (int i = 0; i < n_hm; ++i) {
+      const fides_hmult_item& s = hm[i];
+      for (const void* p : {(const void*)s.a0, (const void*)s.a1, (const void*)s.b0, (const void*)s.b1,
+                            (const void*)s.out0, (const void*)s.out1})
+        need(p, "hmult item operand");
+      vh[i] = fides::HMultItem{s.a0, s.a1, s.b0, s.b1, s.out0, s.out1, s.level};
+    }
+    std::vector<fides::RotateItem> vr(n_rot);
+    for (int i = 0; i < n_rot; ++i) {
+      const fides_rotate_item& s = rot[i];
+      for (const void* p : {(const void*)s.c0, (const void*)s.c1, (const void*)s.out0, (const void*)s.out1})
+        need(p, "rotate item operand");
+      if ((s.auto_index & 1) == 0 || s.auto_index >= 2u * (uint32_t)c->N)
+        throw fides::Error(FIDES_ERR_ARG, "automorphism index must be odd and < 2N");
+      vr[i] = fides::RotateItem{s.c0, s.c1, s.out0, s.out1, s.key, s.level, s.auto_index};
+    }
+    fides::op_mixed_batch(c, vh.data(), n_hm, relin_key, rescale != 0, vr.data(), n_rot, S(stream));
+  });
+}
+
 int fides_rotate_batch(fides_ctx* x, const fides_rotate_item* items, int n, void* stream) {
   return guard([&] {
     auto* c = C(x);

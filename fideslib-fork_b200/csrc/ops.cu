@@ -39,10 +39,9 @@ void check_level(Context* c, int l, int min_l = 1) {
   if (l < min_l || l > c->n_q) throw Error(-4, "level " + std::to_string(l) + " out of range");
 }
 
-// ModUp of n inputs: INTT of xs[i] (times ys[i] when given) into tmps[i], conversion of each
-// digit into digits[i], NTT of the new limbs.  Own-digit limbs of digits[i] are not written.
-void modup_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
-                 uint64_t* const* tmps, uint64_t* const* digits, int n, cudaStream_t s) {
+// ModUp, first phase: INTT of xs[i] (times ys[i] when given) into tmps[i].
+void modup_intt(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
+                uint64_t* const* tmps, int n, cudaStream_t s) {
   const size_t N = c->N;
   std::vector<LimbRef> refs;
   for (int i = 0; i < n; ++i)
@@ -53,8 +52,16 @@ void modup_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* y
       refs.push_back(r);
     }
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s, ys ? IN_MUL : IN_PLAIN);
+}
+
+// ModUp, second phase: conversion of each digit of tmps[i] into digits[i], NTT of the new
+// limbs (one conversion launch and one NTT launch sequence for all n inputs).  Own-digit
+// limbs of digits[i] are not written.
+void modup_convert(Context* c, const int* ls, uint64_t* const* tmps, uint64_t* const* digits, int n,
+                   cudaStream_t s) {
+  const size_t N = c->N;
   std::vector<ConvJob> jobs;
-  refs.clear();
+  std::vector<LimbRef> refs;
   for (int i = 0; i < n; ++i) {
     const int l = ls[i], ext = l + c->K, b = c->beta(l);
     for (int d = 0; d < b; ++d) {
@@ -70,10 +77,18 @@ void modup_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* y
   ntt_limbs(c, refs.data(), (int)refs.size(), false, s);
 }
 
-// ModDown of extended polys exts[i] (special limbs are transformed in place) into outs[i],
-// adding adds[i] when given.
-void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs, uint64_t* const* outs,
-                   const uint64_t* const* adds, int n, cudaStream_t s) {
+// ModUp of n inputs: INTT of xs[i] (times ys[i] when given) into tmps[i], conversion of each
+// digit into digits[i], NTT of the new limbs.  Own-digit limbs of digits[i] are not written.
+void modup_stage(Context* c, const uint64_t* const* xs, const uint64_t* const* ys, const int* ls,
+                 uint64_t* const* tmps, uint64_t* const* digits, int n, cudaStream_t s) {
+  modup_intt(c, xs, ys, ls, tmps, n, s);
+  modup_convert(c, ls, tmps, digits, n, s);
+}
+
+// ModDown, first phase: INTT of the special limbs of the extended polys exts[i] (in place)
+// and their conversion to the Q basis into convs[i] (coefficient form).
+void moddown_prep(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs, int n,
+                  cudaStream_t s) {
   const size_t N = c->N;
   const int K = c->K;
   if (K == 0) throw Error(-1, "ModDown needs special primes");
@@ -82,10 +97,17 @@ void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* c
     for (int k = 0; k < K; ++k) refs.push_back(lref(exts[i] + (ls[i] + k) * N, c->n_q + k));
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
   std::vector<ConvJob> jobs;
-  refs.clear();
+  for (int i = 0; i < n; ++i) jobs.push_back(ConvJob{c->moddown_tab[ls[i]], exts[i] + ls[i] * N, convs[i]});
+  launch_conv(c, jobs.data(), (int)jobs.size(), s);
+}
+
+// ModDown, second phase: out = (x - NTT(conv)) P^-1 (+ adds[i]) in one NTT launch sequence.
+void moddown_finish(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs,
+                    uint64_t* const* outs, const uint64_t* const* adds, int n, cudaStream_t s) {
+  const size_t N = c->N;
+  std::vector<LimbRef> refs;
   for (int i = 0; i < n; ++i) {
     const int l = ls[i];
-    jobs.push_back(ConvJob{c->moddown_tab[l], exts[i] + l * N, convs[i]});
     for (int j = 0; j < l; ++j) {
       LimbRef r = lref(outs[i] + j * N, j);
       r.src = convs[i] + j * N;
@@ -94,8 +116,15 @@ void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* c
       refs.push_back(r);
     }
   }
-  launch_conv(c, jobs.data(), (int)jobs.size(), s);
   ntt_limbs(c, refs.data(), (int)refs.size(), false, s, IN_PLAIN, OUT_MODDOWN);
+}
+
+// ModDown of extended polys exts[i] (special limbs are transformed in place) into outs[i],
+// adding adds[i] when given.
+void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs, uint64_t* const* outs,
+                   const uint64_t* const* adds, int n, cudaStream_t s) {
+  moddown_prep(c, exts, ls, convs, n, s);
+  moddown_finish(c, exts, ls, convs, outs, adds, n, s);
 }
 
 // ModDown fused with the rescale that follows it.  With u = ModDown(x) + add the value
@@ -106,22 +135,16 @@ void moddown_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* c
 // so the result equals ModDown followed by Rescale (reference: NTT<NTT_MODDOWN> then
 // rescale, src/CKKS/LimbPartitionMGPU.cu:89-232) bit for bit, with one INTT and l - 1 NTTs
 // in place of l NTTs, one INTT and l - 1 NTTs.
-void moddown_rescale_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs,
-                           uint64_t* const* tops, uint64_t* const* outs, const uint64_t* const* adds, int n,
-                           cudaStream_t s) {
+// Second phase of a ModDown fused with the rescale (after moddown_prep): the top limb's INTT
+// and the forward transforms of the other limbs with the conv + P SwitchModulus(top) prologue.
+void moddown_rescale_finish(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs,
+                            uint64_t* const* tops, uint64_t* const* outs, const uint64_t* const* adds, int n,
+                            cudaStream_t s) {
   const size_t N = c->N;
-  const int K = c->K;
-  if (K == 0) throw Error(-1, "ModDown needs special primes");
-  std::vector<LimbRef> refs;
-  for (int i = 0; i < n; ++i)
-    for (int k = 0; k < K; ++k) refs.push_back(lref(exts[i] + (ls[i] + k) * N, c->n_q + k));
-  ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
-  std::vector<ConvJob> jobs;
   std::vector<LimbRef> top_add, top_plain, fwd;
   for (int i = 0; i < n; ++i) {
     const int l = ls[i];
     const uint64_t* add = adds ? adds[i] : nullptr;
-    jobs.push_back(ConvJob{c->moddown_tab[l], exts[i] + l * N, convs[i]});
     LimbRef t = lref(tops[i], l - 1);
     t.src = exts[i] + (size_t)(l - 1) * N;
     t.pro = add ? add + (size_t)(l - 1) * N : nullptr;
@@ -137,10 +160,16 @@ void moddown_rescale_stage(Context* c, uint64_t* const* exts, const int* ls, uin
       fwd.push_back(r);
     }
   }
-  launch_conv(c, jobs.data(), (int)jobs.size(), s);
   ntt_limbs(c, top_add.data(), (int)top_add.size(), true, s, IN_ADD_PMUL, OUT_SUB_PINV);
   ntt_limbs(c, top_plain.data(), (int)top_plain.size(), true, s, IN_PLAIN, OUT_SUB_PINV);
   ntt_limbs(c, fwd.data(), (int)fwd.size(), false, s, IN_CONV_SW, OUT_MDRS);
+}
+
+void moddown_rescale_stage(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* convs,
+                           uint64_t* const* tops, uint64_t* const* outs, const uint64_t* const* adds, int n,
+                           cudaStream_t s) {
+  moddown_prep(c, exts, ls, convs, n, s);
+  moddown_rescale_finish(c, exts, ls, convs, tops, outs, adds, n, s);
 }
 
 // Scratch limbs of one key switch at level l: INTT copy, digits, A, B, two conversions,
@@ -373,6 +402,82 @@ void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s)
   modup_stage(c, xs.data(), nullptr, ls.data(), tmp.data(), dig.data(), n, s);
   launch_ksk(c, kj.data(), n, s);
   moddown_stage(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * n, s);
+}
+
+void op_mixed_batch(Context* c, const HMultItem* hm, int nh, const uint64_t* relin_key, bool rescale,
+                    const RotateItem* ro, int nr, cudaStream_t s) {
+  // HMults and rotations share the stages that do not depend on the kind: one conversion and
+  // one NTT launch sequence for every ModUp, one KSK launch (groups by key), one special-limb
+  // INTT and one conversion for every ModDown.  The kind-specific transforms (the INTT with
+  // the a1 b1 prologue, the final ModDown / ModDown + rescale transforms) stay separate
+  // launches.  Each item's arithmetic is that of op_hmult_batch / op_rotate_batch.
+  if (nh <= 0 && nr <= 0) return;
+  if (nh > 0 && !relin_key) throw Error(-5, "null relinearization key");
+  const size_t N = c->N;
+  size_t total = 0;
+  for (int i = 0; i < nh; ++i) {
+    check_level(c, hm[i].l, rescale ? 2 : 1);
+    total += ks_limbs(c, hm[i].l);
+  }
+  for (int i = 0; i < nr; ++i) {
+    check_level(c, ro[i].l);
+    if (!ro[i].key) throw Error(-5, "null rotation key");
+    total += ks_limbs(c, ro[i].l);
+  }
+  Scratch sc(c, sizeof(uint64_t) * N * total, s);
+  Bump bp{sc.u64(), N};
+  const int n = nh + nr;
+  std::vector<const uint64_t*> hx(nh), hy(nh), rx(nr);
+  std::vector<int> ls(n), ls2(2 * n);
+  std::vector<uint64_t*> tmp(n), dig(n), ex(2 * n), conv(2 * n), tops(2 * n), outs(2 * n);
+  std::vector<KskJob> kj;
+  for (int i = 0; i < n; ++i) {
+    const bool mult = i < nh;
+    const int l = mult ? hm[i].l : ro[i - nh].l, ext = l + c->K;
+    ls[i] = l;
+    tmp[i] = bp.take(l);
+    dig[i] = bp.take((size_t)c->beta(l) * ext);
+    uint64_t* A = bp.take(ext);
+    uint64_t* B = bp.take(ext);
+    if (mult) {
+      const HMultItem& it = hm[i];
+      hx[i] = it.a1;
+      hy[i] = it.b1;
+      KskJob job{it.a1, it.b1, dig[i], relin_key, nullptr, A, B, l, 0};
+      job.a0 = it.a0;
+      job.b0 = it.b0;
+      kj.push_back(job);
+      outs[2 * i] = it.out0;
+      outs[2 * i + 1] = it.out1;
+    } else {
+      const RotateItem& it = ro[i - nh];
+      rx[i - nh] = it.c1;
+      kj.push_back(KskJob{it.c1, nullptr, dig[i], it.key, it.c0, A, B, l, it.k});
+      outs[2 * i] = it.out0;
+      outs[2 * i + 1] = it.out1;
+    }
+    ex[2 * i] = B;
+    ex[2 * i + 1] = A;
+    conv[2 * i] = bp.take(l);
+    conv[2 * i + 1] = bp.take(l);
+    tops[2 * i] = bp.take(1);
+    tops[2 * i + 1] = bp.take(1);
+    ls2[2 * i] = ls2[2 * i + 1] = l;
+  }
+  if (nh) modup_intt(c, hx.data(), hy.data(), ls.data(), tmp.data(), nh, s);
+  if (nr) modup_intt(c, rx.data(), nullptr, ls.data() + nh, tmp.data() + nh, nr, s);
+  modup_convert(c, ls.data(), tmp.data(), dig.data(), n, s);
+  launch_ksk(c, kj.data(), n, s);
+  moddown_prep(c, ex.data(), ls2.data(), conv.data(), 2 * n, s);
+  if (nh) {
+    if (rescale)
+      moddown_rescale_finish(c, ex.data(), ls2.data(), conv.data(), tops.data(), outs.data(), nullptr, 2 * nh, s);
+    else
+      moddown_finish(c, ex.data(), ls2.data(), conv.data(), outs.data(), nullptr, 2 * nh, s);
+  }
+  if (nr)
+    moddown_finish(c, ex.data() + 2 * nh, ls2.data() + 2 * nh, conv.data() + 2 * nh, outs.data() + 2 * nh, nullptr,
+                   2 * nr, s);
 }
 
 namespace {

@@ -69,6 +69,12 @@ void op_rescale_batch(Context* c, const uint64_t* const* xs, const int* ls, uint
 void op_hmult_batch(Context* c, const HMultItem* items, int n, const uint64_t* relin_key, bool rescale,
                     cudaStream_t s);
 void op_rotate_batch(Context* c, const RotateItem* items, int n, cudaStream_t s);
+// HMults (relinearised with relin_key, rescaled when `rescale`) and rotations in one launch
+// sequence: the stages common to both kinds (the ModUp conversion and NTT, the KSK inner
+// product, the ModDown's special-limb INTT and conversion) run once over all items.  Results
+// equal op_hmult_batch / op_rotate_batch item for item.
+void op_mixed_batch(Context* c, const HMultItem* hm, int nh, const uint64_t* relin_key, bool rescale,
+                    const RotateItem* ro, int nr, cudaStream_t s);
 void op_hoisted(Context* c, const HoistItem& item, cudaStream_t s);
 // Hoisted rotations of several ciphertexts (any levels, own rotation lists) in one launch
 // sequence per stage.

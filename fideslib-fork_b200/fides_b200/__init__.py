@@ -163,6 +163,8 @@ def lib():
                                            C.POINTER(vp), C.POINTER(vp), vp]
         L.fides_hmult_batch.argtypes = [vp, C.POINTER(_HMultItem), C.c_int, vp, C.c_int, vp]
         L.fides_rotate_batch.argtypes = [vp, C.POINTER(_RotateItem), C.c_int, vp]
+        L.fides_mixed_batch.argtypes = [vp, C.POINTER(_HMultItem), C.c_int, vp, C.c_int, C.POINTER(_RotateItem),
+                                        C.c_int, vp]
         L.fides_key_upload.argtypes = [vp, u64p, C.POINTER(vp)]
         L.fides_key_free.argtypes = [vp, vp]
         L.fides_hmult_host.argtypes = [vp, u64p, u64p, u64p, u64p, C.c_int, vp, C.c_int, u64p, u64p]
@@ -687,6 +689,26 @@ class Context:
                                    auto_index(self.logN, r))
         _check(lib().fides_rotate_batch(self._h, items, n, _stream()))
         return outs
+
+    def mixed_batch(self, pairs, relin_key, rots, rescale=True) -> tuple[list[Ciphertext], list[Ciphertext]]:
+        """HMults of `pairs` and rotations `rots` ((ciphertext, key, rotation) jobs) in one launch
+        sequence (fides_mixed_batch); returns (products, rotated)."""
+        nh, nr = len(pairs), len(rots)
+        hout, rout = [], []
+        hitems, ritems = (_HMultItem * max(nh, 1))(), (_RotateItem * max(nr, 1))()
+        for i, (a, b) in enumerate(pairs):
+            lo = a.level - 1 if rescale else a.level
+            o = Ciphertext(self.empty(lo), self.empty(lo))
+            hout.append(o)
+            hitems[i] = _HMultItem(_ptr(a.c0), _ptr(a.c1), _ptr(b.c0), _ptr(b.c1), _ptr(o.c0), _ptr(o.c1), a.level)
+        for i, (ct, key, r) in enumerate(rots):
+            o = Ciphertext(self.empty(ct.level), self.empty(ct.level))
+            rout.append(o)
+            ritems[i] = _RotateItem(_ptr(ct.c0), _ptr(ct.c1), _ptr(o.c0), _ptr(o.c1), _ptr(key), ct.level,
+                                    auto_index(self.logN, r))
+        _check(lib().fides_mixed_batch(self._h, hitems, nh, _ptr(relin_key), 1 if rescale else 0, ritems, nr,
+                                       _stream()))
+        return hout, rout
 
     # -- host-buffer path --
     def key_upload(self, host_key) -> int:

@@ -280,6 +280,13 @@ typedef struct fides_rotate_item {
   uint32_t auto_index;
 } fides_rotate_item;
 int fides_rotate_batch(fides_ctx* ctx, const fides_rotate_item* items, int n, void* stream);
+/* HMults and rotations in one launch sequence: the stages common to both kinds (the ModUp's
+ * conversion and NTT, the KSK inner product, the ModDown's special-limb INTT and conversion) run
+ * once over all items, so small stages are launched once instead of twice.  Results equal
+ * fides_hmult_batch / fides_rotate_batch item for item.  No reference counterpart (the
+ * reference issues each operation kind separately). */
+int fides_mixed_batch(fides_ctx* ctx, const fides_hmult_item* hm, int n_hm, const uint64_t* relin_key, int rescale,
+                      const fides_rotate_item* rot, int n_rot, void* stream);
 
 /* ---- CUDA graphs ----------------------------------------------------------------------
  * Record everything the library enqueues on `stream` between begin and end into a graph

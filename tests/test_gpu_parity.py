@@ -383,3 +383,46 @@ def test_elementwise_kernels_config_c(Cfg, level):
     scal = np.array([[v] * Cfg.o.N for v in sc], dtype=np.uint64)
     assert eq(ctx.mul_scalar_poly(A, sc), o.mul(a[0], scal, ids))
     assert eq(ctx.add_scalar_poly(A, sc), o.add(a[0], scal, ids))
+
+
+@pytest.mark.gpu
+def test_mixed_batch_equals_separate_batches_and_oracle(fides):
+    """fides_mixed_batch: HMults (rescaled and not) and rotations at uneven levels in one launch
+    sequence equal fides_hmult_batch / fides_rotate_batch item for item, and the oracle."""
+    import torch
+    from fides_b200 import params as P
+    F = fides
+    prm = P.config_c(4)
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    ctx = F.Context(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=91)
+    rk = kg.relin_key()
+    keys = {r: kg.rotation_key(r) for r in (1, -3)}
+    rk_d = F.to_device(rk)
+    keys_d = {r: F.to_device(k) for r, k in keys.items()}
+    rng = xrng(4500)
+    hl, rl = [30, 9, 17], [6, 30, 12, 21]
+    hcts = [[uniform_limbs(rng, prm.q[:l], prm.N) for _ in range(4)] for l in hl]
+    rcts = [[uniform_limbs(rng, prm.q[:l], prm.N) for _ in range(2)] for l in rl]
+    dev = lambda c: F.Ciphertext(F.to_device(c[0]), F.to_device(c[1]))
+    pairs = [(dev(h[:2]), dev(h[2:])) for h in hcts]
+    rsel = [1, -3, 1, -3]
+    rots = [(dev(c), keys_d[r], r) for c, r in zip(rcts, rsel)]
+    for rescale in (True, False):
+        mh, mr = ctx.mixed_batch(pairs, rk_d, rots, rescale=rescale)
+        sh = ctx.mult_batch(pairs, rk_d, rescale=rescale)
+        sr = ctx.rotate_batch(rots)
+        torch.cuda.synchronize()
+        for a, b in zip(mh + mr, sh + sr):
+            assert torch.equal(a.c0, b.c0) and torch.equal(a.c1, b.c1)
+        for h, out in zip(hcts[:2], mh[:2]):
+            w0, w1 = o.hmult(*h, rk, rescale=rescale)
+            assert np.array_equal(F.to_host(out.c0), w0) and np.array_equal(F.to_host(out.c1), w1)
+    for c, r, out in list(zip(rcts, rsel, mr))[:2]:
+        w0, w1 = o.rotate(c[0], c[1], keys[r], r)
+        assert np.array_equal(F.to_host(out.c0), w0) and np.array_equal(F.to_host(out.c1), w1)
+    # only one kind, and neither
+    mh, mr = ctx.mixed_batch(pairs[:1], rk_d, [], rescale=True)
+    assert len(mh) == 1 and mr == []
+    mh, mr = ctx.mixed_batch([], rk_d, rots[:1])
+    assert mh == [] and len(mr) == 1

@@ -16,7 +16,7 @@
 //     inverse stages 2 S_h^-1), SlotsToCoeffs applies F, each grouped into `level budget`
 //     composed matrices evaluated by BSGS;
 //   * EvalMod: after CoeffsToSlots the real slots hold t = m'/(K q0) with m' = m + q0 I; the
-//     Chebyshev interpolant (degree 63 at the Chebyshev points of the first kind) of
+//     Chebyshev interpolant (degree 31 by default, at the Chebyshev points of the first kind) of
 //     cos(2 pi K t / 2^r - pi / 2^(r+1)) followed by r double-angle steps c -> 2 c^2 - 1 gives
 //     sin(2 pi m' / q0) = sin(2 pi m / q0);
 //   * scales: level l has scale S_l with S_(l-1) = S_l^2 / q_(l-1) (FLEXIBLEAUTO's chain), so

@@ -839,7 +839,7 @@ class NativeBootstrapper:
     of (c0, c1) and returns the output Ciphertext at out_level limbs, scale out_scale."""
 
     def __init__(self, ctx: "Context", top_level: int, top_scale: float, msg_scale: float, budget=(3, 3),
-                 K: int = 12, r: int = 3, degree: int = 63, baby: int = 8, prescale_bits: int = 0,
+                 K: int = 12, r: int = 3, degree: int = 31, baby: int = 8, prescale_bits: int = 0,
                  encapsulation: bool = False, correction_bits: int = 0, double_hoist: bool = True):
         self.ctx = ctx
         p = _BootParams(budget[0], budget[1], top_level, float(top_scale), float(msg_scale), K, r, degree, baby,

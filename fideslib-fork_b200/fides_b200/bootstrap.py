@@ -329,7 +329,7 @@ class Evaluator:
 class Bootstrapper:
     """Precomputed CoeffsToSlots / SlotsToCoeffs diagonals and EvalMod constants."""
 
-    def __init__(self, ev: Evaluator, K: int = 12, r: int = 3, degree: int = 63, cts_levels: int = 3,
+    def __init__(self, ev: Evaluator, K: int = 12, r: int = 3, degree: int = 31, cts_levels: int = 3,
                  stc_levels: int = 3, baby: int = 8, prescale_bits: int = 0, encapsulation=None):
         self.ev = ev
         # sparse-secret encapsulation (Bootstrap.cu keySwitchSparse): device switching keys

@@ -245,7 +245,7 @@ class CryptoContextImpl {
     if (levelBudget.size() != 2) throw Error(FIDES_ERR_ARG, "levelBudget = {CoeffsToSlots, SlotsToCoeffs}");
     if (boot_) fides_boot_destroy(boot_), boot_ = nullptr;
     boot_msg_scale_ = msgScale > 0 ? msgScale : S_[1];
-    fides_boot_params p{(int)levelBudget[0], (int)levelBudget[1], cc_->L, S_[cc_->L], boot_msg_scale_, 12, 3, 63,
+    fides_boot_params p{(int)levelBudget[0], (int)levelBudget[1], cc_->L, S_[cc_->L], boot_msg_scale_, 12, 3, 31,
                         dim1.empty() || dim1[0] == 0 ? 8 : (int)dim1[0], (int)correctionFactor,
                         to_sparse_ && to_dense_ ? 1 : 0, 0, boot_double_hoist_ ? 1 : 0};
     check(fides_boot_create(cc_->handle(), &p, &boot_));

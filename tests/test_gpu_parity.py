@@ -426,3 +426,6 @@ def test_mixed_batch_equals_separate_batches_and_oracle(fides):
     assert len(mh) == 1 and mr == []
     mh, mr = ctx.mixed_batch([], rk_d, rots[:1])
     assert mh == [] and len(mr) == 1
+    assert ctx.mixed_batch([], rk_d, []) == ([], [])
+    with pytest.raises(F.FidesError):  # HMults need the relinearisation key
+        ctx.mixed_batch(pairs[:1], None, [])

@@ -118,6 +118,13 @@ int fides_ctx_create(const fides_params* p, fides_ctx** out) {
 int fides_ctx_destroy(fides_ctx* x) {
   return guard([&] {
     if (!x) return;
+    if (x->h2d_stream) cudaStreamSynchronize(x->h2d_stream);
+    if (x->host_stream) cudaStreamSynchronize(x->host_stream);
+    if (x->d2h_stream) cudaStreamSynchronize(x->d2h_stream);
+    if (x->pipe_mem) cudaFree(x->pipe_mem);
+    for (int i = 0; i < fides_ctx::kPipeSlots; ++i)
+      for (cudaEvent_t e : {x->pipe_free[i], x->pipe_in_ready[i], x->pipe_computed[i]})
+        if (e) cudaEventDestroy(e);
     if (x->host_stream) cudaStreamDestroy(x->host_stream);
     if (x->h2d_stream) cudaStreamDestroy(x->h2d_stream);
     if (x->d2h_stream) cudaStreamDestroy(x->d2h_stream);
@@ -837,18 +844,33 @@ struct HostJob {
   int out_limbs;
 };
 
+// Waits for every pipelined host batch enqueued on the context and reports its status.
+void host_pipeline_wait(fides_ctx* x) {
+  cudaError_t e1 = cudaStreamSynchronize(x->h2d_stream), e2 = cudaStreamSynchronize(x->host_stream),
+              e3 = cudaStreamSynchronize(x->d2h_stream);
+  FIDES_CUDA(e1);
+  FIDES_CUDA(e2);
+  FIDES_CUDA(e3);
+  check_device_status(x->c);
+}
+
 // Pipelined host batch: item k's host->device copies (h2d stream), computation (host
 // stream) and device->host copies (d2h stream) are ordered by events, so copies of
-// neighbouring items run on the copy engines under item k's kernels.  Three device slots
-// rotate; slot reuse waits for the slot's previous device->host copies.  Returns after
-// the last copy completes.  Host buffers should be pinned for the copies to overlap.
+// neighbouring items run on the copy engines under item k's kernels.  The context's device
+// slots rotate across items and across calls; a slot is reused once its previous item's
+// device->host copies are done.  With `wait` it returns after the last copy completes;
+// otherwise it returns once everything is enqueued (the host buffers must stay valid until
+// host_pipeline_wait).  Host buffers should be pinned for the copies to overlap.
 template <typename Op>
-void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op) {
+void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op, bool wait = true) {
   auto* c = C(x);
   const size_t N = c->N;
   const int n = (int)jobs.size();
-  if (n == 0) return;
-  constexpr int SLOTS = 3;
+  if (n == 0) {
+    if (wait) host_pipeline_wait(x);
+    return;
+  }
+  constexpr int SLOTS = fides_ctx::kPipeSlots;
   size_t slot_limbs = 0;
   for (const auto& j : jobs) {
     for (auto* p : j.in) need(p, "host input");
@@ -856,22 +878,25 @@ void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op) {
     slot_limbs = std::max(slot_limbs, j.in.size() * (size_t)j.in_limbs + j.out.size() * (size_t)j.out_limbs);
   }
   cudaStream_t sh = x->h2d_stream, sc = x->host_stream, sd = x->d2h_stream;
-  std::vector<cudaEvent_t> ev;
-  auto event = [&] {
-    cudaEvent_t e;
-    FIDES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    ev.push_back(e);
-    return e;
-  };
-  std::unique_ptr<fides::Scratch> slots;
-  std::exception_ptr err;
+  const size_t slot_bytes = sizeof(uint64_t) * N * slot_limbs;
+  if (x->pipe_slot_bytes < slot_bytes) {  // grow the slots once the earlier items are done
+    host_pipeline_wait(x);
+    if (x->pipe_mem) FIDES_CUDA(cudaFree(x->pipe_mem));
+    x->pipe_mem = nullptr;
+    x->pipe_slot_bytes = 0;
+    FIDES_CUDA(cudaMalloc(&x->pipe_mem, slot_bytes * SLOTS));
+    x->pipe_slot_bytes = slot_bytes;
+    for (bool& u : x->pipe_used) u = false;
+  }
+  for (int i = 0; i < SLOTS; ++i)
+    for (cudaEvent_t* e : {&x->pipe_free[i], &x->pipe_in_ready[i], &x->pipe_computed[i]})
+      if (!*e) FIDES_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   try {
-    slots.reset(new fides::Scratch(c, sizeof(uint64_t) * N * slot_limbs * std::min(n, SLOTS), sh));
-    std::vector<cudaEvent_t> done_d2h(n);
     for (int k = 0; k < n; ++k) {
       const HostJob& j = jobs[k];
-      uint64_t* base = slots->u64() + (size_t)(k % SLOTS) * slot_limbs * N;
-      if (k >= SLOTS) FIDES_CUDA(cudaStreamWaitEvent(sh, done_d2h[k - SLOTS], 0));
+      const int slot = (int)(x->pipe_next++ % SLOTS);
+      uint64_t* base = reinterpret_cast<uint64_t*>(static_cast<char*>(x->pipe_mem) + (size_t)slot * x->pipe_slot_bytes);
+      if (x->pipe_used[slot]) FIDES_CUDA(cudaStreamWaitEvent(sh, x->pipe_free[slot], 0));
       std::vector<uint64_t*> din(j.in.size()), dout(j.out.size());
       uint64_t* p = base;
       for (size_t i = 0; i < j.in.size(); ++i, p += (size_t)j.in_limbs * N) {
@@ -879,31 +904,25 @@ void host_pipeline(fides_ctx* x, const std::vector<HostJob>& jobs, Op&& op) {
         FIDES_CUDA(cudaMemcpyAsync(p, j.in[i], sizeof(uint64_t) * N * j.in_limbs, cudaMemcpyHostToDevice, sh));
       }
       for (size_t i = 0; i < j.out.size(); ++i, p += (size_t)j.out_limbs * N) dout[i] = p;
-      cudaEvent_t in_ready = event();
-      FIDES_CUDA(cudaEventRecord(in_ready, sh));
-      FIDES_CUDA(cudaStreamWaitEvent(sc, in_ready, 0));
+      FIDES_CUDA(cudaEventRecord(x->pipe_in_ready[slot], sh));
+      FIDES_CUDA(cudaStreamWaitEvent(sc, x->pipe_in_ready[slot], 0));
       op(k, din, dout, sc);
-      cudaEvent_t computed = event();
-      FIDES_CUDA(cudaEventRecord(computed, sc));
-      FIDES_CUDA(cudaStreamWaitEvent(sd, computed, 0));
+      FIDES_CUDA(cudaEventRecord(x->pipe_computed[slot], sc));
+      FIDES_CUDA(cudaStreamWaitEvent(sd, x->pipe_computed[slot], 0));
       for (size_t i = 0; i < j.out.size(); ++i)
         FIDES_CUDA(cudaMemcpyAsync(j.out[i], dout[i], sizeof(uint64_t) * N * j.out_limbs, cudaMemcpyDeviceToHost,
                                    sd));
-      done_d2h[k] = event();
-      FIDES_CUDA(cudaEventRecord(done_d2h[k], sd));
+      FIDES_CUDA(cudaEventRecord(x->pipe_free[slot], sd));
+      x->pipe_used[slot] = true;
     }
   } catch (...) {
-    err = std::current_exception();
+    // every stream drains before the error is reported, so no copy outlives the call
+    cudaStreamSynchronize(sh);
+    cudaStreamSynchronize(sc);
+    cudaStreamSynchronize(sd);
+    throw;
   }
-  // every stream drains before the slots are released
-  cudaError_t e1 = cudaStreamSynchronize(sh), e2 = cudaStreamSynchronize(sc), e3 = cudaStreamSynchronize(sd);
-  slots.reset();
-  for (auto e : ev) cudaEventDestroy(e);
-  if (err) std::rethrow_exception(err);
-  FIDES_CUDA(e1);
-  FIDES_CUDA(e2);
-  FIDES_CUDA(e3);
-  check_device_status(c);
+  if (wait) host_pipeline_wait(x);
 }
 }  // namespace
 
@@ -948,9 +967,12 @@ int fides_rotate_host_batch(fides_ctx* x, const fides_rotate_host_item* items, i
   });
 }
 
-int fides_mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
-                           int rescale, const fides_rotate_host_item* rot, int n_rot) {
-  return guard([&] {
+}  // extern "C"
+
+namespace {
+void mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
+                      int rescale, const fides_rotate_host_item* rot, int n_rot, bool wait) {
+  {
     auto* c = C(x);
     if (n_hm < 0 || n_rot < 0) throw fides::Error(FIDES_ERR_ARG, "negative count");
     if (n_hm > 0) {
@@ -990,7 +1012,28 @@ int fides_mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_
                             fides::h_auto_index(c->logN, it.rotation)};
         fides::op_rotate_batch(c, &r, 1, s);
       }
-    });
+    }, wait);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fides_mixed_host_batch(fides_ctx* x, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
+                           int rescale, const fides_rotate_host_item* rot, int n_rot) {
+  return guard([&] { mixed_host_batch(x, hm, n_hm, relin_key_dev, rescale, rot, n_rot, true); });
+}
+
+int fides_mixed_host_batch_async(fides_ctx* x, const fides_hmult_host_item* hm, int n_hm,
+                                 const uint64_t* relin_key_dev, int rescale, const fides_rotate_host_item* rot,
+                                 int n_rot) {
+  return guard([&] { mixed_host_batch(x, hm, n_hm, relin_key_dev, rescale, rot, n_rot, false); });
+}
+
+int fides_host_batch_wait(fides_ctx* x) {
+  return guard([&] {
+    C(x);
+    host_pipeline_wait(x);
   });
 }
 

@@ -173,6 +173,8 @@ def lib():
         L.fides_rotate_host_batch.argtypes = [vp, C.POINTER(_RotateHostItem), C.c_int]
         L.fides_mixed_host_batch.argtypes = [vp, C.POINTER(_HMultHostItem), C.c_int, vp, C.c_int,
                                              C.POINTER(_RotateHostItem), C.c_int]
+        L.fides_mixed_host_batch_async.argtypes = L.fides_mixed_host_batch.argtypes
+        L.fides_host_batch_wait.argtypes = [vp]
         L.fides_rescale_noalloc.argtypes = [vp, vp, C.c_int, vp, vp]
         L.fides_add.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
@@ -761,9 +763,12 @@ class Context:
                                      c0.shape[0], r)
         _check(lib().fides_rotate_host_batch(self._h, arr, len(items)))
 
-    def mixed_host_batch(self, hmult_items, dev_key: int, rotate_items, rescale=True):
+    def mixed_host_batch(self, hmult_items, dev_key: int, rotate_items, rescale=True, wait=True):
         """HMults and rotations of host ciphertexts through one pipeline (items as in
-        mult_host_batch / rotate_host_batch, alternated); outputs are written in place."""
+        mult_host_batch / rotate_host_batch, alternated); outputs are written in place.
+        With wait=False the call returns once everything is enqueued and consecutive calls
+        continue one pipeline: the arrays must stay alive and unchanged, and the outputs
+        unread, until host_batch_wait()."""
         ha = (_HMultHostItem * max(1, len(hmult_items)))()
         for k, (a0, a1, b0, b1, o0, o1) in enumerate(hmult_items):
             ha[k] = _HMultHostItem(a0.ctypes.data, a1.ctypes.data, b0.ctypes.data, b1.ctypes.data,
@@ -772,8 +777,12 @@ class Context:
         for k, (c0, c1, o0, o1, key, r) in enumerate(rotate_items):
             ra[k] = _RotateHostItem(c0.ctypes.data, c1.ctypes.data, o0.ctypes.data, o1.ctypes.data, key,
                                     c0.shape[0], r)
-        _check(lib().fides_mixed_host_batch(self._h, ha, len(hmult_items), dev_key, 1 if rescale else 0, ra,
-                                            len(rotate_items)))
+        fn = lib().fides_mixed_host_batch if wait else lib().fides_mixed_host_batch_async
+        _check(fn(self._h, ha, len(hmult_items), dev_key, 1 if rescale else 0, ra, len(rotate_items)))
+
+    def host_batch_wait(self):
+        """Waits for every pipelined host batch of this context (fides_host_batch_wait)."""
+        _check(lib().fides_host_batch_wait(self._h))
 
 
 def pinned_empty(shape) -> "np.ndarray":

@@ -429,6 +429,18 @@ int fides_rotate_host_batch(fides_ctx* ctx, const fides_rotate_host_item* items,
  * CudaEngine.cpp:1156-1227). */
 int fides_mixed_host_batch(fides_ctx* ctx, const fides_hmult_host_item* hm, int n_hm, const uint64_t* relin_key_dev,
                            int rescale, const fides_rotate_host_item* rot, int n_rot);
+/* fides_mixed_host_batch that returns once its copies and kernels are enqueued.  Consecutive
+ * calls continue one pipeline (the context's device slots rotate across calls), so a call's
+ * first host->device copies run under the previous call's last kernels instead of after its
+ * last device->host copies.  Every host buffer of a call must stay valid and unchanged, and
+ * its outputs unread, until fides_host_batch_wait returns.  Enqueueing errors (bad levels,
+ * null pointers) are reported by the call; device errors by fides_host_batch_wait. */
+int fides_mixed_host_batch_async(fides_ctx* ctx, const fides_hmult_host_item* hm, int n_hm,
+                                 const uint64_t* relin_key_dev, int rescale, const fides_rotate_host_item* rot,
+                                 int n_rot);
+/* Waits for every pipelined host batch enqueued on ctx (copies included) and reports a device
+ * error or a bounded wait that gave up. */
+int fides_host_batch_wait(fides_ctx* ctx);
 
 /* ---- bootstrapping ---------------------------------------------------------------------
  * CKKS bootstrapping driven from the library's C++ host layer: replaces CKKS::Bootstrap

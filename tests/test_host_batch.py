@@ -114,3 +114,52 @@ def test_host_batch_rejects_bad_level(env):
         ctx.mult_host_batch([], key, True)  # empty batch: no-op
     finally:
         ctx.key_free(key)
+
+
+def test_mixed_host_batch_async_continues_pipeline(env):
+    """Calls that return once enqueued (fides_mixed_host_batch_async) continue one pipeline
+    across calls: a later call with larger items grows the slots, a rejected call leaves the
+    enqueued ones intact, and after fides_host_batch_wait every item equals the oracle."""
+    F, prm, o, ctx, rk, rot = env
+    key = ctx.key_upload(rk)
+    keys = {r: ctx.key_upload(k) for r, k in rot.items()}
+    try:
+        calls = []  # per call: (hmult items, rotate items, references)
+        for c, (hl, rl) in enumerate([([3, 2], [(2, 1)]), ([4], [(3, -2), (4, 1)]), ([6, 5], [(6, -2)])]):
+            hm, rt, refs = [], [], []
+            for k, l in enumerate(hl):
+                a, b = host_ct(F, prm, l, 2500 + 10 * c + 2 * k), host_ct(F, prm, l, 2501 + 10 * c + 2 * k)
+                o0, o1 = F.pinned_empty((l - 1, prm.N)), F.pinned_empty((l - 1, prm.N))
+                hm.append((a[0], a[1], b[0], b[1], o0, o1))
+                refs.append(((o0, o1), o.hmult(a[0], a[1], b[0], b[1], rk, rescale=True)))
+            for k, (l, r) in enumerate(rl):
+                x = host_ct(F, prm, l, 2600 + 10 * c + k)
+                o0, o1 = F.pinned_empty((l, prm.N)), F.pinned_empty((l, prm.N))
+                rt.append((x[0], x[1], o0, o1, keys[r], r))
+                refs.append(((o0, o1), o.rotate(x[0], x[1], rot[r], r)))
+            calls.append((hm, rt, refs))
+        ctx.mixed_host_batch(calls[0][0], key, calls[0][1], True, wait=False)
+        ctx.mixed_host_batch(calls[1][0], key, calls[1][1], True, wait=False)
+        bad = host_ct(F, prm, 1, 2700)
+        b0, b1 = F.pinned_empty((1, prm.N)), F.pinned_empty((1, prm.N))
+        with pytest.raises(F.FidesError) as e:  # level 1 cannot rescale: rejected before enqueueing
+            ctx.mixed_host_batch([(bad[0], bad[1], bad[0], bad[1], b0, b1)], key, [], True, wait=False)
+        assert e.value.code == -4
+        ctx.mixed_host_batch(calls[2][0], key, calls[2][1], True, wait=False)  # larger slots
+        ctx.host_batch_wait()
+        for c, (_, _, refs) in enumerate(calls):
+            for k, ((o0, o1), (r0, r1)) in enumerate(refs):
+                assert np.array_equal(o0, r0) and np.array_equal(o1, r1), f"call {c} item {k}"
+        # a waiting call after asynchronous ones continues the same slots
+        hm, rt, refs = calls[1]
+        for (o0, o1), _ in refs:
+            o0[:] = 0
+            o1[:] = 0
+        ctx.mixed_host_batch(hm, key, rt, True)
+        for k, ((o0, o1), (r0, r1)) in enumerate(refs):
+            assert np.array_equal(o0, r0) and np.array_equal(o1, r1), f"repeat item {k}"
+        ctx.host_batch_wait()  # nothing pending: returns at once
+    finally:
+        ctx.key_free(key)
+        for v in keys.values():
+            ctx.key_free(v)

@@ -12,6 +12,8 @@
 // restated here because that file needs OpenFHE headers: natural-order powers of the root
 // (2N of them), their bit-reversed first N, the middle-scale tables, the inverse tables scaled
 // by N^-1, Shoup companions floor(w 2^64 / q), Barrett mu = floor(2^(2 bits + 1) / q).
+// The reduced-noise variant of both conversions (C_.reduced_noise with the DecompAndModUp_negQ
+// table of src/ReducedNoiseConstants.cu) is switched by ref_kernels_set_reduced_noise.
 // It also drives the reference's basis conversions with their geometry (block 64 x 2, one
 // coefficient column per thread, LimbPartitionMGPU.cu:1296-1303 and :1642-1651):
 //   * DecompAndModUpConv<ALGO_SHOUP> (src/CKKS/Conv.cu:274-423) for one digit at one level;
@@ -222,6 +224,18 @@ int ref_kernels_init(int logN, int n_q, int K, int dnum, const uint64_t* primes,
     hc.primeid_digit[j] = j / alpha;
   }
   for (int k = 0; k < K; ++k) hc.primeid_digit[n_q + k] = -1;  // special primes belong to no digit
+  // reduced-noise ModUp constants (src/ReducedNoiseConstants.cu:16-33): -(product of the first
+  // s + 1 primes of digit d) mod p_t at MODUPIDX_SCALE(d, s, t); ModDown's uses P (above)
+  for (int d = 0; d < dnum; ++d) {
+    const int lo = d * alpha, hi = std::min(n_q, (d + 1) * alpha);
+    for (int t = 0; t < np; ++t) {
+      uint64_t Qmod = 1 % primes[t];
+      for (int sidx = 0; sidx < hi - lo; ++sidx) {
+        Qmod = mulm(Qmod, primes[lo + sidx], primes[t]);
+        hg.DecompAndModUp_negQ[FIDESlib_MODUPIDX_SCALE(d, sidx, t)] = (primes[t] - Qmod) % primes[t];
+      }
+    }
+  }
   const int aw = (logN + 1) / 2;
   for (int i = 0; i < np; ++i) {
     const uint64_t q = primes[i], root = psi[i] % q, iroot = inv_h(root, q), ninv = inv_h((uint64_t)N % q, q);
@@ -331,6 +345,14 @@ int ref_ntt(uint64_t* data, uint64_t* aux, int n_polys, int n_limbs, int inverse
 }
 
 // Destination prime ids of digit d (ModUp output row j_ is prime ids[j_]); returns the count.
+// Sets the __constant__ block's reduced_noise flag (reference Parameters::reducedNoise), read by
+// DecompAndModUpConv and ModDown2 (src/CKKS/Conv.cu:76-87, :356-381).
+int ref_kernels_set_reduced_noise(int on) {
+  if (!S.d_globals) return -1;
+  const bool b = on != 0;
+  return run([&] { return cudaMemcpyToSymbol(FIDESlib::constants, &b, sizeof(b), offsetof(Constants, reduced_noise)); });
+}
+
 int ref_modup_dst(int d, int* ids) {
   if (d < 0 || d >= (int)S.to.size()) return -1;
   for (size_t j = 0; j < S.to[d].size(); ++j) ids[j] = S.to[d][j];

@@ -23,6 +23,7 @@ def lib():
                                           C.POINTER(C.c_uint64)]
         _lib.ref_ntt.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         _lib.ref_modup_dst.argtypes = [C.c_int, C.POINTER(C.c_int)]
+        _lib.ref_kernels_set_reduced_noise.argtypes = [C.c_int]
         _lib.ref_modup.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         _lib.ref_moddown.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         vp = C.c_void_p
@@ -42,6 +43,13 @@ def init(logN: int, primes, psi, K: int = 0, dnum: int = 1):
     rc = lib().ref_kernels_init(logN, n - K, K, dnum, (C.c_uint64 * n)(*primes), (C.c_uint64 * n)(*psi))
     if rc:
         raise RuntimeError(f"ref_kernels_init failed: {rc}")
+
+
+def set_reduced_noise(on: bool):
+    """The reduced-noise conversions (reference Parameters::reducedNoise) on or off."""
+    rc = lib().ref_kernels_set_reduced_noise(1 if on else 0)
+    if rc:
+        raise RuntimeError(f"ref_kernels_set_reduced_noise failed: {rc}")
 
 
 def modup_dst(d: int) -> list:

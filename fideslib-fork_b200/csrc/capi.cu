@@ -226,6 +226,15 @@ int fides_ctx_set_conv_engine(fides_ctx* x, int engine) {
   });
 }
 
+int fides_ctx_set_reduced_noise(fides_ctx* x, int on) {
+  return guard([&] {
+    if (on != 0 && on != 1) throw fides::Error(FIDES_ERR_ARG, "reduced_noise must be 0 or 1");
+    auto* c = C(x);
+    if (on && c->K == 0) throw fides::Error(FIDES_ERR_ARG, "reduced noise needs special primes");
+    c->reduced_noise = on != 0;
+  });
+}
+
 int fides_ctx_device_status(fides_ctx* x, uint32_t* status, int clear) {
   return guard([&] {
     auto* c = C(x);

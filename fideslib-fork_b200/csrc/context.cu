@@ -293,18 +293,24 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       std::vector<uint64_t> mat;
       std::vector<uint8_t> tc_b;  // empty: no tensor-core form
       std::vector<TcDest> tc_dst;
-      int kpad = 0, ndp = 0;
+      int kpad = 0, ndp = 0, lift = 0;
     };
     auto build_conv = [&](const std::vector<int>& sp, const std::vector<int>& spr, const std::vector<int>& dp,
-                          const std::vector<int>& dpr) {
+                          const std::vector<int>& dpr, int lift) {
       HostConv h;
       h.src_pos = sp;
       h.src_prime = spr;
       h.dst_pos = dp;
       h.dst_prime = dpr;
+      h.lift = lift;
       int ns = (int)spr.size(), nd = (int)dpr.size();
       h.pre.resize(ns);
-      h.mat.resize((size_t)ns * nd);
+      h.mat.resize((size_t)(ns + lift) * nd);
+      for (int j = 0; j < nd && lift; ++j) {  // row ns: [-Q_src]_{p_j} (reference ReducedNoiseConstants.cu)
+        uint64_t pj = primes[dpr[j]], v = 1 % pj;
+        for (int k = 0; k < ns; ++k) v = h_mulmod(v, primes[spr[k]] % pj, pj);
+        h.mat[(size_t)ns * nd + j] = v ? pj - v : 0;
+      }
       for (int i = 0; i < ns; ++i) {
         uint64_t qi = primes[spr[i]], hq = 1;
         for (int k = 0; k < ns; ++k)
@@ -317,29 +323,33 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
           h.mat[(size_t)i * nd + j] = v;
         }
       }
-      if (conv_tc_fits(logN, ns, nd, primes, dpr)) build_tc_image(h.mat.data(), ns, nd, dpr, primes, h.tc_b, h.tc_dst, h.kpad, h.ndp);
+      if (conv_tc_fits(logN, ns + lift, nd, primes, dpr))
+        build_tc_image(h.mat.data(), ns + lift, nd, dpr, primes, h.tc_b, h.tc_dst, h.kpad, h.ndp);
       return h;
     };
-    std::vector<std::vector<HostConv>> hmu(n_q + 1);
-    std::vector<HostConv> hmd(n_q + 1);
-    for (int l = 1; l <= n_q; ++l) {
-      int b = c->beta(l);
-      for (int d = 0; d < b; ++d) {
-        int s0 = d * c->alpha, s1 = std::min((d + 1) * c->alpha, l);
-        std::vector<int> sp, spr, dp, dpr;
-        for (int i = s0; i < s1; ++i) sp.push_back(i), spr.push_back(i);
-        for (int i = 0; i < l; ++i)
-          if (i < s0 || i >= s1) dp.push_back(i), dpr.push_back(i);
-        for (int k = 0; k < K; ++k) dp.push_back(l + k), dpr.push_back(n_q + k);
-        hmu[l].push_back(build_conv(sp, spr, dp, dpr));
+    // [lift][l]: the plain tables and the reduced-noise ones
+    std::vector<std::vector<HostConv>> hmu[2] = {std::vector<std::vector<HostConv>>(n_q + 1),
+                                                 std::vector<std::vector<HostConv>>(n_q + 1)};
+    std::vector<HostConv> hmd[2] = {std::vector<HostConv>(n_q + 1), std::vector<HostConv>(n_q + 1)};
+    for (int lift = 0; lift < 2; ++lift)
+      for (int l = 1; l <= n_q; ++l) {
+        int b = c->beta(l);
+        for (int d = 0; d < b; ++d) {
+          int s0 = d * c->alpha, s1 = std::min((d + 1) * c->alpha, l);
+          std::vector<int> sp, spr, dp, dpr;
+          for (int i = s0; i < s1; ++i) sp.push_back(i), spr.push_back(i);
+          for (int i = 0; i < l; ++i)
+            if (i < s0 || i >= s1) dp.push_back(i), dpr.push_back(i);
+          for (int k = 0; k < K; ++k) dp.push_back(l + k), dpr.push_back(n_q + k);
+          hmu[lift][l].push_back(build_conv(sp, spr, dp, dpr, lift));
+        }
+        if (K > 0) {
+          std::vector<int> sp, spr, dp, dpr;
+          for (int k = 0; k < K; ++k) sp.push_back(k), spr.push_back(n_q + k);
+          for (int j = 0; j < l; ++j) dp.push_back(j), dpr.push_back(j);
+          hmd[lift][l] = build_conv(sp, spr, dp, dpr, lift);
+        }
       }
-      if (K > 0) {
-        std::vector<int> sp, spr, dp, dpr;
-        for (int k = 0; k < K; ++k) sp.push_back(k), spr.push_back(n_q + k);
-        for (int j = 0; j < l; ++j) dp.push_back(j), dpr.push_back(j);
-        hmd[l] = build_conv(sp, spr, dp, dpr);
-      }
-    }
     // ---- pack everything into one device blob
     std::vector<char> blob;
     size_t o_prime, o_tf, o_ti, o_il, o_pinv, o_pmod, o_rs, o_pq, o_tff, o_tfi, o_f64, o_tww, o_twwi;
@@ -358,7 +368,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     append(blob, f64, o_f64);
     struct Off {
       size_t sp, spr, pre, dp, dpr, mat, tcb, tcd;
-      int ns, nd, kpad, ndp;
+      int ns, nd, kpad, ndp, lift;
     };
     auto put = [&](const HostConv& h) {
       Off o;
@@ -374,14 +384,17 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       o.nd = (int)h.dst_prime.size();
       o.kpad = h.tc_b.empty() ? 0 : h.kpad;
       o.ndp = h.ndp;
+      o.lift = h.lift;
       return o;
     };
-    std::vector<std::vector<Off>> omu(n_q + 1);
-    std::vector<Off> omd(n_q + 1);
-    for (int l = 1; l <= n_q; ++l) {
-      for (auto& h : hmu[l]) omu[l].push_back(put(h));
-      if (K > 0) omd[l] = put(hmd[l]);
-    }
+    std::vector<std::vector<Off>> omu[2] = {std::vector<std::vector<Off>>(n_q + 1),
+                                            std::vector<std::vector<Off>>(n_q + 1)};
+    std::vector<Off> omd[2] = {std::vector<Off>(n_q + 1), std::vector<Off>(n_q + 1)};
+    for (int lift = 0; lift < 2; ++lift)
+      for (int l = 1; l <= n_q; ++l) {
+        for (auto& h : hmu[lift][l]) omu[lift][l].push_back(put(h));
+        if (K > 0) omd[lift][l] = put(hmd[lift][l]);
+      }
     FIDES_CUDA(cudaMalloc(&c->d_tables, blob.size()));
     FIDES_CUDA(cudaMemcpy(c->d_tables, blob.data(), blob.size(), cudaMemcpyHostToDevice));
     char* base = static_cast<char*>(c->d_tables);
@@ -408,6 +421,7 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
       t.dst_pos = reinterpret_cast<const int*>(base + o.dp);
       t.dst_prime = reinterpret_cast<const int*>(base + o.dpr);
       t.mat = reinterpret_cast<const uint64_t*>(base + o.mat);
+      t.lift = o.lift;
       if (o.kpad) {
         t.tc_b = reinterpret_cast<const uint8_t*>(base + o.tcb);
         t.tc_dst = reinterpret_cast<const TcDest*>(base + o.tcd);
@@ -418,9 +432,15 @@ Context* create_context(int logN, int n_q, int K, int dnum, const uint64_t* prim
     };
     c->modup_tab.resize(n_q + 1);
     c->moddown_tab.resize(n_q + 1);
+    c->modup_tab_rn.resize(n_q + 1);
+    c->moddown_tab_rn.resize(n_q + 1);
     for (int l = 1; l <= n_q; ++l) {
-      for (auto& o : omu[l]) c->modup_tab[l].push_back(mk(o));
-      if (K > 0) c->moddown_tab[l] = mk(omd[l]);
+      for (auto& o : omu[0][l]) c->modup_tab[l].push_back(mk(o));
+      for (auto& o : omu[1][l]) c->modup_tab_rn[l].push_back(mk(o));
+      if (K > 0) {
+        c->moddown_tab[l] = mk(omd[0][l]);
+        c->moddown_tab_rn[l] = mk(omd[1][l]);
+      }
     }
     // ---- scratch pool: keep freed blocks cached for reuse
     FIDES_CUDA(cudaDeviceGetDefaultMemPool(&c->pool, device));

@@ -58,8 +58,13 @@ struct ConvTable {
   //         (s * nd_pad * 8 + n) * 16.
   const uint8_t* tc_b = nullptr;
   const TcDest* tc_dst = nullptr;  // [nd_pad]
-  int tc_kpad = 0;                 // K = 8 n_src rounded up to a multiple of 32
+  int tc_kpad = 0;                 // K = 8 (n_src + lift) rounded up to a multiple of 32
   int tc_nd_pad = 0;               // n_dst rounded up to even
+  // Reduced-noise lift (reference src/CKKS/Conv.cu:76-87 and :356-381, ReducedNoise.cuh:14-16):
+  // with lift = 1 the conversion also adds cnt * [-Q_src]_{p_j}, cnt = the number of pre-scaled
+  // sources y_i above q_i / 2, i.e. it converts the centred representatives y_i - q_i.  Row
+  // n_src of mat (and of the B image) holds [-Q_src]_{p_j}.
+  int lift = 0;
 };
 
 // Basis-conversion engine: tensor cores (INT8 split on tcgen05) or 64-bit SIMT.
@@ -108,6 +113,13 @@ struct Context {
   void* d_tables = nullptr;          // backing store of the conversion tables
   std::vector<std::vector<ConvTable>> modup_tab;  // [l][d]
   std::vector<ConvTable> moddown_tab;              // [l]
+  // The same tables with the reduced-noise lift; used while reduced_noise is set (reference
+  // Parameters::reducedNoise, src/CKKS/Parameters.cuh:31, off by default).
+  std::vector<std::vector<ConvTable>> modup_tab_rn;
+  std::vector<ConvTable> moddown_tab_rn;
+  bool reduced_noise = false;
+  const ConvTable& modup_table(int l, int d) const { return (reduced_noise ? modup_tab_rn : modup_tab)[l][d]; }
+  const ConvTable& moddown_table(int l) const { return (reduced_noise ? moddown_tab_rn : moddown_tab)[l]; }
   int conv_engine = CONV_AUTO;
   // NTT tile shapes: sub-transforms per CTA (4, 8 or 16) of each pass, by direction (0 =
   // forward, 1 = inverse), pass (0 = column, 1 = row) and launch-size class (limbs in the

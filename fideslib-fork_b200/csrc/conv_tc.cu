@@ -240,16 +240,21 @@ __global__ void __launch_bounds__(TC_M, 7)
 #pragma unroll
     for (int i = 0; i < TC_MAX_SRC; ++i)
       if (i < ns) x[i] = J.src[(size_t)T.src_pos[i] * N + coef];
+    uint64_t lifted = 0;  // reduced-noise lift: the count is source row ns of the product
 #pragma unroll
     for (int i = 0; i < TC_MAX_SRC; ++i)
       if (i < ns) {
         const ShoupConst pc = T.pre[i];
-        x[i] = shoup(x[i], pc.w, pc.ws, primes[T.src_prime[i]].q);
+        const uint64_t q = primes[T.src_prime[i]].q;
+        x[i] = shoup(x[i], pc.w, pc.ws, q);
+        lifted += x[i] > (q >> 1);
       }
+    if (!T.lift) lifted = 0;
 #pragma unroll
     for (int p = 0; p < TC_MAX_SRC / 2; ++p) {
       if (p >= kpad / 16) break;
-      const uint64_t lo = 2 * p < ns ? x[2 * p] : 0, hi = 2 * p + 1 < ns ? x[2 * p + 1] : 0;
+      const uint64_t lo = 2 * p < ns ? x[2 * p] : (2 * p == ns ? lifted : 0),
+                     hi = 2 * p + 1 < ns ? x[2 * p + 1] : (2 * p + 1 == ns ? lifted : 0);
       *reinterpret_cast<ulonglong2*>(sA + p * (TC_M * 16) + tid * 16) = make_ulonglong2(lo, hi);
     }
   }

@@ -30,12 +30,12 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
   const ConvJob& J = L.j[blockIdx.y];
   const ConvTable& T = J.t;
   extern __shared__ uint64_t sm[];
-  const int ns = NS ? NS : T.n_src, nd = T.n_dst;
+  const int ns = NS ? NS : T.n_src, nd = T.n_dst, lift = T.lift;
   ShoupConst* pre = reinterpret_cast<ShoupConst*>(sm);       // [ns]
   DevPrime* dp = reinterpret_cast<DevPrime*>(sm + 2 * ns);   // [nd]
-  uint64_t* mat = sm + 2 * ns + 8 * nd;                      // [ns][nd]
-  int* dpos = reinterpret_cast<int*>(mat + ns * nd);         // [nd]
-  for (int i = threadIdx.x; i < ns * nd; i += blockDim.x) mat[i] = T.mat[i];
+  uint64_t* mat = sm + 2 * ns + 8 * nd;                      // [ns + lift][nd]
+  int* dpos = reinterpret_cast<int*>(mat + (ns + lift) * nd); // [nd]
+  for (int i = threadIdx.x; i < (ns + lift) * nd; i += blockDim.x) mat[i] = T.mat[i];
   for (int i = threadIdx.x; i < ns; i += blockDim.x) pre[i] = T.pre[i];
   for (int j = threadIdx.x; j < nd; j += blockDim.x) {
     dp[j] = primes[T.dst_prime[j]];
@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
   const int n = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   constexpr int R = NS ? NS : MAX_SRC;
   uint64_t y0[R], y1[R];
+  uint64_t lift0 = 0, lift1 = 0;  // reduced-noise lift: sources above q_i / 2
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     if (NS == 0 && i >= ns) break;
@@ -53,6 +54,8 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
     const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(J.src + (size_t)T.src_pos[i] * N + n);
     y0[i] = shoup(v.x, pre[i].w, pre[i].ws, q);
     y1[i] = shoup(v.y, pre[i].w, pre[i].ws, q);
+    lift0 += y0[i] > (q >> 1);
+    lift1 += y1[i] > (q >> 1);
   }
   uint64_t* dst = J.dst + n;
   for (int j = 0; j < nd; ++j) {
@@ -68,6 +71,11 @@ __global__ void __launch_bounds__(EW_THREADS) conv_kernel(const __grid_constant_
       const uint64_t m = mat[i * nd + j];
       mac128(a0, y0[i], m);
       mac128(a1, y1[i], m);
+    }
+    if (lift) {  // count (<= 64) times [-Q_src]_{p_j}: below 2^69, no reduction needed first
+      const uint64_t m = mat[ns * nd + j];
+      mac128(a0, lift0, m);
+      mac128(a1, lift1, m);
     }
     *reinterpret_cast<ulonglong2*>(dst + (size_t)dpos[j] * N) = make_ulonglong2(reduce128(a0, p), reduce128(a1, p));
   }
@@ -582,7 +590,7 @@ void launch_conv(Context* c, const ConvJob* jobs, int n, cudaStream_t s) {
       double bytes = 0;
       for (int i = 0; i < m; ++i) {
         const ConvTable& t = L.j[i].t;
-        smem = std::max(smem, (size_t)t.n_src * t.n_dst * 8 + (size_t)t.n_src * 16 + (size_t)t.n_dst * 68);
+        smem = std::max(smem, (size_t)(t.n_src + t.lift) * t.n_dst * 8 + (size_t)t.n_src * 16 + (size_t)t.n_dst * 68);
         bytes += 8.0 * c->N * (t.n_src + t.n_dst);
       }
       dim3 grid(c->N / (2 * EW_THREADS), m);

@@ -66,7 +66,7 @@ void modup_convert(Context* c, const int* ls, uint64_t* const* tmps, uint64_t* c
     const int l = ls[i], ext = l + c->K, b = c->beta(l);
     for (int d = 0; d < b; ++d) {
       uint64_t* D = digits[i] + (size_t)d * ext * N;
-      jobs.push_back(ConvJob{c->modup_tab[l][d], tmps[i], D});
+      jobs.push_back(ConvJob{c->modup_table(l, d), tmps[i], D});
       const int s0 = d * c->alpha, s1 = std::min(l, (d + 1) * c->alpha);
       for (int j = 0; j < l; ++j)
         if (j < s0 || j >= s1) refs.push_back(lref(D + j * N, j));
@@ -97,7 +97,7 @@ void moddown_prep(Context* c, uint64_t* const* exts, const int* ls, uint64_t* co
     for (int k = 0; k < K; ++k) refs.push_back(lref(exts[i] + (ls[i] + k) * N, c->n_q + k));
   ntt_limbs(c, refs.data(), (int)refs.size(), true, s);
   std::vector<ConvJob> jobs;
-  for (int i = 0; i < n; ++i) jobs.push_back(ConvJob{c->moddown_tab[ls[i]], exts[i] + ls[i] * N, convs[i]});
+  for (int i = 0; i < n; ++i) jobs.push_back(ConvJob{c->moddown_table(ls[i]), exts[i] + ls[i] * N, convs[i]});
   launch_conv(c, jobs.data(), (int)jobs.size(), s);
 }
 

@@ -112,6 +112,7 @@ def lib():
         L.fides_ctx_launch_count.restype = C.c_uint64
         L.fides_ctx_profile.argtypes = [vp, C.c_int]
         L.fides_ctx_set_conv_engine.argtypes = [vp, C.c_int]
+        L.fides_ctx_set_reduced_noise.argtypes = [vp, C.c_int]
         L.fides_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.fides_f64_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.fides_ctx_ntt_counts.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
@@ -265,7 +266,8 @@ class Ciphertext:
 class Context:
     """One parameter set on one GPU (reference: CKKS::Context / ContextData)."""
 
-    def __init__(self, logN: int, q_primes, p_primes, dnum: int, psi=None, device: int = 0):
+    def __init__(self, logN: int, q_primes, p_primes, dnum: int, psi=None, device: int = 0,
+                 reduced_noise: bool = False):
         import numpy as np
         self.logN, self.N = logN, 1 << logN
         self.q, self.p = [int(x) for x in q_primes], [int(x) for x in p_primes]
@@ -282,6 +284,8 @@ class Context:
         ps = np.zeros(len(self._primes), dtype=np.uint64)
         _check(lib().fides_ctx_psi(h, ps.ctypes.data_as(u64p)))
         self.psi = [int(x) for x in ps]
+        if reduced_noise:
+            self.set_reduced_noise(True)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -352,6 +356,11 @@ class Context:
         """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer
         units) or 'tensor' (exact INT8-split product on the tcgen05 tensor cores)."""
         _check(lib().fides_ctx_set_conv_engine(self._h, self.CONV_ENGINES[engine]))
+
+    def set_reduced_noise(self, on: bool):
+        """Reduced-noise ModUp/ModDown conversions (reference Parameters::reducedNoise): pre-scaled
+        source residues above q_i / 2 are converted as y_i - q_i.  Off by default."""
+        _check(lib().fides_ctx_set_reduced_noise(self._h, 1 if on else 0))
 
     def device_status(self, clear: bool = True) -> int:
         """Synchronises and returns the device status word (bit 0: a bounded device wait

@@ -62,6 +62,7 @@ struct Parameters {
   std::vector<uint64_t> Sprimes;  // special primes
   std::vector<uint64_t> psi;      // optional roots (Q then special); empty = derived
   int device = 0;
+  bool reducedNoise = false;  // reduced-noise ModUp / ModDown (src/CKKS/Parameters.cuh:31)
 };
 
 // Device buffer of limbs (RAII).
@@ -130,6 +131,7 @@ class Context {
     primes.insert(primes.end(), p.Sprimes.begin(), p.Sprimes.end());
     fides_params fp{p.logN, L, K, p.dnum, primes.data(), p.psi.empty() ? nullptr : p.psi.data(), p.device};
     check(fides_ctx_create(&fp, &h_));
+    if (p.reducedNoise) check(fides_ctx_set_reduced_noise(h_, 1));
     check_cuda(cudaSetDevice(p.device), "cudaSetDevice");
     check_cuda(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking), "cudaStreamCreate");
   }

@@ -44,8 +44,8 @@ static void emit(FILE* f, const Ciphertext& ct) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 3) {
-    fprintf(stderr, "usage: %s input.bin output.bin\n", argv[0]);
+  if (argc != 3 && argc != 4) {
+    fprintf(stderr, "usage: %s input.bin output.bin [reduced-noise]\n", argv[0]);
     return 2;
   }
   FILE* in = fopen(argv[1], "rb");
@@ -65,6 +65,7 @@ int main(int argc, char** argv) {
     p.dnum = dnum;
     p.primes.assign(primes.begin(), primes.begin() + nq);
     p.Sprimes.assign(primes.begin() + nq, primes.end());
+    p.reducedNoise = argc == 4;
     Context cc(p);
     {
       KeySwitchingKey k(cc);

@@ -75,6 +75,15 @@ uint64_t fides_ctx_launch_count(const fides_ctx* ctx);
  * matrix fits in shared memory; wider ones stay on SIMT).  Results are identical. No reference
  * counterpart: the reference has one conversion kernel family (src/Conv.cu:27-423). */
 int fides_ctx_set_conv_engine(fides_ctx* ctx, int engine);
+/* Reduced-noise basis conversion (reference Parameters::reducedNoise, src/CKKS/Parameters.cuh:31,
+ * read as C_.reduced_noise by ModDown2 / DecompAndModUpConv, src/CKKS/Conv.cu:76-87 and
+ * :356-381; ReducedNoise.cuh:14-16; tables as src/ReducedNoiseConstants.cu).  With on = 1 every
+ * ModUp and ModDown conversion reads each pre-scaled source residue y_i above q_i / 2 as
+ * y_i - q_i: the converted value gains cnt * [-Q_src]_{p_j}, cnt the number of such sources,
+ * which removes the conversion's q-overflow term for those coefficients (OpenFHE's
+ * WITH_REDUCED_NOISE build).  Off (0) by default, as in the reference.  Applies to operations
+ * launched after the call (a CUDA graph keeps the tables it was captured with). */
+int fides_ctx_set_reduced_noise(fides_ctx* ctx, int on);
 /* NTT tile-shape autotuner.  Each NTT pass groups 4, 8 or 16 sub-transforms per CTA; the
  * context keeps one choice per direction (0 forward, 1 inverse), pass (0 column, 1 row) and
  * launch-size class (limbs per launch <= 8, <= 32, <= 128, more).  fides_ctx_autotune times

@@ -140,6 +140,7 @@ struct or_ctx {
   /* per prime: psi_rev, psi_rev_shoup, ipsi_rev, ipsi_rev_shoup (N each), n_inv */
   uint64_t** tw;
   uint64_t* n_inv;
+  int reduced_noise; /* reference Parameters::reducedNoise (src/CKKS/Parameters.cuh:31) */
 };
 
 static uint64_t shoup_pre(uint64_t w, uint64_t q) { return (uint64_t)(((u128)w << 64) / q); }
@@ -292,8 +293,25 @@ void or_ntt(const or_ctx* c, uint64_t* a, int n_limbs, const int* prime_ids, int
  *   y_i   = [x_i * (Qhat_i)^-1]_{q_i}                 (pre-scale, Qhat_i = prod_{k != i} q_k)
  *   out_j = [ sum_i y_i * [Qhat_i]_{p_j} ]_{p_j}       (128-bit accumulate, one reduction)
  * Tables as reference src/Math.cu:94-130 (q_hat_inv, p_hat). */
+static void switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out, int n_dst,
+                         const int* dst_ids, int lift);
+
 void or_switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out, int n_dst,
                      const int* dst_ids) {
+  switch_basis(c, in, n_src, src_ids, out, n_dst, dst_ids, 0);
+}
+
+void or_switch_basis_lift(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out,
+                          int n_dst, const int* dst_ids) {
+  switch_basis(c, in, n_src, src_ids, out, n_dst, dst_ids, 1);
+}
+
+/* With lift (the reduced-noise conversion, reference src/CKKS/Conv.cu:76-87 and :356-381,
+ * src/CKKS/ReducedNoise.cuh:14-16, tables src/ReducedNoiseConstants.cu:16-33): a pre-scaled
+ * y_i above q_i / 2 (q_i >> 1, strictly) stands for y_i - q_i, so out_j gains
+ * cnt * [-Q_src]_{p_j}, cnt the number of such y_i of the coefficient. */
+static void switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out, int n_dst,
+                         const int* dst_ids, int lift) {
   const int N = c->N;
   uint64_t* pre = (uint64_t*)malloc(sizeof(uint64_t) * n_src);
   uint64_t* mat = (uint64_t*)malloc(sizeof(uint64_t) * n_src * (n_dst ? n_dst : 1));
@@ -311,15 +329,26 @@ void or_switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* 
       mat[i * n_dst + j] = hj;
     }
   }
+  uint64_t* negq = (uint64_t*)malloc(sizeof(uint64_t) * (n_dst ? n_dst : 1));
+  for (int j = 0; j < n_dst; ++j) {
+    uint64_t pj = c->primes[dst_ids[j]], v = 1 % pj;
+    for (int k = 0; k < n_src; ++k) v = or_mulmod(v, c->primes[src_ids[k]] % pj, pj);
+    negq[j] = v ? pj - v : 0;
+  }
 #pragma omp parallel
   {
     uint64_t* y = (uint64_t*)malloc(sizeof(uint64_t) * (n_src ? n_src : 1));
 #pragma omp for schedule(static)
     for (int n = 0; n < N; ++n) {
-      for (int i = 0; i < n_src; ++i) y[i] = or_mulmod(in[(size_t)i * N + n], pre[i], c->primes[src_ids[i]]);
+      uint64_t cnt = 0;
+      for (int i = 0; i < n_src; ++i) {
+        y[i] = or_mulmod(in[(size_t)i * N + n], pre[i], c->primes[src_ids[i]]);
+        cnt += y[i] > (c->primes[src_ids[i]] >> 1);
+      }
       for (int j = 0; j < n_dst; ++j) {
         u128 acc = 0;
         for (int i = 0; i < n_src; ++i) acc += (u128)y[i] * mat[i * n_dst + j];
+        if (lift) acc += (u128)cnt * negq[j];
         out[(size_t)j * N + n] = (uint64_t)(acc % c->primes[dst_ids[j]]);
       }
     }
@@ -327,7 +356,10 @@ void or_switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* 
   }
   free(pre);
   free(mat);
+  free(negq);
 }
+
+void or_ctx_set_reduced_noise(or_ctx* c, int on) { c->reduced_noise = on != 0; }
 
 /* ------------------------------------------------------------------------- */
 /* elementwise                                                                */
@@ -446,7 +478,7 @@ void or_modup(const or_ctx* c, const uint64_t* x, int l, uint64_t* digits) {
     memcpy(coeff, x + (size_t)s0 * N, sizeof(uint64_t) * ns * N);
     or_ntt(c, coeff, ns, src, 1);
     uint64_t* conv = (uint64_t*)malloc(sizeof(uint64_t) * (nd ? nd : 1) * N);
-    or_switch_basis(c, coeff, ns, src, conv, nd, dst);
+    switch_basis(c, coeff, ns, src, conv, nd, dst, c->reduced_noise);
     or_ntt(c, conv, nd, dst, 0);
     uint64_t* D = digits + (size_t)d * ext * N;
     for (int i = 0; i < ns; ++i) memcpy(D + (size_t)(s0 + i) * N, x + (size_t)(s0 + i) * N, sizeof(uint64_t) * N);
@@ -498,7 +530,7 @@ void or_moddown(const or_ctx* c, const uint64_t* in_ext, int l, uint64_t* out) {
   memcpy(sp, in_ext + (size_t)l * N, sizeof(uint64_t) * K * N);
   or_ntt(c, sp, K, src, 1);
   uint64_t* conv = (uint64_t*)malloc(sizeof(uint64_t) * l * N);
-  or_switch_basis(c, sp, K, src, conv, l, dst);
+  switch_basis(c, sp, K, src, conv, l, dst, c->reduced_noise);
   or_ntt(c, conv, l, dst, 0);
 #pragma omp parallel for schedule(static)
   for (int j = 0; j < l; ++j) {

@@ -43,6 +43,8 @@ or_ctx* or_ctx_create(int logN, int n_q, int n_p, const uint64_t* primes, const 
 void or_ctx_destroy(or_ctx* c);
 int or_ctx_alpha(const or_ctx* c);
 uint64_t or_ctx_psi(const or_ctx* c, int prime_id);
+/* Reduced-noise ModUp / ModDown conversions (reference Parameters::reducedNoise): off by default. */
+void or_ctx_set_reduced_noise(or_ctx* c, int on);
 /* Set the number of OpenMP threads the oracle uses (<=0: all). */
 void or_set_threads(int n);
 int or_get_threads(void);
@@ -54,6 +56,9 @@ void or_ntt(const or_ctx* c, uint64_t* a, int n_limbs, const int* prime_ids, int
 /* ApproxSwitchCRTBasis: coefficient-domain limbs over src primes -> dst primes. */
 void or_switch_basis(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out, int n_dst,
                      const int* dst_ids);
+/* The same with the reduced-noise lift: sources above q_i / 2 taken as y_i - q_i. */
+void or_switch_basis_lift(const or_ctx* c, const uint64_t* in, int n_src, const int* src_ids, uint64_t* out,
+                          int n_dst, const int* dst_ids);
 
 /* ---- elementwise ---- */
 void or_poly_mul(const or_ctx* c, const uint64_t* a, const uint64_t* b, uint64_t* out, int n_limbs, const int* prime_ids);

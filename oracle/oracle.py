@@ -48,6 +48,7 @@ def lib():
         L.or_ctx_create.restype = C.c_void_p
         L.or_ctx_create.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int]
         L.or_ctx_destroy.argtypes = [C.c_void_p]
+        L.or_ctx_set_reduced_noise.argtypes = [C.c_void_p, C.c_int]
         L.or_ctx_alpha.restype = C.c_int
         L.or_ctx_alpha.argtypes = [C.c_void_p]
         L.or_ctx_psi.restype = C.c_uint64
@@ -56,6 +57,7 @@ def lib():
         L.or_get_threads.restype = C.c_int
         L.or_ntt.argtypes = [C.c_void_p, u64p, C.c_int, i32p, C.c_int]
         L.or_switch_basis.argtypes = [C.c_void_p, u64p, C.c_int, i32p, u64p, C.c_int, i32p]
+        L.or_switch_basis_lift.argtypes = L.or_switch_basis.argtypes
         for f in ("or_poly_mul", "or_poly_add", "or_poly_sub"):
             getattr(L, f).argtypes = [C.c_void_p, u64p, u64p, u64p, C.c_int, i32p]
         L.or_tensor.argtypes = [C.c_void_p, u64p, u64p, u64p, u64p, C.c_int, u64p, u64p, u64p]
@@ -116,7 +118,7 @@ def rotation_auto_index(logN: int, r: int) -> int:
 class Oracle:
     """CPU restatement of the CKKS evaluation path on one parameter set."""
 
-    def __init__(self, logN: int, q_primes, p_primes, dnum: int, psi=None):
+    def __init__(self, logN: int, q_primes, p_primes, dnum: int, psi=None, reduced_noise: bool = False):
         self.logN, self.N = logN, 1 << logN
         self.q = [int(x) for x in q_primes]
         self.p = [int(x) for x in p_primes]
@@ -127,6 +129,8 @@ class Oracle:
         self.alpha = lib().or_ctx_alpha(self._h)
         self.psi = [int(lib().or_ctx_psi(self._h, i)) for i in range(len(primes))]
         self.primes = [int(x) for x in primes]
+        self.reduced_noise = bool(reduced_noise)
+        lib().or_ctx_set_reduced_noise(self._h, int(self.reduced_noise))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -158,12 +162,15 @@ class Oracle:
         lib().or_ntt(self._h, _p(out), len(ids), ip, 1 if inverse else 0)
         return out
 
-    def switch_basis(self, a: np.ndarray, src_ids, dst_ids) -> np.ndarray:
+    def switch_basis(self, a: np.ndarray, src_ids, dst_ids, lift: bool = False) -> np.ndarray:
+        """ApproxSwitchCRTBasis; lift=True: the reduced-noise form (sources above q_i / 2 taken
+        as y_i - q_i)."""
         a = np.ascontiguousarray(a, dtype=np.uint64)
         s, sp = _ip(src_ids)
         d, dp = _ip(dst_ids)
         out = self._new(len(d))
-        lib().or_switch_basis(self._h, _p(a), len(s), sp, _p(out), len(d), dp)
+        fn = lib().or_switch_basis_lift if lift else lib().or_switch_basis
+        fn(self._h, _p(a), len(s), sp, _p(out), len(d), dp)
         return out
 
     def _elt(self, fn, a, b, prime_ids):

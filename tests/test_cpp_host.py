@@ -14,12 +14,14 @@ from conftest import ROOT
 pytestmark = pytest.mark.gpu
 
 
-def test_cpp_host_api_matches_oracle(fides, tmp_path):
+@pytest.mark.parametrize("reduced_noise", [False, True])
+def test_cpp_host_api_matches_oracle(fides, tmp_path, reduced_noise):
+    """reduced_noise: Parameters::reducedNoise set on the C++ side, the oracle's flag likewise."""
     from fides_b200 import params as P
     pkg = os.path.join(ROOT, "fideslib-fork_b200")
     subprocess.run(["make", "-s", "-C", pkg, "host_test"], check=True)
     prm = P.config_a()
-    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum, reduced_noise=reduced_noise)
     kg = KeyGen(o, seed_stream=71)
     rot = 3
     rk, kr = kg.relin_key(), kg.rotation_key(rot)
@@ -33,7 +35,8 @@ def test_cpp_host_api_matches_oracle(fides, tmp_path):
         np.array(prm.q + prm.p, dtype=np.uint64).tofile(f)
         for arr in (rk, kr, a[0], a[1], b[0], b[1]):
             np.ascontiguousarray(arr, dtype=np.uint64).tofile(f)
-    r = subprocess.run([os.path.join(pkg, "host_test"), str(inp), str(outp)], capture_output=True, text=True)
+    r = subprocess.run([os.path.join(pkg, "host_test"), str(inp), str(outp)] + (["rn"] if reduced_noise else []),
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr + r.stdout
     data = np.fromfile(outp, dtype=np.uint64)
     pos = 0

@@ -79,6 +79,47 @@ def test_reference_conversions_equal_oracle(fides, level):
     assert np.array_equal(fides.to_host(out), ref)
 
 
+@pytest.mark.parametrize("level", [30, 17, 5])
+def test_reference_reduced_noise_conversions_equal_oracle(fides, level):
+    """With the reference's reduced_noise flag (Parameters::reducedNoise, read by
+    DecompAndModUpConv and ModDown2), its conversions equal the oracle's lifted conversion and
+    differ from the plain one; this project's ModUp with the flag equals the oracle too."""
+    import torch
+    from fides_b200 import params as P
+    prm = P.config_c(4)
+    ctx = fides.Context(prm.logN, prm.q, prm.p, prm.dnum, reduced_noise=True)
+    R.init(prm.logN, prm.q + prm.p, ctx.psi, K=prm.K, dnum=prm.dnum)
+    R.set_reduced_noise(True)
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum, reduced_noise=True)
+    N = prm.N
+    x = uniform_limbs(xrng(2800 + level), prm.q[:level], N)
+    xd = fides.to_device(x)
+    s = torch.cuda.current_stream().cuda_stream
+    alpha = -(-prm.n_q // prm.dnum)
+    for d in range(-(-level // alpha)):
+        lo, hi = d * alpha, min(level, (d + 1) * alpha)
+        dst = R.modup_dst(d)
+        out = torch.zeros((len(dst), N), dtype=torch.int64, device="cuda").view(torch.uint64)
+        R.modup(xd, level, d, out, s)
+        torch.cuda.synchronize()
+        got = fides.to_host(out)
+        active = [j for j, pid in enumerate(dst) if pid < level or pid >= prm.n_q]
+        ids = [dst[j] for j in active]
+        ref = o.switch_basis(x[lo:hi], list(range(lo, hi)), ids, lift=True)
+        assert np.array_equal(got[active], ref), f"digit {d}"
+        assert not np.array_equal(ref, o.switch_basis(x[lo:hi], list(range(lo, hi)), ids))
+    sp = uniform_limbs(xrng(2900 + level), prm.p, N)
+    out = torch.empty((level, N), dtype=torch.int64, device="cuda").view(torch.uint64)
+    R.moddown(fides.to_device(sp), level, out, s)
+    torch.cuda.synchronize()
+    ref = o.switch_basis(sp, list(range(prm.n_q, prm.n_q + prm.K)), list(range(level)), lift=True)
+    assert np.array_equal(fides.to_host(out), ref)
+    R.set_reduced_noise(False)
+    # the whole ModUp of this project with the flag (INTT, lifted conversion, NTT)
+    x_eval = o.ntt(x, list(range(level)))
+    assert np.array_equal(fides.to_host(ctx.modup(fides.to_device(x_eval))), o.modup(x_eval))
+
+
 # ---------------------------------------------------------------- key switching, automorphism,
 # SwitchModulus, tensor and elementwise kernels of the reference, against the oracle and ours
 def _config_c(fides):

@@ -731,3 +731,44 @@ def test_native_double_hoisted_n4096(fides, baby):
         nb.close()
     print(f"N=2^12 baby {baby}: single-hoisted {bits[False]:.2f} bits, double-hoisted {bits[True]:.2f} bits")
     assert bits[True] > 12 and bits[True] >= bits[False] - 0.5
+
+
+@pytest.mark.gpu
+def test_native_bootstrap_reduced_noise_n4096(fides):
+    """N = 2^12, the C++ bootstrapper on a context with the reduced-noise conversions (the
+    reference's Parameters::reducedNoise): every key switch of the bootstrap uses the lifted
+    ModUp / ModDown, the result differs from the plain context's and keeps its precision
+    (within half a bit, above 12 bits)."""
+    import torch
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    delta = 2.0 ** 50
+    rng = xrng(73)
+    n = prm.N // 2
+    zs, cts = [], []
+    for _ in range(2):
+        z = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        c0, c1 = kg.encrypt(encode(z, prm.N, delta).astype(np.int64), 1)
+        zs.append(z)
+        cts.append(F.Ciphertext(F.to_device(c0), F.to_device(c1)))
+    bits, outs = {}, {}
+    for rn in (False, True):
+        ctx.set_reduced_noise(rn)
+        nb = F.NativeBootstrapper(ctx, top_level=prm.n_q, top_scale=ev.S[prm.n_q], msg_scale=delta, K=bs.K, r=bs.r,
+                                  degree=bs.degree, prescale_bits=bs.prescale.bit_length() - 1)
+        nb.set_keys(ev.rk, ev.conj_key)
+        for r in nb.rotations():
+            if r not in ev.rot_keys:
+                ev.rot_keys[r] = F.to_device(kg.rotation_key(r))
+            nb.set_rotation_key(r, ev.rot_keys[r])
+        nb.prepare()
+        batch = nb.bootstrap_batch(cts)
+        torch.cuda.synchronize()
+        outs[rn] = [(F.to_host(x.c0), F.to_host(x.c1)) for x in batch]
+        errs = [np.abs(decode(kg.decrypt_limb0(*h), prm.N, nb.out_scale) - z).max() for h, z in zip(outs[rn], zs)]
+        bits[rn] = -math.log2(max(errs))
+        nb.close()
+    ctx.set_reduced_noise(False)
+    print(f"N=2^12 bootstrap: plain {bits[False]:.2f} bits, reduced noise {bits[True]:.2f} bits")
+    assert not np.array_equal(outs[True][0][0], outs[False][0][0])
+    assert bits[True] > 12 and bits[True] >= bits[False] - 0.5

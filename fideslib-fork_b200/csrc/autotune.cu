@@ -1,8 +1,10 @@
 // NTT tile-shape autotuner.  For each direction, pass and launch-size class, time the
 // transform on device-resident synthetic limbs with every supported sub-transforms-per-CTA
-// (4, 8, 16) and keep the fastest in the context's shape table (Context::ntt_g).  The
-// shape changes only how the sub-transforms are grouped into CTAs, never the arithmetic,
-// so results are identical whatever the table holds.
+// (4, 8, 16) and residues per thread (16; also 8 at N >= 2^15, i.e. three butterfly stages
+// per register chunk instead of four) and keep the fastest in the context's tables
+// (Context::ntt_g, Context::ntt_r).  Both change only how the butterflies are distributed
+// over threads and CTAs, never the arithmetic, so results are identical whatever the tables
+// hold.
 #include <algorithm>
 #include <vector>
 
@@ -37,8 +39,10 @@ void autotune_ntt(Context* c, float* best_ms) {
   FIDES_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   FIDES_CUDA(cudaEventCreate(&e0));
   FIDES_CUDA(cudaEventCreate(&e1));
-  uint8_t saved[2][2][4];
+  uint8_t saved[2][2][4], saved_r[2][2][4];
   std::copy(&c->ntt_g[0][0][0], &c->ntt_g[0][0][0] + 16, &saved[0][0][0]);
+  std::copy(&c->ntt_r[0][0][0], &c->ntt_r[0][0][0] + 16, &saved_r[0][0][0]);
+  const bool r8 = c->logN >= 15;  // passes with 8 residues per thread exist (ntt_impl.cuh HasLe3)
   const int saved_chunk = c->ntt_chunk;
   c->ntt_chunk = 0;  // the shapes are timed on unsplit launches
   try {
@@ -71,18 +75,23 @@ void autotune_ntt(Context* c, float* best_ms) {
           }
           return best;
         };
-        // coordinate descent: the column pass with the row pass at 16, then the row pass
+        // coordinate descent: the column pass with the row pass at (16, 16), then the row pass
         float best = 0;
         for (int pass = 0; pass < 2; ++pass) {
-          int pick = 16;
+          int pick = 16, pick_r = 16;
           best = 1e30f;
-          for (int g : SHAPES) {
-            c->ntt_g[inv][pass][cls] = (uint8_t)g;
-            if (pass == 0) c->ntt_g[inv][1][cls] = 16;
-            const float t = time_it();
-            if (t < best) best = t, pick = g;
+          for (int r : {16, 8}) {
+            if (r == 8 && !r8) continue;
+            for (int g : SHAPES) {
+              c->ntt_g[inv][pass][cls] = (uint8_t)g;
+              c->ntt_r[inv][pass][cls] = (uint8_t)r;
+              if (pass == 0) c->ntt_g[inv][1][cls] = 16, c->ntt_r[inv][1][cls] = 16;
+              const float t = time_it();
+              if (t < best) best = t, pick = g, pick_r = r;
+            }
           }
           c->ntt_g[inv][pass][cls] = (uint8_t)pick;
+          c->ntt_r[inv][pass][cls] = (uint8_t)pick_r;
         }
         // the other direction of the timing pair uses its current table entries
         if (best_ms) best_ms[inv * 4 + cls] = best;
@@ -113,6 +122,7 @@ void autotune_ntt(Context* c, float* best_ms) {
   } catch (...) {
     c->ntt_chunk = saved_chunk;
     std::copy(&saved[0][0][0], &saved[0][0][0] + 16, &c->ntt_g[0][0][0]);
+    std::copy(&saved_r[0][0][0], &saved_r[0][0][0] + 16, &c->ntt_r[0][0][0]);
     cudaStreamSynchronize(s);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

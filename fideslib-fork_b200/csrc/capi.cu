@@ -208,6 +208,26 @@ int fides_ctx_set_ntt_shape(fides_ctx* x, int inverse, int pass, int size_class,
   });
 }
 
+int fides_ctx_ntt_residues(fides_ctx* x, uint8_t* residues) {
+  return guard([&] {
+    auto* c = C(x);
+    need(residues, "residues");
+    std::memcpy(residues, &c->ntt_r[0][0][0], 16);
+  });
+}
+
+int fides_ctx_set_ntt_residues(fides_ctx* x, int inverse, int pass, int size_class, int residues_per_thread) {
+  return guard([&] {
+    auto* c = C(x);
+    if (inverse < 0 || inverse > 1 || pass < 0 || pass > 1 || size_class < 0 || size_class > 3 ||
+        (residues_per_thread != 8 && residues_per_thread != 16))
+      throw fides::Error(FIDES_ERR_ARG, "bad NTT residues per thread");
+    if (residues_per_thread == 8 && c->logN < 15)
+      throw fides::Error(FIDES_ERR_ARG, "8 residues per thread are built for N >= 2^15 only");
+    c->ntt_r[inverse][pass][size_class] = (uint8_t)residues_per_thread;
+  });
+}
+
 int fides_ctx_ntt_chunk(fides_ctx* x, int set_limbs) {
   int out = 0;
   const int rc = guard([&] {

@@ -133,6 +133,10 @@ struct Context {
   // largest launch (MAX_NTT_LIMBS); fides_ctx_autotune picks it by timing.
   int ntt_chunk = 0;
   int ntt_shape(bool inverse, int pass, int limbs) const { return ntt_g[inverse][pass][ntt_size_class(limbs)]; }
+  // Residues per thread (16 or 8) of each pass, indexed like ntt_g.  8 exists at N >= 2^15 only
+  // (elsewhere 16 is used whatever the table holds); 16 by default, fides_ctx_autotune times both.
+  uint8_t ntt_r[2][2][4] = {{{16, 16, 16, 16}, {16, 16, 16, 16}}, {{16, 16, 16, 16}, {16, 16, 16, 16}}};
+  int ntt_residues(bool inverse, int pass, int limbs) const { return ntt_r[inverse][pass][ntt_size_class(limbs)]; }
   uint32_t* d_status = nullptr;  // device word: bit 0 = a bounded device wait gave up,
                                  // bit 1 = an encoded coefficient exceeded 2^62
   // special-FFT twiddles of the slot encoder, [N/2] (double, double) pairs: entry h + j

@@ -8,8 +8,9 @@
 //   * N = 2^LOG1 x 2^LOG2.  Pass COL runs global stages [0, LOG1) on strided columns,
 //     pass ROW runs stages [LOG1, logN) on contiguous rows.  Forward = COL then ROW,
 //     inverse = ROW then COL; each pass reads and writes every limb once.
-//   * each thread keeps 2^LOGE elements in registers and runs LOGE stages per chunk;
-//     chunks exchange through padded shared memory (conflict-free);
+//   * each thread keeps 2^LE elements in registers (16, or 8 at N >= 2^15 where the
+//     autotuner picks it) and runs LE stages per chunk; chunks exchange through padded
+//     shared memory;
 //   * lazy butterflies with one 64-bit Shoup product each (primes < 2^62): the forward
 //     transform skips every conditional subtraction for q < 2^58 (values stay below 35q)
 //     and uses Harvey's [0, 4q) form otherwise; the inverse tracks a bound B (a multiple

@@ -10,10 +10,11 @@ namespace nttk {
 
 constexpr int COL = 0, ROW = 1;
 
-constexpr int LOGE = 4;  // 16 elements per thread
-// Sub-transforms per CTA (G) is a template parameter of every pass: 4, 8 or 16, chosen per
-// launch by the context's tile-shape table (fides_ctx_autotune).  The butterflies and their
-// order are the same for every G, so the results are identical.
+// Residues per thread, 2^LE (LE = 4: 16, four butterfly stages per register chunk; LE = 3: 8,
+// three stages per chunk, one more shared-memory exchange per pass, twice the threads), and
+// sub-transforms per CTA (G: 4, 8 or 16) are template parameters of every pass, chosen per
+// launch by the context's tables (fides_ctx_autotune).  The butterflies, their pairs and
+// twiddles and their order are the same for every LE and G, so the results are identical.
 
 // Asynchronous 16-byte global -> shared copies (cp.async), used to fetch an epilogue operand
 // while the butterflies run.
@@ -142,24 +143,24 @@ struct PassArgs {
 };
 
 // Element index u of register r for thread t, when the register index spans bits
-// [lo, lo + LOGE) of u.
-template <int LO>
+// [lo, lo + LE) of u.
+template <int LO, int LE>
 __device__ __forceinline__ int u_of(int t, int r) {
   // disjoint bit fields: '+' lets the compiler fold the register-index part into offsets
-  return ((t >> LO) << (LO + LOGE)) + (r << LO) + (t & ((1 << LO) - 1));
+  return ((t >> LO) << (LO + LE)) + (r << LO) + (t & ((1 << LO) - 1));
 }
 
-template <int LOGP>
+template <int LE>
 __device__ __forceinline__ int padu(int u) {
-  return u + (u >> LOGE);
+  return u + (u >> LE);
 }
 
 // Butterflies of pair bits [BLO, BHI] (in u) for a thread whose registers span bits
-// [LO, LO + LOGE).  FWD walks bits high -> low, inverse low -> high.
-template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS, bool SMALL>
-__device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int sub, int sbase, const ShoupConst* tw,
+// [LO, LO + LE).  FWD walks bits high -> low, inverse low -> high.
+template <int LE, int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS, bool SMALL>
+__device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LE], int t, int sub, int sbase, const ShoupConst* tw,
                                           const DevPrime& pr, ShoupConst last, uint64_t& B, uint64_t pol) {
-  constexpr int E = 1 << LOGE;
+  constexpr int E = 1 << LE;
   const int th = t >> LO;
 #pragma unroll
   for (int k = 0; k <= BHI - BLO; ++k) {
@@ -167,7 +168,7 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
     const int rb = b - LO;
     const int sig = LOGP - 1 - b;  // stage within this pass
     const int s = sbase + sig;     // global stage
-    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LOGE - b - 1));
+    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LE - b - 1));
     const bool red = !FWD && B > (1ull << 62);
 #pragma unroll
     for (int hi = 0; hi < (E >> (rb + 1)); ++hi) {
@@ -199,10 +200,10 @@ __device__ __forceinline__ void run_chunk(uint64_t (&x)[1 << LOGE], int t, int s
 }
 
 // run_chunk on FP64 residues (q < 2^50): the same stages, pairs and twiddles.
-template <int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS>
-__device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int sub, int sbase, const double2* tw,
+template <int LE, int LOGP, int LO, int BHI, int BLO, bool FWD, int PASS>
+__device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LE], int t, int sub, int sbase, const double2* tw,
                                               const double* tww, const F64Prime& fp, uint64_t pol) {
-  constexpr int E = 1 << LOGE;
+  constexpr int E = 1 << LE;
   const int th = t >> LO;
 #pragma unroll
   for (int k = 0; k <= BHI - BLO; ++k) {
@@ -210,7 +211,7 @@ __device__ __forceinline__ void run_chunk_f64(double (&x)[1 << LOGE], int t, int
     const int rb = b - LO;
     const int sig = LOGP - 1 - b;
     const int s = sbase + sig;
-    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LOGE - b - 1));
+    const uint32_t base = (1u << s) + ((uint32_t)sub << sig) + ((uint32_t)th << (LO + LE - b - 1));
 #pragma unroll
     for (int hi = 0; hi < (E >> (rb + 1)); ++hi) {
       if (!FWD && PASS == COL && b == LOGP - 1) {
@@ -261,77 +262,77 @@ __device__ __forceinline__ uint64_t inv_bound(uint64_t q, int stages) {
 
 
 // Register span of chunk c.
-template <int LOGP, bool FWD, int C>
+template <int LE, int LOGP, bool FWD, int C>
 struct Chunk {
   // forward: bits from the top; inverse: bits from the bottom
-  static constexpr int BHI = FWD ? (LOGP - 1 - C * LOGE) : (C * LOGE + LOGE - 1 < LOGP - 1 ? C * LOGE + LOGE - 1 : LOGP - 1);
-  static constexpr int BLO = FWD ? (LOGP - (C + 1) * LOGE > 0 ? LOGP - (C + 1) * LOGE : 0) : C * LOGE;
-  static constexpr int LO = FWD ? BLO : (BLO + LOGE <= LOGP ? BLO : LOGP - LOGE);
+  static constexpr int BHI = FWD ? (LOGP - 1 - C * LE) : (C * LE + LE - 1 < LOGP - 1 ? C * LE + LE - 1 : LOGP - 1);
+  static constexpr int BLO = FWD ? (LOGP - (C + 1) * LE > 0 ? LOGP - (C + 1) * LE : 0) : C * LE;
+  static constexpr int LO = FWD ? BLO : (BLO + LE <= LOGP ? BLO : LOGP - LE);
 };
 
 // The register chunks of one pass, separated by shared-memory exchanges.
-template <int LOGP, int PASS, bool FWD, bool SMALL, typename SIDX>
-__device__ __forceinline__ void chunks(uint64_t (&x)[1 << LOGE], uint64_t* sm, SIDX sidx, int g, int t, int subtw,
+template <int LE, int LOGP, int PASS, bool FWD, bool SMALL, typename SIDX>
+__device__ __forceinline__ void chunks(uint64_t (&x)[1 << LE], uint64_t* sm, SIDX sidx, int g, int t, int subtw,
                                        int sbase, const ShoupConst* tw, const DevPrime& pr, ShoupConst last,
                                        uint64_t& B, bool direct_load, uint64_t pol) {
-  constexpr int E = 1 << LOGE;
-  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
-  using C0 = Chunk<LOGP, FWD, 0>;
-  run_chunk<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
+  constexpr int E = 1 << LE;
+  constexpr int NCH = (LOGP + LE - 1) / LE;
+  using C0 = Chunk<LE, LOGP, FWD, 0>;
+  run_chunk<LE, LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   if constexpr (NCH > 1) {
-    using C1 = Chunk<LOGP, FWD, 1>;
+    using C1 = Chunk<LE, LOGP, FWD, 1>;
     if (!direct_load) __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO>(t, r))] = x[r];
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO, LE>(t, r))] = x[r];
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
-    run_chunk<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO, LE>(t, r))];
+    run_chunk<LE, LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   }
   if constexpr (NCH > 2) {
-    using C1 = Chunk<LOGP, FWD, 1>;
-    using C2 = Chunk<LOGP, FWD, 2>;
+    using C1 = Chunk<LE, LOGP, FWD, 1>;
+    using C2 = Chunk<LE, LOGP, FWD, 2>;
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO>(t, r))] = x[r];
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO, LE>(t, r))] = x[r];
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
-    run_chunk<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO, LE>(t, r))];
+    run_chunk<LE, LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS, SMALL>(x, t, subtw, sbase, tw, pr, last, B, pol);
   }
   static_assert(NCH <= 3, "sub-transform too large");
 }
 
 // chunks() on FP64 residues; the shared-memory exchanges move the doubles' bits.
-template <int LOGP, int PASS, bool FWD, typename SIDX>
-__device__ __forceinline__ void chunks_f64(double (&x)[1 << LOGE], uint64_t* smu, SIDX sidx, int g, int t, int subtw,
+template <int LE, int LOGP, int PASS, bool FWD, typename SIDX>
+__device__ __forceinline__ void chunks_f64(double (&x)[1 << LE], uint64_t* smu, SIDX sidx, int g, int t, int subtw,
                                            int sbase, const double2* tw, const double* tww, const F64Prime& fp,
                                            bool direct_load, uint64_t pol) {
-  constexpr int E = 1 << LOGE;
-  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
+  constexpr int E = 1 << LE;
+  constexpr int NCH = (LOGP + LE - 1) / LE;
   double* sm = reinterpret_cast<double*>(smu);
-  using C0 = Chunk<LOGP, FWD, 0>;
-  run_chunk_f64<LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
+  using C0 = Chunk<LE, LOGP, FWD, 0>;
+  run_chunk_f64<LE, LOGP, C0::LO, C0::BHI, C0::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   if constexpr (NCH > 1) {
-    using C1 = Chunk<LOGP, FWD, 1>;
+    using C1 = Chunk<LE, LOGP, FWD, 1>;
     if (!direct_load) __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO>(t, r))] = x[r];
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C0::LO, LE>(t, r))] = x[r];
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO>(t, r))];
-    run_chunk_f64<LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C1::LO, LE>(t, r))];
+    run_chunk_f64<LE, LOGP, C1::LO, C1::BHI, C1::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   }
   if constexpr (NCH > 2) {
-    using C1 = Chunk<LOGP, FWD, 1>;
-    using C2 = Chunk<LOGP, FWD, 2>;
+    using C1 = Chunk<LE, LOGP, FWD, 1>;
+    using C2 = Chunk<LE, LOGP, FWD, 2>;
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO>(t, r))] = x[r];
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<C1::LO, LE>(t, r))] = x[r];
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO>(t, r))];
-    run_chunk_f64<LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<C2::LO, LE>(t, r))];
+    run_chunk_f64<LE, LOGP, C2::LO, C2::BHI, C2::BLO, FWD, PASS>(x, t, subtw, sbase, tw, tww, fp, pol);
   }
 }
 
@@ -343,24 +344,32 @@ struct PassShape {
 
 // One pass of a transform of 2^LOGN points.  Every index is a compile-time function of
 // LOGN, so global and shared addresses are a per-thread base plus immediate offsets.
-// Threads of a pass CTA, and CTAs per SM the register budget is sized for (by default 768
-// threads = 24 warps per SM, i.e. 80 registers; FIDES_NTT_THREADS_PER_SM overrides it).
+// Threads of a pass CTA, and CTAs per SM the register budget is sized for: with 16 residues
+// per thread 768 threads = 24 warps per SM, i.e. 80 registers (FIDES_NTT_THREADS_PER_SM
+// overrides it); with 8, 1024 threads = 32 warps, 64 registers (no spills in the plain passes).
 #ifndef FIDES_NTT_THREADS_PER_SM
 #define FIDES_NTT_THREADS_PER_SM 768
 #endif
-template <int LOGN, int PASS, int G>
+template <int LOGN, int PASS, int G, int LE>
 struct PassThreads {
-  static constexpr int TPS = FIDES_NTT_THREADS_PER_SM;
-  static constexpr int NT = (1 << (PassShape<LOGN, PASS>::LOGP - LOGE)) * G;
+  static constexpr int TPS = LE == 3 ? 1024 : FIDES_NTT_THREADS_PER_SM;
+  static constexpr int NT = (1 << (PassShape<LOGN, PASS>::LOGP - LE)) * G;
   static constexpr int MINB = NT >= TPS ? 1 : (TPS / NT > 32 ? 32 : TPS / NT);
 };
 
-template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G>
-__global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LOGN, PASS, G>::MINB)
+// Ring dimensions whose passes are also built with 8 residues per thread (measured faster for
+// small launches at N >= 2^15; smaller rings keep 16 only).
+template <int LOGN>
+struct HasLe3 {
+  static constexpr bool value = LOGN >= 15;
+};
+
+template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G, int LE>
+__global__ void __launch_bounds__(PassThreads<LOGN, PASS, G, LE>::NT, PassThreads<LOGN, PASS, G, LE>::MINB)
     ntt_pass(const PassArgs a, const __grid_constant__ NttLimbList L) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
-  constexpr int P = 1 << LOGP, E = 1 << LOGE, T = P / E, NT = T * G;
-  constexpr int NCH = (LOGP + LOGE - 1) / LOGE;
+  constexpr int P = 1 << LOGP, E = 1 << LE, T = P / E, NT = T * G;
+  constexpr int NCH = (LOGP + LE - 1) / LE;
   constexpr int PADP = P + P / E;
   extern __shared__ uint64_t sm[];
 
@@ -386,7 +395,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   const int subtw = PASS == COL ? 0 : sub;
 
   auto gidx = [&](int s_, int u) -> int { return PASS == COL ? s_ + u * S : s_ * P + u; };
-  auto sidx = [&](int gg, int u) -> int { return PASS == COL ? u * G + gg : gg * PADP + padu<LOGP>(u); };
+  auto sidx = [&](int gg, int u) -> int { return PASS == COL ? u * G + gg : gg * PADP + padu<LE>(u); };
 
   uint64_t x[E];
 
@@ -407,8 +416,8 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   };
 
   // ---- load chunk 0 (direct when lanes map to consecutive addresses, else staged)
-  constexpr int LO0 = Chunk<LOGP, FWD, 0>::LO;
-  constexpr bool direct_load = (PASS == COL) || (LO0 == LOGP - LOGE);
+  constexpr int LO0 = Chunk<LE, LOGP, FWD, 0>::LO;
+  constexpr bool direct_load = (PASS == COL) || (LO0 == LOGP - LE);
   // conv + P SwitchModulus(top) (a column pass): the tile of the top limb is copied into the
   // exchange buffer by cp.async while the conv loads are in flight, so the prologue waits for
   // memory once (loading both operands per element serialised the loads: long-scoreboard
@@ -425,13 +434,13 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   }
   if (direct_load) {
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = load(gidx(sub, u_of<LO0>(t, r)));
+    for (int r = 0; r < E; ++r) x[r] = load(gidx(sub, u_of<LO0, LE>(t, r)));
     if constexpr (STAGE_PRO) {
       cp_async_wait_all();
       __syncthreads();
 #pragma unroll
       for (int r = 0; r < E; ++r)
-        x[r] = addmod(x[r], shoup(switch_modulus(sm[u_of<LO0>(t, r) * G + g], opr, pr), pm.w, pm.ws, pr.q), pr.q);
+        x[r] = addmod(x[r], shoup(switch_modulus(sm[u_of<LO0, LE>(t, r) * G + g], opr, pr), pm.w, pm.ws, pr.q), pr.q);
     }
   } else {
 #pragma unroll
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<LO0>(t, r))];
+    for (int r = 0; r < E; ++r) x[r] = sm[sidx(g, u_of<LO0, LE>(t, r))];
   }
 
   // ---- epilogue operand: start fetching it into shared memory (after the data region)
@@ -471,7 +480,7 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
 #pragma unroll
       for (int r = 0; r < E; ++r) xf[r] = __longlong_as_double((long long)x[r]);  // the first pass's doubles
     }
-    chunks_f64<LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N,
+    chunks_f64<LE, LOGP, PASS, FWD>(xf, sm, sidx, g, t, subtw, sbase, a.twf + (size_t)lr.prime * N,
                                 a.tww + (size_t)lr.prime * N, fp, direct_load && !STAGE_PRO, pol);
     if (first_pass) {
 #pragma unroll
@@ -485,9 +494,9 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
   uint64_t B = pr.q;  // inverse: bound of the values (a multiple of q)
   if (!FWD && PASS == COL) B = inv_bound(pr.q, PassShape<LOGN, ROW>::LOGP);
   if (FWD && pr.q < (1ull << 58))
-    chunks<LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
+    chunks<LE, LOGP, PASS, FWD, true>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
   else
-    chunks<LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
+    chunks<LE, LOGP, PASS, FWD, false>(x, sm, sidx, g, t, subtw, sbase, tw, pr, last, B, direct_load && !STAGE_PRO, pol);
 
   // ---- final reduction of the completed transform
   if (FWD && PASS == ROW) {
@@ -525,19 +534,19 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
     }
     data[i] = v;
   };
-  constexpr int LOL = Chunk<LOGP, FWD, NCH - 1>::LO;
-  constexpr bool direct_store = (PASS == COL) || (LOL == LOGP - LOGE);
+  constexpr int LOL = Chunk<LE, LOGP, FWD, NCH - 1>::LO;
+  constexpr bool direct_store = (PASS == COL) || (LOL == LOGP - LE);
   if constexpr (EPS) {
     cp_async_wait_all();
     if (direct_store) __syncthreads();  // the staged store below synchronises anyway
   }
   if (direct_store) {
 #pragma unroll
-    for (int r = 0; r < E; ++r) store(gidx(sub, u_of<LOL>(t, r)), x[r]);
+    for (int r = 0; r < E; ++r) store(gidx(sub, u_of<LOL, LE>(t, r)), x[r]);
   } else {
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<LOL>(t, r))] = x[r];
+    for (int r = 0; r < E; ++r) sm[sidx(g, u_of<LOL, LE>(t, r))] = x[r];
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < E; ++k) {
@@ -549,33 +558,44 @@ __global__ void __launch_bounds__(PassThreads<LOGN, PASS, G>::NT, PassThreads<LO
 }
 
 
-template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G>
+template <int LOGN, int PASS, bool FWD, int IN, int OUT, int G, int LE>
 void launch_pass_g(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
   constexpr int LOGP = PassShape<LOGN, PASS>::LOGP;
-  constexpr int P = 1 << LOGP, T = P / (1 << LOGE);
-  constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LOGE))) * (int)sizeof(uint64_t) +
+  constexpr int P = 1 << LOGP, T = P / (1 << LE);
+  constexpr int smem = (PASS == COL ? P * G : G * (P + P / (1 << LE))) * (int)sizeof(uint64_t) +
                        (EpStage<PASS, FWD, OUT>::on ? G * P * (int)sizeof(uint64_t) : 0);
   static bool attr_set = false;  // per instantiation; set before first launch
   if (!attr_set) {
-    FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT, G>,
+    FIDES_CUDA(cudaFuncSetAttribute(ntt_pass<LOGN, PASS, FWD, IN, OUT, G, LE>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set = true;
   }
   dim3 grid(((1 << LOGN) >> LOGP) / G, L.n);
   // algorithmic bytes: half of a transform's read + write of each limb (two passes)
   LaunchScope ls(c, s, KK_NTT, 8.0 * (1 << LOGN) * L.n);
-  ntt_pass<LOGN, PASS, FWD, IN, OUT, G><<<grid, T * G, smem, s>>>(a, L);
+  ntt_pass<LOGN, PASS, FWD, IN, OUT, G, LE><<<grid, T * G, smem, s>>>(a, L);
   FIDES_CUDA(cudaGetLastError());
 }
 
-// The pass with the sub-transforms-per-CTA the context's shape table picks for this launch.
+// The pass with the sub-transforms-per-CTA and residues per thread the context's tables pick
+// for this launch.
+template <int LOGN, int PASS, bool FWD, int IN, int OUT, int LE>
+void launch_pass_le(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
+  switch (c->ntt_shape(!FWD, PASS, L.n)) {
+    case 4: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 4, LE>(c, a, L, s); break;
+    case 8: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 8, LE>(c, a, L, s); break;
+    default: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 16, LE>(c, a, L, s);
+  }
+}
 template <int LOGN, int PASS, bool FWD, int IN, int OUT>
 void launch_pass(Context* c, const PassArgs& a, const NttLimbList& L, cudaStream_t s) {
-  switch (c->ntt_shape(!FWD, PASS, L.n)) {
-    case 4: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 4>(c, a, L, s); break;
-    case 8: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 8>(c, a, L, s); break;
-    default: launch_pass_g<LOGN, PASS, FWD, IN, OUT, 16>(c, a, L, s);
+  if constexpr (HasLe3<LOGN>::value) {
+    if (c->ntt_residues(!FWD, PASS, L.n) == 8) {
+      launch_pass_le<LOGN, PASS, FWD, IN, OUT, 3>(c, a, L, s);
+      return;
+    }
   }
+  launch_pass_le<LOGN, PASS, FWD, IN, OUT, 4>(c, a, L, s);
 }
 
 // The pass sequence of one transform for a given ring dimension.

@@ -125,6 +125,8 @@ def lib():
         L.fides_rotate_hoisted_batch.argtypes = [vp, C.POINTER(_HoistItem), C.c_int, vp]
         L.fides_ctx_ntt_shapes.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.fides_ctx_set_ntt_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.fides_ctx_ntt_residues.argtypes = [vp, C.POINTER(C.c_uint8)]
+        L.fides_ctx_set_ntt_residues.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.fides_ctx_device_status.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int]
         L.fides_ctx_synchronize.argtypes = [vp, vp]
         L.fides_ctx_ntt_chunk.argtypes = [vp, C.c_int]
@@ -327,12 +329,13 @@ class Context:
     NTT_SIZE_CLASSES = (8, 32, 128, None)  # upper bounds of limbs per launch
 
     def autotune(self) -> dict:
-        """Time the NTT tile shapes on the device and keep the fastest (fides_ctx_autotune).
-        Returns the shape table and each class's representative transform time."""
+        """Time the NTT tile shapes and residues per thread on the device and keep the fastest
+        (fides_ctx_autotune).  Returns both tables and each class's representative transform
+        time."""
         ms = (C.c_float * 8)()
         _check(lib().fides_ctx_autotune(self._h, ms))
-        return {"shapes": self.ntt_shapes(), "transform_ms": {"forward": list(ms[0:4]), "inverse": list(ms[4:8])},
-                "chunk_limbs": self.ntt_chunk()}
+        return {"shapes": self.ntt_shapes(), "residues_per_thread": self.ntt_residues(),
+                "transform_ms": {"forward": list(ms[0:4]), "inverse": list(ms[4:8])}, "chunk_limbs": self.ntt_chunk()}
 
     def ntt_chunk(self, set_limbs: int = -1) -> int:
         """Limbs per NTT launch pair (fides_ctx_ntt_chunk): set_limbs > 0 sets it, 0 restores
@@ -351,6 +354,16 @@ class Context:
 
     def set_ntt_shape(self, inverse: bool, pass_: int, size_class: int, subs_per_cta: int):
         _check(lib().fides_ctx_set_ntt_shape(self._h, int(inverse), pass_, size_class, subs_per_cta))
+
+    def ntt_residues(self) -> dict:
+        """Residues per thread (16 or 8) by direction / pass / launch-size class."""
+        v = (C.c_uint8 * 16)()
+        _check(lib().fides_ctx_ntt_residues(self._h, v))
+        return {d: {p: list(v[8 * i + 4 * j: 8 * i + 4 * j + 4]) for j, p in enumerate(("column", "row"))}
+                for i, d in enumerate(("forward", "inverse"))}
+
+    def set_ntt_residues(self, inverse: bool, pass_: int, size_class: int, residues_per_thread: int):
+        _check(lib().fides_ctx_set_ntt_residues(self._h, int(inverse), pass_, size_class, residues_per_thread))
 
     def set_conv_engine(self, engine: str):
         """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer

@@ -102,6 +102,12 @@ int fides_ctx_ntt_chunk(fides_ctx* ctx, int set_limbs);
 /* The 16 shape entries, index [inverse][pass][size class]. */
 int fides_ctx_ntt_shapes(fides_ctx* ctx, uint8_t* shapes);
 int fides_ctx_set_ntt_shape(fides_ctx* ctx, int inverse, int pass, int size_class, int subs_per_cta);
+/* Residues per thread of each pass (16, or 8 = three butterfly stages per register chunk and
+ * twice the threads, built for N >= 2^15), in the same [inverse][pass][size class] layout;
+ * fides_ctx_autotune times both with every shape.  Results never depend on them.  The
+ * reference's counterpart is its fixed per-thread radix (src/NTT.cu:331-756). */
+int fides_ctx_ntt_residues(fides_ctx* ctx, uint8_t* residues);
+int fides_ctx_set_ntt_residues(fides_ctx* ctx, int inverse, int pass, int size_class, int residues_per_thread);
 /* Compute roofline of the NTT: butterflies per second that `device` sustains running the
  * forward NTT butterfly (one 64-bit Shoup product, two 64-bit additions) on register-resident
  * data, with no memory traffic.  Takes about 100 ms.  No reference counterpart. */

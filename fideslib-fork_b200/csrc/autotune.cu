@@ -45,6 +45,8 @@ void autotune_ntt(Context* c, float* best_ms) {
   const bool r8 = c->logN >= 15;  // passes with 8 residues per thread exist (ntt_impl.cuh HasLe3)
   const int saved_chunk = c->ntt_chunk;
   c->ntt_chunk = 0;  // the shapes are timed on unsplit launches
+  const bool saved_profiling = c->profiling;
+  c->profiling = false;  // no profiling events inside the timing graphs
   try {
     Scratch data(c, c->limb_bytes() * max_limbs, s);
     Scratch ids(c, sizeof(int) * max_limbs, s);
@@ -60,20 +62,49 @@ void autotune_ntt(Context* c, float* best_ms) {
     for (int inv = 0; inv < 2; ++inv)
       for (int cls = 0; cls < 4; ++cls) {
         const int n = SIZES[cls];
+        // Device time of one transform: kReps round trips (the tuned direction, then the other
+        // one, which keeps the data reduced) replayed from a CUDA graph, so that host launch
+        // overhead, which exceeds the GPU time of a launch of a few limbs, does not decide
+        // between the candidates.  One round trip runs uncaptured first (each kernel's first
+        // launch sets its shared-memory attribute).
         auto time_it = [&] {
-          float best = 1e30f;
-          for (int rep = 0; rep < 4; ++rep) {  // the first repetition warms up
-            FIDES_CUDA(cudaEventRecord(e0, s));
-            // a forward+inverse pair keeps the data reduced for the next repetition
-            ntt_limbs(c, refs.data(), n, inv != 0, s);
-            FIDES_CUDA(cudaEventRecord(e1, s));
-            ntt_limbs(c, refs.data(), n, inv == 0, s);
-            FIDES_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            FIDES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (rep) best = std::min(best, ms);
+          constexpr int kReps = 8;
+          ntt_limbs(c, refs.data(), n, inv != 0, s);
+          ntt_limbs(c, refs.data(), n, inv == 0, s);
+          cudaGraph_t graph = nullptr;
+          cudaGraphExec_t exec = nullptr;
+          FIDES_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+          try {
+            for (int k = 0; k < kReps; ++k) {
+              ntt_limbs(c, refs.data(), n, inv != 0, s);
+              ntt_limbs(c, refs.data(), n, inv == 0, s);
+            }
+          } catch (...) {
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
           }
-          return best;
+          FIDES_CUDA(cudaStreamEndCapture(s, &graph));
+          const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+          if (ie != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            FIDES_CUDA(ie);
+          }
+          float best = 1e30f;
+          cudaError_t err = cudaSuccess;
+          for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {  // the first replay warms up
+            err = cudaEventRecord(e0, s);
+            if (err == cudaSuccess) err = cudaGraphLaunch(exec, s);
+            if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+            if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+            if (rep && err == cudaSuccess) best = std::min(best, ms);
+          }
+          cudaGraphExecDestroy(exec);
+          cudaGraphDestroy(graph);
+          FIDES_CUDA(err);
+          return best / (2 * kReps);
         };
         // coordinate descent: the column pass with the row pass at (16, 16), then the row pass
         float best = 0;
@@ -120,6 +151,7 @@ void autotune_ntt(Context* c, float* best_ms) {
     }
     FIDES_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
+    c->profiling = saved_profiling;
     c->ntt_chunk = saved_chunk;
     std::copy(&saved[0][0][0], &saved[0][0][0] + 16, &c->ntt_g[0][0][0]);
     std::copy(&saved_r[0][0][0], &saved_r[0][0][0] + 16, &c->ntt_r[0][0][0]);
@@ -129,6 +161,7 @@ void autotune_ntt(Context* c, float* best_ms) {
     cudaStreamDestroy(s);
     throw;
   }
+  c->profiling = saved_profiling;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaStreamDestroy(s);

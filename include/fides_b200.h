@@ -87,7 +87,8 @@ int fides_ctx_set_reduced_noise(fides_ctx* ctx, int on);
 /* NTT tile-shape autotuner.  Each NTT pass groups 4, 8 or 16 sub-transforms per CTA; the
  * context keeps one choice per direction (0 forward, 1 inverse), pass (0 column, 1 row) and
  * launch-size class (limbs per launch <= 8, <= 32, <= 128, more).  fides_ctx_autotune times
- * every shape on the device (about 0.2 s at N = 2^16) and keeps the fastest; best_ms
+ * every shape (and residues per thread, below) on the device from CUDA-graph replays (under a
+ * second at N = 2^16) and keeps the fastest; best_ms
  * (optional, 8 floats [inverse][class]) receives one transform's time of each class's
  * representative launch (4, 16, 64, 256 limbs).  Results never depend on the shapes.  Do
  * not run it concurrently with other work on the context.  No reference counterpart: the

@@ -1,7 +1,8 @@
 // The evaluation facade of the B200 CKKS core, shaped like the reference's
 // fideslib::CryptoContextImpl<DCRTPoly> (api/CryptoContext.hpp:306-458, bodies in
 // api/CryptoContext.cpp:1120-1299 over CudaEngine, api/engine/cuda/CudaEngine.cpp:429-1150):
-// EvalAdd / EvalSub (ciphertexts and real constants), EvalMult / EvalSquare, Rescale,
+// MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
+// real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare, Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -23,6 +24,7 @@
 #pragma once
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <memory>
 #include <vector>
 
@@ -32,6 +34,17 @@ namespace FIDESlib {
 namespace B200 {
 
 enum ScalingTechnique { FIXEDMANUAL = 0, FLEXIBLEAUTO = 1 };
+
+// An encoded CKKS plaintext (the reference's Plaintext from MakeCKKSPackedPlaintext,
+// api/Plaintext.hpp, CKKSPackedEncoding): `level` limbs in EVALUATION form on the device, at
+// scale `scale`, holding `slots` slots.
+struct Plaintext {
+  DeviceLimbs limbs;  // [level][N]
+  int level = 0;
+  double scale = 0;
+  int slots = 0;
+  const uint64_t* data() const { return limbs.get(); }
+};
 
 // The ModUp of a ciphertext's c1, kept for any number of EvalFastRotation calls (the
 // reference's EvalFastRotationPrecompute result).
@@ -102,6 +115,20 @@ class CryptoContextImpl {
     return o;
   }
 
+  Ciphertext add_sub_pt(const Ciphertext& a, const Plaintext& p, bool sub) const {
+    const int l = std::min(a.getLevel(), p.level);
+    Ciphertext A = tech_ == FLEXIBLEAUTO ? AdjustToLevel(a, l) : copy_of(a, l);
+    if (!same_scale(A.NoiseFactor, p.scale))
+      throw Error(FIDES_ERR_ARG, "the plaintext's scale differs from the ciphertext's");
+    Ciphertext o = fresh(l, A.NoiseFactor, A.NoiseLevel, a.slots);
+    check((sub ? fides_sub : fides_add)(cc_->handle(), A.c0(), p.data(), l, o.c0(), cc_->stream()));
+    check_cuda(cudaMemcpyAsync(o.c1(), A.c1(), sizeof(uint64_t) * (size_t)N() * l, cudaMemcpyDeviceToDevice,
+                               cc_->stream()),
+               "D2D");
+    cc_->synchronize();  // A is released at scope exit
+    return o;
+  }
+
   Ciphertext copy_of(const Ciphertext& a, int level) const {
     Ciphertext o = fresh(level, a.NoiseFactor, a.NoiseLevel, a.slots);
     const size_t bytes = sizeof(uint64_t) * (size_t)N() * level;
@@ -142,11 +169,48 @@ class CryptoContextImpl {
     return mul_int_rescale(a, level + 1, k, S_[level]);
   }
 
+  // ---- plaintexts (CryptoContextImpl::MakeCKKSPackedPlaintext, api/CryptoContext.hpp; encoded
+  // on the device by fides_encode, the reference's DeviceEncodeBatch.cu path)
+  // `z` is padded with zeros to a power of two of slots (at most N/2); level 0 = the top level,
+  // scale 0 = that level's canonical scale (OpenFHE's default for the level).
+  Plaintext MakeCKKSPackedPlaintext(const std::vector<std::complex<double>>& z, int level = 0,
+                                    double scale = 0) const {
+    const int L = (int)S_.size() - 1;
+    if (level == 0) level = L;
+    if (level < 1 || level > L) throw Error(FIDES_ERR_LEVEL, "plaintext level out of range");
+    if (z.empty() || (int)z.size() > N() / 2) throw Error(FIDES_ERR_ARG, "1..N/2 slots");
+    int n = 1;
+    while (n < (int)z.size()) n <<= 1;
+    std::vector<double> host(2 * (size_t)n, 0.0);
+    for (size_t i = 0; i < z.size(); ++i) host[2 * i] = z[i].real(), host[2 * i + 1] = z[i].imag();
+    DeviceLimbs dev(2 * (size_t)n);  // n complex slots as doubles
+    check_cuda(cudaMemcpyAsync(dev.get(), host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice,
+                               cc_->stream()),
+               "H2D");
+    Plaintext p;
+    p.level = level;
+    p.scale = scale > 0 ? scale : S_[level];
+    p.slots = n;
+    p.limbs = DeviceLimbs((size_t)N() * level);
+    check(fides_encode(cc_->handle(), reinterpret_cast<const double*>(dev.get()), n, 1, p.scale, level, p.limbs.get(),
+                       cc_->stream()));
+    cc_->synchronize();  // the slot buffer is released at scope exit
+    return p;
+  }
+  Plaintext MakeCKKSPackedPlaintext(const std::vector<double>& x, int level = 0, double scale = 0) const {
+    return MakeCKKSPackedPlaintext(std::vector<std::complex<double>>(x.begin(), x.end()), level, scale);
+  }
+
   // ---- additive operations (CryptoContextImpl::EvalAdd / EvalSub)
   Ciphertext EvalAdd(const Ciphertext& a, const Ciphertext& b) const { return add_sub(a, b, false); }
   Ciphertext EvalSub(const Ciphertext& a, const Ciphertext& b) const { return add_sub(a, b, true); }
   Ciphertext EvalAdd(const Ciphertext& a, double c) const { return add_const(a, c); }
   Ciphertext EvalSub(const Ciphertext& a, double c) const { return add_const(a, -c); }
+  // with a plaintext (Ciphertext::addPt / subPt): the plaintext's scale must equal the
+  // ciphertext's (FIXEDMANUAL) or the common level's canonical scale (FLEXIBLEAUTO, where the
+  // ciphertext is first brought to the lower of the two levels)
+  Ciphertext EvalAdd(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, false); }
+  Ciphertext EvalSub(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, true); }
 
   // ---- multiplicative operations (EvalMult, EvalSquare, Rescale)
   Ciphertext EvalMult(const Ciphertext& a, const Ciphertext& b) const {
@@ -169,6 +233,29 @@ class CryptoContextImpl {
     return o;
   }
   Ciphertext EvalSquare(const Ciphertext& a) const { return EvalMult(a, a); }
+  // Multiplication by a plaintext (Ciphertext::multPt): both components times the plaintext on
+  // the lower of the two levels.  FIXEDMANUAL: scale product, degree + 1, no rescale.
+  // FLEXIBLEAUTO: the ciphertext at its canonical scale, the product rescaled (level l - 1,
+  // scale S_l p.scale / q_(l-1), which is S_(l-1) for a plaintext at the canonical S_l).
+  Ciphertext EvalMult(const Ciphertext& a, const Plaintext& p) const {
+    const int l = std::min(a.getLevel(), p.level);
+    if (tech_ == FIXEDMANUAL) {
+      Ciphertext o = fresh(l, a.NoiseFactor * p.scale, a.NoiseLevel + 1, a.slots);
+      check(fides_mul(cc_->handle(), a.c0(), p.data(), l, o.c0(), cc_->stream()));
+      check(fides_mul(cc_->handle(), a.c1(), p.data(), l, o.c1(), cc_->stream()));
+      return o;
+    }
+    if (l < 2) throw Error(FIDES_ERR_LEVEL, "no level left for the product's rescale");
+    Ciphertext A = AdjustToLevel(a, l);
+    Ciphertext t = fresh(l, 0, 1, a.slots);
+    check(fides_mul(cc_->handle(), A.c0(), p.data(), l, t.c0(), cc_->stream()));
+    check(fides_mul(cc_->handle(), A.c1(), p.data(), l, t.c1(), cc_->stream()));
+    Ciphertext o = fresh(l - 1, S_[l] * p.scale / (double)q(l - 1), 1, a.slots);
+    check(fides_rescale(cc_->handle(), t.c0(), l, o.c0(), cc_->stream()));
+    check(fides_rescale(cc_->handle(), t.c1(), l, o.c1(), cc_->stream()));
+    cc_->synchronize();  // t is released at scope exit
+    return o;
+  }
   // Multiplication by a real constant: FLEXIBLEAUTO lands on level l - 1 at S_(l-1); FIXEDMANUAL
   // multiplies by round(c q_(l-1)) and raises the degree (the next Rescale divides q_(l-1) out).
   Ciphertext EvalMult(const Ciphertext& a, double c) const {

@@ -152,4 +152,61 @@ int facade_arith(int logN, int n_q, int K, int dnum, const uint64_t* primes, dou
   }
 }
 
+// Plaintext operations of the facade on ciphertext (a0, a1) at l limbs: the plaintext of the
+// n complex slots z = [n][re, im] encoded at level l (canonical scale S_l of top_scale), then,
+// packed into out in this order: the plaintext's limbs [l] | FLEXIBLEAUTO EvalMult(A, P) [l-1] |
+// EvalAdd(A, P) [l] | EvalSub(A, P) [l] | FIXEDMANUAL EvalMult(A, P) [l] (at scale 1 x S_l,
+// degree 2), each ciphertext as c0 limbs then c1 limbs.
+int facade_plain(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, int l,
+                 const uint64_t* a0, const uint64_t* a1, const double* z, int n, uint64_t* out, char* err,
+                 int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    std::vector<std::complex<double>> slots(n);
+    for (int i = 0; i < n; ++i) slots[i] = {z[2 * i], z[2 * i + 1]};
+    uint64_t* w = out;
+    {
+      CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+      const double S = ev.GetScalingFactorReal(l);
+      Plaintext P = ev.MakeCKKSPackedPlaintext(slots, l);
+      if (P.level != l || P.scale != S) throw Error(FIDES_ERR_STATE, "plaintext metadata");
+      check_cuda(cudaMemcpy(w, P.data(), sizeof(uint64_t) * (size_t)N * l, cudaMemcpyDeviceToHost), "D2H");
+      w += (size_t)N * l;
+      Ciphertext A(cc, raw_of(a0, a1, l, N, S));
+      Ciphertext M = ev.EvalMult(A, P);
+      if (M.getLevel() != l - 1 || std::abs(M.NoiseFactor / ev.GetScalingFactorReal(l - 1) - 1) > 1e-12)
+        throw Error(FIDES_ERR_STATE, "EvalMult(plaintext) metadata");
+      put(M, w);
+      put(ev.EvalAdd(A, P), w);
+      put(ev.EvalSub(A, P), w);
+      bool refused = false;  // a plaintext at another scale is refused
+      try {
+        Plaintext Q = ev.MakeCKKSPackedPlaintext(slots, l, 2 * S);
+        ev.EvalAdd(A, Q);
+      } catch (const Error& e) {
+        refused = e.code == FIDES_ERR_ARG;
+      }
+      if (!refused) throw Error(FIDES_ERR_STATE, "EvalAdd with a mismatched scale was not refused");
+    }
+    {
+      CryptoContextImpl man(cc, FIXEDMANUAL, top_scale);
+      Plaintext P = man.MakeCKKSPackedPlaintext(slots, l);
+      Ciphertext A(cc, raw_of(a0, a1, l, N, 1.0));
+      Ciphertext M = man.EvalMult(A, P);
+      if (M.NoiseLevel != 2 || M.getLevel() != l) throw Error(FIDES_ERR_STATE, "FIXEDMANUAL plaintext product");
+      put(M, w);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from ckks_host import KeyGen, decode, encode, uniform_limbs, xrng
+from ckks_host import KeyGen, decode, encode, small_to_limbs, uniform_limbs, xrng
 
 
 def _u0(n):
@@ -512,6 +512,8 @@ def _facade_lib():
                                      dp, C.c_char_p, C.c_int]
     lib.facade_arith.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, C.c_int, vp, C.c_int,
                                  u64p, u64p, u64p, u64p, u64p, u64p, C.c_char_p, C.c_int]
+    lib.facade_plain.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, C.c_int, u64p, u64p, dp,
+                                 C.c_int, u64p, C.c_char_p, C.c_int]
     return lib
 
 
@@ -772,3 +774,63 @@ def test_native_bootstrap_reduced_noise_n4096(fides):
     print(f"N=2^12 bootstrap: plain {bits[False]:.2f} bits, reduced noise {bits[True]:.2f} bits")
     assert not np.array_equal(outs[True][0][0], outs[False][0][0])
     assert bits[True] > 12 and bits[True] >= bits[False] - 0.5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_slots", [2048, 100])
+def test_cpp_facade_plaintexts(fides, n_slots):
+    """The C++ facade's MakeCKKSPackedPlaintext (device encode at the level's canonical scale;
+    fewer slots than N/2 are zero-padded to a power of two) and EvalMult / EvalAdd / EvalSub
+    with that plaintext under FLEXIBLEAUTO (product rescaled to S_(l-1)) and FIXEDMANUAL (degree
+    2, not rescaled): the plaintext's coefficients are within 1 of the host encoder's, its
+    limbs are one integer polynomial, and every ciphertext result equals the oracle's
+    operations on those limbs residue for residue; a plaintext at another scale is refused."""
+    import ctypes as C
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 50, 8, 2, name="facade")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    N, L, q = prm.N, prm.n_q, prm.q
+    l = L - 1
+    S = [0.0] * (L + 1)
+    S[L] = 2.0 ** 45
+    for k in range(L, 1, -1):
+        S[k - 1] = S[k] * S[k] / q[k - 1]
+    rng = xrng(80 + n_slots)
+    a = [uniform_limbs(rng, q[:l], N) for _ in range(2)]
+    z = rng.uniform(-1, 1, n_slots) + 1j * rng.uniform(-1, 1, n_slots)
+    zz = np.stack([z.real, z.imag], axis=1).reshape(-1).copy()
+    sizes = [l, l - 1, l, l, l]  # plaintext limbs, then 4 ciphertexts
+    out = np.zeros((sizes[0] + 2 * sum(sizes[1:])) * N, dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    u64 = lambda x: np.ascontiguousarray(x, dtype=np.uint64).ctypes.data_as(C.POINTER(C.c_uint64))
+    primes = np.array(q + prm.p, dtype=np.uint64)
+    rc = _facade_lib().facade_plain(prm.logN, L, prm.K, prm.dnum, u64(primes), S[L], l, u64(a[0]), u64(a[1]),
+                                    zz.ctypes.data_as(C.POINTER(C.c_double)), n_slots, u64(out), err, 512)
+    assert rc == 0, err.value.decode()
+    ids = list(range(l))
+    pt = out[:l * N].reshape(l, N)
+    # the encoded polynomial: n_slots zero-padded to n (a power of two), the 2n-ring encoding's
+    # coefficients spread with gap N / 2n
+    n = 1 << (n_slots - 1).bit_length()
+    zp = np.zeros(n, dtype=np.complex128)
+    zp[:n_slots] = z
+    ref = np.zeros(N)
+    ref[::N // (2 * n)] = encode(zp, 2 * n, S[l])
+    m = o.ntt(pt, ids, inverse=True)[0].astype(object)
+    m = np.array([int(v) - q[0] if int(v) > q[0] // 2 else int(v) for v in m], dtype=np.int64)
+    diff = np.abs(m - ref.astype(np.int64))
+    assert diff.max() <= 1 and np.count_nonzero(diff) <= max(1, N // 1000)
+    assert np.array_equal(pt, o.ntt(small_to_limbs(m, q[:l]), ids))
+    pos, got = l * N, []
+    for s_ in sizes[1:]:
+        got.append((out[pos:pos + s_ * N].reshape(s_, N), out[pos + s_ * N:pos + 2 * s_ * N].reshape(s_, N)))
+        pos += 2 * s_ * N
+    prod = [o.mul(a[i], pt, ids) for i in range(2)]
+    want = [(o.rescale(prod[0]), o.rescale(prod[1])),
+            (o.add(a[0], pt, ids), a[1]),
+            (o.sub(a[0], pt, ids), a[1]),
+            (prod[0], prod[1])]
+    for name, (g0, g1), (w0, w1) in zip(["EvalMult(pt)", "EvalAdd(pt)", "EvalSub(pt)", "FIXEDMANUAL EvalMult(pt)"],
+                                        got, want):
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name

@@ -2,7 +2,8 @@
 // fideslib::CryptoContextImpl<DCRTPoly> (api/CryptoContext.hpp:306-458, bodies in
 // api/CryptoContext.cpp:1120-1299 over CudaEngine, api/engine/cuda/CudaEngine.cpp:429-1150):
 // MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
-// real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare, Rescale,
+// real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare,
+// EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -111,6 +112,13 @@ class CryptoContextImpl {
     Ciphertext o = fresh(level - 1, new_scale, 1, a.slots);
     check(fides_rescale(cc_->handle(), t.c0(), level, o.c0(), cc_->stream()));
     check(fides_rescale(cc_->handle(), t.c1(), level, o.c1(), cc_->stream()));
+    if (a.hasC2()) {  // a third component is scaled the same way
+      DeviceLimbs t2((size_t)N() * level);
+      o.c2_ = DeviceLimbs((size_t)N() * (level - 1));
+      check(fides_mul_scalar(cc_->handle(), a.c2(), level, s.data(), t2.get(), cc_->stream()));
+      check(fides_rescale(cc_->handle(), t2.get(), level, o.c2(), cc_->stream()));
+      cc_->synchronize();
+    }
     cc_->synchronize();  // t is released at scope exit
     return o;
   }
@@ -120,11 +128,8 @@ class CryptoContextImpl {
     Ciphertext A = tech_ == FLEXIBLEAUTO ? AdjustToLevel(a, l) : copy_of(a, l);
     if (!same_scale(A.NoiseFactor, p.scale))
       throw Error(FIDES_ERR_ARG, "the plaintext's scale differs from the ciphertext's");
-    Ciphertext o = fresh(l, A.NoiseFactor, A.NoiseLevel, a.slots);
+    Ciphertext o = copy_of(A, l);  // c1 (and c2) as they are
     check((sub ? fides_sub : fides_add)(cc_->handle(), A.c0(), p.data(), l, o.c0(), cc_->stream()));
-    check_cuda(cudaMemcpyAsync(o.c1(), A.c1(), sizeof(uint64_t) * (size_t)N() * l, cudaMemcpyDeviceToDevice,
-                               cc_->stream()),
-               "D2D");
     cc_->synchronize();  // A is released at scope exit
     return o;
   }
@@ -134,6 +139,10 @@ class CryptoContextImpl {
     const size_t bytes = sizeof(uint64_t) * (size_t)N() * level;
     check_cuda(cudaMemcpyAsync(o.c0(), a.c0(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
     check_cuda(cudaMemcpyAsync(o.c1(), a.c1(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+    if (a.hasC2()) {
+      o.c2_ = DeviceLimbs((size_t)N() * level);
+      check_cuda(cudaMemcpyAsync(o.c2(), a.c2(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+    }
     return o;
   }
 
@@ -160,9 +169,15 @@ class CryptoContextImpl {
   // same value on fewer limbs (FIXEDMANUAL, scale unchanged).
   Ciphertext AdjustToLevel(const Ciphertext& a, int level) const {
     if (level < 1 || level > a.getLevel()) throw Error(FIDES_ERR_LEVEL, "cannot raise a ciphertext's level");
+    if (tech_ == FIXEDMANUAL) return copy_of(a, level);  // limbs dropped, scale and degree unchanged
+    if (a.NoiseLevel == 2) {
+      // an unrescaled product (EvalMultNoRelin / Relinearize): kept as it is at its own level,
+      // otherwise rescaled first, as OpenFHE does before the next operation
+      if (level == a.getLevel()) return copy_of(a, level);
+      return AdjustToLevel(Rescale(a), level);
+    }
     if (a.NoiseLevel != 1) throw Error(FIDES_ERR_STATE, "adjust a degree-2 ciphertext after Rescale");
-    if (tech_ == FIXEDMANUAL || (a.getLevel() == level && same_scale(a.NoiseFactor, S_[level])))
-      return copy_of(a, level);
+    if (a.getLevel() == level && same_scale(a.NoiseFactor, S_[level])) return copy_of(a, level);
     if (a.getLevel() == level)
       throw Error(FIDES_ERR_LEVEL, "scale differs from the level's canonical scale and no level is left to adjust it");
     const double k = round_even(S_[level] * (double)q(level) / a.NoiseFactor);
@@ -211,9 +226,28 @@ class CryptoContextImpl {
   // ciphertext is first brought to the lower of the two levels)
   Ciphertext EvalAdd(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, false); }
   Ciphertext EvalSub(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, true); }
+  // EvalNegate (CryptoContextImpl::EvalNegate): every component times -1
+  Ciphertext EvalNegate(const Ciphertext& a) const {
+    const int l = a.getLevel();
+    const auto m1 = residues(-1.0, l);
+    Ciphertext o = copy_of(a, l);
+    check(fides_mul_scalar(cc_->handle(), a.c0(), l, m1.data(), o.c0(), cc_->stream()));
+    check(fides_mul_scalar(cc_->handle(), a.c1(), l, m1.data(), o.c1(), cc_->stream()));
+    if (a.hasC2()) check(fides_mul_scalar(cc_->handle(), a.c2(), l, m1.data(), o.c2(), cc_->stream()));
+    return o;
+  }
+  // EvalAddMany (CryptoContextImpl::EvalAddMany): the sum of the ciphertexts, left to right
+  Ciphertext EvalAddMany(const std::vector<const Ciphertext*>& cts) const {
+    if (cts.empty()) throw Error(FIDES_ERR_ARG, "no ciphertexts");
+    Ciphertext acc = copy_of(*cts[0], cts[0]->getLevel());
+    for (size_t i = 1; i < cts.size(); ++i) acc = EvalAdd(acc, *cts[i]);
+    return acc;
+  }
 
   // ---- multiplicative operations (EvalMult, EvalSquare, Rescale)
   Ciphertext EvalMult(const Ciphertext& a, const Ciphertext& b) const {
+    a.need_two();
+    b.need_two();
     if (tech_ == FIXEDMANUAL) {
       const int l = std::min(a.getLevel(), b.getLevel());
       Ciphertext A = copy_of(a, l), B = copy_of(b, l);
@@ -238,6 +272,7 @@ class CryptoContextImpl {
   // FLEXIBLEAUTO: the ciphertext at its canonical scale, the product rescaled (level l - 1,
   // scale S_l p.scale / q_(l-1), which is S_(l-1) for a plaintext at the canonical S_l).
   Ciphertext EvalMult(const Ciphertext& a, const Plaintext& p) const {
+    a.need_two();
     const int l = std::min(a.getLevel(), p.level);
     if (tech_ == FIXEDMANUAL) {
       Ciphertext o = fresh(l, a.NoiseFactor * p.scale, a.NoiseLevel + 1, a.slots);
@@ -259,6 +294,7 @@ class CryptoContextImpl {
   // Multiplication by a real constant: FLEXIBLEAUTO lands on level l - 1 at S_(l-1); FIXEDMANUAL
   // multiplies by round(c q_(l-1)) and raises the degree (the next Rescale divides q_(l-1) out).
   Ciphertext EvalMult(const Ciphertext& a, double c) const {
+    a.need_two();
     const int l = a.getLevel();
     if (tech_ == FIXEDMANUAL) {
       const double k = round_even(c * (double)q(l - 1));
@@ -272,21 +308,56 @@ class CryptoContextImpl {
     const double k = round_even(c * S_[l - 1] * (double)q(l - 1) / a.NoiseFactor);
     return mul_int_rescale(a, l, k, S_[l - 1]);
   }
+  // FIXEDMANUAL: divides by the top prime and drops it.  FLEXIBLEAUTO: products are already
+  // rescaled (a copy), except the unrescaled ones of EvalMultNoRelin, which land on S_(l-1).
   Ciphertext Rescale(const Ciphertext& a) const {
-    if (tech_ == FLEXIBLEAUTO) return copy_of(a, a.getLevel());
+    if (tech_ == FLEXIBLEAUTO && a.NoiseLevel != 2) return copy_of(a, a.getLevel());
     Ciphertext o = copy_of(a, a.getLevel());
     o.rescale();
     return o;
   }
 
+  // EvalMultNoRelin (CryptoContextImpl::EvalMultNoRelin): the tensor product (a0 b0, a0 b1 +
+  // a1 b0, a1 b1) of two ciphertexts on the lower level, without key switching: three components
+  // until Relinearize.  Scale = product of the operands' (FLEXIBLEAUTO: operands first brought to
+  // that level's canonical scale, so S_l^2), degree = sum.
+  Ciphertext EvalMultNoRelin(const Ciphertext& a, const Ciphertext& b) const {
+    a.need_two();
+    b.need_two();
+    const int l = std::min(a.getLevel(), b.getLevel());
+    Ciphertext A = tech_ == FLEXIBLEAUTO ? AdjustToLevel(a, l) : copy_of(a, l);
+    Ciphertext B = tech_ == FLEXIBLEAUTO ? AdjustToLevel(b, l) : copy_of(b, l);
+    Ciphertext o = fresh(l, A.NoiseFactor * B.NoiseFactor, A.NoiseLevel + B.NoiseLevel, a.slots);
+    o.c2_ = DeviceLimbs((size_t)N() * l);
+    check(fides_tensor(cc_->handle(), A.c0(), A.c1(), B.c0(), B.c1(), l, o.c0(), o.c1(), o.c2(), cc_->stream()));
+    cc_->synchronize();  // A and B are released at scope exit
+    return o;
+  }
+  // Relinearize (CryptoContextImpl::Relinearize): the third component key-switched with the
+  // relinearisation key and added, (c0 + f0, c1 + f1); level, scale and degree unchanged.  Equal
+  // residue for residue to EvalMult's product before its rescale.
+  Ciphertext Relinearize(const Ciphertext& a) const {
+    const int l = a.getLevel();
+    if (!a.hasC2()) return copy_of(a, l);
+    Ciphertext o = fresh(l, a.NoiseFactor, a.NoiseLevel, a.slots);
+    DeviceLimbs f0((size_t)N() * l), f1((size_t)N() * l);
+    check(fides_keyswitch(cc_->handle(), a.c2(), l, cc_->GetEvalKey().device(), f0.get(), f1.get(), cc_->stream()));
+    check(fides_add(cc_->handle(), a.c0(), f0.get(), l, o.c0(), cc_->stream()));
+    check(fides_add(cc_->handle(), a.c1(), f1.get(), l, o.c1(), cc_->stream()));
+    cc_->synchronize();  // f0 and f1 are released at scope exit
+    return o;
+  }
+
   // ---- rotations (EvalRotate, EvalFastRotationPrecompute, EvalFastRotation)
   Ciphertext EvalRotate(const Ciphertext& a, int index) const {
+    a.need_two();
     Ciphertext o = fresh(a.getLevel(), a.NoiseFactor, a.NoiseLevel, a.slots);
     check(fides_rotate(cc_->handle(), a.c0(), a.c1(), a.getLevel(), cc_->GetRotationKey(index).device(), index,
                        o.c0(), o.c1(), cc_->stream()));
     return o;
   }
   std::shared_ptr<FastRotationPrecompute> EvalFastRotationPrecompute(const Ciphertext& a) const {
+    a.need_two();
     auto p = std::make_shared<FastRotationPrecompute>();
     const int l = a.getLevel(), beta = (l + fides_ctx_alpha(cc_->handle()) - 1) / fides_ctx_alpha(cc_->handle());
     p->level = l;
@@ -300,6 +371,23 @@ class CryptoContextImpl {
     (void)m;
     auto v = EvalFastRotation(a, std::vector<int>{index}, pre);
     return std::move(v.at(0));
+  }
+  // EvalRotateMany (CryptoContextImpl::EvalRotateMany, CudaEngine::evalRotateMany): every
+  // ciphertext rotated by the same index, all in one launch sequence (fides_rotate_batch).
+  std::vector<Ciphertext> EvalRotateMany(const std::vector<const Ciphertext*>& cts, int index) const {
+    std::vector<Ciphertext> outs;
+    std::vector<fides_rotate_item> items;
+    const uint64_t* key = cc_->GetRotationKey(index).device();
+    const uint32_t k = fides_rotation_auto_index(cc_->logN, index);
+    for (const Ciphertext* c : cts) {
+      c->need_two();
+      outs.push_back(fresh(c->getLevel(), c->NoiseFactor, c->NoiseLevel, c->slots));
+    }
+    for (size_t i = 0; i < cts.size(); ++i)
+      items.push_back(fides_rotate_item{cts[i]->c0(), cts[i]->c1(), outs[i].c0(), outs[i].c1(), key,
+                                        cts[i]->getLevel(), k});
+    if (!items.empty()) check(fides_rotate_batch(cc_->handle(), items.data(), (int)items.size(), cc_->stream()));
+    return outs;
   }
   // Several indexes from one precomputation, in one launch sequence.
   std::vector<Ciphertext> EvalFastRotation(const Ciphertext& a, const std::vector<int>& indexes,
@@ -365,6 +453,7 @@ class CryptoContextImpl {
   }
   // The input's limb q_0 is bootstrapped; its slots must be at the setup's msgScale.
   Ciphertext EvalBootstrap(const Ciphertext& a) const {
+    a.need_two();
     if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
     int lo = 0;
     double sc = 0;
@@ -399,14 +488,33 @@ class CryptoContextImpl {
 
  private:
   Ciphertext add_sub(const Ciphertext& a, const Ciphertext& b, bool sub) const {
+    if (tech_ == FLEXIBLEAUTO && (a.NoiseLevel == 2 || b.NoiseLevel == 2) &&
+        !(a.NoiseLevel == 2 && b.NoiseLevel == 2 && a.getLevel() == b.getLevel())) {
+      // unrescaled products meet only their like at the same level; otherwise rescale first
+      if (a.NoiseLevel == 2 && b.NoiseLevel == 2) return add_sub(Rescale(a), Rescale(b), sub);
+      if (a.NoiseLevel == 2) return add_sub(Rescale(a), b, sub);
+      return add_sub(a, Rescale(b), sub);
+    }
     const int l = std::min(a.getLevel(), b.getLevel());
     Ciphertext A = AdjustToLevel(a, l), B = AdjustToLevel(b, l);
-    if (tech_ == FIXEDMANUAL && (A.NoiseLevel != B.NoiseLevel || !same_scale(A.NoiseFactor, B.NoiseFactor)))
+    if (A.NoiseLevel != B.NoiseLevel || !same_scale(A.NoiseFactor, B.NoiseFactor))
       throw Error(FIDES_ERR_STATE, "operands at different scales (rescale first)");
     Ciphertext o = fresh(l, A.NoiseFactor, A.NoiseLevel, a.slots);
     auto f = sub ? fides_sub : fides_add;
     check(f(cc_->handle(), A.c0(), B.c0(), l, o.c0(), cc_->stream()));
     check(f(cc_->handle(), A.c1(), B.c1(), l, o.c1(), cc_->stream()));
+    if (A.hasC2() || B.hasC2()) {  // a missing third component is zero
+      o.c2_ = DeviceLimbs((size_t)N() * l);
+      const size_t bytes = sizeof(uint64_t) * (size_t)N() * l;
+      if (A.hasC2() && B.hasC2())
+        check(f(cc_->handle(), A.c2(), B.c2(), l, o.c2(), cc_->stream()));
+      else if (A.hasC2())
+        check_cuda(cudaMemcpyAsync(o.c2(), A.c2(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+      else if (!sub)
+        check_cuda(cudaMemcpyAsync(o.c2(), B.c2(), bytes, cudaMemcpyDeviceToDevice, cc_->stream()), "D2D");
+      else
+        check(fides_mul_scalar(cc_->handle(), B.c2(), l, residues(-1.0, l).data(), o.c2(), cc_->stream()));
+    }
     cc_->synchronize();
     return o;
   }

@@ -206,12 +206,14 @@ class Ciphertext {
   friend class CryptoContextImpl;
   Context* cc_;
   DeviceLimbs c0_, c1_;
+  DeviceLimbs c2_;  // third component of an unrelinearised product (CryptoContextImpl::EvalMultNoRelin)
   int level_ = 0;
 
   void alloc(int level) {
     level_ = level;
     c0_ = DeviceLimbs((size_t)level * cc_->N);
     c1_ = DeviceLimbs((size_t)level * cc_->N);
+    c2_ = DeviceLimbs();
   }
 
  public:
@@ -227,6 +229,11 @@ class Ciphertext {
   int getLevel() const { return level_; }  // active Q limbs
   uint64_t* c0() const { return c0_.get(); }
   uint64_t* c1() const { return c1_.get(); }
+  uint64_t* c2() const { return c2_.get(); }
+  bool hasC2() const { return c2_.get() != nullptr; }  // three components (not relinearised)
+  void need_two() const {
+    if (hasC2()) throw Error(FIDES_ERR_STATE, "three-component ciphertext: relinearize first");
+  }
 
   // reference Ciphertext::load / store (Ciphertext.cpp; CudaEngine.cpp:1768-1795, 1156-1227)
   void load(const RawCipherText& raw) {
@@ -250,6 +257,7 @@ class Ciphertext {
   }
 
   void store(RawCipherText& raw) const {
+    need_two();
     const int N = cc_->N;
     raw.N = N;
     raw.numRes = level_;
@@ -272,6 +280,7 @@ class Ciphertext {
 
   // reference Ciphertext::mult(b, rescale) (Ciphertext.cpp:660-869): tensor + relinearize
   void mult(const Ciphertext& b, bool rescale = false) {
+    need_two();
     if (b.level_ != level_) throw Error(FIDES_ERR_LEVEL, "operands at different levels");
     const int lo = rescale ? level_ - 1 : level_;
     Ciphertext out(*cc_);
@@ -284,9 +293,11 @@ class Ciphertext {
       f /= (double)cc_->primes[level_ - 1];
       nl -= 1;
     }
+    const int sl = slots;
     *this = std::move(out);
     NoiseFactor = f;
     NoiseLevel = nl;
+    slots = sl;
   }
   void square(bool rescale = false) { mult(*this, rescale); }
 
@@ -297,26 +308,35 @@ class Ciphertext {
     out.alloc(level_ - 1);
     check(fides_rescale(cc_->handle(), c0(), level_, out.c0(), cc_->stream()));
     check(fides_rescale(cc_->handle(), c1(), level_, out.c1(), cc_->stream()));
+    if (hasC2()) {  // every component is divided by the same prime
+      out.c2_ = DeviceLimbs((size_t)(level_ - 1) * cc_->N);
+      check(fides_rescale(cc_->handle(), c2(), level_, out.c2(), cc_->stream()));
+    }
     const double f = NoiseFactor / (double)cc_->primes[level_ - 1];
-    const int nl = NoiseLevel - 1;
+    const int nl = NoiseLevel - 1, sl = slots;
+    cc_->synchronize();  // the old buffers are released below
     *this = std::move(out);
     NoiseFactor = f;
     NoiseLevel = nl;
+    slots = sl;
   }
 
   // reference Ciphertext::rotate(index) (Ciphertext.cpp:1102-1168)
   void rotate(int index) {
+    need_two();
     check(fides_rotate(cc_->handle(), c0(), c1(), level_, cc_->GetRotationKey(index).device(), index, c0(), c1(),
                        cc_->stream()));
   }
   // reference Ciphertext::conjugate (Ciphertext.cpp:1175-1219)
   void conjugate() {
+    need_two();
     const uint32_t k = 2u * cc_->N - 1;
     check(fides_rotate_auto(cc_->handle(), c0(), c1(), level_, cc_->GetRotationKey(2 * cc_->N - 1).device(), k,
                             c0(), c1(), cc_->stream()));
   }
   // reference Ciphertext::add / sub (Ciphertext.cpp:244-330)
   void add(const Ciphertext& b) {
+    need_two();
     if (b.level_ != level_) throw Error(FIDES_ERR_LEVEL, "operands at different levels");
     check(fides_add(cc_->handle(), c0(), b.c0(), level_, c0(), cc_->stream()));
     check(fides_add(cc_->handle(), c1(), b.c1(), level_, c1(), cc_->stream()));
@@ -329,6 +349,7 @@ class Ciphertext {
 
   // reference Ciphertext::keySwitch (Ciphertext.cpp:1893-1907): (c0 + f0, f1)
   void keySwitch(const KeySwitchingKey& ksk) {
+    need_two();
     DeviceLimbs f0((size_t)level_ * cc_->N), f1((size_t)level_ * cc_->N);
     check(fides_keyswitch(cc_->handle(), c1(), level_, ksk.device(), f0.get(), f1.get(), cc_->stream()));
     check(fides_add(cc_->handle(), c0(), f0.get(), level_, c0(), cc_->stream()));
@@ -338,6 +359,7 @@ class Ciphertext {
 
   // reference Ciphertext::rotate_hoisted (Ciphertext.cpp:1221-1394)
   void rotate_hoisted(const std::vector<int>& indexes, std::vector<Ciphertext*> results) const {
+    need_two();
     if (results.size() != indexes.size()) throw Error(FIDES_ERR_ARG, "one result per index");
     std::vector<const uint64_t*> keys;
     std::vector<uint64_t*> o0, o1;

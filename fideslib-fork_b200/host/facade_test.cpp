@@ -209,4 +209,62 @@ int facade_plain(int logN, int n_q, int K, int dnum, const uint64_t* primes, dou
   }
 }
 
+// Unrelinearised products and the other CryptoContextImpl forms, on ciphertexts a, b at l limbs
+// (top_scale as in facade_arith), packed into out in this order, each as c0 then c1 limbs:
+//   FIXEDMANUAL Relinearize(EvalMultNoRelin(a, b)) [l] |
+//   FIXEDMANUAL Relinearize(EvalAdd(EvalMultNoRelin(a, b), EvalMultNoRelin(a, a))) [l] |
+//   FLEXIBLEAUTO Rescale(Relinearize(EvalMultNoRelin(a, b))) [l-1] | EvalNegate(a) [l] |
+//   EvalAddMany({a, b, a}) [l] | EvalRotateMany({a, b}, rot) [l] [l]
+int facade_more(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, const uint64_t* relin,
+                int rot, const uint64_t* rot_key, int l, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
+                const uint64_t* b1, uint64_t* out, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    cc.AddEvalKey(key_from(cc, relin));
+    cc.AddRotationKey(rot, key_from(cc, rot_key));
+    uint64_t* w = out;
+    {
+      CryptoContextImpl man(cc, FIXEDMANUAL, top_scale);
+      Ciphertext A(cc, raw_of(a0, a1, l, N, 1.0)), B(cc, raw_of(b0, b1, l, N, 1.0));
+      Ciphertext X = man.EvalMultNoRelin(A, B);
+      if (!X.hasC2() || X.NoiseLevel != 2 || X.getLevel() != l) throw Error(FIDES_ERR_STATE, "EvalMultNoRelin");
+      bool refused = false;  // three components go through Relinearize first
+      try {
+        man.EvalRotate(X, rot);
+      } catch (const Error& e) {
+        refused = e.code == FIDES_ERR_STATE;
+      }
+      if (!refused) throw Error(FIDES_ERR_STATE, "a three-component rotation was not refused");
+      Ciphertext R = man.Relinearize(X);
+      if (R.hasC2()) throw Error(FIDES_ERR_STATE, "Relinearize left a third component");
+      put(R, w);
+      put(man.Relinearize(man.EvalAdd(X, man.EvalMultNoRelin(A, A))), w);
+    }
+    {
+      CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+      const double S = ev.GetScalingFactorReal(l);
+      Ciphertext A(cc, raw_of(a0, a1, l, N, S)), B(cc, raw_of(b0, b1, l, N, S));
+      Ciphertext R = ev.Rescale(ev.Relinearize(ev.EvalMultNoRelin(A, B)));
+      if (R.getLevel() != l - 1 || R.NoiseLevel != 1 || std::abs(R.NoiseFactor / ev.GetScalingFactorReal(l - 1) - 1) > 1e-12)
+        throw Error(FIDES_ERR_STATE, "FLEXIBLEAUTO relinearised product metadata");
+      put(R, w);
+      put(ev.EvalNegate(A), w);
+      put(ev.EvalAddMany({&A, &B, &A}), w);
+      auto rs = ev.EvalRotateMany({&A, &B}, rot);
+      put(rs.at(0), w);
+      put(rs.at(1), w);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

@@ -514,6 +514,8 @@ def _facade_lib():
                                  u64p, u64p, u64p, u64p, u64p, u64p, C.c_char_p, C.c_int]
     lib.facade_plain.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, C.c_int, u64p, u64p, dp,
                                  C.c_int, u64p, C.c_char_p, C.c_int]
+    lib.facade_more.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, C.c_int, vp, C.c_int,
+                                u64p, u64p, u64p, u64p, u64p, C.c_char_p, C.c_int]
     return lib
 
 
@@ -833,4 +835,54 @@ def test_cpp_facade_plaintexts(fides, n_slots):
             (prod[0], prod[1])]
     for name, (g0, g1), (w0, w1) in zip(["EvalMult(pt)", "EvalAdd(pt)", "EvalSub(pt)", "FIXEDMANUAL EvalMult(pt)"],
                                         got, want):
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name
+
+
+@pytest.mark.gpu
+def test_cpp_facade_norelin_and_many(fides):
+    """The C++ facade's EvalMultNoRelin + Relinearize (three-component ciphertexts; a lazily
+    relinearised sum of two products), EvalNegate, EvalAddMany and EvalRotateMany (one batched
+    launch sequence) against the oracle residue for residue, and the FLEXIBLEAUTO
+    Rescale(Relinearize(EvalMultNoRelin)) against the fused product."""
+    import ctypes as C
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 50, 8, 2, name="facade")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=69)
+    rk, rot = kg.relin_key(), 3
+    kr = kg.rotation_key(rot)
+    rk_d, kr_d = F.to_device(rk), F.to_device(kr)
+    N, l, q = prm.N, prm.n_q, prm.q
+    rng = xrng(90)
+    a = [uniform_limbs(rng, q, N) for _ in range(2)]
+    b = [uniform_limbs(rng, q, N) for _ in range(2)]
+    sizes = [l, l, l - 1, l, l, l, l]
+    out = np.zeros(2 * sum(sizes) * N, dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    u64 = lambda x: np.ascontiguousarray(x, dtype=np.uint64).ctypes.data_as(C.POINTER(C.c_uint64))
+    primes = np.array(q + prm.p, dtype=np.uint64)
+    rc = _facade_lib().facade_more(prm.logN, l, prm.K, prm.dnum, u64(primes), 2.0 ** 45, rk_d.data_ptr(), rot,
+                                   kr_d.data_ptr(), l, u64(a[0]), u64(a[1]), u64(b[0]), u64(b[1]), u64(out), err, 512)
+    assert rc == 0, err.value.decode()
+    got, pos = [], 0
+    for s_ in sizes:
+        got.append((out[pos:pos + s_ * N].reshape(s_, N), out[pos + s_ * N:pos + 2 * s_ * N].reshape(s_, N)))
+        pos += 2 * s_ * N
+    ids = list(range(l))
+    x0, x1, x2 = o.tensor(a[0], a[1], b[0], b[1])
+    y0, y1, y2 = o.tensor(a[0], a[1], a[0], a[1])
+    s0, s1, s2 = o.add(x0, y0, ids), o.add(x1, y1, ids), o.add(x2, y2, ids)
+    f0, f1 = o.keyswitch(s2, rk)
+    neg = [o.sub(np.zeros_like(a[i]), a[i], ids) for i in range(2)]
+    want = [o.hmult(a[0], a[1], b[0], b[1], rk, rescale=False),
+            (o.add(s0, f0, ids), o.add(s1, f1, ids)),
+            o.hmult(a[0], a[1], b[0], b[1], rk, rescale=True),
+            (neg[0], neg[1]),
+            (o.add(o.add(a[0], b[0], ids), a[0], ids), o.add(o.add(a[1], b[1], ids), a[1], ids)),
+            o.rotate(a[0], a[1], kr, rot),
+            o.rotate(b[0], b[1], kr, rot)]
+    names = ["Relinearize(EvalMultNoRelin)", "lazy relinearisation of a sum", "FLEXIBLEAUTO NoRelin+Relinearize+Rescale",
+             "EvalNegate", "EvalAddMany", "EvalRotateMany[0]", "EvalRotateMany[1]"]
+    for name, (g0, g1), (w0, w1) in zip(names, got, want):
         assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name

@@ -1040,7 +1040,8 @@ struct Bootstrapper {
     return it->second;
   }
 
-  Powers cheb_powers(const std::vector<boot::Ct>& ts, cudaStream_t s) const {
+  // T_1 .. T_min(PS_BABY, degree) and the doublings T_32, T_64, ... up to `degree`
+  Powers cheb_powers(const std::vector<boot::Ct>& ts, int degree, cudaStream_t s) const {
     Powers P;
     P.T[1] = ts;
     auto make = [&](int k) {
@@ -1061,8 +1062,8 @@ struct Bootstrapper {
         P.T[k] = lincomb_many(lanes, {2, -1}, 0.0, s);
       }
     };
-    for (int k = 2; k <= PS_BABY; ++k) make(k);
-    for (int m = 2 * PS_BABY; m <= prm.degree; m *= 2) make(m);
+    for (int k = 2; k <= std::min(PS_BABY, degree); ++k) make(k);
+    for (int m = 2 * PS_BABY; m <= degree; m *= 2) make(m);
     return P;
   }
 
@@ -1097,7 +1098,7 @@ struct Bootstrapper {
   }
 
   std::vector<boot::Ct> eval_mod_many(const std::vector<boot::Ct>& ts, cudaStream_t s) const {
-    Powers P = cheb_powers(ts, s);
+    Powers P = cheb_powers(ts, prm.degree, s);
     const int depth = (int)std::ceil(std::log2((double)prm.degree)) + 1;
     auto cs = ps(cheb, ts[0].level - depth, P, (int)ts.size(), s);
     for (int k = 0; k < prm.r; ++k) {
@@ -1109,6 +1110,33 @@ struct Bootstrapper {
       cs = lincomb_many(lanes, {2}, -1.0, s);
     }
     return cs;
+  }
+
+  // Chebyshev series in OpenFHE's convention, p(x) = c_0 / 2 + sum_(k >= 1) c_k T_k(t) with
+  // t = (2 x - (lo + hi)) / (hi - lo) (reference evalChebyshevSeries, src/CKKS/ApproxModEval.cu:
+  // 527; CryptoContext::EvalChebyshevSeries), by the Paterson-Stockmeyer evaluation above.
+  // Inputs at their level's canonical scale (else brought there one level down).  Levels
+  // consumed: ceil(log2 d) + 1 for degree d, one more when [lo, hi] is not [-1, 1].
+  std::vector<boot::Ct> eval_chebyshev_many(std::vector<boot::Ct> xs, std::vector<double> coeffs, double lo, double hi,
+                                            cudaStream_t s) const {
+    while (coeffs.size() > 1 && coeffs.back() == 0.0) coeffs.pop_back();
+    if (coeffs.empty()) throw Error(-1, "chebyshev: no coefficients");
+    coeffs[0] /= 2;
+    if (!(hi > lo)) throw Error(-1, "chebyshev: empty interval");
+    const int d = (int)coeffs.size() - 1;
+    const int depth = d <= 1 ? 1 : (int)std::ceil(std::log2((double)d)) + 1;
+    const bool affine = std::abs(lo + 1.0) > 1e-12 || std::abs(hi - 1.0) > 1e-12;
+    int l = xs[0].level;
+    if (std::abs(xs[0].scale / S[l] - 1) > 1e-12) xs = to_level_many(xs, --l, s);
+    if (l - depth - (affine ? 1 : 0) < 1) throw Error(-4, "chebyshev: not enough levels for this degree");
+    if (affine) {
+      std::vector<std::vector<boot::Ct>> lanes;
+      for (const auto& x : xs) lanes.push_back({x});
+      xs = lincomb_to_many(lanes, {2.0 / (hi - lo)}, -(hi + lo) / (hi - lo), l - 1, s);
+      --l;
+    }
+    Powers P = cheb_powers(xs, std::max(d, 1), s);
+    return ps(coeffs, l - depth, P, (int)xs.size(), s);
   }
 
   // ---------------------------------------------------------------- the bootstrap
@@ -1219,6 +1247,42 @@ fides::Bootstrapper* B(fides_boot* b) {
 }  // namespace
 
 extern "C" {
+
+int fides_eval_chebyshev(fides_ctx* ctx, const uint64_t* relin_key, double top_scale, const uint64_t* c0,
+                         const uint64_t* c1, int level, double scale, const double* coeffs, int n_coeffs, double lo,
+                         double hi, uint64_t* out0, uint64_t* out1, int* out_level, double* out_scale,
+                         void* stream) {
+  return bguard(__func__, [&] {
+    if (!ctx || !ctx->c || !relin_key || !c0 || !c1 || !coeffs || !out0 || !out1)
+      throw fides::Error(FIDES_ERR_ARG, "null argument");
+    fides::Context* c = ctx->c;
+    FIDES_CUDA(cudaSetDevice(c->device));
+    if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "relinearisation needs special primes");
+    if (level < 2 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (n_coeffs < 1 || n_coeffs > 1025) throw fides::Error(FIDES_ERR_ARG, "1..1025 coefficients");
+    if (!(top_scale > 0) || !(scale > 0)) throw fides::Error(FIDES_ERR_ARG, "scales must be positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an evaluator over the context: the canonical scale chain of top_scale and the relinearisation
+    // key (no bootstrapping tables)
+    fides::Bootstrapper ev{};
+    ev.c = c;
+    ev.relin = relin_key;
+    ev.S.assign(c->n_q + 1, 0.0);
+    ev.S[c->n_q] = top_scale;
+    for (int l = c->n_q; l > 1; --l) ev.S[l - 1] = ev.S[l] * ev.S[l] / (double)c->primes[l - 1];
+    fides::boot::Ct x;
+    x.c0 = c0;
+    x.c1 = c1;
+    x.level = level;
+    x.scale = scale;
+    auto r = ev.eval_chebyshev_many({x}, std::vector<double>(coeffs, coeffs + n_coeffs), lo, hi, s);
+    const size_t bytes = sizeof(uint64_t) * (size_t)c->N * r[0].level;
+    FIDES_CUDA(cudaMemcpyAsync(out0, r[0].c0, bytes, cudaMemcpyDeviceToDevice, s));
+    FIDES_CUDA(cudaMemcpyAsync(out1, r[0].c1, bytes, cudaMemcpyDeviceToDevice, s));
+    if (out_level) *out_level = r[0].level;
+    if (out_scale) *out_scale = r[0].scale;
+  });
+}
 
 int fides_boot_create(fides_ctx* ctx, const fides_boot_params* p, fides_boot** out) {
   return bguard(__func__, [&] {

@@ -131,6 +131,9 @@ def lib():
         L.fides_ctx_synchronize.argtypes = [vp, vp]
         L.fides_ctx_ntt_chunk.argtypes = [vp, C.c_int]
         L.fides_boot_create.argtypes = [vp, C.POINTER(_BootParams), C.POINTER(vp)]
+        L.fides_eval_chebyshev.argtypes = [vp, vp, C.c_double, vp, vp, C.c_int, C.c_double,
+                                           C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp,
+                                           C.POINTER(C.c_int), C.POINTER(C.c_double), vp]
         L.fides_boot_destroy.argtypes = [vp]
         L.fides_boot_rotations.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
         L.fides_boot_set_keys.argtypes = [vp, vp, vp, vp, vp]
@@ -369,6 +372,21 @@ class Context:
         """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer
         units) or 'tensor' (exact INT8-split product on the tcgen05 tensor cores)."""
         _check(lib().fides_ctx_set_conv_engine(self._h, self.CONV_ENGINES[engine]))
+
+    def eval_chebyshev(self, ct: "Ciphertext", relin_key, top_scale: float, scale: float, coeffs, lo=-1.0,
+                       hi=1.0):
+        """Chebyshev series of ct (fides_eval_chebyshev; OpenFHE's convention c_0 / 2 + sum c_k T_k
+        on [lo, hi]) on the canonical scale chain of top_scale.  ct at its level with scale
+        `scale`.  Returns (Ciphertext at the output level, its scale)."""
+        import numpy as np
+        l = ct.c0.shape[0]
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        o0, o1 = self.empty(l), self.empty(l)
+        lvl, sc = C.c_int(0), C.c_double(0)
+        _check(lib().fides_eval_chebyshev(self._h, _ptr(relin_key), top_scale, _ptr(ct.c0), _ptr(ct.c1), l, scale,
+                                          cf.ctypes.data_as(C.POINTER(C.c_double)), len(cf), lo, hi, _ptr(o0),
+                                          _ptr(o1), C.byref(lvl), C.byref(sc), _stream()))
+        return Ciphertext(o0[:lvl.value], o1[:lvl.value]), sc.value
 
     def set_reduced_noise(self, on: bool):
         """Reduced-noise ModUp/ModDown conversions (reference Parameters::reducedNoise): pre-scaled

@@ -3,7 +3,8 @@
 // api/CryptoContext.cpp:1120-1299 over CudaEngine, api/engine/cuda/CudaEngine.cpp:429-1150):
 // MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
 // real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare,
-// EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, Rescale,
+// EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, EvalChebyshevSeries,
+// Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -226,6 +227,24 @@ class CryptoContextImpl {
   // ciphertext is first brought to the lower of the two levels)
   Ciphertext EvalAdd(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, false); }
   Ciphertext EvalSub(const Ciphertext& a, const Plaintext& p) const { return add_sub_pt(a, p, true); }
+  // EvalChebyshevSeries (CryptoContextImpl::EvalChebyshevSeries): OpenFHE's convention
+  // c_0 / 2 + sum_(k >= 1) c_k T_k on [lo, hi], evaluated on the device (fides_eval_chebyshev)
+  // with the relinearisation key; the result sits at its level's canonical scale S_l,
+  // ceil(log2 d) + 1 levels below the input for degree d (one more for [lo, hi] != [-1, 1]).
+  Ciphertext EvalChebyshevSeries(const Ciphertext& a, const std::vector<double>& coeffs, double lo, double hi) const {
+    a.need_two();
+    if (a.NoiseLevel == 2) return EvalChebyshevSeries(Rescale(a), coeffs, lo, hi);
+    int lvl = 0;
+    double sc = 0;
+    Ciphertext o = fresh(a.getLevel(), 0, 1, a.slots);
+    check(fides_eval_chebyshev(cc_->handle(), cc_->GetEvalKey().device(), S_.back(), a.c0(), a.c1(), a.getLevel(),
+                               a.NoiseFactor, coeffs.data(), (int)coeffs.size(), lo, hi, o.c0(), o.c1(), &lvl, &sc,
+                               cc_->stream()));
+    cc_->synchronize();
+    o.level_ = lvl;  // the first lvl limbs of the buffers
+    o.NoiseFactor = sc;
+    return o;
+  }
   // EvalNegate (CryptoContextImpl::EvalNegate): every component times -1
   Ciphertext EvalNegate(const Ciphertext& a) const {
     const int l = a.getLevel();

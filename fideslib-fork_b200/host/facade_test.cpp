@@ -267,4 +267,33 @@ int facade_more(int logN, int n_q, int K, int dnum, const uint64_t* primes, doub
   }
 }
 
+// EvalChebyshevSeries under FLEXIBLEAUTO on (a0, a1) at l limbs, canonical scale S_l of
+// top_scale: out = the result's c0 then c1 limbs; *out_level / *out_scale its level and scale.
+int facade_chebyshev(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale,
+                     const uint64_t* relin, int l, const uint64_t* a0, const uint64_t* a1, const double* coeffs,
+                     int n_coeffs, double lo, double hi, uint64_t* out, int* out_level, double* out_scale, char* err,
+                     int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    cc.AddEvalKey(key_from(cc, relin));
+    CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+    Ciphertext A(cc, raw_of(a0, a1, l, N, ev.GetScalingFactorReal(l)));
+    Ciphertext R = ev.EvalChebyshevSeries(A, std::vector<double>(coeffs, coeffs + n_coeffs), lo, hi);
+    uint64_t* w = out;
+    put(R, w);
+    *out_level = R.getLevel();
+    *out_scale = R.NoiseFactor;
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

@@ -494,6 +494,20 @@ typedef struct fides_boot_params {
 } fides_boot_params;
 typedef struct fides_boot fides_boot;
 int fides_boot_create(fides_ctx* ctx, const fides_boot_params* params, fides_boot** out);
+/* Chebyshev series of a ciphertext (replaces evalChebyshevSeries, src/CKKS/ApproxModEval.cu:527,
+ * behind CryptoContext::EvalChebyshevSeries, api/CryptoContext.hpp:406): OpenFHE's convention
+ * p(x) = c_0 / 2 + sum_(k >= 1) c_k T_k(t), t = (2 x - (lo + hi)) / (hi - lo), for the n_coeffs
+ * coefficients c.  Evaluated by Paterson-Stockmeyer in the Chebyshev basis (the bootstrapper's
+ * EvalMod evaluator) with the relinearisation key, on the scale chain S_L = top_scale,
+ * S_(l-1) = S_l^2 / q_(l-1).  The input (c0, c1) at `level` limbs and `scale` (brought to the
+ * canonical S_level one level down if it differs); the result goes to out0 / out1 (room for
+ * `level` limbs each) at *out_level = level - ceil(log2 d) - 1 limbs for degree d (one fewer
+ * when [lo, hi] != [-1, 1], one fewer again for a non-canonical input scale), at scale
+ * *out_scale (that level's canonical scale). */
+int fides_eval_chebyshev(fides_ctx* ctx, const uint64_t* relin_key, double top_scale, const uint64_t* c0,
+                         const uint64_t* c1, int level, double scale, const double* coeffs, int n_coeffs, double lo,
+                         double hi, uint64_t* out0, uint64_t* out1, int* out_level, double* out_scale,
+                         void* stream);
 int fides_boot_destroy(fides_boot* b);
 /* Rotation amounts (slots, in [1, N/2)) whose keys the linear transforms use: writes up to cap
  * of them and returns the count (EvalBootstrapKeyGen's rotation list). */

@@ -4,7 +4,7 @@
 // MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
 // real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare,
 // EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, EvalChebyshevSeries,
-// Rescale,
+// MultByMonomial, Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -243,6 +243,27 @@ class CryptoContextImpl {
     cc_->synchronize();
     o.level_ = lvl;  // the first lvl limbs of the buffers
     o.NoiseFactor = sc;
+    return o;
+  }
+  // MultByMonomial (CryptoContextImpl::MultByMonomial): every component times X^power in
+  // Z_q[X]/(X^N + 1) (X^N = -1, so power is taken modulo 2N); level, scale and degree unchanged.
+  // The monomial's limbs are transformed on the device and multiplied in, one product per limb.
+  Ciphertext MultByMonomial(const Ciphertext& a, uint32_t power) const {
+    const int l = a.getLevel(), n = N();
+    power %= 2u * (uint32_t)n;
+    const bool neg = power >= (uint32_t)n;
+    std::vector<uint64_t> host((size_t)l * n, 0);
+    for (int i = 0; i < l; ++i) host[(size_t)i * n + power % n] = neg ? q(i) - 1 : 1;
+    DeviceLimbs mono((size_t)l * n);
+    check_cuda(cudaMemcpyAsync(mono.get(), host.data(), sizeof(uint64_t) * host.size(), cudaMemcpyHostToDevice,
+                               cc_->stream()),
+               "H2D");
+    check(fides_ntt_polys(cc_->handle(), mono.get(), 1, l, 0, cc_->stream()));
+    Ciphertext o = copy_of(a, l);
+    check(fides_mul(cc_->handle(), a.c0(), mono.get(), l, o.c0(), cc_->stream()));
+    check(fides_mul(cc_->handle(), a.c1(), mono.get(), l, o.c1(), cc_->stream()));
+    if (a.hasC2()) check(fides_mul(cc_->handle(), a.c2(), mono.get(), l, o.c2(), cc_->stream()));
+    cc_->synchronize();  // the host and device monomials are released at scope exit
     return o;
   }
   // EvalNegate (CryptoContextImpl::EvalNegate): every component times -1

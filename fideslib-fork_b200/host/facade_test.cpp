@@ -214,7 +214,7 @@ int facade_plain(int logN, int n_q, int K, int dnum, const uint64_t* primes, dou
 //   FIXEDMANUAL Relinearize(EvalMultNoRelin(a, b)) [l] |
 //   FIXEDMANUAL Relinearize(EvalAdd(EvalMultNoRelin(a, b), EvalMultNoRelin(a, a))) [l] |
 //   FLEXIBLEAUTO Rescale(Relinearize(EvalMultNoRelin(a, b))) [l-1] | EvalNegate(a) [l] |
-//   EvalAddMany({a, b, a}) [l] | EvalRotateMany({a, b}, rot) [l] [l]
+//   EvalAddMany({a, b, a}) [l] | EvalRotateMany({a, b}, rot) [l] [l] | MultByMonomial(a, N + 5) [l]
 int facade_more(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, const uint64_t* relin,
                 int rot, const uint64_t* rot_key, int l, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
                 const uint64_t* b1, uint64_t* out, char* err, int err_len) {
@@ -259,6 +259,7 @@ int facade_more(int logN, int n_q, int K, int dnum, const uint64_t* primes, doub
       auto rs = ev.EvalRotateMany({&A, &B}, rot);
       put(rs.at(0), w);
       put(rs.at(1), w);
+      put(ev.MultByMonomial(A, (uint32_t)N + 5), w);
     }
     return 0;
   } catch (const std::exception& e) {

@@ -841,9 +841,9 @@ def test_cpp_facade_plaintexts(fides, n_slots):
 @pytest.mark.gpu
 def test_cpp_facade_norelin_and_many(fides):
     """The C++ facade's EvalMultNoRelin + Relinearize (three-component ciphertexts; a lazily
-    relinearised sum of two products), EvalNegate, EvalAddMany and EvalRotateMany (one batched
-    launch sequence) against the oracle residue for residue, and the FLEXIBLEAUTO
-    Rescale(Relinearize(EvalMultNoRelin)) against the fused product."""
+    relinearised sum of two products), EvalNegate, EvalAddMany, EvalRotateMany (one batched
+    launch sequence) and MultByMonomial against the oracle residue for residue, and the
+    FLEXIBLEAUTO Rescale(Relinearize(EvalMultNoRelin)) against the fused product."""
     import ctypes as C
     from fides_b200 import params as P
     F = fides
@@ -857,7 +857,7 @@ def test_cpp_facade_norelin_and_many(fides):
     rng = xrng(90)
     a = [uniform_limbs(rng, q, N) for _ in range(2)]
     b = [uniform_limbs(rng, q, N) for _ in range(2)]
-    sizes = [l, l, l - 1, l, l, l, l]
+    sizes = [l, l, l - 1, l, l, l, l, l]
     out = np.zeros(2 * sum(sizes) * N, dtype=np.uint64)
     err = C.create_string_buffer(512)
     u64 = lambda x: np.ascontiguousarray(x, dtype=np.uint64).ctypes.data_as(C.POINTER(C.c_uint64))
@@ -875,14 +875,20 @@ def test_cpp_facade_norelin_and_many(fides):
     s0, s1, s2 = o.add(x0, y0, ids), o.add(x1, y1, ids), o.add(x2, y2, ids)
     f0, f1 = o.keyswitch(s2, rk)
     neg = [o.sub(np.zeros_like(a[i]), a[i], ids) for i in range(2)]
+    # X^(N + 5) = -X^5: its limbs in EVALUATION form (the oracle's NTT of the coefficient vector)
+    mono = np.zeros((l, N), dtype=np.uint64)
+    for i in range(l):
+        mono[i, 5] = q[i] - 1
+    mono = o.ntt(mono, ids)
     want = [o.hmult(a[0], a[1], b[0], b[1], rk, rescale=False),
             (o.add(s0, f0, ids), o.add(s1, f1, ids)),
             o.hmult(a[0], a[1], b[0], b[1], rk, rescale=True),
             (neg[0], neg[1]),
             (o.add(o.add(a[0], b[0], ids), a[0], ids), o.add(o.add(a[1], b[1], ids), a[1], ids)),
             o.rotate(a[0], a[1], kr, rot),
-            o.rotate(b[0], b[1], kr, rot)]
+            o.rotate(b[0], b[1], kr, rot),
+            (o.mul(a[0], mono, ids), o.mul(a[1], mono, ids))]
     names = ["Relinearize(EvalMultNoRelin)", "lazy relinearisation of a sum", "FLEXIBLEAUTO NoRelin+Relinearize+Rescale",
-             "EvalNegate", "EvalAddMany", "EvalRotateMany[0]", "EvalRotateMany[1]"]
+             "EvalNegate", "EvalAddMany", "EvalRotateMany[0]", "EvalRotateMany[1]", "MultByMonomial"]
     for name, (g0, g1), (w0, w1) in zip(names, got, want):
         assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name

@@ -688,6 +688,37 @@ int fides_rotate_hoisted(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, i
   });
 }
 
+int fides_accumulate_rotations(int radix, int stride, int size, int* indices, int cap) {
+  if (radix < 2 || (radix & (radix - 1)) || stride < 1 || size < 1 || (cap > 0 && !indices)) return FIDES_ERR_ARG;
+  int n = 0;
+  for (long t = 1; t < size; t *= radix)
+    for (int k = 1; k < radix && (long)stride * t * k < (long)stride * size; ++k) {
+      if (n < cap) indices[n] = (int)(stride * t * k);
+      ++n;
+    }
+  return n;
+}
+
+int fides_accumulate(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, int level, int radix, int stride, int size,
+                     const int* key_rotations, const uint64_t* const* keys, int n_keys, uint64_t* out0,
+                     uint64_t* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(c0, "c0");
+    need(c1, "c1");
+    need(out0, "out0");
+    need(out1, "out1");
+    if (n_keys < 0 || (n_keys > 0 && (!key_rotations || !keys))) throw fides::Error(FIDES_ERR_ARG, "bad key table");
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    std::vector<std::pair<int, const uint64_t*>> kt;
+    for (int i = 0; i < n_keys; ++i) {
+      need(keys[i], "key");
+      kt.push_back({key_rotations[i], keys[i]});
+    }
+    fides::op_accumulate(c, c0, c1, level, radix, stride, size, kt, out0, out1, S(stream));
+  });
+}
+
 int fides_rotate_hoisted_digits(fides_ctx* x, const uint64_t* c0, const uint64_t* digits, int level,
                                 const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
                                 uint64_t* const* out1, void* stream) {

@@ -580,6 +580,95 @@ void op_moddown_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t
   moddown_stage(c, exts, ls, conv.data(), outs, nullptr, n, s);
 }
 
+// Rotation sum (reference Accumulate, src/CKKS/AccumulateBroadcast.cu:122-160, behind
+// CryptoContext::AccumulateSum): rounds t = 1, radix, radix^2, ... < size; round t rotates the
+// running value by stride t k (k = 1 .. radix - 1, while below stride size) as hoisted rotations
+// left in the extended basis and adds them.  As in the reference, c0 stays in the extended basis
+// (P c0 plus the rotations' extended c0 parts, each rotation adding the running extended c0
+// instead of P c0) until one ModDown at the end, while c1 (P c1 + the rotations' c1 parts) is
+// brought back by a ModDown every round, because the next round's ModUp reads it.
+void op_accumulate(Context* c, const uint64_t* c0, const uint64_t* c1, int l, int radix, int stride, int size,
+                   const std::vector<std::pair<int, const uint64_t*>>& keys, uint64_t* out0, uint64_t* out1,
+                   cudaStream_t s) {
+  check_level(c, l);
+  if (radix < 2 || (radix & (radix - 1))) throw Error(-1, "accumulate: radix must be a power of two >= 2");
+  if (stride < 1 || size < 1 || (long)stride * size > c->N / 2) throw Error(-1, "accumulate: stride / size out of range");
+  const int K = c->K, ext = l + K;
+  if (K < 1) throw Error(-1, "accumulate: needs special primes");
+  if (ext > MAX_LC_LIMBS || radix > MAX_LC_TERMS) throw Error(-1, "accumulate: too many limbs or terms");
+  const size_t N = c->N, lb = sizeof(uint64_t) * N;
+  if (out0 != c0) FIDES_CUDA(cudaMemcpyAsync(out0, c0, lb * l, cudaMemcpyDeviceToDevice, s));
+  if (out1 != c1) FIDES_CUDA(cudaMemcpyAsync(out1, c1, lb * l, cudaMemcpyDeviceToDevice, s));
+  if (size <= 1) return;
+  auto key_of = [&](int r) {
+    for (const auto& kv : keys)
+      if (kv.first == r) return kv.second;
+    throw Error(-5, "accumulate: no key for rotation " + std::to_string(r));
+  };
+  // P mod each limb's prime (0 on the special limbs)
+  std::vector<uint64_t> pm(ext, 0);
+  for (int j = 0; j < l; ++j) {
+    uint64_t v = 1;
+    for (int k = 0; k < K; ++k) v = h_mulmod(v, c->primes[c->n_q + k] % c->primes[j], c->primes[j]);
+    pm[j] = v;
+  }
+  // extended buffers: x0e (running c0), x1e (P c1 operand), a1 (c1 sum), radix - 1 rotation pairs
+  Scratch sc(c, lb * ext * (3 + 2 * (size_t)(radix - 1)), s);
+  Bump bp{sc.u64(), N};
+  uint64_t *x0e = bp.take(ext), *x1e = bp.take(ext), *a1 = bp.take(ext);
+  std::vector<uint64_t*> r0(radix - 1), r1(radix - 1);
+  for (int k = 0; k < radix - 1; ++k) r0[k] = bp.take(ext), r1[k] = bp.take(ext);
+  static thread_local LinCombJob j;
+  auto combine = [&](const uint64_t* first, const uint64_t* first_scale, int m, uint64_t* const* parts,
+                     uint64_t* out) {  // out = first (times first_scale per limb, or 1) + sum parts
+    j.n = m + 1;
+    j.l = ext;
+    j.lanes = 1;
+    j.lq = l;
+    j.nq = c->n_q;
+    for (int i = 0; i < ext; ++i) {
+      j.s[0][i] = first_scale ? first_scale[i] : 1;
+      j.add0[i] = 0;
+    }
+    j.x0[0][0] = j.x1[0][0] = first;
+    for (int t = 0; t < m; ++t) {
+      for (int i = 0; i < ext; ++i) j.s[t + 1][i] = 1;
+      j.x0[0][t + 1] = j.x1[0][t + 1] = parts[t];
+    }
+    j.out0[0] = j.out1[0] = out;  // one polynomial per lane: both halves name the same buffers
+    launch_lincomb(c, j, s);
+  };
+  // x0e = P c0 (its special limbs are zero)
+  FIDES_CUDA(cudaMemcpyAsync(x1e, c0, lb * l, cudaMemcpyDeviceToDevice, s));
+  FIDES_CUDA(cudaMemsetAsync(x1e + (size_t)l * N, 0, lb * K, s));
+  combine(x1e, pm.data(), 0, nullptr, x0e);
+  for (long t = 1; t < size; t *= radix) {
+    HoistItem it;
+    it.c0 = nullptr;
+    it.c1 = out1;
+    it.l = l;
+    it.c0x = x0e;
+    for (int k = 1; k < radix && (long)stride * t * k < (long)stride * size; ++k) {
+      const int r = (int)(stride * t * k);
+      it.keys.push_back(key_of(r));
+      it.ks.push_back(h_auto_index(c->logN, r));
+      it.out0.push_back(r0[k - 1]);
+      it.out1.push_back(r1[k - 1]);
+    }
+    const int m = (int)it.ks.size();
+    op_hoisted_ext_batch(c, &it, 1, s);
+    combine(x0e, nullptr, m, r0.data(), a1);  // the extended c0 sum, then back into x0e
+    FIDES_CUDA(cudaMemcpyAsync(x0e, a1, lb * ext, cudaMemcpyDeviceToDevice, s));
+    FIDES_CUDA(cudaMemcpyAsync(x1e, out1, lb * l, cudaMemcpyDeviceToDevice, s));
+    FIDES_CUDA(cudaMemsetAsync(x1e + (size_t)l * N, 0, lb * K, s));
+    combine(x1e, pm.data(), m, r1.data(), a1);  // P c1 + the rotations' c1 parts
+    int lv = l;
+    op_moddown_batch(c, &a1, &lv, &out1, 1, s);
+  }
+  int lv = l;
+  op_moddown_batch(c, &x0e, &lv, &out0, 1, s);
+}
+
 void op_moddown_rescale_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n,
                               cudaStream_t s) {
   if (n <= 0) return;

@@ -86,6 +86,11 @@ void op_hoisted_ext_batch(Context* c, const HoistItem* items, int n_items, cudaS
 // ModDown of n extended-basis polynomials exts[i] (l_i + K limbs; their special limbs are
 // transformed in place) into outs[i] (l_i limbs), EVAL in and out.
 void op_moddown_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n, cudaStream_t s);
+// Rotation sum x + sum of its rotations by stride t k over rounds t = 1, radix, radix^2, ... <
+// size (reference Accumulate); keys = (rotation index, device key) pairs.
+void op_accumulate(Context* c, const uint64_t* c0, const uint64_t* c1, int l, int radix, int stride, int size,
+                   const std::vector<std::pair<int, const uint64_t*>>& keys, uint64_t* out0, uint64_t* out1,
+                   cudaStream_t s);
 // ModDown followed by the rescale by q_(l_i - 1), fused (outs[i]: l_i - 1 limbs).
 void op_moddown_rescale_batch(Context* c, uint64_t* const* exts, const int* ls, uint64_t* const* outs, int n,
                               cudaStream_t s);

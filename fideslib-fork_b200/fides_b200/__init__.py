@@ -131,6 +131,9 @@ def lib():
         L.fides_ctx_synchronize.argtypes = [vp, vp]
         L.fides_ctx_ntt_chunk.argtypes = [vp, C.c_int]
         L.fides_boot_create.argtypes = [vp, C.POINTER(_BootParams), C.POINTER(vp)]
+        L.fides_accumulate.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(vp), C.c_int, vp, vp, vp]
+        L.fides_accumulate_rotations.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int]
         L.fides_eval_chebyshev.argtypes = [vp, vp, C.c_double, vp, vp, C.c_int, C.c_double,
                                            C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp,
                                            C.POINTER(C.c_int), C.POINTER(C.c_double), vp]
@@ -372,6 +375,28 @@ class Context:
         """Basis-conversion engine for ModUp/ModDown: 'auto', 'simt' (64-bit integer
         units) or 'tensor' (exact INT8-split product on the tcgen05 tensor cores)."""
         _check(lib().fides_ctx_set_conv_engine(self._h, self.CONV_ENGINES[engine]))
+
+    @staticmethod
+    def accumulate_rotations(radix: int, stride: int, size: int) -> list:
+        """Rotation indices accumulate() needs (fides_accumulate_rotations)."""
+        n = lib().fides_accumulate_rotations(radix, stride, size, None, 0)
+        if n < 0:
+            _check(n)
+        out = (C.c_int * max(1, n))()
+        lib().fides_accumulate_rotations(radix, stride, size, out, n)
+        return list(out[:n])
+
+    def accumulate(self, ct: "Ciphertext", radix: int, stride: int, size: int, keys: dict) -> "Ciphertext":
+        """Rotation sum (fides_accumulate, the reference's AccumulateSum): slot i gathers
+        slots i + j stride, j < size.  keys: rotation index -> device key."""
+        l = ct.c0.shape[0]
+        rots = list(keys)
+        kr = (C.c_int * max(1, len(rots)))(*rots)
+        kp = (vp * max(1, len(rots)))(*[_ptr(keys[r]) for r in rots])
+        o0, o1 = self.empty(l), self.empty(l)
+        _check(lib().fides_accumulate(self._h, _ptr(ct.c0), _ptr(ct.c1), l, radix, stride, size, kr, kp, len(rots),
+                                      _ptr(o0), _ptr(o1), _stream()))
+        return Ciphertext(o0, o1)
 
     def eval_chebyshev(self, ct: "Ciphertext", relin_key, top_scale: float, scale: float, coeffs, lo=-1.0,
                        hi=1.0):

@@ -4,7 +4,7 @@
 // MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
 // real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare,
 // EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, EvalChebyshevSeries,
-// MultByMonomial, Rescale,
+// MultByMonomial, AccumulateSum, Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -243,6 +243,23 @@ class CryptoContextImpl {
     cc_->synchronize();
     o.level_ = lvl;  // the first lvl limbs of the buffers
     o.NoiseFactor = sc;
+    return o;
+  }
+  // AccumulateSum (CryptoContextImpl::AccumulateSum, CudaEngine::accumulateSum): slot i gathers
+  // slots i + j stride, j < slots, by rounds of hoisted rotations summed in the extended basis
+  // (fides_accumulate, radix 4 as the reference's default PARTIAL_SUM_RADIX); the rotation keys
+  // of fides_accumulate_rotations must be registered.  Level and scale unchanged.
+  Ciphertext AccumulateSum(const Ciphertext& a, int slots, int stride = 1, int radix = 4) const {
+    a.need_two();
+    const int n = fides_accumulate_rotations(radix, stride, slots, nullptr, 0);
+    if (n < 0) throw Error(n, "AccumulateSum: bad radix, stride or slot count");
+    std::vector<int> rots(n);
+    fides_accumulate_rotations(radix, stride, slots, rots.data(), n);
+    std::vector<const uint64_t*> keys;
+    for (int r : rots) keys.push_back(cc_->GetRotationKey(r).device());
+    Ciphertext o = fresh(a.getLevel(), a.NoiseFactor, a.NoiseLevel, a.slots);
+    check(fides_accumulate(cc_->handle(), a.c0(), a.c1(), a.getLevel(), radix, stride, slots, rots.data(),
+                           keys.data(), n, o.c0(), o.c1(), cc_->stream()));
     return o;
   }
   // MultByMonomial (CryptoContextImpl::MultByMonomial): every component times X^power in

@@ -297,4 +297,29 @@ int facade_chebyshev(int logN, int n_q, int K, int dnum, const uint64_t* primes,
   }
 }
 
+// AccumulateSum(a, size, stride) under FLEXIBLEAUTO with the rotation keys (rots[i], keys[i]):
+// out = the result's c0 then c1 limbs (l each).
+int facade_accumulate(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, int n_keys,
+                      const int* rots, const uint64_t* const* keys, int l, const uint64_t* a0, const uint64_t* a1,
+                      int size, int stride, uint64_t* out, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    for (int i = 0; i < n_keys; ++i) cc.AddRotationKey(rots[i], key_from(cc, keys[i]));
+    CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+    Ciphertext A(cc, raw_of(a0, a1, l, N, ev.GetScalingFactorReal(l)));
+    uint64_t* w = out;
+    put(ev.AccumulateSum(A, size, stride), w);
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

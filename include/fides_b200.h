@@ -252,6 +252,21 @@ int fides_rotate_auto(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, in
 int fides_rotate_hoisted(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                          const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
                          uint64_t* const* out1, void* stream);
+/* Rotation sum (replaces Accumulate, src/CKKS/AccumulateBroadcast.cu:122-160, behind
+ * CryptoContext::AccumulateSum, api/CryptoContext.hpp:456): x + sum of its rotations by
+ * stride t k for rounds t = 1, radix, radix^2, ... < size and k = 1 .. radix - 1 (while
+ * stride t k < stride size), i.e. slot i gathers slots i + j stride, j < size.  Each round's
+ * rotations are hoisted and summed in the extended basis; as in the reference, c0 stays there
+ * until one ModDown at the end and c1 is brought back every round.  radix: a power of two >= 2
+ * (the reference's PARTIAL_SUM_RADIX, 4 by default); keys: one device rotation key per index of
+ * fides_accumulate_rotations, key_rotations[i] naming the rotation of keys[i].  out0 / out1 may
+ * alias c0 / c1. */
+int fides_accumulate(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, int radix, int stride,
+                     int size, const int* key_rotations, const uint64_t* const* keys, int n_keys, uint64_t* out0,
+                     uint64_t* out1, void* stream);
+/* The rotation indices fides_accumulate needs (reference GetAccumulateRotationIndices): writes up
+ * to cap of them and returns their count (negative status for bad arguments). */
+int fides_accumulate_rotations(int radix, int stride, int size, int* indices, int cap);
 /* Hoisted rotations from a ModUp computed earlier: digits = fides_modup(c1) ([beta][level+K][N]),
  * reused for any number of calls.  The reference's EvalFastRotationPrecompute (the ModUp) and
  * EvalFastRotation (KSK with P c0, automorphism, ModDown), CudaEngine.cpp:536-585 over

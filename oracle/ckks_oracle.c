@@ -694,6 +694,85 @@ void or_rotate_auto(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int
   free(digits);
 }
 
+/* Rotation sum, reference src/CKKS/AccumulateBroadcast.cu:122-160 (Accumulate) over the hoisted
+ * rotations left in the extended basis (Ciphertext.cpp:1221-1300 with ext): rounds t = 1, radix,
+ * radix^2, ... < size rotate the running value by stride t k (k < radix, stride t k < stride
+ * size).  Each rotation's c0 part is automorph(B_k + x0e), x0e the running extended c0 (P c0
+ * before the first round), its c1 part automorph(A_k); x0e gains the c0 parts (ModDown once at
+ * the end), P c1 + the c1 parts is brought down every round. */
+static const uint64_t* key_for(const int* key_rot, const uint64_t* const* keys, int n_keys, int r) {
+  for (int i = 0; i < n_keys; ++i)
+    if (key_rot[i] == r) return keys[i];
+  return NULL;
+}
+
+int or_accumulate(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int l, int radix, int stride, int size,
+                  const int* key_rot, const uint64_t* const* keys, int n_keys, uint64_t* out0, uint64_t* out1) {
+  const size_t N = (size_t)c->N;
+  const int K = c->n_p, ext = l + K, beta = or_num_digits(c, l);
+  if (radix < 2 || (radix & (radix - 1)) || stride < 1 || size < 1) return -1;
+  for (long t = 1; t < size; t *= radix)  /* every key first: -2 when one is missing */
+    for (int k = 1; k < radix && (long)stride * t * k < (long)stride * size; ++k)
+      if (!key_for(key_rot, keys, n_keys, (int)(stride * t * k))) return -2;
+  memcpy(out0, c0, sizeof(uint64_t) * l * N);
+  memcpy(out1, c1, sizeof(uint64_t) * l * N);
+  if (size <= 1) return 0;
+  uint64_t* pm = (uint64_t*)malloc(sizeof(uint64_t) * ext);
+  int* pid = (int*)malloc(sizeof(int) * ext);
+  for (int j = 0; j < ext; ++j) {
+    pid[j] = j < l ? j : c->n_q + (j - l);
+    uint64_t q = c->primes[pid[j]], P = 1;
+    for (int k = 0; k < K; ++k) P = or_mulmod(P, c->primes[c->n_q + k] % q, q);
+    pm[j] = j < l ? P : 0;
+  }
+  uint64_t* x0e = (uint64_t*)calloc((size_t)ext * N, sizeof(uint64_t));
+  uint64_t* s0 = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* s1 = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* A = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* B = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* As = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* Bs = (uint64_t*)malloc(sizeof(uint64_t) * ext * N);
+  uint64_t* digits = (uint64_t*)malloc(sizeof(uint64_t) * beta * ext * N);
+  for (int j = 0; j < l; ++j)
+    for (size_t n = 0; n < N; ++n) x0e[j * N + n] = or_mulmod(c0[j * N + n], pm[j], c->primes[pid[j]]);
+  for (long t = 1; t < size; t *= radix) {
+    or_modup(c, out1, l, digits);
+    memcpy(s0, x0e, sizeof(uint64_t) * ext * N);
+    memset(s1, 0, sizeof(uint64_t) * ext * N);
+    for (int j = 0; j < l; ++j)
+      for (size_t n = 0; n < N; ++n) s1[j * N + n] = or_mulmod(out1[j * N + n], pm[j], c->primes[pid[j]]);
+    for (int k = 1; k < radix && (long)stride * t * k < (long)stride * size; ++k) {
+      const int r = (int)(stride * t * k);
+      or_ksk_ip(c, digits, l, key_for(key_rot, keys, n_keys, r), A, B);
+      for (int j = 0; j < ext; ++j)
+        for (size_t n = 0; n < N; ++n) B[j * N + n] = addmod(B[j * N + n], x0e[j * N + n], c->primes[pid[j]]);
+      const uint32_t ka = or_rotation_auto_index(c->logN, r);
+      or_automorph(c, A, As, ext, ka);
+      or_automorph(c, B, Bs, ext, ka);
+      for (int j = 0; j < ext; ++j)
+        for (size_t n = 0; n < N; ++n) {
+          const uint64_t q = c->primes[pid[j]];
+          s0[j * N + n] = addmod(s0[j * N + n], Bs[j * N + n], q);
+          s1[j * N + n] = addmod(s1[j * N + n], As[j * N + n], q);
+        }
+    }
+    memcpy(x0e, s0, sizeof(uint64_t) * ext * N);
+    or_moddown(c, s1, l, out1);
+  }
+  or_moddown(c, x0e, l, out0);
+  free(pm);
+  free(pid);
+  free(x0e);
+  free(s0);
+  free(s1);
+  free(A);
+  free(B);
+  free(As);
+  free(Bs);
+  free(digits);
+  return 0;
+}
+
 /* Hoisted rotations: reference src/CKKS/Ciphertext.cpp:1221-1394 (one ModUp, one fused
  * KSK/automorph pass over all indices, ModDown per result). */
 void or_rotate_hoisted(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int l, const uint64_t* const* keys,

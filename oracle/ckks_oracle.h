@@ -95,6 +95,9 @@ void or_hmult(const or_ctx* c, const uint64_t* a0, const uint64_t* a1, const uin
 void or_rotate_auto(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int l, const uint64_t* key, uint32_t k,
                     uint64_t* out0, uint64_t* out1);
 /* Hoisted rotations: one ModUp of c1, n automorphism indices / keys. */
+/* Rotation sum (reference Accumulate): see ckks_oracle.c. */
+int or_accumulate(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int l, int radix, int stride, int size,
+                  const int* key_rot, const uint64_t* const* keys, int n_keys, uint64_t* out0, uint64_t* out1);
 void or_rotate_hoisted(const or_ctx* c, const uint64_t* c0, const uint64_t* c1, int l, const uint64_t* const* keys,
                        const uint32_t* ks, int n, uint64_t* const* out0, uint64_t* const* out1);
 

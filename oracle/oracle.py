@@ -74,6 +74,8 @@ def lib():
         L.or_switch_modulus.argtypes = [C.c_void_p, u64p, C.c_int, C.c_int, C.c_int, u64p]
         L.or_hmult.argtypes = [C.c_void_p, u64p, u64p, u64p, u64p, C.c_int, u64p, C.c_int, u64p, u64p]
         L.or_rotate_auto.argtypes = [C.c_void_p, u64p, u64p, C.c_int, u64p, C.c_uint32, u64p, u64p]
+        L.or_accumulate.argtypes = [C.c_void_p, u64p, u64p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(C.c_int), C.POINTER(u64p), C.c_int, u64p, u64p]
         L.or_rotate_hoisted.argtypes = [C.c_void_p, u64p, u64p, C.c_int, C.POINTER(u64p), C.POINTER(C.c_uint32),
                                         C.c_int, C.POINTER(u64p), C.POINTER(u64p)]
         _lib = L
@@ -262,6 +264,20 @@ class Oracle:
 
     def rotate(self, c0, c1, key, r: int):
         return self.rotate_auto(c0, c1, key, self.auto_index(r))
+
+    def accumulate(self, c0, c1, radix: int, stride: int, size: int, keys: dict):
+        """Rotation sum (reference Accumulate); keys: rotation index -> switching key."""
+        l = c0.shape[0]
+        rots = list(keys)
+        karr = [np.ascontiguousarray(keys[r], dtype=np.uint64) for r in rots]
+        kp = (u64p * max(1, len(rots)))(*[_p(k) for k in karr])
+        kr = (C.c_int * max(1, len(rots)))(*rots)
+        o0, o1 = self._new(l), self._new(l)
+        rc = lib().or_accumulate(self._h, _p(np.ascontiguousarray(c0)), _p(np.ascontiguousarray(c1)), l, radix, stride,
+                                 size, kr, kp, len(rots), _p(o0), _p(o1))
+        if rc:
+            raise ValueError(f"or_accumulate: bad arguments or a missing key ({rc})")
+        return o0, o1
 
     def rotate_hoisted(self, c0, c1, keys, rs):
         l, n = c0.shape[0], len(rs)

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -60,6 +61,8 @@ class CryptoContextImpl {
   ScalingTechnique tech_;
   std::vector<double> S_;  // canonical scale of each level (FLEXIBLEAUTO)
   fides_boot* boot_ = nullptr;
+  fides_boot_params boot_params_{};
+  std::map<int, fides_boot*> short_boot_;  // EvalBootstrapToLevel: bootstrappers on shorter chains
   double boot_msg_scale_ = 0;
   bool boot_double_hoist_ = true;
   std::unique_ptr<KeySwitchingKey> to_sparse_, to_dense_;
@@ -157,6 +160,7 @@ class CryptoContextImpl {
     for (int l = L; l > 1; --l) S_[l - 1] = S_[l] * S_[l] / (double)cc.primes[l - 1];
   }
   ~CryptoContextImpl() {
+    drop_short_boots();
     if (boot_) fides_boot_destroy(boot_);
   }
   CryptoContextImpl(const CryptoContextImpl&) = delete;
@@ -475,12 +479,14 @@ class CryptoContextImpl {
     if (numSlots != 0 && (int)numSlots != N() / 2)
       throw Error(FIDES_ERR_ARG, "bootstrapping supports full packing (N/2 slots) only");
     if (levelBudget.size() != 2) throw Error(FIDES_ERR_ARG, "levelBudget = {CoeffsToSlots, SlotsToCoeffs}");
+    drop_short_boots();
     if (boot_) fides_boot_destroy(boot_), boot_ = nullptr;
     boot_msg_scale_ = msgScale > 0 ? msgScale : S_[1];
     fides_boot_params p{(int)levelBudget[0], (int)levelBudget[1], cc_->L, S_[cc_->L], boot_msg_scale_, 12, 3, 31,
                         dim1.empty() || dim1[0] == 0 ? 8 : (int)dim1[0], (int)correctionFactor,
                         to_sparse_ && to_dense_ ? 1 : 0, 0, boot_double_hoist_ ? 1 : 0};
     check(fides_boot_create(cc_->handle(), &p, &boot_));
+    boot_params_ = p;
   }
   // Double-hoisted linear transforms in the bootstrap (fides_boot_params::double_hoist; on by
   // default, about 8-10 % faster).  Set before EvalBootstrapSetup; off gives the single-hoisted
@@ -520,6 +526,48 @@ class CryptoContextImpl {
     cc_->synchronize();
     return o;
   }
+  // EvalBootstrapToLevel (CryptoContextImpl::EvalBootstrapToLevel): the refreshed ciphertext at
+  // `outputLevel` consumed towers (OpenFHE's level: L minus the limbs kept), or at EvalBootstrap's
+  // own level when that consumes at least as many.  A deeper request runs the same circuit on a
+  // chain cut short at the top (ModRaise to fewer limbs), so every step moves fewer limbs; that
+  // bootstrapper is built and prepared with the same parameters and keys on first use of each
+  // depth and kept.  Precision is the bootstrap's own: the scales of the shorter chain are the
+  // canonical ones of its levels.
+  Ciphertext EvalBootstrapToLevel(const Ciphertext& a, uint32_t outputLevel) {
+    a.need_two();
+    if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
+    int lo = 0;
+    double sc = 0;
+    check(fides_boot_levels(boot_, &lo, &sc));
+    const int L = cc_->L, consumed = L - lo;
+    if ((int)outputLevel <= consumed) return EvalBootstrap(a);
+    if ((int)outputLevel >= L) throw Error(FIDES_ERR_LEVEL, "the output level leaves no limb");
+    const int top = L - ((int)outputLevel - consumed);
+    fides_boot*& b = short_boot_[top];
+    if (!b) {
+      fides_boot_params p = boot_params_;
+      p.top_level = top;  // top_scale stays the chain's S_L: the bootstrapper indexes scales by level
+      try {
+        check(fides_boot_create(cc_->handle(), &p, &b));
+        check(fides_boot_set_keys(b, cc_->GetEvalKey().device(), cc_->GetRotationKey(2 * N() - 1).device(),
+                                  to_sparse_ ? to_sparse_->device() : nullptr,
+                                  to_dense_ ? to_dense_->device() : nullptr));
+        std::vector<int> r(fides_boot_rotations(b, nullptr, 0));
+        fides_boot_rotations(b, r.data(), (int)r.size());
+        for (int x : r) check(fides_boot_set_rotation_key(b, x, cc_->GetRotationKey(x).device()));
+        check(fides_boot_prepare(b, cc_->stream()));
+      } catch (...) {
+        if (b) fides_boot_destroy(b);
+        short_boot_.erase(top);
+        throw;
+      }
+    }
+    check(fides_boot_levels(b, &lo, &sc));
+    Ciphertext o = fresh(lo, sc, 1, a.slots);
+    check(fides_bootstrap(b, a.c0(), a.c1(), o.c0(), o.c1(), cc_->stream()));
+    cc_->synchronize();
+    return o;
+  }
   // Several inputs bootstrapped concurrently (one stream each); results equal EvalBootstrap's.
   std::vector<Ciphertext> EvalBootstrap(const std::vector<const Ciphertext*>& in) const {
     if (!boot_) throw Error(FIDES_ERR_STATE, "EvalBootstrapSetup first");
@@ -544,6 +592,11 @@ class CryptoContextImpl {
   }
 
  private:
+  void drop_short_boots() {
+    for (auto& kv : short_boot_)
+      if (kv.second) fides_boot_destroy(kv.second);
+    short_boot_.clear();
+  }
   Ciphertext add_sub(const Ciphertext& a, const Ciphertext& b, bool sub) const {
     if (tech_ == FLEXIBLEAUTO && (a.NoiseLevel == 2 || b.NoiseLevel == 2) &&
         !(a.NoiseLevel == 2 && b.NoiseLevel == 2 && a.getLevel() == b.getLevel())) {

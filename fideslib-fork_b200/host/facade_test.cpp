@@ -96,6 +96,53 @@ int facade_bootstrap(int logN, int n_q, int K, int dnum, const uint64_t* primes,
   }
 }
 
+// EvalBootstrap and EvalBootstrapToLevel of one level-1 ciphertext (setup as facade_bootstrap,
+// dense secret, no encapsulation): out_d0/1 = EvalBootstrap [*lvl_d limbs], out_s0/1 =
+// EvalBootstrapToLevel(consumed, the default's consumed towers) [same], out_t0/1 =
+// EvalBootstrapToLevel(consumed + extra) [*lvl_t limbs]; *sc_t its scale.
+int facade_bootstrap_to_level(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale,
+                              const uint64_t* relin, const uint64_t* conj, int n_rot, const int* rots,
+                              const uint64_t* const* rot_keys, double msg_scale, int prescale_bits, int extra,
+                              const uint64_t* c0, const uint64_t* c1, uint64_t* out_d0, uint64_t* out_d1,
+                              uint64_t* out_s0, uint64_t* out_s1, uint64_t* out_t0, uint64_t* out_t1, int* lvl_d,
+                              int* lvl_t, double* sc_t, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    cc.AddEvalKey(key_from(cc, relin));
+    cc.AddRotationKey(2 * N - 1, key_from(cc, conj));
+    for (int i = 0; i < n_rot; ++i) cc.AddRotationKey(rots[i], key_from(cc, rot_keys[i]));
+    CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+    ev.EvalBootstrapSetup({3, 3}, {0, 0}, (uint32_t)(N / 2), (uint32_t)prescale_bits, msg_scale);
+    ev.EvalBootstrapPrepare();
+    Ciphertext in(cc, raw_of(c0, c1, 1, N, msg_scale));
+    auto dump = [&](const Ciphertext& o, uint64_t* w0, uint64_t* w1) {
+      RawCipherText r;
+      o.store(r);
+      for (auto& v : r.sub_0) w0 = std::copy(v.begin(), v.end(), w0);
+      for (auto& v : r.sub_1) w1 = std::copy(v.begin(), v.end(), w1);
+    };
+    Ciphertext d = ev.EvalBootstrap(in);
+    *lvl_d = d.getLevel();
+    dump(d, out_d0, out_d1);
+    const uint32_t consumed = (uint32_t)(n_q - d.getLevel());
+    dump(ev.EvalBootstrapToLevel(in, consumed), out_s0, out_s1);
+    Ciphertext t = ev.EvalBootstrapToLevel(in, consumed + (uint32_t)extra);
+    *lvl_t = t.getLevel();
+    *sc_t = t.NoiseFactor;
+    dump(t, out_t0, out_t1);
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 // The facade's arithmetic on a and b (host, level l, scale S_l of a FLEXIBLEAUTO chain from
 // top_scale), results packed into out in this order:
 //   EvalMult(a, b) [l-1] | EvalRotate(a, rot) [l] | EvalFastRotation(a, rot) from

@@ -892,3 +892,50 @@ def test_cpp_facade_norelin_and_many(fides):
              "EvalNegate", "EvalAddMany", "EvalRotateMany[0]", "EvalRotateMany[1]", "MultByMonomial"]
     for name, (g0, g1), (w0, w1) in zip(names, got, want):
         assert np.array_equal(g0, w0) and np.array_equal(g1, w1), name
+
+
+@pytest.mark.gpu
+def test_cpp_facade_bootstrap_to_level_n4096(fides):
+    """The facade's EvalBootstrapToLevel at N = 2^12: a request for no more consumed levels than
+    EvalBootstrap's gives its result bit for bit; three more consumed levels run the circuit on a
+    chain cut short by three limbs at the top (ModRaise to fewer limbs), land exactly three limbs
+    lower at that level's canonical scale and keep the precision (> 12 bits, within half a bit)."""
+    import ctypes as C
+    F = fides
+    prm, o, kg, ctx, ev, bs = make_boot(F, 12)
+    N, L = prm.N, prm.n_q
+    delta = 2.0 ** 50
+    rng = xrng(88)
+    z = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    c0, c1 = kg.encrypt(encode(z, N, delta).astype(np.int64), 1)
+    lib = _facade_lib()
+    vp, u64p = C.c_void_p, C.POINTER(C.c_uint64)
+    lib.facade_bootstrap_to_level.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, vp, vp, C.c_int,
+                                              C.POINTER(C.c_int), C.POINTER(vp), C.c_double, C.c_int, C.c_int, u64p,
+                                              u64p, u64p, u64p, u64p, u64p, u64p, u64p, C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_char_p, C.c_int]
+    rots = sorted(ev.rot_keys)
+    outs = [np.zeros((L, N), dtype=np.uint64) for _ in range(6)]
+    u64 = lambda x: np.ascontiguousarray(x, dtype=np.uint64).ctypes.data_as(u64p)
+    lvl_d, lvl_t, sc_t = C.c_int(), C.c_int(), C.c_double()
+    err = C.create_string_buffer(512)
+    primes = np.array(prm.q + prm.p, dtype=np.uint64)
+    rc = lib.facade_bootstrap_to_level(prm.logN, L, prm.K, prm.dnum, u64(primes), ev.S[L], ev.rk.data_ptr(),
+                                       ev.conj_key.data_ptr(), len(rots), (C.c_int * len(rots))(*rots),
+                                       (vp * len(rots))(*[ev.rot_keys[r].data_ptr() for r in rots]), delta,
+                                       bs.prescale.bit_length() - 1, 3, u64(c0), u64(c1), *[u64(x) for x in outs],
+                                       C.byref(lvl_d), C.byref(lvl_t), C.byref(sc_t), err, 512)
+    assert rc == 0, err.value.decode()
+    ld, lt = lvl_d.value, lvl_t.value
+    assert lt == ld - 3
+    assert np.array_equal(outs[0][:ld], outs[2][:ld]) and np.array_equal(outs[1][:ld], outs[3][:ld])
+    S = [0.0] * (L + 1)
+    S[L] = ev.S[L]
+    for k in range(L, 1, -1):
+        S[k - 1] = S[k] * S[k] / prm.q[k - 1]
+    assert abs(sc_t.value / S[lt] - 1) < 1e-12
+    bits = lambda x0, x1, l, sc: -math.log2(np.abs(decode(kg.decrypt_limb0(x0[:l], x1[:l]), N, sc) - z).max())
+    b_d = bits(outs[0], outs[1], ld, S[ld])
+    b_t = bits(outs[4], outs[5], lt, sc_t.value)
+    print(f"N=2^12 bootstrap: {ld} limbs {b_d:.2f} bits; to level (3 deeper): {lt} limbs {b_t:.2f} bits")
+    assert b_t > 12 and b_t >= b_d - 0.5

@@ -4,7 +4,7 @@
 // MakeCKKSPackedPlaintext (encoded on the device), EvalAdd / EvalSub (ciphertexts, plaintexts and
 // real constants), EvalMult (ciphertexts, plaintexts, real constants) / EvalSquare,
 // EvalMultNoRelin + Relinearize, EvalNegate, EvalAddMany, EvalRotateMany, EvalChebyshevSeries,
-// MultByMonomial, AccumulateSum, Rescale,
+// MultByMonomial, AccumulateSum, LinearTransform(InPlace / Many), Rescale,
 // EvalRotate, EvalFastRotationPrecompute + EvalFastRotation, EvalBootstrapSetup +
 // EvalBootstrap, with the reference's level and scale management:
 //   * FIXEDMANUAL: EvalMult leaves a degree-2 result at the operands' level (scale product);
@@ -248,6 +248,105 @@ class CryptoContextImpl {
     o.level_ = lvl;  // the first lvl limbs of the buffers
     o.NoiseFactor = sc;
     return o;
+  }
+  // LinearTransform / LinearTransformInPlace (CryptoContextImpl, api/CryptoContext.hpp:460-517):
+  // ct <- sum_(k < rowSize) Rot(ct, k stride + offset) * D_k by baby steps and giant steps, with
+  // the reference's diagonal contract: diagonals[k] encodes Rot(D_k, r_k), r_k = -bStep (k / bStep)
+  // stride - offset (GetLinearTransformPlaintextRotationIndices), at the level the products are
+  // taken (ct's, one below for an unrescaled input, which is rescaled first).  The bStep baby
+  // rotations by j stride are hoisted (one ModUp); each giant step's inner product
+  // sum_j Rot(ct, j stride) * diagonals[g bStep + j] is one launch (fides_dot_plain, the reference's
+  // LTdotProductPtBatch); the giant steps fold from the top, the running sum rotated by
+  // bStep stride before each is added, and by offset at the end.  Keys: j stride (1 <= j <= bStep)
+  // and offset (GetLinearTransformRotationIndices).  The result keeps the level, at scale
+  // ct x diagonal scale and degree + 1 (un-rescaled).
+  static std::vector<int> GetLinearTransformRotationIndices(int bStep, int stride = 1, int offset = 0) {
+    std::vector<int> r;
+    for (int i = 1; i <= bStep; ++i) r.push_back(i * stride);
+    if (offset != 0) r.push_back(offset);
+    return r;
+  }
+  static std::vector<int> GetLinearTransformPlaintextRotationIndices(int rowSize, int bStep, int stride = 1,
+                                                                    int offset = 0) {
+    std::vector<int> r;
+    for (int k = 0; k < rowSize; ++k) r.push_back(-bStep * (k / bStep) * stride - offset);
+    return r;
+  }
+  std::vector<Ciphertext> LinearTransformMany(const Ciphertext& ct_in, int rowSize, int bStep,
+                                              const std::vector<std::vector<const Plaintext*>>& sets, int stride = 1,
+                                              int offset = 0) const {
+    ct_in.need_two();
+    if (rowSize <= 0 || bStep <= 0) throw Error(FIDES_ERR_ARG, "LinearTransform: rowSize and bStep must be positive");
+    if (ct_in.NoiseLevel == 2) return LinearTransformMany(Rescale(ct_in), rowSize, bStep, sets, stride, offset);
+    const int l = ct_in.getLevel();
+    for (const auto& d : sets) {
+      if ((int)d.size() < rowSize) throw Error(FIDES_ERR_ARG, "LinearTransform: fewer diagonals than rowSize");
+      for (int k = 0; k < rowSize; ++k) {
+        if (!d[k]) throw Error(FIDES_ERR_ARG, "LinearTransform: null diagonal");
+        if (d[k]->level != l) throw Error(FIDES_ERR_LEVEL, "LinearTransform: diagonals must be at the ciphertext's level");
+      }
+    }
+    const int nb = std::min(bStep, rowSize), gs = (rowSize + bStep - 1) / bStep;
+    // baby steps: the input and its hoisted rotations by j stride
+    std::vector<Ciphertext> baby;
+    baby.push_back(copy_of(ct_in, l));
+    if (nb > 1) {
+      std::vector<int> rots;
+      std::vector<const uint64_t*> keys;
+      std::vector<uint64_t *> o0, o1;
+      for (int j = 1; j < nb; ++j) {
+        rots.push_back(j * stride);
+        keys.push_back(cc_->GetRotationKey(j * stride).device());
+        baby.push_back(fresh(l, ct_in.NoiseFactor, ct_in.NoiseLevel, ct_in.slots));
+      }
+      for (int j = 1; j < nb; ++j) o0.push_back(baby[j].c0()), o1.push_back(baby[j].c1());
+      check(fides_rotate_hoisted(cc_->handle(), ct_in.c0(), ct_in.c1(), l, keys.data(), rots.data(), nb - 1,
+                                 o0.data(), o1.data(), cc_->stream()));
+    }
+    std::vector<Ciphertext> outs;
+    for (const auto& d : sets) {
+      const double sc = ct_in.NoiseFactor * d[0]->scale;
+      Ciphertext acc = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
+      for (int g = gs - 1; g >= 0; --g) {
+        std::vector<const uint64_t *> c0s, c1s, pts;
+        for (int j = 0; j < nb && g * bStep + j < rowSize; ++j) {
+          c0s.push_back(baby[j].c0());
+          c1s.push_back(baby[j].c1());
+          pts.push_back(d[g * bStep + j]->data());
+        }
+        if (g == gs - 1) {
+          check(fides_dot_plain(cc_->handle(), c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l, acc.c0(),
+                                acc.c1(), cc_->stream()));
+          continue;
+        }
+        Ciphertext inner = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
+        check(fides_dot_plain(cc_->handle(), c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l, inner.c0(),
+                              inner.c1(), cc_->stream()));
+        Ciphertext r = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
+        check(fides_rotate(cc_->handle(), acc.c0(), acc.c1(), l, cc_->GetRotationKey(bStep * stride).device(),
+                           bStep * stride, r.c0(), r.c1(), cc_->stream()));
+        check(fides_add(cc_->handle(), r.c0(), inner.c0(), l, acc.c0(), cc_->stream()));
+        check(fides_add(cc_->handle(), r.c1(), inner.c1(), l, acc.c1(), cc_->stream()));
+        cc_->synchronize();  // inner and r are released at the end of the iteration
+      }
+      if (offset != 0) {
+        Ciphertext r = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
+        check(fides_rotate(cc_->handle(), acc.c0(), acc.c1(), l, cc_->GetRotationKey(offset).device(), offset, r.c0(),
+                           r.c1(), cc_->stream()));
+        acc = std::move(r);
+      }
+      outs.push_back(std::move(acc));
+    }
+    cc_->synchronize();  // the baby steps are released at scope exit
+    return outs;
+  }
+  Ciphertext LinearTransform(const Ciphertext& ct, int rowSize, int bStep, const std::vector<const Plaintext*>& diagonals,
+                             int stride = 1, int offset = 0) const {
+    return std::move(LinearTransformMany(ct, rowSize, bStep, {diagonals}, stride, offset).at(0));
+  }
+  void LinearTransformInPlace(Ciphertext& ct, int rowSize, int bStep, const std::vector<const Plaintext*>& diagonals,
+                              int stride = 1, int offset = 0) const {
+    ct = LinearTransform(ct, rowSize, bStep, diagonals, stride, offset);
   }
   // AccumulateSum (CryptoContextImpl::AccumulateSum, CudaEngine::accumulateSum): slot i gathers
   // slots i + j stride, j < slots, by rounds of hoisted rotations summed in the extended basis

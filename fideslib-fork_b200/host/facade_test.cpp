@@ -369,4 +369,54 @@ int facade_accumulate(int logN, int n_q, int K, int dnum, const uint64_t* primes
   }
 }
 
+// LinearTransform under FLEXIBLEAUTO of (a0, a1) at l limbs (canonical scale), the rowSize
+// diagonals given as slot vectors dz = [rowSize][n][re, im] (already pre-rotated by the caller),
+// encoded at level l; and LinearTransformMany with the same diagonals and their negation.
+// Each result is rescaled (Rescale: the transform leaves degree 2) and packed into out as c0
+// then c1 limbs (l - 1 each): LinearTransform's, then LinearTransformMany's two; *out_scale the
+// rescaled scale.
+int facade_linear_transform(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, int n_keys,
+                            const int* rots, const uint64_t* const* keys, int l, const uint64_t* a0,
+                            const uint64_t* a1, int row_size, int b_step, int stride, int offset, const double* dz,
+                            int n, uint64_t* out, double* out_scale, char* err, int err_len) {
+  try {
+    Parameters p;
+    p.logN = logN;
+    p.dnum = dnum;
+    p.primes.assign(primes, primes + n_q);
+    p.Sprimes.assign(primes + n_q, primes + n_q + K);
+    Context cc(p);
+    const int N = 1 << logN;
+    for (int i = 0; i < n_keys; ++i) cc.AddRotationKey(rots[i], key_from(cc, keys[i]));
+    CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+    Ciphertext A(cc, raw_of(a0, a1, l, N, ev.GetScalingFactorReal(l)));
+    std::vector<Plaintext> pts, neg;
+    for (int k = 0; k < row_size; ++k) {
+      std::vector<std::complex<double>> v(n), w(n);
+      for (int i = 0; i < n; ++i) {
+        v[i] = {dz[((size_t)k * n + i) * 2], dz[((size_t)k * n + i) * 2 + 1]};
+        w[i] = -v[i];
+      }
+      pts.push_back(ev.MakeCKKSPackedPlaintext(v, l));
+      neg.push_back(ev.MakeCKKSPackedPlaintext(w, l));
+    }
+    std::vector<const Plaintext *> d, dn;
+    for (auto& x : pts) d.push_back(&x);
+    for (auto& x : neg) dn.push_back(&x);
+    uint64_t* w = out;
+    Ciphertext R = ev.LinearTransform(A, row_size, b_step, d, stride, offset);
+    if (R.NoiseLevel != 2 || R.getLevel() != l) throw Error(FIDES_ERR_STATE, "LinearTransform result metadata");
+    Ciphertext Rr = ev.Rescale(R);
+    *out_scale = Rr.NoiseFactor;
+    put(Rr, w);
+    auto many = ev.LinearTransformMany(A, row_size, b_step, {d, dn}, stride, offset);
+    put(ev.Rescale(many.at(0)), w);
+    put(ev.Rescale(many.at(1)), w);
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

@@ -939,3 +939,58 @@ def test_cpp_facade_bootstrap_to_level_n4096(fides):
     b_t = bits(outs[4], outs[5], lt, sc_t.value)
     print(f"N=2^12 bootstrap: {ld} limbs {b_d:.2f} bits; to level (3 deeper): {lt} limbs {b_t:.2f} bits")
     assert b_t > 12 and b_t >= b_d - 0.5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("row_size,b_step,stride,offset", [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2)])
+def test_cpp_facade_linear_transform(fides, row_size, b_step, stride, offset):
+    """The facade's LinearTransform / LinearTransformMany (the reference's BSGS contract:
+    pre-rotated diagonals r_k = -bStep (k / bStep) stride - offset, hoisted baby steps, giant
+    steps folded from the top, the offset rotation last) decrypt, after Rescale, to the FP64
+    y[i] = sum_k x[i + k stride + offset] D_k[i]; the batched form's first set equals the single
+    transform bit for bit and its second (negated diagonals) gives -y."""
+    import ctypes as C
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 50, 8, 2, name="facade")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    kg = KeyGen(o, seed_stream=91)
+    N, l = prm.N, prm.n_q
+    n = N // 2
+    rots = sorted(set([i * stride for i in range(1, b_step + 1)] + ([offset] if offset else [])))
+    keys = {r: F.to_device(kg.rotation_key(r)) for r in rots}
+    top = 2.0 ** 45
+    S = [0.0] * (l + 1)
+    S[l] = top
+    for k in range(l, 1, -1):
+        S[k - 1] = S[k] * S[k] / prm.q[k - 1]
+    rng = xrng(92 + row_size)
+    x = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    D = rng.uniform(-1, 1, (row_size, n)) + 1j * rng.uniform(-1, 1, (row_size, n))
+    # diagonals[k] = Rot(D_k, r_k): slot i holds D_k[i + r_k]
+    pre = [np.roll(D[k], b_step * (k // b_step) * stride + offset) for k in range(row_size)]
+    dz = np.stack([np.stack([p_.real, p_.imag], axis=1) for p_ in pre]).reshape(-1).copy()
+    c0, c1 = kg.encrypt(encode(x, N, S[l]).astype(np.int64), l)
+    lib = _facade_lib()
+    u64p, dp = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
+    lib.facade_linear_transform.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, C.c_int,
+                                            C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int, u64p, u64p, C.c_int,
+                                            C.c_int, C.c_int, C.c_int, dp, C.c_int, u64p, dp, C.c_char_p, C.c_int]
+    lo = l - 1
+    out = np.zeros(3 * 2 * lo * N, dtype=np.uint64)
+    sc = C.c_double()
+    err = C.create_string_buffer(512)
+    u64 = lambda a: np.ascontiguousarray(a, dtype=np.uint64).ctypes.data_as(u64p)
+    primes = np.array(prm.q + prm.p, dtype=np.uint64)
+    rc = lib.facade_linear_transform(prm.logN, l, prm.K, prm.dnum, u64(primes), top, len(rots),
+                                     (C.c_int * len(rots))(*rots), (C.c_void_p * len(rots))(*[keys[r].data_ptr() for r in rots]),
+                                     l, u64(c0), u64(c1), row_size, b_step, stride, offset, dz.ctypes.data_as(dp), n,
+                                     u64(out), C.byref(sc), err, 512)
+    assert rc == 0, err.value.decode()
+    res = [out[i * 2 * lo * N:(i + 1) * 2 * lo * N].reshape(2, lo, N) for i in range(3)]
+    want = sum(np.roll(x, -(k * stride + offset)) * D[k] for k in range(row_size))
+    got = decode(kg.decrypt_limb0(res[0][0], res[0][1]), N, sc.value)
+    assert np.abs(got - want).max() < 1e-6
+    assert np.array_equal(res[1], res[0])
+    got_neg = decode(kg.decrypt_limb0(res[2][0], res[2][1]), N, sc.value)
+    assert np.abs(got_neg + want).max() < 1e-6

@@ -348,6 +348,28 @@ class CryptoContextImpl {
                               int stride = 1, int offset = 0) const {
     ct = LinearTransform(ct, rowSize, bStep, diagonals, stride, offset);
   }
+  // In-place forms (CryptoContextImpl::*InPlace): the operand is replaced by the result.
+  void EvalAddInPlace(Ciphertext& a, const Ciphertext& b) const { a = EvalAdd(a, b); }
+  void EvalAddInPlace(Ciphertext& a, const Plaintext& p) const { a = EvalAdd(a, p); }
+  void EvalAddInPlace(Ciphertext& a, double c) const { a = EvalAdd(a, c); }
+  void EvalSubInPlace(Ciphertext& a, const Ciphertext& b) const { a = EvalSub(a, b); }
+  void EvalSubInPlace(Ciphertext& a, const Plaintext& p) const { a = EvalSub(a, p); }
+  void EvalSubInPlace(Ciphertext& a, double c) const { a = EvalSub(a, c); }
+  void EvalMultInPlace(Ciphertext& a, const Ciphertext& b) const { a = EvalMult(a, b); }
+  void EvalMultInPlace(Ciphertext& a, const Plaintext& p) const { a = EvalMult(a, p); }
+  void EvalMultInPlace(Ciphertext& a, double c) const { a = EvalMult(a, c); }
+  void EvalSquareInPlace(Ciphertext& a) const { a = EvalSquare(a); }
+  void EvalNegateInPlace(Ciphertext& a) const { a = EvalNegate(a); }
+  void RelinearizeInPlace(Ciphertext& a) const { a = Relinearize(a); }
+  void RescaleInPlace(Ciphertext& a) const { a = Rescale(a); }
+  void EvalRotateInPlace(Ciphertext& a, int index) const { a = EvalRotate(a, index); }
+  void EvalChebyshevSeriesInPlace(Ciphertext& a, const std::vector<double>& coeffs, double lo, double hi) const {
+    a = EvalChebyshevSeries(a, coeffs, lo, hi);
+  }
+  void MultByMonomialInPlace(Ciphertext& a, uint32_t power) const { a = MultByMonomial(a, power); }
+  void AccumulateSumInPlace(Ciphertext& a, int slots, int stride = 1) const { a = AccumulateSum(a, slots, stride); }
+  void EvalBootstrapInPlace(Ciphertext& a) const { a = EvalBootstrap(a); }
+  void EvalBootstrapToLevelInPlace(Ciphertext& a, uint32_t outputLevel) { a = EvalBootstrapToLevel(a, outputLevel); }
   // AccumulateSum (CryptoContextImpl::AccumulateSum, CudaEngine::accumulateSum): slot i gathers
   // slots i + j stride, j < slots, by rounds of hoisted rotations summed in the extended basis
   // (fides_accumulate, radix 4 as the reference's default PARTIAL_SUM_RADIX); the rotation keys

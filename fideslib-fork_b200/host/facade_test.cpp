@@ -290,6 +290,14 @@ int facade_more(int logN, int n_q, int K, int dnum, const uint64_t* primes, doub
       if (!refused) throw Error(FIDES_ERR_STATE, "a three-component rotation was not refused");
       Ciphertext R = man.Relinearize(X);
       if (R.hasC2()) throw Error(FIDES_ERR_STATE, "Relinearize left a third component");
+      {  // the in-place form gives the same residues
+        Ciphertext Y = man.EvalMultNoRelin(A, B);
+        man.RelinearizeInPlace(Y);
+        RawCipherText r1, r2;
+        Y.store(r1);
+        R.store(r2);
+        if (r1.sub_0 != r2.sub_0 || r1.sub_1 != r2.sub_1) throw Error(FIDES_ERR_STATE, "RelinearizeInPlace differs");
+      }
       put(R, w);
       put(man.Relinearize(man.EvalAdd(X, man.EvalMultNoRelin(A, A))), w);
     }

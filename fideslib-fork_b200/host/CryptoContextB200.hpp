@@ -220,6 +220,44 @@ class CryptoContextImpl {
   Plaintext MakeCKKSPackedPlaintext(const std::vector<double>& x, int level = 0, double scale = 0) const {
     return MakeCKKSPackedPlaintext(std::vector<std::complex<double>>(x.begin(), x.end()), level, scale);
   }
+  // A plaintext from / to the reference's raw exchange format (GetRawPlainText /
+  // GetOpenFHEPlaintext, RawCiphertext.cuh:106-109): the limbs converted by fides_ct_import /
+  // fides_ct_export (COEFFICIENT limbs transformed on the device; OpenFHE's bit-reversed
+  // EVALUATION order unless natural_order).
+  Plaintext LoadPlaintext(const RawPlainText& raw, bool natural_order = false) const {
+    if (raw.numRes < 1 || raw.numRes > (int)S_.size() - 1 || raw.N != N() || (int)raw.sub_0.size() != raw.numRes)
+      throw Error(FIDES_ERR_ARG, "RawPlainText does not match the context");
+    std::vector<const uint64_t*> limbs;
+    for (const auto& v : raw.sub_0) {
+      if ((int)v.size() != N()) throw Error(FIDES_ERR_ARG, "bad plaintext limb");
+      limbs.push_back(v.data());
+    }
+    Plaintext p;
+    p.level = raw.numRes;
+    p.scale = raw.Noise;
+    p.slots = raw.slots;
+    p.limbs = DeviceLimbs((size_t)N() * raw.numRes);
+    check(fides_ct_import(cc_->handle(), 1, limbs.data(), raw.moduli.empty() ? nullptr : raw.moduli.data(),
+                          raw.numRes, raw.format == COEFFICIENT ? 1 : 0, natural_order ? 1 : 0, p.limbs.get(),
+                          cc_->stream()));
+    cc_->synchronize();
+    return p;
+  }
+  void StorePlaintext(const Plaintext& p, RawPlainText& raw, RawFormat format = EVALUATION,
+                      bool natural_order = false) const {
+    raw.N = N();
+    raw.numRes = p.level;
+    raw.moduli.assign(cc_->primes.begin(), cc_->primes.begin() + p.level);
+    raw.format = format;
+    raw.Noise = p.scale;
+    raw.slots = p.slots;
+    raw.NoiseLevel = 1;
+    raw.sub_0.assign(p.level, std::vector<uint64_t>(N()));
+    std::vector<uint64_t*> limbs;
+    for (auto& v : raw.sub_0) limbs.push_back(v.data());
+    check(fides_ct_export(cc_->handle(), 1, p.data(), p.level, format == COEFFICIENT ? 1 : 0, natural_order ? 1 : 0,
+                          limbs.data(), cc_->stream()));
+  }
 
   // ---- additive operations (CryptoContextImpl::EvalAdd / EvalSub)
   Ciphertext EvalAdd(const Ciphertext& a, const Ciphertext& b) const { return add_sub(a, b, false); }

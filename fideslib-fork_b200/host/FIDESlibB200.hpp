@@ -55,6 +55,29 @@ struct RawKeySwitchKey {
   std::vector<std::vector<std::vector<std::vector<uint64_t>>>> r_key;
 };
 
+// reference RawPlainText (RawCiphertext.cuh:39-50), without the OpenFHE object: one polynomial
+// of numRes limbs in OpenFHE's layout (bit-reversed EVALUATION, or COEFFICIENT).
+enum RawFormat { EVALUATION = 0, COEFFICIENT = 1 };
+struct RawPlainText {
+  std::vector<std::vector<uint64_t>> sub_0;
+  std::vector<uint64_t> moduli;
+  int numRes = 0;
+  int N = 0;
+  RawFormat format = EVALUATION;
+  double Noise = 1.0;  // scaling factor
+  int slots = 0;
+  int NoiseLevel = 1;
+};
+
+// reference RawParams (RawCiphertext.cuh:52-88): the fields a context is built from (the
+// precomputed tables OpenFHE also exports are rebuilt by the library from the primes).
+struct RawParams {
+  int N = 0, L = 0, K = 0, logN = 0, dnum = 1;
+  std::vector<uint64_t> moduli, root_of_unity;                // Q primes and their 2N-th roots
+  std::vector<uint64_t> SPECIALmoduli, SPECIALroot_of_unity;  // special primes and roots
+  std::vector<double> ScalingFactorReal;                     // per level (FLEXIBLEAUTO chains)
+};
+
 struct Parameters {
   int logN = 0;
   int dnum = 1;
@@ -63,6 +86,20 @@ struct Parameters {
   std::vector<uint64_t> psi;      // optional roots (Q then special); empty = derived
   int device = 0;
   bool reducedNoise = false;  // reduced-noise ModUp / ModDown (src/CKKS/Parameters.cuh:31)
+
+  // reference Parameters::adaptTo(RawParams&) (src/CKKS/Parameters.cu): the chain, the roots and
+  // dnum of an OpenFHE context; device and reducedNoise stay as set here
+  Parameters adaptTo(const RawParams& raw) const {
+    Parameters p = *this;
+    p.logN = raw.logN;
+    p.dnum = raw.dnum;
+    p.primes = raw.moduli;
+    p.Sprimes = raw.SPECIALmoduli;
+    p.psi = raw.root_of_unity;
+    p.psi.insert(p.psi.end(), raw.SPECIALroot_of_unity.begin(), raw.SPECIALroot_of_unity.end());
+    if ((int)p.psi.size() != (int)(p.primes.size() + p.Sprimes.size())) p.psi.clear();  // derive them instead
+    return p;
+  }
 };
 
 // Device buffer of limbs (RAII).

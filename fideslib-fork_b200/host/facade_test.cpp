@@ -427,4 +427,54 @@ int facade_linear_transform(int logN, int n_q, int K, int dnum, const uint64_t* 
   }
 }
 
+// The reference's raw formats: a context from RawParams (Parameters::adaptTo), a plaintext of the
+// n slots z encoded at the top level, exported with StorePlaintext as EVALUATION (eval_out),
+// COEFFICIENT (coeff_out) and natural-order EVALUATION (nat_out), each [L][N]; the COEFFICIENT and
+// natural-order exports are loaded back with LoadPlaintext and must equal the plaintext.
+int facade_raw_plaintext(int logN, int n_q, int K, int dnum, const uint64_t* primes, const uint64_t* psi,
+                         double top_scale, const double* z, int n, uint64_t* eval_out, uint64_t* coeff_out,
+                         uint64_t* nat_out, char* err, int err_len) {
+  try {
+    RawParams raw;
+    raw.logN = logN;
+    raw.N = 1 << logN;
+    raw.L = n_q;
+    raw.K = K;
+    raw.dnum = dnum;
+    raw.moduli.assign(primes, primes + n_q);
+    raw.SPECIALmoduli.assign(primes + n_q, primes + n_q + K);
+    raw.root_of_unity.assign(psi, psi + n_q);
+    raw.SPECIALroot_of_unity.assign(psi + n_q, psi + n_q + K);
+    Context cc(Parameters{}.adaptTo(raw));
+    const int N = 1 << logN;
+    CryptoContextImpl ev(cc, FLEXIBLEAUTO, top_scale);
+    std::vector<std::complex<double>> v(n);
+    for (int i = 0; i < n; ++i) v[i] = {z[2 * i], z[2 * i + 1]};
+    Plaintext P = ev.MakeCKKSPackedPlaintext(v);
+    const size_t words = (size_t)N * n_q;
+    std::vector<uint64_t> dev(words);
+    check_cuda(cudaMemcpy(dev.data(), P.data(), words * 8, cudaMemcpyDeviceToHost), "D2H");
+    auto flat = [&](const RawPlainText& r, uint64_t* out) {
+      for (const auto& limb : r.sub_0) out = std::copy(limb.begin(), limb.end(), out);
+    };
+    RawPlainText re, rc, rn;
+    ev.StorePlaintext(P, re);
+    ev.StorePlaintext(P, rc, COEFFICIENT);
+    ev.StorePlaintext(P, rn, EVALUATION, true);
+    flat(re, eval_out);
+    flat(rc, coeff_out);
+    flat(rn, nat_out);
+    for (const RawPlainText* r : {&rc, &rn}) {
+      Plaintext Q = ev.LoadPlaintext(*r, r == &rn);
+      std::vector<uint64_t> back(words);
+      check_cuda(cudaMemcpy(back.data(), Q.data(), words * 8, cudaMemcpyDeviceToHost), "D2H");
+      if (back != dev || Q.level != P.level || Q.scale != P.scale) throw Error(FIDES_ERR_STATE, "plaintext round trip");
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+}
+
 }  // extern "C"

@@ -994,3 +994,43 @@ def test_cpp_facade_linear_transform(fides, row_size, b_step, stride, offset):
     assert np.array_equal(res[1], res[0])
     got_neg = decode(kg.decrypt_limb0(res[2][0], res[2][1]), N, sc.value)
     assert np.abs(got_neg + want).max() < 1e-6
+
+
+@pytest.mark.gpu
+def test_cpp_facade_raw_plaintext_and_params(fides):
+    """The reference's raw exchange formats in the C++ layer: a context built from RawParams
+    (Parameters::adaptTo), a device-encoded plaintext exported as RawPlainText in EVALUATION,
+    COEFFICIENT and natural-order EVALUATION form and loaded back unchanged; the COEFFICIENT
+    export is the encoder's integer polynomial (within 1 of the host encoder's coefficients) and
+    the EVALUATION export its NTT (the oracle's), the natural-order one the same residues permuted."""
+    import ctypes as C
+    from fides_b200 import params as P
+    F = fides
+    prm = P.chain(12, 60, 50, 6, 2, name="raw")
+    o = O.Oracle(prm.logN, prm.q, prm.p, prm.dnum)
+    N, L = prm.N, prm.n_q
+    rng = xrng(95)
+    z = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    zz = np.stack([z.real, z.imag], axis=1).reshape(-1).copy()
+    outs = [np.zeros((L, N), dtype=np.uint64) for _ in range(3)]
+    lib = _facade_lib()
+    u64p, dp = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
+    lib.facade_raw_plaintext.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_double, dp, C.c_int,
+                                         u64p, u64p, u64p, C.c_char_p, C.c_int]
+    u64 = lambda a: np.ascontiguousarray(a, dtype=np.uint64).ctypes.data_as(u64p)
+    err = C.create_string_buffer(512)
+    primes = np.array(prm.q + prm.p, dtype=np.uint64)
+    psi = np.array(o.psi, dtype=np.uint64)
+    top = 2.0 ** 45
+    rc = lib.facade_raw_plaintext(prm.logN, L, prm.K, prm.dnum, u64(primes), u64(psi), top, zz.ctypes.data_as(dp),
+                                  N // 2, *[u64(x) for x in outs], err, 512)
+    assert rc == 0, err.value.decode()
+    ev_, co_, na_ = outs
+    ids = list(range(L))
+    assert np.array_equal(o.ntt(co_, ids), ev_)
+    m = np.array([int(v) - prm.q[0] if int(v) > prm.q[0] // 2 else int(v) for v in co_[0]], dtype=np.int64)
+    ref = encode(z, N, top).astype(np.int64)
+    diff = np.abs(m - ref)
+    assert diff.max() <= 1 and np.count_nonzero(diff) <= max(1, N // 1000)
+    for j in range(L):
+        assert np.array_equal(np.sort(na_[j]), np.sort(ev_[j]))

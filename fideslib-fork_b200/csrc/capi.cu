@@ -420,9 +420,22 @@ int fides_mul(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uin
   return addsub(x, a, b, level, out, stream, fides::EW_MUL);
 }
 
-int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* const* c1s,
-                    const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
-                    void* stream) {
+int fides_add_ext(fides_ctx* x, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(a, "a");
+    need(b, "b");
+    need(out, "out");
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "extended basis needs special primes");
+    fides::AddSubJob j{a, b, out, level + c->K, fides::EW_ADD, level, c->n_q};
+    fides::launch_addsub(c, &j, 1, S(stream));
+  });
+}
+
+static int dot_plain_impl(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                          const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
+                          void* stream, bool ext) {
   return guard([&] {
     auto* c = C(x);
     if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
@@ -444,10 +457,26 @@ int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* co
     j.out0[0] = out0;
     j.out1[0] = out1;
     j.n = n_terms;
-    j.l = level;
+    j.l = ext ? level + c->K : level;
+    if (ext) {
+      if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "extended basis needs special primes");
+      j.lq = level;
+      j.nq = c->n_q;
+    }
     j.lanes = 1;
     fides::launch_dot_plain(c, j, S(stream));
   });
+}
+
+int fides_dot_plain(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* const* c1s, const uint64_t* const* pts,
+                    int n_terms, int level, uint64_t* out0, uint64_t* out1, void* stream) {
+  return dot_plain_impl(x, c0s, c1s, pts, n_terms, level, out0, out1, stream, false);
+}
+
+int fides_dot_plain_ext(fides_ctx* x, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                        const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
+                        void* stream) {
+  return dot_plain_impl(x, c0s, c1s, pts, n_terms, level, out0, out1, stream, true);
 }
 
 int fides_lincomb(fides_ctx* x, int n_lanes, const uint64_t* const* c0s, const uint64_t* const* c1s,
@@ -522,6 +551,17 @@ int fides_encode(fides_ctx* x, const double* slots, int n_slots, int n_pts, doub
     need(slots, "slots");
     need(out, "out");
     fides::op_encode(c, slots, n_slots, n_pts, scale, level, out, S(stream));
+  });
+}
+
+int fides_encode_ext(fides_ctx* x, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
+                     void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(slots, "slots");
+    need(out, "out");
+    if (c->K < 1) throw fides::Error(FIDES_ERR_ARG, "extended basis needs special primes");
+    fides::op_encode_ext(c, slots, n_slots, n_pts, scale, level, c->K, out, S(stream));
   });
 }
 
@@ -685,6 +725,37 @@ int fides_rotate_hoisted(fides_ctx* x, const uint64_t* c0, const uint64_t* c1, i
       it.out1.push_back(out1[j]);
     }
     fides::op_hoisted(c, it, S(stream));
+  });
+}
+
+int fides_rotate_hoisted_ext(fides_ctx* x, const uint64_t* c0, int c0_ext, const uint64_t* c1, int level,
+                             const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                             uint64_t* const* out1, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    need(c0, "c0");
+    need(c1, "c1");
+    need(keys, "keys");
+    need(rotations, "rotations");
+    need(out0, "out0");
+    need(out1, "out1");
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (n < 1) throw fides::Error(FIDES_ERR_ARG, "need at least one rotation");
+    fides::HoistItem it;
+    it.c0 = c0_ext ? nullptr : c0;
+    it.c0x = c0_ext ? c0 : nullptr;
+    it.c1 = c1;
+    it.l = level;
+    for (int j = 0; j < n; ++j) {
+      need(out0[j], "out0[j]");
+      need(out1[j], "out1[j]");
+      need(keys[j], "keys[j]");
+      it.keys.push_back(keys[j]);
+      it.ks.push_back(fides::h_auto_index(c->logN, rotations[j]));
+      it.out0.push_back(out0[j]);
+      it.out1.push_back(out1[j]);
+    }
+    fides::op_hoisted_ext_batch(c, &it, 1, S(stream));
   });
 }
 

@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(EW_THREADS) addsub_kernel(const __grid_constan
   const int j = blockIdx.y;
   if (j >= J.l) return;
   const size_t off = ((size_t)j << logN) + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const DevPrime p = primes[j];
+  const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
   const uint64_t q = p.q;
   const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(J.a + off);
   ulonglong2 y;

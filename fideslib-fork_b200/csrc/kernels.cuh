@@ -127,6 +127,7 @@ struct AddSubJob {
   uint64_t* out;
   int l;
   int sub;  // EwOp
+  int lq = 0, nq = 0;  // extended-basis operands (ext_prime); lq = 0: Q limbs only
 };
 constexpr int MAX_ADDSUB_JOBS = 128;
 struct AddSubJobList {

@@ -189,6 +189,11 @@ def lib():
         L.fides_mul.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         L.fides_mul_scalar.argtypes = [vp, vp, C.c_int, u64p, vp, vp]
         L.fides_dot_plain.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        L.fides_dot_plain_ext.argtypes = L.fides_dot_plain.argtypes
+        L.fides_add_ext.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_encode_ext.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]
+        L.fides_rotate_hoisted_ext.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_int),
+                                               C.c_int, C.POINTER(vp), C.POINTER(vp), vp]
         L.fides_lincomb.argtypes = [vp, C.c_int, vp, vp, u64p, u64p, C.c_int, C.c_int, vp, vp, vp]
         L.fides_rescale_batch.argtypes = [vp, vp, vp, vp, C.c_int, vp]
         L.fides_encode.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]
@@ -560,6 +565,22 @@ class Context:
         _check(lib().fides_rotate_hoisted(self._h, _ptr(ct.c0), _ptr(ct.c1), l, kp, rs, n, o0, o1, _stream()))
         return outs
 
+    def rotate_hoisted_ext(self, ct: Ciphertext, keys, rotations, c0_ext=None) -> list[Ciphertext]:
+        """Hoisted rotations left in the extended basis: each result has level + K limbs per
+        component (P times the rotation, before ModDown); moddown() of both gives
+        rotate_hoisted's results.  c0_ext: an extended c0 added instead of P ct.c0 (ct.c0 is
+        then ignored)."""
+        n, l = len(rotations), ct.c1.shape[0]
+        e = l + self.K
+        outs = [Ciphertext(self.empty(e), self.empty(e)) for _ in range(n)]
+        kp = (vp * n)(*[_ptr(k) for k in keys])
+        rs = (C.c_int * n)(*rotations)
+        o0 = (vp * n)(*[_ptr(o.c0) for o in outs])
+        o1 = (vp * n)(*[_ptr(o.c1) for o in outs])
+        c0, x = (ct.c0, 0) if c0_ext is None else (c0_ext, 1)
+        _check(lib().fides_rotate_hoisted_ext(self._h, _ptr(c0), x, _ptr(ct.c1), l, kp, rs, n, o0, o1, _stream()))
+        return outs
+
     def rotate_hoisted_batch(self, cts, keys, rotations) -> list[list[Ciphertext]]:
         """Hoisted rotations of several ciphertexts (any levels) in one launch sequence per
         stage.  keys / rotations: per-ciphertext lists (or one list shared by all)."""
@@ -607,6 +628,23 @@ class Context:
         c1 = (vp * n)(*[_ptr(c.c1) for c in cts])
         pp = (vp * n)(*[_ptr(p) for p in pts])
         _check(lib().fides_dot_plain(self._h, c0, c1, pp, n, l, _ptr(out.c0), _ptr(out.c1), _stream()))
+        return out
+
+    def add_ext(self, a, b, level: int, out=None):
+        """a + b over extended-basis polynomials ([level + K, N])."""
+        out = self.empty(level + self.K) if out is None else out
+        _check(lib().fides_add_ext(self._h, _ptr(a), _ptr(b), level, _ptr(out), _stream()))
+        return out
+
+    def dot_plain_ext(self, cts, pts, level: int, out=None):
+        """dot_plain over extended-basis operands: cts and pts carry level Q limbs followed by
+        the K special limbs (rotate_hoisted_ext, encode_ext); out has level + K limbs."""
+        n, e = len(cts), level + self.K
+        out = Ciphertext(self.empty(e), self.empty(e)) if out is None else out
+        c0 = (vp * n)(*[_ptr(c.c0) for c in cts])
+        c1 = (vp * n)(*[_ptr(c.c1) for c in cts])
+        pp = (vp * n)(*[_ptr(p) for p in pts])
+        _check(lib().fides_dot_plain_ext(self._h, c0, c1, pp, n, level, _ptr(out.c0), _ptr(out.c1), _stream()))
         return out
 
     # -- interop with per-limb host arrays (the reference's RawCipherText / RawKeySwitchKey) --
@@ -671,6 +709,19 @@ class Context:
         out = torch.empty((n_pts, level, self.N), dtype=torch.int64, device=self.device).view(torch.uint64)
         _check(lib().fides_encode(self._h, torch.view_as_real(z).data_ptr(), n, n_pts, float(scale), level, _ptr(out),
                                   _stream()))
+        return out[0] if single else out
+
+    def encode_ext(self, slots, scale: float, level: int):
+        """encode over the extended basis (MakeCKKSPackedPlaintextExtended): [level + K, N] (or
+        [n_pts, level + K, N]), the level Q limbs then the K special limbs of one integer
+        polynomial."""
+        z = torch.as_tensor(slots).to(device=self.device, dtype=torch.complex128).contiguous()
+        single = z.dim() == 1
+        z = z.reshape(1, -1) if single else z
+        n_pts, n = z.shape
+        out = torch.empty((n_pts, level + self.K, self.N), dtype=torch.int64, device=self.device).view(torch.uint64)
+        _check(lib().fides_encode_ext(self._h, torch.view_as_real(z).data_ptr(), n, n_pts, float(scale), level,
+                                      _ptr(out), _stream()))
         return out[0] if single else out
 
     def decode(self, pts, scale: float, n_slots=None):

@@ -42,10 +42,13 @@ enum ScalingTechnique { FIXEDMANUAL = 0, FLEXIBLEAUTO = 1 };
 // api/Plaintext.hpp, CKKSPackedEncoding): `level` limbs in EVALUATION form on the device, at
 // scale `scale`, holding `slots` slots.
 struct Plaintext {
-  DeviceLimbs limbs;  // [level][N]
+  DeviceLimbs limbs;  // [level][N], or [level + K][N] when ext
   int level = 0;
   double scale = 0;
   int slots = 0;
+  // encoded over Q.P as well (MakeCKKSPackedPlaintextExtended): the K special limbs follow the
+  // level Q limbs, which are those of the plain encoding
+  bool ext = false;
   const uint64_t* data() const { return limbs.get(); }
 };
 
@@ -195,6 +198,19 @@ class CryptoContextImpl {
   // scale 0 = that level's canonical scale (OpenFHE's default for the level).
   Plaintext MakeCKKSPackedPlaintext(const std::vector<std::complex<double>>& z, int level = 0,
                                     double scale = 0) const {
+    return encode_packed(z, level, scale, false);
+  }
+  // MakeCKKSPackedPlaintextExtended (api/CryptoContext.hpp:171): the same integer polynomial
+  // over Q.P (fides_encode_ext), for the diagonals of a LinearTransform that keeps its baby
+  // steps and giant-step sums in the extended basis.
+  Plaintext MakeCKKSPackedPlaintextExtended(const std::vector<std::complex<double>>& z, int level = 0,
+                                            double scale = 0) const {
+    return encode_packed(z, level, scale, true);
+  }
+  Plaintext MakeCKKSPackedPlaintextExtended(const std::vector<double>& x, int level = 0, double scale = 0) const {
+    return encode_packed(std::vector<std::complex<double>>(x.begin(), x.end()), level, scale, true);
+  }
+  Plaintext encode_packed(const std::vector<std::complex<double>>& z, int level, double scale, bool ext) const {
     const int L = (int)S_.size() - 1;
     if (level == 0) level = L;
     if (level < 1 || level > L) throw Error(FIDES_ERR_LEVEL, "plaintext level out of range");
@@ -211,9 +227,10 @@ class CryptoContextImpl {
     p.level = level;
     p.scale = scale > 0 ? scale : S_[level];
     p.slots = n;
-    p.limbs = DeviceLimbs((size_t)N() * level);
-    check(fides_encode(cc_->handle(), reinterpret_cast<const double*>(dev.get()), n, 1, p.scale, level, p.limbs.get(),
-                       cc_->stream()));
+    p.ext = ext;
+    p.limbs = DeviceLimbs((size_t)N() * (level + (ext ? cc_->K : 0)));
+    check((ext ? fides_encode_ext : fides_encode)(cc_->handle(), reinterpret_cast<const double*>(dev.get()), n, 1,
+                                                  p.scale, level, p.limbs.get(), cc_->stream()));
     cc_->synchronize();  // the slot buffer is released at scope exit
     return p;
   }
@@ -324,6 +341,10 @@ class CryptoContextImpl {
         if (d[k]->level != l) throw Error(FIDES_ERR_LEVEL, "LinearTransform: diagonals must be at the ciphertext's level");
       }
     }
+    bool ext = cc_->K > 0;  // every diagonal extended: the Q.P path (the reference's ext flag)
+    for (const auto& d : sets)
+      for (int k = 0; k < rowSize; ++k) ext = ext && d[k]->ext;
+    if (ext) return linear_transform_ext(ct_in, rowSize, bStep, sets, stride, offset);
     const int nb = std::min(bStep, rowSize), gs = (rowSize + bStep - 1) / bStep;
     // baby steps: the input and its hoisted rotations by j stride
     std::vector<Ciphertext> baby;
@@ -376,6 +397,90 @@ class CryptoContextImpl {
       outs.push_back(std::move(acc));
     }
     cc_->synchronize();  // the baby steps are released at scope exit
+    return outs;
+  }
+  // P mod q_i for the first l Q primes (P: the product of the special primes)
+  std::vector<uint64_t> p_mod_q(int l) const {
+    std::vector<uint64_t> v(l);
+    for (int i = 0; i < l; ++i) {
+      unsigned __int128 r = 1;
+      for (int k = 0; k < cc_->K; ++k) r = r * (cc_->primes[cc_->L + k] % q(i)) % q(i);
+      v[i] = (uint64_t)r;
+    }
+    return v;
+  }
+  // LinearTransform over extended diagonals (the reference's fused branch with ext = true,
+  // LinearTransform.cu:84-196): the baby steps are P ct and the hoisted rotations left in Q.P
+  // (fides_rotate_hoisted_ext), each giant step's inner product is taken there
+  // (fides_dot_plain_ext), and the giant-step fold keeps c0 in Q.P: before each step the running
+  // sum's c1 is brought down and the sum rotated by bStep stride without ModDown, its extended c0
+  // added as it is (a rotation by a multiple of N/2 slots is the identity and is skipped, as
+  // there).  The transform ends with one ModDown of each component, or of c1 before the rotation
+  // by offset, whose ModDown closes it.  Same diagonal contract, keys and result scale as the
+  // Q-basis path; the rounding differs (one ModDown per component instead of one per rotation).
+  std::vector<Ciphertext> linear_transform_ext(const Ciphertext& ct_in, int rowSize, int bStep,
+                                               const std::vector<std::vector<const Plaintext*>>& sets, int stride,
+                                               int offset) const {
+    const int l = ct_in.getLevel(), e = l + cc_->K;
+    const size_t Ne = (size_t)N() * e, Nq = (size_t)N() * l;
+    auto* h = cc_->handle();
+    auto st = cc_->stream();
+    const int nb = std::min(bStep, rowSize), gs = (rowSize + bStep - 1) / bStep;
+    std::vector<DeviceLimbs> b0, b1;  // baby steps in Q.P: P ct, then Rot(ct, j stride) before ModDown
+    for (int j = 0; j < nb; ++j) b0.emplace_back(Ne), b1.emplace_back(Ne);
+    const auto pm = p_mod_q(l);
+    check(fides_mul_scalar(h, ct_in.c0(), l, pm.data(), b0[0].get(), st));
+    check(fides_mul_scalar(h, ct_in.c1(), l, pm.data(), b1[0].get(), st));
+    check_cuda(cudaMemsetAsync(b0[0].get() + Nq, 0, sizeof(uint64_t) * (Ne - Nq), st), "memset");
+    check_cuda(cudaMemsetAsync(b1[0].get() + Nq, 0, sizeof(uint64_t) * (Ne - Nq), st), "memset");
+    if (nb > 1) {
+      std::vector<int> rots;
+      std::vector<const uint64_t*> keys;
+      std::vector<uint64_t *> o0, o1;
+      for (int j = 1; j < nb; ++j) {
+        rots.push_back(j * stride);
+        keys.push_back(cc_->GetRotationKey(j * stride).device());
+        o0.push_back(b0[j].get());
+        o1.push_back(b1[j].get());
+      }
+      check(fides_rotate_hoisted_ext(h, ct_in.c0(), 0, ct_in.c1(), l, keys.data(), rots.data(), nb - 1, o0.data(),
+                                     o1.data(), st));
+    }
+    DeviceLimbs a0(Ne), a1(Ne), t0(Ne), t1(Ne), c1q(Nq);
+    // a rotation of the running sum (c0 in Q.P, c1 brought down first), into a0 / a1
+    auto rotate_sum = [&](int r) {
+      check(fides_moddown(h, a1.get(), l, c1q.get(), st));
+      const uint64_t* key = cc_->GetRotationKey(r).device();
+      uint64_t* r0 = t0.get();
+      uint64_t* r1 = t1.get();
+      check(fides_rotate_hoisted_ext(h, a0.get(), 1, c1q.get(), l, &key, &r, 1, &r0, &r1, st));
+      std::swap(a0, t0);
+      std::swap(a1, t1);
+    };
+    std::vector<Ciphertext> outs;
+    for (const auto& d : sets) {
+      for (int g = gs - 1; g >= 0; --g) {
+        std::vector<const uint64_t *> c0s, c1s, pts;
+        for (int j = 0; j < nb && g * bStep + j < rowSize; ++j) {
+          c0s.push_back(b0[j].get());
+          c1s.push_back(b1[j].get());
+          pts.push_back(d[g * bStep + j]->data());
+        }
+        const bool first = g == gs - 1;
+        if (!first && (bStep * stride) % (N() / 2) != 0) rotate_sum(bStep * stride);
+        check(fides_dot_plain_ext(h, c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l,
+                                  first ? a0.get() : t0.get(), first ? a1.get() : t1.get(), st));
+        if (first) continue;
+        check(fides_add_ext(h, a0.get(), t0.get(), l, a0.get(), st));
+        check(fides_add_ext(h, a1.get(), t1.get(), l, a1.get(), st));
+      }
+      if (offset != 0) rotate_sum(offset);
+      Ciphertext o = fresh(l, ct_in.NoiseFactor * d[0]->scale, ct_in.NoiseLevel + 1, ct_in.slots);
+      check(fides_moddown(h, a0.get(), l, o.c0(), st));
+      check(fides_moddown(h, a1.get(), l, o.c1(), st));
+      outs.push_back(std::move(o));
+    }
+    cc_->synchronize();  // the Q.P buffers are released at scope exit
     return outs;
   }
   Ciphertext LinearTransform(const Ciphertext& ct, int rowSize, int bStep, const std::vector<const Plaintext*>& diagonals,

@@ -382,11 +382,12 @@ int facade_accumulate(int logN, int n_q, int K, int dnum, const uint64_t* primes
 // encoded at level l; and LinearTransformMany with the same diagonals and their negation.
 // Each result is rescaled (Rescale: the transform leaves degree 2) and packed into out as c0
 // then c1 limbs (l - 1 each): LinearTransform's, then LinearTransformMany's two; *out_scale the
-// rescaled scale.
+// rescaled scale.  ext != 0: the diagonals are encoded over Q.P (MakeCKKSPackedPlaintextExtended),
+// which takes the extended-basis path.
 int facade_linear_transform(int logN, int n_q, int K, int dnum, const uint64_t* primes, double top_scale, int n_keys,
                             const int* rots, const uint64_t* const* keys, int l, const uint64_t* a0,
                             const uint64_t* a1, int row_size, int b_step, int stride, int offset, const double* dz,
-                            int n, uint64_t* out, double* out_scale, char* err, int err_len) {
+                            int n, int ext, uint64_t* out, double* out_scale, char* err, int err_len) {
   try {
     Parameters p;
     p.logN = logN;
@@ -405,8 +406,8 @@ int facade_linear_transform(int logN, int n_q, int K, int dnum, const uint64_t* 
         v[i] = {dz[((size_t)k * n + i) * 2], dz[((size_t)k * n + i) * 2 + 1]};
         w[i] = -v[i];
       }
-      pts.push_back(ev.MakeCKKSPackedPlaintext(v, l));
-      neg.push_back(ev.MakeCKKSPackedPlaintext(w, l));
+      pts.push_back(ext ? ev.MakeCKKSPackedPlaintextExtended(v, l) : ev.MakeCKKSPackedPlaintext(v, l));
+      neg.push_back(ext ? ev.MakeCKKSPackedPlaintextExtended(w, l) : ev.MakeCKKSPackedPlaintext(w, l));
     }
     std::vector<const Plaintext *> d, dn;
     for (auto& x : pts) d.push_back(&x);

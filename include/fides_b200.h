@@ -197,6 +197,16 @@ int fides_add_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_
 int fides_dot_plain(fides_ctx* ctx, const uint64_t* const* c0s, const uint64_t* const* c1s,
                     const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
                     void* stream);
+/* out = a + b over extended-basis polynomials ([level + K][N]: the level Q limbs, then the K
+ * special limbs); Ciphertext::add of two operands still in Q.P (LinearTransform.cu:168-173). */
+int fides_add_ext(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);
+/* The same over extended-basis operands (level Q limbs followed by the K special limbs): the
+ * inner product of hoisted rotations kept in Q.P (fides_rotate_hoisted_ext) with diagonals
+ * encoded over Q.P (fides_encode_ext); one ModDown (fides_moddown) per result then replaces one
+ * per rotation (the reference's LinearTransformInPlace with ext = true). */
+int fides_dot_plain_ext(fides_ctx* ctx, const uint64_t* const* c0s, const uint64_t* const* c1s,
+                        const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
+                        void* stream);
 /* Ciphertext linear combination with integer constants (EVAL, level limbs), over n_lanes
  * independent operand sets that share the constants:
  *   out0s[a] = sum_t s_t * c0s[a * n_terms + t] + add0,  out1s[a] = sum_t s_t * c1s[a * n_terms + t]
@@ -223,6 +233,11 @@ int fides_rescale_batch(fides_ctx* ctx, const uint64_t* const* xs, const int* le
  * and sets bit 1 of the device status word (fides_ctx_device_status). */
 int fides_encode(fides_ctx* ctx, const double* slots, int n_slots, int n_pts, double scale, int level, uint64_t* out,
                  void* stream);
+/* fides_encode over the extended basis (the reference's MakeCKKSPackedPlaintextExtended,
+ * api/CryptoContext.hpp:171): out = [n_pts][level + K][N], the level Q limbs followed by the K
+ * special limbs of the same integer polynomial. */
+int fides_encode_ext(fides_ctx* ctx, const double* slots, int n_slots, int n_pts, double scale, int level,
+                     uint64_t* out, void* stream);
 /* CKKS slot decode on the device: n_pts plaintexts [n_pts][level][N] in EVALUATION form ->
  * n_slots complex slots each divided by `scale` (slots = [n_pts][n_slots][re, im] doubles in
  * device memory).  Reads limb 0 only, so the coefficients must lie below q_0 / 2 in magnitude
@@ -252,6 +267,16 @@ int fides_rotate_auto(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, in
 int fides_rotate_hoisted(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level,
                          const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
                          uint64_t* const* out1, void* stream);
+/* Hoisted rotations left in the extended basis (Ciphertext::rotate_hoisted with ext = true,
+ * Ciphertext.cpp:1221-1300): out0[j] / out1[j] = [level + K][N], P times rotation j of (c0, c1)
+ * up to the ModDown rounding (the key-switch outputs with P c0 added, automorphism applied, no
+ * ModDown); fides_moddown of each gives fides_rotate_hoisted's results.  c0_ext != 0: c0 is
+ * already extended ([level + K][N]) and is added as it is instead of P c0 -- a rotation without
+ * ModDown of a ciphertext whose c0 stayed in Q.P (Ciphertext::rotate(r, false) after
+ * c1.moddown, the giant-step fold of LinearTransform, LinearTransform.cu:164-195). */
+int fides_rotate_hoisted_ext(fides_ctx* ctx, const uint64_t* c0, int c0_ext, const uint64_t* c1, int level,
+                             const uint64_t* const* keys, const int* rotations, int n, uint64_t* const* out0,
+                             uint64_t* const* out1, void* stream);
 /* Rotation sum (replaces Accumulate, src/CKKS/AccumulateBroadcast.cu:122-160, behind
  * CryptoContext::AccumulateSum, api/CryptoContext.hpp:456): x + sum of its rotations by
  * stride t k for rounds t = 1, radix, radix^2, ... < size and k = 1 .. radix - 1 (while

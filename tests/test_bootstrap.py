@@ -975,7 +975,8 @@ def test_cpp_facade_linear_transform(fides, row_size, b_step, stride, offset):
     u64p, dp = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
     lib.facade_linear_transform.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, u64p, C.c_double, C.c_int,
                                             C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int, u64p, u64p, C.c_int,
-                                            C.c_int, C.c_int, C.c_int, dp, C.c_int, u64p, dp, C.c_char_p, C.c_int]
+                                            C.c_int, C.c_int, C.c_int, dp, C.c_int, C.c_int, u64p, dp, C.c_char_p,
+                                            C.c_int]
     lo = l - 1
     out = np.zeros(3 * 2 * lo * N, dtype=np.uint64)
     sc = C.c_double()
@@ -985,7 +986,7 @@ def test_cpp_facade_linear_transform(fides, row_size, b_step, stride, offset):
     rc = lib.facade_linear_transform(prm.logN, l, prm.K, prm.dnum, u64(primes), top, len(rots),
                                      (C.c_int * len(rots))(*rots), (C.c_void_p * len(rots))(*[keys[r].data_ptr() for r in rots]),
                                      l, u64(c0), u64(c1), row_size, b_step, stride, offset, dz.ctypes.data_as(dp), n,
-                                     u64(out), C.byref(sc), err, 512)
+                                     0, u64(out), C.byref(sc), err, 512)
     assert rc == 0, err.value.decode()
     res = [out[i * 2 * lo * N:(i + 1) * 2 * lo * N].reshape(2, lo, N) for i in range(3)]
     want = sum(np.roll(x, -(k * stride + offset)) * D[k] for k in range(row_size))

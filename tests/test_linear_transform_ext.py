@@ -154,7 +154,7 @@ def test_encode_ext_is_the_plain_encoding_over_qp(env, level):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("level", [8, 5])
+@pytest.mark.parametrize("level", [8, 5, 1])
 def test_rotate_hoisted_ext_and_dot_equal_oracle(env, level):
     F, prm, o, kg, ctx, _ = env
     rots = [1, 3, -2]
@@ -187,12 +187,14 @@ def test_rotate_hoisted_ext_and_dot_equal_oracle(env, level):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("row_size,b_step,stride,offset", [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2)])
+@pytest.mark.parametrize("row_size,b_step,stride,offset",
+                         [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2), (4, 2, 1024, 0), (3, 4, 1, 1)])
 def test_cpp_facade_linear_transform_ext(env, row_size, b_step, stride, offset):
     """The facade's LinearTransform / LinearTransformMany on extended diagonals equal the
     restatement above residue for residue (after the facade's Rescale, applied to the
     restatement too), decrypt to the FP64 transform, and the batched form's first set equals
-    the single transform."""
+    the single transform.  Cases: several giant steps with and without offset, one giant step
+    (bStep > rowSize), and giant-step rotations by N/2 slots (the identity, skipped)."""
     F, prm, o, kg, ctx, _ = env
     from test_bootstrap import _facade_lib
     N, l = prm.N, prm.n_q

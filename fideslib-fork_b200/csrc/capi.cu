@@ -479,6 +479,46 @@ int fides_dot_plain_ext(fides_ctx* x, const uint64_t* const* c0s, const uint64_t
   return dot_plain_impl(x, c0s, c1s, pts, n_terms, level, out0, out1, stream, true);
 }
 
+int fides_dot_plain_bsgs(fides_ctx* x, const uint64_t* const* x0s, const uint64_t* const* x1s, int n_baby,
+                         const uint64_t* const* pts, int n_giant, int level, int ext, uint64_t* const* out0s,
+                         uint64_t* const* out1s, void* stream) {
+  return guard([&] {
+    auto* c = C(x);
+    if (level < 1 || level > c->n_q) throw fides::Error(FIDES_ERR_LEVEL, "level out of range");
+    if (n_baby < 1 || n_baby > fides::MAX_BSGS_BABY || n_giant < 1 || n_giant > fides::MAX_BSGS_GIANT)
+      throw fides::Error(FIDES_ERR_ARG, "need 1..16 baby steps and 1..16 giant steps");
+    if (ext && c->K < 1) throw fides::Error(FIDES_ERR_ARG, "extended basis needs special primes");
+    need(x0s, "x0s");
+    need(x1s, "x1s");
+    need(pts, "pts");
+    need(out0s, "out0s");
+    need(out1s, "out1s");
+    fides::BsgsJob j{};
+    for (int k = 0; k < n_baby; ++k) {
+      need(x0s[k], "x0s[k]");
+      need(x1s[k], "x1s[k]");
+      j.x0[0][k] = x0s[k];
+      j.x1[0][k] = x1s[k];
+    }
+    for (int i = 0; i < n_giant; ++i) {
+      need(out0s[i], "out0s[i]");
+      need(out1s[i], "out1s[i]");
+      j.out0[0][i] = out0s[i];
+      j.out1[0][i] = out1s[i];
+      for (int k = 0; k < n_baby; ++k) j.pt[i][k] = pts[(size_t)i * n_baby + k];
+    }
+    j.nb = n_baby;
+    j.ng = n_giant;
+    j.lanes = 1;
+    j.l = ext ? level + c->K : level;
+    if (ext) {
+      j.lq = level;
+      j.nq = c->n_q;
+    }
+    fides::launch_bsgs_dot(c, j, S(stream));
+  });
+}
+
 int fides_lincomb(fides_ctx* x, int n_lanes, const uint64_t* const* c0s, const uint64_t* const* c1s,
                   const uint64_t* scalars, const uint64_t* add0, int n_terms, int level, uint64_t* const* out0s,
                   uint64_t* const* out1s, void* stream) {

@@ -191,6 +191,8 @@ def lib():
         L.fides_dot_plain.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         L.fides_dot_plain_ext.argtypes = L.fides_dot_plain.argtypes
         L.fides_add_ext.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        L.fides_dot_plain_bsgs.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(vp), C.c_int, C.c_int,
+                                           C.c_int, C.POINTER(vp), C.POINTER(vp), vp]
         L.fides_encode_ext.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]
         L.fides_rotate_hoisted_ext.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_int),
                                                C.c_int, C.POINTER(vp), C.POINTER(vp), vp]
@@ -635,6 +637,20 @@ class Context:
         out = self.empty(level + self.K) if out is None else out
         _check(lib().fides_add_ext(self._h, _ptr(a), _ptr(b), level, _ptr(out), _stream()))
         return out
+
+    def dot_plain_bsgs(self, babies, pts, level: int, ext: bool = False):
+        """Every giant step's inner product in one launch: pts[i][k] (None: no term) times
+        babies[k], summed over k, for each giant step i.  ext: Q.P operands and results."""
+        nb, ng = len(babies), len(pts)
+        e = level + (self.K if ext else 0)
+        outs = [Ciphertext(self.empty(e), self.empty(e)) for _ in range(ng)]
+        x0 = (vp * nb)(*[_ptr(b.c0) for b in babies])
+        x1 = (vp * nb)(*[_ptr(b.c1) for b in babies])
+        pp = (vp * (nb * ng))(*[None if p is None else _ptr(p) for row in pts for p in row])
+        o0 = (vp * ng)(*[_ptr(o.c0) for o in outs])
+        o1 = (vp * ng)(*[_ptr(o.c1) for o in outs])
+        _check(lib().fides_dot_plain_bsgs(self._h, x0, x1, nb, pp, ng, level, int(ext), o0, o1, _stream()))
+        return outs
 
     def dot_plain_ext(self, cts, pts, level: int, out=None):
         """dot_plain over extended-basis operands: cts and pts carry level Q limbs followed by

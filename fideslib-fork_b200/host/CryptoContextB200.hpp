@@ -309,9 +309,9 @@ class CryptoContextImpl {
   // the reference's diagonal contract: diagonals[k] encodes Rot(D_k, r_k), r_k = -bStep (k / bStep)
   // stride - offset (GetLinearTransformPlaintextRotationIndices), at the level the products are
   // taken (ct's, one below for an unrescaled input, which is rescaled first).  The bStep baby
-  // rotations by j stride are hoisted (one ModUp); each giant step's inner product
-  // sum_j Rot(ct, j stride) * diagonals[g bStep + j] is one launch (fides_dot_plain, the reference's
-  // LTdotProductPtBatch); the giant steps fold from the top, the running sum rotated by
+  // rotations by j stride are hoisted (one ModUp); the giant steps' inner products
+  // sum_j Rot(ct, j stride) * diagonals[g bStep + j], of every diagonal set, are taken together
+  // (dot_giant_steps, the reference's DotProductPtInternal); the giant steps fold from the top, the running sum rotated by
   // bStep stride before each is added, and by offset at the end.  Keys: j stride (1 <= j <= bStep)
   // and offset (GetLinearTransformRotationIndices).  The result keeps the level, at scale
   // ct x diagonal scale and degree + 1 (un-rescaled).
@@ -362,42 +362,67 @@ class CryptoContextImpl {
       check(fides_rotate_hoisted(cc_->handle(), ct_in.c0(), ct_in.c1(), l, keys.data(), rots.data(), nb - 1,
                                  o0.data(), o1.data(), cc_->stream()));
     }
+    // every giant step's inner product of every set first (fides_dot_plain_bsgs), then the folds
+    const int ns = (int)sets.size();
+    std::vector<Ciphertext> inner;  // [set][giant step]
+    std::vector<const uint64_t *> x0, x1;
+    std::vector<uint64_t *> o0, o1;
+    for (int j = 0; j < nb; ++j) x0.push_back(baby[j].c0()), x1.push_back(baby[j].c1());
+    for (int t = 0; t < ns * gs; ++t) {
+      inner.push_back(fresh(l, ct_in.NoiseFactor * sets[t / gs][0]->scale, ct_in.NoiseLevel + 1, ct_in.slots));
+      o0.push_back(inner.back().c0());
+      o1.push_back(inner.back().c1());
+    }
+    dot_giant_steps(x0, x1, sets, rowSize, bStep, l, false, o0, o1);
     std::vector<Ciphertext> outs;
-    for (const auto& d : sets) {
-      const double sc = ct_in.NoiseFactor * d[0]->scale;
-      Ciphertext acc = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
-      for (int g = gs - 1; g >= 0; --g) {
-        std::vector<const uint64_t *> c0s, c1s, pts;
-        for (int j = 0; j < nb && g * bStep + j < rowSize; ++j) {
-          c0s.push_back(baby[j].c0());
-          c1s.push_back(baby[j].c1());
-          pts.push_back(d[g * bStep + j]->data());
-        }
-        if (g == gs - 1) {
-          check(fides_dot_plain(cc_->handle(), c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l, acc.c0(),
-                                acc.c1(), cc_->stream()));
-          continue;
-        }
-        Ciphertext inner = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
-        check(fides_dot_plain(cc_->handle(), c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l, inner.c0(),
-                              inner.c1(), cc_->stream()));
-        Ciphertext r = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
+    for (int si = 0; si < ns; ++si) {
+      Ciphertext acc = std::move(inner[(size_t)si * gs + gs - 1]);
+      Ciphertext r = fresh(l, acc.NoiseFactor, acc.NoiseLevel, acc.slots);
+      for (int g = gs - 2; g >= 0; --g) {
+        const Ciphertext& in = inner[(size_t)si * gs + g];
         check(fides_rotate(cc_->handle(), acc.c0(), acc.c1(), l, cc_->GetRotationKey(bStep * stride).device(),
                            bStep * stride, r.c0(), r.c1(), cc_->stream()));
-        check(fides_add(cc_->handle(), r.c0(), inner.c0(), l, acc.c0(), cc_->stream()));
-        check(fides_add(cc_->handle(), r.c1(), inner.c1(), l, acc.c1(), cc_->stream()));
-        cc_->synchronize();  // inner and r are released at the end of the iteration
+        check(fides_add(cc_->handle(), r.c0(), in.c0(), l, acc.c0(), cc_->stream()));
+        check(fides_add(cc_->handle(), r.c1(), in.c1(), l, acc.c1(), cc_->stream()));
       }
       if (offset != 0) {
-        Ciphertext r = fresh(l, sc, ct_in.NoiseLevel + 1, ct_in.slots);
         check(fides_rotate(cc_->handle(), acc.c0(), acc.c1(), l, cc_->GetRotationKey(offset).device(), offset, r.c0(),
                            r.c1(), cc_->stream()));
-        acc = std::move(r);
+        std::swap(acc, r);
       }
+      cc_->synchronize();  // r is released at the end of the iteration
       outs.push_back(std::move(acc));
     }
-    cc_->synchronize();  // the baby steps are released at scope exit
+    cc_->synchronize();  // the baby steps and inner products are released at scope exit
     return outs;
+  }
+  // Every giant step's inner product of every diagonal set, sets x giant steps outputs in that
+  // order: up to 16 giant steps per launch (fides_dot_plain_bsgs, the reference's
+  // DotProductPtInternal over all giant steps); more than 16 baby steps: one launch per giant
+  // step (fides_dot_plain / fides_dot_plain_ext, up to 32 terms).
+  void dot_giant_steps(const std::vector<const uint64_t*>& x0, const std::vector<const uint64_t*>& x1,
+                       const std::vector<std::vector<const Plaintext*>>& sets, int rowSize, int bStep, int l, bool ext,
+                       const std::vector<uint64_t*>& o0, const std::vector<uint64_t*>& o1) const {
+    const int nb = (int)x0.size(), gs = (rowSize + bStep - 1) / bStep, total = (int)sets.size() * gs;
+    constexpr int kGiant = 16, kBaby = 16;
+    for (int t0 = 0; t0 < total; t0 += (nb <= kBaby ? kGiant : 1)) {
+      const int ng = nb <= kBaby ? std::min(kGiant, total - t0) : 1;
+      std::vector<const uint64_t*> pts((size_t)ng * nb, nullptr);
+      int terms = 0;
+      for (int i = 0; i < ng; ++i) {
+        const int t = t0 + i, g = t % gs;
+        const auto& d = sets[t / gs];
+        for (int j = 0; j < nb && g * bStep + j < rowSize; ++j) pts[(size_t)i * nb + j] = d[g * bStep + j]->data();
+      }
+      if (nb <= kBaby) {
+        check(fides_dot_plain_bsgs(cc_->handle(), x0.data(), x1.data(), nb, pts.data(), ng, l, ext ? 1 : 0,
+                                   o0.data() + t0, o1.data() + t0, cc_->stream()));
+        continue;
+      }
+      while (terms < nb && pts[terms]) ++terms;  // the last giant step may have fewer terms
+      check((ext ? fides_dot_plain_ext : fides_dot_plain)(cc_->handle(), x0.data(), x1.data(), pts.data(), terms, l,
+                                                          o0[t0], o1[t0], cc_->stream()));
+    }
   }
   // P mod q_i for the first l Q primes (P: the product of the special primes)
   std::vector<uint64_t> p_mod_q(int l) const {
@@ -457,25 +482,29 @@ class CryptoContextImpl {
       std::swap(a0, t0);
       std::swap(a1, t1);
     };
+    const int ns = (int)sets.size();
+    std::vector<DeviceLimbs> i0, i1;  // every giant step's inner product in Q.P, [set][giant step]
+    std::vector<const uint64_t *> x0, x1;
+    std::vector<uint64_t *> o0, o1;
+    for (int j = 0; j < nb; ++j) x0.push_back(b0[j].get()), x1.push_back(b1[j].get());
+    for (int t = 0; t < ns * gs; ++t) {
+      i0.emplace_back(Ne), i1.emplace_back(Ne);
+      o0.push_back(i0.back().get());
+      o1.push_back(i1.back().get());
+    }
+    dot_giant_steps(x0, x1, sets, rowSize, bStep, l, true, o0, o1);
     std::vector<Ciphertext> outs;
-    for (const auto& d : sets) {
-      for (int g = gs - 1; g >= 0; --g) {
-        std::vector<const uint64_t *> c0s, c1s, pts;
-        for (int j = 0; j < nb && g * bStep + j < rowSize; ++j) {
-          c0s.push_back(b0[j].get());
-          c1s.push_back(b1[j].get());
-          pts.push_back(d[g * bStep + j]->data());
-        }
-        const bool first = g == gs - 1;
-        if (!first && (bStep * stride) % (N() / 2) != 0) rotate_sum(bStep * stride);
-        check(fides_dot_plain_ext(h, c0s.data(), c1s.data(), pts.data(), (int)pts.size(), l,
-                                  first ? a0.get() : t0.get(), first ? a1.get() : t1.get(), st));
-        if (first) continue;
-        check(fides_add_ext(h, a0.get(), t0.get(), l, a0.get(), st));
-        check(fides_add_ext(h, a1.get(), t1.get(), l, a1.get(), st));
+    for (int si = 0; si < ns; ++si) {
+      const size_t top = (size_t)si * gs + gs - 1;
+      std::swap(a0, i0[top]);
+      std::swap(a1, i1[top]);
+      for (int g = gs - 2; g >= 0; --g) {
+        if ((bStep * stride) % (N() / 2) != 0) rotate_sum(bStep * stride);
+        check(fides_add_ext(h, a0.get(), i0[(size_t)si * gs + g].get(), l, a0.get(), st));
+        check(fides_add_ext(h, a1.get(), i1[(size_t)si * gs + g].get(), l, a1.get(), st));
       }
       if (offset != 0) rotate_sum(offset);
-      Ciphertext o = fresh(l, ct_in.NoiseFactor * d[0]->scale, ct_in.NoiseLevel + 1, ct_in.slots);
+      Ciphertext o = fresh(l, ct_in.NoiseFactor * sets[si][0]->scale, ct_in.NoiseLevel + 1, ct_in.slots);
       check(fides_moddown(h, a0.get(), l, o.c0(), st));
       check(fides_moddown(h, a1.get(), l, o.c1(), st));
       outs.push_back(std::move(o));

@@ -197,6 +197,14 @@ int fides_add_scalar(fides_ctx* ctx, const uint64_t* a, int level, const uint64_
 int fides_dot_plain(fides_ctx* ctx, const uint64_t* const* c0s, const uint64_t* const* c1s,
                     const uint64_t* const* pts, int n_terms, int level, uint64_t* out0, uint64_t* out1,
                     void* stream);
+/* Every giant step's inner product of a BSGS linear transform in one launch (the reference's
+ * DotProductPtInternal over all giant steps, LinearTransform.cu:148): out0s[i] / out1s[i] =
+ * sum_k pts[i n_baby + k] * (x0s[k], x1s[k]) for giant steps i < n_giant (1..16) over the baby
+ * steps k < n_baby (1..16); a null pts entry is no term (a row of nulls gives zero).  ext != 0:
+ * operands and results over Q.P ([level + K][N]), as fides_dot_plain_ext. */
+int fides_dot_plain_bsgs(fides_ctx* ctx, const uint64_t* const* x0s, const uint64_t* const* x1s, int n_baby,
+                         const uint64_t* const* pts, int n_giant, int level, int ext, uint64_t* const* out0s,
+                         uint64_t* const* out1s, void* stream);
 /* out = a + b over extended-basis polynomials ([level + K][N]: the level Q limbs, then the K
  * special limbs); Ciphertext::add of two operands still in Q.P (LinearTransform.cu:168-173). */
 int fides_add_ext(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, int level, uint64_t* out, void* stream);

@@ -187,6 +187,32 @@ def test_rotate_hoisted_ext_and_dot_equal_oracle(env, level):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ext", [False, True])
+def test_dot_plain_bsgs_equals_oracle(env, ext):
+    """All giant steps' inner products in one launch (fides_dot_plain_bsgs): each output is the
+    oracle's sum over the giant step's non-null diagonals; a giant step without terms is zero."""
+    F, prm, o, kg, ctx, _ = env
+    level, nb, ng = 6, 5, 4
+    primes = prm.q[:level] + (prm.p if ext else [])
+    ids = o.ext_ids(level) if ext else o.ids(level)
+    rng = xrng(80 + ext)
+    xs = [[uniform_limbs(rng, primes, prm.N) for _ in range(2)] for _ in range(nb)]
+    pts = [[uniform_limbs(rng, primes, prm.N) if (i * nb + k) % 7 != 3 else None for k in range(nb)]
+           for i in range(ng - 1)] + [[None] * nb]
+    babies = [F.Ciphertext(F.to_device(a), F.to_device(b)) for a, b in xs]
+    got = ctx.dot_plain_bsgs(babies, [[None if p is None else F.to_device(p) for p in row] for row in pts], level,
+                             ext=ext)
+    for i in range(ng):
+        w0 = np.zeros((len(primes), prm.N), dtype=np.uint64)
+        w1 = np.zeros_like(w0)
+        for k in range(nb):
+            if pts[i][k] is not None:
+                w0 = o.add(w0, o.mul(xs[k][0], pts[i][k], ids), ids)
+                w1 = o.add(w1, o.mul(xs[k][1], pts[i][k], ids), ids)
+        assert np.array_equal(F.to_host(got[i].c0), w0) and np.array_equal(F.to_host(got[i].c1), w1), f"giant {i}"
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("row_size,b_step,stride,offset",
                          [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2), (4, 2, 1024, 0), (3, 4, 1, 1)])
 def test_cpp_facade_linear_transform_ext(env, row_size, b_step, stride, offset):

@@ -942,7 +942,7 @@ def test_cpp_facade_bootstrap_to_level_n4096(fides):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("row_size,b_step,stride,offset", [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2)])
+@pytest.mark.parametrize("row_size,b_step,stride,offset", [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2), (38, 18, 1, 0)])
 def test_cpp_facade_linear_transform(fides, row_size, b_step, stride, offset):
     """The facade's LinearTransform / LinearTransformMany (the reference's BSGS contract:
     pre-rotated diagonals r_k = -bStep (k / bStep) stride - offset, hoisted baby steps, giant

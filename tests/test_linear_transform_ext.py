@@ -214,13 +214,15 @@ def test_dot_plain_bsgs_equals_oracle(env, ext):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("row_size,b_step,stride,offset",
-                         [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2), (4, 2, 1024, 0), (3, 4, 1, 1)])
+                         [(14, 4, 1, 3), (8, 8, 2, 0), (5, 2, 3, -2), (4, 2, 1024, 0), (3, 4, 1, 1),
+                          (38, 18, 1, 0)])
 def test_cpp_facade_linear_transform_ext(env, row_size, b_step, stride, offset):
     """The facade's LinearTransform / LinearTransformMany on extended diagonals equal the
     restatement above residue for residue (after the facade's Rescale, applied to the
     restatement too), decrypt to the FP64 transform, and the batched form's first set equals
     the single transform.  Cases: several giant steps with and without offset, one giant step
-    (bStep > rowSize), and giant-step rotations by N/2 slots (the identity, skipped)."""
+    (bStep > rowSize), giant-step rotations by N/2 slots (the identity, skipped), and more than
+    16 baby steps (one inner-product launch per giant step)."""
     F, prm, o, kg, ctx, _ = env
     from test_bootstrap import _facade_lib
     N, l = prm.N, prm.n_q

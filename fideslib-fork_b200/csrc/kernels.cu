@@ -509,6 +509,37 @@ __global__ void __launch_bounds__(EW_THREADS) bsgs_dot_kernel(const __grid_const
   J.out1[lane][i][off] = reduce128(s1, p);
 }
 
+// bsgs_dot_kernel with two consecutive coefficients per thread (16-byte loads and stores), for
+// at most 8 baby steps (the products stay below 2^128 without an intermediate reduction) and
+// operands whose addresses are 16-byte aligned (checked by the launcher).
+__global__ void __launch_bounds__(EW_THREADS) bsgs_dot2_kernel(const __grid_constant__ BsgsJob J,
+                                                               const DevPrime* primes, int logN) {
+  constexpr int NB = 8;
+  const int i = blockIdx.x % J.ng, lane = blockIdx.x / J.ng, j = blockIdx.z;
+  const DevPrime p = primes[ext_prime(j, J.lq, J.nq)];
+  const size_t off = ((size_t)j << logN) + 2 * ((size_t)blockIdx.y * blockDim.x + threadIdx.x);
+  auto ld2 = [](const uint64_t* q) { return *reinterpret_cast<const ulonglong2*>(q); };
+  ulonglong2 a[NB], b[NB], w[NB];
+#pragma unroll
+  for (int k = 0; k < NB; ++k)
+    if (k < J.nb && J.pt[i][k]) {
+      w[k] = ld2(J.pt[i][k] + off);
+      a[k] = ld2(J.x0[lane][k] + off);
+      b[k] = ld2(J.x1[lane][k] + off);
+    }
+  U128 s0x{0, 0}, s0y{0, 0}, s1x{0, 0}, s1y{0, 0};
+#pragma unroll
+  for (int k = 0; k < NB; ++k)
+    if (k < J.nb && J.pt[i][k]) {
+      mac128(s0x, w[k].x, a[k].x);
+      mac128(s0y, w[k].y, a[k].y);
+      mac128(s1x, w[k].x, b[k].x);
+      mac128(s1y, w[k].y, b[k].y);
+    }
+  *reinterpret_cast<ulonglong2*>(J.out0[lane][i] + off) = ulonglong2{reduce128(s0x, p), reduce128(s0y, p)};
+  *reinterpret_cast<ulonglong2*>(J.out1[lane][i] + off) = ulonglong2{reduce128(s1x, p), reduce128(s1y, p)};
+}
+
 __global__ void __launch_bounds__(EW_THREADS) lincomb_kernel(const __grid_constant__ LinCombJob J,
                                                              const DevPrime* primes, int logN) {
   const int j = blockIdx.y, lane = blockIdx.z;
@@ -641,8 +672,23 @@ void launch_bsgs_dot(Context* c, const BsgsJob& job, cudaStream_t s) {
   int terms = 0;
   for (int i = 0; i < job.ng; ++i)
     for (int k = 0; k < job.nb; ++k) terms += job.pt[i][k] != nullptr;
-  dim3 grid(job.lanes * job.ng, c->N / EW_THREADS, job.l);
+  bool aligned = c->N >= 2 * EW_THREADS;  // the paired form: 16-byte aligned operands, a whole tile of pairs
+  auto al = [&](const void* q) { aligned = aligned && (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  for (int i = 0; i < job.ng; ++i)
+    for (int k = 0; k < job.nb; ++k)
+      if (job.pt[i][k]) al(job.pt[i][k]);
+  for (int ln = 0; ln < job.lanes; ++ln) {
+    for (int k = 0; k < job.nb; ++k) al(job.x0[ln][k]), al(job.x1[ln][k]);
+    for (int i = 0; i < job.ng; ++i) al(job.out0[ln][i]), al(job.out1[ln][i]);
+  }
   LaunchScope ls(c, s, KK_ELEM, 8.0 * c->N * job.l * (terms + job.lanes * 2.0 * (job.nb + job.ng)));
+  if (job.nb <= 8 && aligned) {
+    dim3 grid2(job.lanes * job.ng, c->N / (2 * EW_THREADS), job.l);
+    bsgs_dot2_kernel<<<grid2, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
+    FIDES_CUDA(cudaGetLastError());
+    return;
+  }
+  dim3 grid(job.lanes * job.ng, c->N / EW_THREADS, job.l);
   if (job.nb <= 8)
     bsgs_dot_kernel<8><<<grid, EW_THREADS, 0, s>>>(job, c->d_prime, c->logN);
   else
